@@ -1,0 +1,139 @@
+"""ctypes binding of ``libfgkl_b200.so`` (the C ABI of ``include/fgkl_b200.h``).
+
+The library is the only compute path: there is no CPU fallback. If it cannot be loaded, importing
+the compute API raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = _PKG / "libfgkl_b200.so"
+
+FGKL_OK = 0
+FGKL_E_EMPTY_READ = -1
+FGKL_E_MISMATCHED_READ_ARRAYS = -2
+FGKL_E_EMPTY_HAPLOTYPE = -3
+FGKL_E_MISMATCHED_HAPLOTYPE_ARRAYS = -4
+FGKL_E_OUTPUT_LENGTH = -5
+FGKL_E_BAD_OFFSETS = -6
+FGKL_E_INVALID_ARGUMENT = -7
+FGKL_E_UNSUPPORTED = -8
+FGKL_E_NO_DEVICE = -9
+FGKL_E_CUDA = -10
+
+u8p = C.POINTER(C.c_uint8)
+i32p = C.POINTER(C.c_int32)
+i64p = C.POINTER(C.c_int64)
+f64p = C.POINTER(C.c_double)
+
+
+class Config(C.Structure):
+    _fields_ = [("double_precision", C.c_int32), ("double_fallback", C.c_int32), ("share_suffixes", C.c_int32)]
+
+
+class Stats(C.Structure):
+    _fields_ = [
+        ("fallback_pairs", C.c_uint64),
+        ("rescue_reads", C.c_uint64),
+        ("nominal_cells", C.c_uint64),
+        ("computed_cells", C.c_uint64),
+        ("forward_cells", C.c_uint64),
+        ("backward_cells", C.c_uint64),
+        ("prefix_only_cells", C.c_uint64),
+        ("kernel_launches", C.c_uint64),
+    ]
+
+
+class Reads(C.Structure):
+    _fields_ = [
+        ("bases", u8p), ("bases_len", C.c_int64),
+        ("quals", u8p), ("quals_len", C.c_int64),
+        ("ins_gop", u8p), ("ins_gop_len", C.c_int64),
+        ("del_gop", u8p), ("del_gop_len", C.c_int64),
+        ("gcp", u8p), ("gcp_len", C.c_int64),
+        ("offsets", i32p), ("offsets_len", C.c_int64),
+    ]
+
+
+class Haplotypes(C.Structure):
+    _fields_ = [
+        ("bases", u8p), ("bases_len", C.c_int64),
+        ("flags", u8p), ("flags_len", C.c_int64),
+        ("offsets", i32p), ("offsets_len", C.c_int64),
+    ]
+
+
+class Batch(C.Structure):
+    _fields_ = [
+        ("num_regions", C.c_int32),
+        ("region_reads", i32p),
+        ("region_haps", i32p),
+        ("bases", u8p),
+        ("quals", u8p),
+        ("ins_gop", u8p),
+        ("del_gop", u8p),
+        ("gcp", u8p),
+        ("read_offsets", i64p),
+        ("hap_bases", u8p),
+        ("hap_flags", u8p),
+        ("hap_offsets", i64p),
+    ]
+
+
+_lib: C.CDLL | None = None
+
+
+def lib() -> C.CDLL:
+    """The loaded library; raises OSError when it is missing (run ``__graft_entry__.build()``)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = os.environ.get("FGKL_B200_LIB", str(LIB_PATH))
+    if not Path(path).exists():
+        raise OSError(f"{path} is missing; build it with `python -c 'import __graft_entry__ as g; g.build()'`")
+    L = C.CDLL(path)
+    L.fgkl_pairhmm_compute.argtypes = [C.POINTER(Reads), C.POINTER(Haplotypes), C.c_int32, f64p, C.c_int64]
+    L.fgkl_pairhmm_compute_config.argtypes = [C.POINTER(Reads), C.POINTER(Haplotypes), C.POINTER(Config), f64p, C.c_int64,
+                                              C.POINTER(Stats)]
+    L.fgkl_pdhmm_compute.argtypes = L.fgkl_pairhmm_compute.argtypes
+    L.fgkl_pdhmm_compute_config.argtypes = L.fgkl_pairhmm_compute_config.argtypes
+    for f in (L.fgkl_pairhmm_compute, L.fgkl_pairhmm_compute_config, L.fgkl_pdhmm_compute, L.fgkl_pdhmm_compute_config):
+        f.restype = C.c_int
+    L.fgkl_backend.restype = C.c_char_p
+    L.fgkl_last_error.restype = C.c_char_p
+    L.fgkl_context_create.argtypes = [C.c_int32, C.c_void_p]
+    L.fgkl_context_create.restype = C.c_void_p
+    L.fgkl_context_destroy.argtypes = [C.c_void_p]
+    L.fgkl_batch_prepare.argtypes = [C.c_void_p, C.POINTER(Batch), C.POINTER(Config)]
+    L.fgkl_batch_run.argtypes = [C.c_void_p]
+    L.fgkl_batch_fetch.argtypes = [C.c_void_p, f64p, C.c_int64, C.POINTER(Stats)]
+    L.fgkl_batch_compute.argtypes = [C.c_void_p, C.POINTER(Batch), C.POINTER(Config), f64p, C.c_int64, C.POINTER(Stats)]
+    L.fgkl_batch_output_len.argtypes = [C.c_void_p]
+    L.fgkl_batch_output_len.restype = C.c_int64
+    L.fgkl_synth_config.argtypes = [C.c_int32, C.c_uint64, C.c_int32, C.c_int32]
+    L.fgkl_synth_config.restype = C.c_void_p
+    L.fgkl_synth_reference_region.argtypes = [C.c_uint64, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int32]
+    L.fgkl_synth_reference_region.restype = C.c_void_p
+    L.fgkl_synth_view.argtypes = [C.c_void_p, C.POINTER(Batch), i64p]
+    L.fgkl_synth_free.argtypes = [C.c_void_p]
+    L.fgkl_plan_describe.argtypes = [u8p, i32p, C.c_int32, C.c_int32, i32p, i32p, u8p, i32p, i32p, i32p, i32p,
+                                     C.POINTER(C.c_uint64)]
+    L.fgkl_plan_sweeps.argtypes = [u8p, i32p, C.c_int32, i32p, C.c_int32, i32p, C.c_int32]
+    _lib = L
+    return L
+
+
+def last_error() -> str:
+    return lib().fgkl_last_error().decode()
+
+
+# Symbols include/fgkl_b200.h declares; the CPU test suite checks the library exports each one.
+EXPORTED = [
+    "fgkl_pairhmm_compute", "fgkl_pairhmm_compute_config", "fgkl_pdhmm_compute", "fgkl_pdhmm_compute_config",
+    "fgkl_backend", "fgkl_last_error", "fgkl_context_create", "fgkl_context_destroy", "fgkl_batch_prepare",
+    "fgkl_batch_run", "fgkl_batch_fetch", "fgkl_batch_compute", "fgkl_batch_output_len", "fgkl_synth_config",
+    "fgkl_synth_reference_region", "fgkl_synth_view", "fgkl_synth_free", "fgkl_plan_describe", "fgkl_plan_sweeps",
+]

@@ -1,0 +1,392 @@
+// The extern "C" boundary (include/fgkl_b200.h).
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/fgkl_b200.h"
+#include "engine.h"
+#include "planner.h"
+#include "synthetic.h"
+
+namespace {
+
+thread_local std::string t_error;
+
+int set_error(int code, const std::string& msg) {
+  t_error = msg;
+  return code;
+}
+
+// The device this process computes on: FGKL_DEVICE, else 0. An sm_100 part is required; there is
+// no CPU path.
+int pick_device(int* device) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return set_error(FGKL_E_NO_DEVICE, "no CUDA device is visible");
+  int d = 0;
+  if (const char* env = std::getenv("FGKL_DEVICE")) d = std::atoi(env);
+  if (d < 0 || d >= n) return set_error(FGKL_E_NO_DEVICE, "FGKL_DEVICE names no visible device");
+  cudaDeviceProp prop{};
+  if (cudaGetDeviceProperties(&prop, d) != cudaSuccess) return set_error(FGKL_E_NO_DEVICE, "cannot query the CUDA device");
+  if (prop.major != 10 || prop.minor != 0)
+    return set_error(FGKL_E_NO_DEVICE, std::string("the kernels are built for sm_100a; device is ") + prop.name);
+  *device = d;
+  return FGKL_OK;
+}
+
+// One engine per calling thread for the per-call entry points.
+fgkl::Engine* thread_engine(int* rc) {
+  thread_local std::unique_ptr<fgkl::Engine> engine;
+  if (!engine) {
+    int d = 0;
+    if ((*rc = pick_device(&d)) != FGKL_OK) return nullptr;
+    engine = std::make_unique<fgkl::Engine>(d);
+  }
+  *rc = FGKL_OK;
+  return engine.get();
+}
+
+// Offset table -> (start, end) checks of crates/jni/src/lib.rs:343-363.
+int check_offsets(const int32_t* offsets, int64_t n, int64_t total, const char* what) {
+  if (n < 1 || offsets == nullptr || offsets[0] != 0)
+    return set_error(FGKL_E_BAD_OFFSETS, std::string(what) + " offset table must start at zero");
+  if (offsets[n - 1] < 0 || static_cast<int64_t>(offsets[n - 1]) != total)
+    return set_error(FGKL_E_BAD_OFFSETS, std::string(what) + " offset table must end at the array length");
+  for (int64_t i = 1; i < n; ++i)
+    if (offsets[i] < offsets[i - 1]) return set_error(FGKL_E_BAD_OFFSETS, std::string(what) + " offset table must be non-decreasing");
+  return FGKL_OK;
+}
+
+int per_call(const fgkl_reads* reads, const fgkl_haplotypes* haps, const fgkl_config* cfg, bool pd, double* out, int64_t out_len,
+             fgkl_stats* stats) {
+  t_error.clear();
+  if (!reads || !haps || !cfg || (out_len > 0 && !out) || out_len < 0) return set_error(FGKL_E_INVALID_ARGUMENT, "null argument");
+  // ReadBatch::fetch (jni/src/lib.rs:104-133): the five read arrays must have one total length.
+  const int64_t n = reads->bases_len;
+  if (reads->quals_len != n || reads->ins_gop_len != n || reads->del_gop_len != n || reads->gcp_len != n)
+    return set_error(FGKL_E_MISMATCHED_READ_ARRAYS, "read bases, qualities and penalties differ in total length");
+  if (n < 0 || haps->bases_len < 0) return set_error(FGKL_E_INVALID_ARGUMENT, "negative array length");
+  int rc;
+  if ((rc = check_offsets(reads->offsets, reads->offsets_len, n, "read"))) return rc;
+  if (pd && haps->flags_len != haps->bases_len)
+    return set_error(FGKL_E_MISMATCHED_HAPLOTYPE_ARRAYS, "haplotype bases and PD flags differ in total length");
+  if ((rc = check_offsets(haps->offsets, haps->offsets_len, haps->bases_len, "haplotype"))) return rc;
+  const int64_t n_reads = reads->offsets_len - 1, n_haps = haps->offsets_len - 1;
+  const int64_t expected = n_reads * n_haps;
+  if (out_len != expected)
+    return set_error(FGKL_E_OUTPUT_LENGTH,
+                     "output has " + std::to_string(out_len) + " elements but reads x haplotypes is " + std::to_string(expected));
+  // PairHmm::compute_log10_likelihoods validation order (lib.rs:278-290).
+  for (int64_t r = 0; r < n_reads; ++r)
+    if (reads->offsets[r + 1] == reads->offsets[r]) return set_error(FGKL_E_EMPTY_READ, "read " + std::to_string(r) + " has no bases");
+  for (int64_t h = 0; h < n_haps; ++h)
+    if (haps->offsets[h + 1] == haps->offsets[h])
+      return set_error(FGKL_E_EMPTY_HAPLOTYPE, "haplotype " + std::to_string(h) + " has no bases");
+  if (stats) std::memset(stats, 0, sizeof *stats);
+  if (expected == 0) return FGKL_OK;
+  if (pd) return set_error(FGKL_E_UNSUPPORTED, "the PD-HMM kernel is not available in this build");
+  fgkl::Engine* e = thread_engine(&rc);
+  if (!e) return rc;
+  std::vector<int64_t> roff(static_cast<size_t>(n_reads) + 1), hoff(static_cast<size_t>(n_haps) + 1);
+  for (int64_t i = 0; i <= n_reads; ++i) roff[i] = reads->offsets[i];
+  for (int64_t i = 0; i <= n_haps; ++i) hoff[i] = haps->offsets[i];
+  const int32_t nr = static_cast<int32_t>(n_reads), nh = static_cast<int32_t>(n_haps);
+  fgkl::BatchInput in;
+  in.num_regions = 1;
+  in.region_reads = &nr;
+  in.region_haps = &nh;
+  in.bases = reads->bases;
+  in.quals = reads->quals;
+  in.ins = reads->ins_gop;
+  in.del = reads->del_gop;
+  in.gcp = reads->gcp;
+  in.read_off = roff.data();
+  in.hap_bases = haps->bases;
+  in.hap_off = hoff.data();
+  fgkl::EngineConfig ec;
+  ec.double_precision = cfg->double_precision != 0;
+  ec.double_fallback = cfg->double_fallback != 0;
+  ec.share_suffixes = cfg->share_suffixes != 0;
+  fgkl::BatchStats bs;
+  rc = e->compute(in, ec, out, out_len, &bs);
+  if (rc) return set_error(rc, e->error());
+  if (stats) {
+    stats->fallback_pairs = bs.fallback_pairs;
+    stats->rescue_reads = bs.rescue_reads;
+    stats->nominal_cells = bs.nominal_cells;
+    stats->computed_cells = bs.computed_cells;
+    stats->forward_cells = bs.forward_cells;
+    stats->backward_cells = bs.backward_cells;
+    stats->prefix_only_cells = bs.prefix_only_cells;
+    stats->kernel_launches = bs.kernel_launches;
+  }
+  return FGKL_OK;
+}
+
+fgkl_config default_config(int32_t double_precision) {
+  fgkl_config c;
+  c.double_precision = double_precision;
+  c.double_fallback = 1;
+  c.share_suffixes = 1;
+  return c;
+}
+
+void to_stats(const fgkl::BatchStats& bs, fgkl_stats* s) {
+  s->fallback_pairs = bs.fallback_pairs;
+  s->rescue_reads = bs.rescue_reads;
+  s->nominal_cells = bs.nominal_cells;
+  s->computed_cells = bs.computed_cells;
+  s->forward_cells = bs.forward_cells;
+  s->backward_cells = bs.backward_cells;
+  s->prefix_only_cells = bs.prefix_only_cells;
+  s->kernel_launches = bs.kernel_launches;
+}
+
+}  // namespace
+
+struct fgkl_context {
+  std::unique_ptr<fgkl::Engine> engine;
+  cudaGraphExec_t graph = nullptr;
+  bool prepared = false;
+};
+
+extern "C" {
+
+int fgkl_pairhmm_compute(const fgkl_reads* reads, const fgkl_haplotypes* haps, int32_t double_precision, double* out,
+                         int64_t out_len) {
+  const fgkl_config c = default_config(double_precision);
+  return per_call(reads, haps, &c, false, out, out_len, nullptr);
+}
+
+int fgkl_pairhmm_compute_config(const fgkl_reads* reads, const fgkl_haplotypes* haps, const fgkl_config* config, double* out,
+                                int64_t out_len, fgkl_stats* stats) {
+  return per_call(reads, haps, config, false, out, out_len, stats);
+}
+
+int fgkl_pdhmm_compute(const fgkl_reads* reads, const fgkl_haplotypes* haps, int32_t double_precision, double* out,
+                       int64_t out_len) {
+  const fgkl_config c = default_config(double_precision);
+  return per_call(reads, haps, &c, true, out, out_len, nullptr);
+}
+
+int fgkl_pdhmm_compute_config(const fgkl_reads* reads, const fgkl_haplotypes* haps, const fgkl_config* config, double* out,
+                              int64_t out_len, fgkl_stats* stats) {
+  return per_call(reads, haps, config, true, out, out_len, stats);
+}
+
+const char* fgkl_backend(void) { return "cuda-sm100a"; }
+
+const char* fgkl_last_error(void) { return t_error.c_str(); }
+
+fgkl_context* fgkl_context_create(int32_t device, void* stream) {
+  t_error.clear();
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+    set_error(FGKL_E_NO_DEVICE, "no such CUDA device");
+    return nullptr;
+  }
+  auto* ctx = new fgkl_context;
+  ctx->engine = std::make_unique<fgkl::Engine>(device, static_cast<cudaStream_t>(stream));
+  return ctx;
+}
+
+void fgkl_context_destroy(fgkl_context* ctx) {
+  if (!ctx) return;
+  if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
+  delete ctx;
+}
+
+int fgkl_batch_prepare(fgkl_context* ctx, const fgkl_batch* b, const fgkl_config* config) {
+  t_error.clear();
+  if (!ctx || !b || !config) return set_error(FGKL_E_INVALID_ARGUMENT, "null argument");
+  if (b->hap_flags) return set_error(FGKL_E_UNSUPPORTED, "the PD-HMM kernel is not available in this build");
+  if (ctx->graph) {
+    cudaGraphExecDestroy(ctx->graph);
+    ctx->graph = nullptr;
+  }
+  fgkl::BatchInput in;
+  in.num_regions = b->num_regions;
+  in.region_reads = b->region_reads;
+  in.region_haps = b->region_haps;
+  in.bases = b->bases;
+  in.quals = b->quals;
+  in.ins = b->ins_gop;
+  in.del = b->del_gop;
+  in.gcp = b->gcp;
+  in.read_off = b->read_offsets;
+  in.hap_bases = b->hap_bases;
+  in.hap_off = b->hap_offsets;
+  fgkl::EngineConfig ec;
+  ec.double_precision = config->double_precision != 0;
+  ec.double_fallback = config->double_fallback != 0;
+  ec.share_suffixes = config->share_suffixes != 0;
+  const int rc = ctx->engine->prepare(in, ec);
+  ctx->prepared = rc == FGKL_OK;
+  return rc ? set_error(rc, ctx->engine->error()) : FGKL_OK;
+}
+
+int fgkl_batch_run(fgkl_context* ctx) {
+  t_error.clear();
+  if (!ctx || !ctx->prepared) return set_error(FGKL_E_INVALID_ARGUMENT, "no prepared batch");
+  fgkl::Engine& e = *ctx->engine;
+  if (e.output_len() == 0) return FGKL_OK;
+  cudaStream_t s = e.stream();
+  if (!ctx->graph) {
+    cudaGraph_t g = nullptr;
+    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+      return set_error(FGKL_E_CUDA, "cannot capture the launch sequence");
+    const int rc = e.run();
+    const cudaError_t end = cudaStreamEndCapture(s, &g);
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      return set_error(rc, e.error());
+    }
+    if (end != cudaSuccess) return set_error(FGKL_E_CUDA, std::string("capture: ") + cudaGetErrorString(end));
+    const cudaError_t inst = cudaGraphInstantiate(&ctx->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (inst != cudaSuccess) {
+      ctx->graph = nullptr;
+      return set_error(FGKL_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(inst));
+    }
+  }
+  const cudaError_t err = cudaGraphLaunch(ctx->graph, s);
+  if (err != cudaSuccess) return set_error(FGKL_E_CUDA, std::string("graph launch: ") + cudaGetErrorString(err));
+  return FGKL_OK;
+}
+
+int fgkl_batch_fetch(fgkl_context* ctx, double* out, int64_t out_len, fgkl_stats* stats) {
+  t_error.clear();
+  if (!ctx || !ctx->prepared) return set_error(FGKL_E_INVALID_ARGUMENT, "no prepared batch");
+  fgkl::BatchStats bs;
+  const int rc = ctx->engine->fetch(out, out_len, &bs);
+  if (rc) return set_error(rc, ctx->engine->error());
+  if (stats) to_stats(bs, stats);
+  return FGKL_OK;
+}
+
+int fgkl_batch_compute(fgkl_context* ctx, const fgkl_batch* batch, const fgkl_config* config, double* out, int64_t out_len,
+                       fgkl_stats* stats) {
+  int rc = fgkl_batch_prepare(ctx, batch, config);
+  if (rc) return rc;
+  if (out_len != ctx->engine->output_len())
+    return set_error(FGKL_E_OUTPUT_LENGTH, "output has " + std::to_string(out_len) + " elements but the batch produces " +
+                                               std::to_string(ctx->engine->output_len()));
+  if ((rc = fgkl_batch_run(ctx))) return rc;
+  return fgkl_batch_fetch(ctx, out, out_len, stats);
+}
+
+int64_t fgkl_batch_output_len(const fgkl_context* ctx) { return ctx && ctx->prepared ? ctx->engine->output_len() : 0; }
+
+// ---------------------------------------------------------------------------------------------
+// Synthetic workloads and planner diagnostics (test and benchmark support).
+// ---------------------------------------------------------------------------------------------
+
+struct fgkl_synth {
+  fgkl::SynthBatch batch;
+};
+
+fgkl_synth* fgkl_synth_config(int32_t which, uint64_t seed, int32_t regions, int32_t threads) {
+  try {
+    auto* s = new fgkl_synth;
+    s->batch = fgkl::config_batch(which, seed, regions, threads);
+    return s;
+  } catch (const std::exception& e) {
+    set_error(FGKL_E_INVALID_ARGUMENT, e.what());
+    return nullptr;
+  }
+}
+
+fgkl_synth* fgkl_synth_reference_region(uint64_t seed, int64_t reads, int64_t read_len, int64_t haps, int64_t hap_len, int32_t pd) {
+  auto* s = new fgkl_synth;
+  const auto r = pd ? fgkl::reference_pd_region(seed, reads, read_len, haps, hap_len)
+                    : fgkl::reference_region(seed, reads, read_len, haps, hap_len);
+  s->batch.append(r);
+  s->batch.pd = pd != 0;
+  return s;
+}
+
+void fgkl_synth_view(const fgkl_synth* s, fgkl_batch* out, int64_t sizes[4]) {
+  const auto& b = s->batch;
+  out->num_regions = static_cast<int32_t>(b.region_reads.size());
+  out->region_reads = b.region_reads.data();
+  out->region_haps = b.region_haps.data();
+  out->bases = b.bases.data();
+  out->quals = b.quals.data();
+  out->ins_gop = b.ins.data();
+  out->del_gop = b.del.data();
+  out->gcp = b.gcp.data();
+  out->read_offsets = b.read_off.data();
+  out->hap_bases = b.hap_bases.data();
+  out->hap_flags = b.pd ? b.hap_flags.data() : nullptr;
+  out->hap_offsets = b.hap_off.data();
+  sizes[0] = static_cast<int64_t>(b.read_off.size()) - 1;
+  sizes[1] = static_cast<int64_t>(b.bases.size());
+  sizes[2] = static_cast<int64_t>(b.hap_off.size()) - 1;
+  sizes[3] = static_cast<int64_t>(b.hap_bases.size());
+}
+
+void fgkl_synth_free(fgkl_synth* s) { delete s; }
+
+// Sorted order, LCP, duplicate flags, cuts, node count and SharedColumns of one haplotype set;
+// sweeps are reported through fgkl_plan_sweeps. Arrays are num_haps long.
+int fgkl_plan_describe(const uint8_t* hap_bases, const int32_t* hap_offsets, int32_t num_haps, int32_t share_suffixes,
+                       int32_t* order, int32_t* lcp, uint8_t* dup, int32_t* cut_column, int32_t* cut_node, int32_t* num_sweeps,
+                       int32_t* num_nodes, uint64_t columns[3]) {
+  try {
+    std::vector<fgkl::HapView> views(static_cast<size_t>(num_haps));
+    for (int h = 0; h < num_haps; ++h) views[h] = fgkl::HapView{hap_bases + hap_offsets[h], hap_offsets[h + 1] - hap_offsets[h]};
+    const auto s = fgkl::SortedHaps::make(views, share_suffixes != 0);
+    for (int k = 0; k < num_haps; ++k) {
+      order[k] = s.order[k];
+      lcp[k] = s.lcp[k];
+      dup[k] = s.dup[k];
+      cut_column[k] = s.plan.cuts[k].column;
+      cut_node[k] = s.plan.cuts[k].node;
+    }
+    *num_sweeps = static_cast<int32_t>(s.plan.sweeps.size());
+    *num_nodes = s.plan.nodes;
+    const auto c = s.columns();
+    columns[0] = c.prefix_only;
+    columns[1] = c.forward;
+    columns[2] = c.backward;
+    return FGKL_OK;
+  } catch (const std::exception& e) {
+    return set_error(FGKL_E_INVALID_ARGUMENT, e.what());
+  }
+}
+
+// The sweeps of a plan: per sweep (hap, resume, need, start, first write, write count) in
+// `sweeps` (6 ints each) and the (depth, node) writes in `writes` (2 ints each).
+int fgkl_plan_sweeps(const uint8_t* hap_bases, const int32_t* hap_offsets, int32_t num_haps, int32_t* sweeps, int32_t max_sweeps,
+                     int32_t* writes, int32_t max_writes) {
+  try {
+    std::vector<fgkl::HapView> views(static_cast<size_t>(num_haps));
+    for (int h = 0; h < num_haps; ++h) views[h] = fgkl::HapView{hap_bases + hap_offsets[h], hap_offsets[h + 1] - hap_offsets[h]};
+    const auto s = fgkl::SortedHaps::make(views, true);
+    if (static_cast<int32_t>(s.plan.sweeps.size()) > max_sweeps) return set_error(FGKL_E_INVALID_ARGUMENT, "too many sweeps");
+    int w = 0;
+    for (size_t i = 0; i < s.plan.sweeps.size(); ++i) {
+      const auto& sw = s.plan.sweeps[i];
+      int32_t* o = sweeps + 6 * i;
+      o[0] = sw.hap;
+      o[1] = sw.resume;
+      o[2] = sw.need;
+      o[3] = sw.start;
+      o[4] = w;
+      o[5] = static_cast<int32_t>(sw.writes.size());
+      for (const auto& wr : sw.writes) {
+        if (w >= max_writes) return set_error(FGKL_E_INVALID_ARGUMENT, "too many writes");
+        writes[2 * w] = wr.first;
+        writes[2 * w + 1] = wr.second;
+        ++w;
+      }
+    }
+    return FGKL_OK;
+  } catch (const std::exception& e) {
+    return set_error(FGKL_E_INVALID_ARGUMENT, e.what());
+  }
+}
+
+}  // extern "C"

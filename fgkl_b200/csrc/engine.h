@@ -1,0 +1,125 @@
+// Host orchestration of the sm_100a PairHMM kernels: plans a batch of regions, uploads it, runs the
+// first pass and the double-precision recomputation, and brings the results back. One Engine owns a
+// device stream and grow-only device buffers (fgkl keeps per-thread workspaces the same way,
+// kernel.rs:144-163).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+#include "program.h"
+
+namespace fgkl {
+
+struct EngineConfig {
+  bool double_precision = false;  // Precision::Double (lib.rs:72-77)
+  bool double_fallback = true;    // recompute lost pairs (lib.rs:218-222)
+  bool share_suffixes = true;     // suffix sharing (lib.rs:223-226)
+};
+
+// A batch of regions in host memory (reads and haplotypes concatenated, region sizes apart).
+struct BatchInput {
+  int32_t num_regions = 0;
+  const int32_t* region_reads = nullptr;
+  const int32_t* region_haps = nullptr;
+  const uint8_t *bases = nullptr, *quals = nullptr, *ins = nullptr, *del = nullptr, *gcp = nullptr;
+  const int64_t* read_off = nullptr;  // total_reads + 1
+  const uint8_t* hap_bases = nullptr;
+  const int64_t* hap_off = nullptr;   // total_haps + 1
+};
+
+struct BatchStats {
+  uint64_t fallback_pairs = 0;
+  uint64_t rescue_reads = 0;
+  uint64_t nominal_cells = 0;       // Σ per region of Σ read lengths x Σ haplotype lengths
+  uint64_t computed_cells = 0;      // forward + backward cells of the first pass
+  uint64_t forward_cells = 0;
+  uint64_t backward_cells = 0;
+  uint64_t prefix_only_cells = 0;   // forward cells prefix sharing alone would compute
+  uint64_t device_fwd_columns = 0;  // stream positions the kernels walked (cross-check)
+  uint64_t device_bwd_columns = 0;
+  uint64_t kernel_launches = 0;     // launches issued by the last run()
+};
+
+class Engine {
+ public:
+  explicit Engine(int device, cudaStream_t stream = nullptr);
+  ~Engine();
+  Engine(const Engine&) = delete;
+  Engine& operator=(const Engine&) = delete;
+
+  // Plans `in` and uploads it; returns 0 or a negative FGKL_E_* code (message in error()).
+  int prepare(const BatchInput& in, const EngineConfig& cfg);
+  // Enqueues the first pass and the recomputation on the stream (no host synchronisation).
+  int run();
+  // Copies the results (and counters) back and waits for the stream.
+  int fetch(double* out, int64_t out_len, BatchStats* stats);
+  // prepare + run + fetch.
+  int compute(const BatchInput& in, const EngineConfig& cfg, double* out, int64_t out_len, BatchStats* stats);
+
+  const std::string& error() const { return error_; }
+  cudaStream_t stream() const { return stream_; }
+  int64_t output_len() const { return out_len_; }
+  // Host-side planning statistics of the prepared batch.
+  const BatchStats& planned() const { return planned_; }
+  // Device pointer to the output, for callers that keep results on the device.
+  const double* device_output() const { return d_out_; }
+
+ private:
+  struct Bin {
+    Kind kind;
+    int rows;
+    int task_off;  // into the device task array
+    int n_tasks;
+    int blocks;
+  };
+  template <class T>
+  T* grow(T*& ptr, size_t& cap, size_t n);
+  int fail(int code, const std::string& msg);
+  int check(cudaError_t e, const char* what);
+
+  int device_ = 0;
+  int sms_ = 0;
+  cudaStream_t stream_ = nullptr;
+  bool own_stream_ = false;
+  std::string error_;
+  EngineConfig cfg_;
+  BatchStats planned_;
+
+  // Device buffers (grow-only).
+  uint8_t* d_reads_ = nullptr;
+  size_t cap_reads_ = 0;
+  int64_t* d_read_off_ = nullptr;
+  size_t cap_read_off_ = 0;
+  uint8_t* d_plan_ = nullptr;  // regions, haps, stream, segs, slot/node lists, code tables
+  size_t cap_plan_ = 0;
+  Task* d_tasks_ = nullptr;
+  size_t cap_tasks_ = 0;
+  Task* d_queue_ = nullptr;
+  size_t cap_queue_ = 0;
+  int* d_small_ = nullptr;  // task counters, queue offsets and tails
+  size_t cap_small_ = 0;
+  double* d_out_ = nullptr;
+  size_t cap_out_ = 0;
+  Counters* d_counters_ = nullptr;
+  char* d_scratch_ = nullptr;
+  size_t cap_scratch_ = 0;
+  double* d_err_ = nullptr;
+  double* d_m2m_ = nullptr;
+
+  // Pinned host staging.
+  uint8_t* h_stage_ = nullptr;
+  size_t cap_stage_ = 0;
+
+  // Prepared batch.
+  BatchView view_{};
+  std::vector<Bin> bins_, rescue_bins_;
+  size_t scratch_stride_ = 0;
+  int64_t out_len_ = 0;
+  int n_small_ = 0;
+};
+
+}  // namespace fgkl

@@ -1,0 +1,312 @@
+#include "planner.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <map>
+#include <stdexcept>
+
+namespace fgkl {
+
+namespace {
+
+constexpr uint8_t kStandard[5] = {'A', 'C', 'G', 'T', 'N'};
+// A backward sweep must skip at least this many forward columns to pay for its join (plan.rs:9).
+constexpr int32_t kMinSaving = 4;
+
+int standard_code(uint8_t b) {
+  for (int i = 0; i < 5; ++i)
+    if (kStandard[i] == b) return i;
+  return -1;
+}
+
+bool lex_less(const HapView& a, const HapView& b) {
+  return std::lexicographical_compare(a.bases, a.bases + a.len, b.bases, b.bases + b.len);
+}
+
+// Ordering of the reversed byte strings (plan.rs:128).
+bool rev_less(const HapView& a, const HapView& b) {
+  const int32_t n = std::min(a.len, b.len);
+  for (int32_t i = 0; i < n; ++i) {
+    const uint8_t x = a.bases[a.len - 1 - i], y = b.bases[b.len - 1 - i];
+    if (x != y) return x < y;
+  }
+  return a.len < b.len;
+}
+
+int32_t common_prefix(const HapView& a, const HapView& b) {
+  const int32_t n = std::min(a.len, b.len);
+  int32_t i = 0;
+  while (i < n && a.bases[i] == b.bases[i]) ++i;
+  return i;
+}
+
+int32_t common_suffix(const HapView& a, const HapView& b) {
+  const int32_t n = std::min(a.len, b.len);
+  int32_t i = 0;
+  while (i < n && a.bases[a.len - 1 - i] == b.bases[b.len - 1 - i]) ++i;
+  return i;
+}
+
+bool same(const HapView& a, const HapView& b) {
+  return a.len == b.len && std::memcmp(a.bases, b.bases, a.len) == 0;
+}
+
+// Distinct haplotypes ordered by reversed bases (plan.rs:116-144).
+struct SuffixOrder {
+  std::vector<int32_t> order, lcs, pos;
+
+  SuffixOrder(const std::vector<HapView>& bases, const std::vector<int32_t>& distinct) {
+    order = distinct;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int32_t a, int32_t b) { return rev_less(bases[a], bases[b]); });
+    lcs.assign(order.size(), 0);
+    for (size_t r = 1; r < order.size(); ++r) lcs[r] = common_suffix(bases[order[r - 1]], bases[order[r]]);
+    pos.assign(bases.size(), 0);
+    for (size_t r = 0; r < order.size(); ++r) pos[order[r]] = static_cast<int32_t>(r);
+  }
+
+  int32_t longest_shared(int32_t r) const {
+    const int32_t next = (static_cast<size_t>(r) + 1 < lcs.size()) ? lcs[r + 1] : 0;
+    return std::max(lcs[r], next);
+  }
+};
+
+// Node numbering in call order (plan.rs:200-235); ids are deterministic because they depend only on
+// the order of node_for calls.
+struct NodeNumbering {
+  std::map<std::pair<int32_t, int32_t>, int32_t> ids;
+
+  int32_t node_for(const std::vector<BackwardSweep>& sweeps, const std::vector<int32_t>& sweep_at,
+                   const std::vector<int32_t>& lcs, int32_t r, int32_t depth) {
+    if (depth == 0) return 0;
+    int32_t p = r;
+    int32_t shared = std::numeric_limits<int32_t>::max();
+    for (;;) {
+      const int32_t s = sweep_at[p];
+      if (s >= 0 && sweeps[s].resume < depth && depth <= sweeps[s].need) {
+        auto key = std::make_pair(s, depth);
+        auto it = ids.find(key);
+        if (it != ids.end()) return it->second;
+        const int32_t next = static_cast<int32_t>(ids.size()) + 1;
+        ids.emplace(key, next);
+        return next;
+      }
+      shared = std::min(shared, lcs[p]);
+      if (!(p > 0 && shared >= depth)) throw std::logic_error("backward depth is never computed");
+      --p;
+    }
+  }
+};
+
+SuffixPlan forward_only(size_t n) {
+  SuffixPlan p;
+  p.cuts.assign(n, Cut{-1, -1});
+  p.nodes = 1;
+  return p;
+}
+
+// SuffixPlan::new, plan.rs:61-89.
+SuffixPlan suffix_plan(const std::vector<HapView>& bases, const std::vector<int32_t>& lcp,
+                       const std::vector<uint8_t>& dup) {
+  const size_t n = bases.size();
+  std::vector<int32_t> distinct;
+  for (size_t k = 0; k < n; ++k)
+    if (!dup[k]) distinct.push_back(static_cast<int32_t>(k));
+  SuffixOrder suffixes(bases, distinct);
+
+  // cut_depths, plan.rs:148-168.
+  std::vector<int32_t> depth(n, 0);
+  for (size_t t = 0; t < distinct.size(); ++t) {
+    const int32_t k = distinct[t];
+    const int32_t next_lcp = (t + 1 < distinct.size()) ? lcp[distinct[t + 1]] : 0;
+    const int32_t shared_prefix = std::max(lcp[k], next_lcp);
+    const int32_t len = bases[k].len;
+    if (shared_prefix < len) {
+      const int32_t d = std::min(suffixes.longest_shared(suffixes.pos[k]), len - shared_prefix - 1);
+      if (d >= kMinSaving) depth[k] = d;
+    }
+  }
+
+  // backward_sweeps, plan.rs:173-196.
+  SuffixPlan plan;
+  std::vector<int32_t> sweep_at(suffixes.order.size(), -1);
+  int32_t reach = 0;
+  for (size_t r = 0; r < suffixes.order.size(); ++r) {
+    const int32_t k = suffixes.order[r];
+    const int32_t resume = std::min(suffixes.lcs[r], reach);
+    if (depth[k] > resume) {
+      sweep_at[r] = static_cast<int32_t>(plan.sweeps.size());
+      plan.sweeps.push_back(BackwardSweep{k, resume, depth[k], 0, {}});
+    }
+    reach = std::max(resume, depth[k]);
+  }
+
+  NodeNumbering numbering;
+  std::vector<int32_t> starts;
+  for (const auto& s : plan.sweeps)
+    starts.push_back(numbering.node_for(plan.sweeps, sweep_at, suffixes.lcs, suffixes.pos[s.hap], s.resume));
+  plan.cuts.assign(n, Cut{-1, -1});
+  for (int32_t k : distinct) {
+    if (depth[k] > 0) {
+      const int32_t node = numbering.node_for(plan.sweeps, sweep_at, suffixes.lcs, suffixes.pos[k], depth[k]);
+      plan.cuts[k] = Cut{bases[k].len - depth[k], node};
+    }
+  }
+  for (size_t i = 0; i < plan.sweeps.size(); ++i) plan.sweeps[i].start = starts[i];
+  for (const auto& [key, node] : numbering.ids) plan.sweeps[key.first].writes.emplace_back(key.second, node);
+  for (auto& s : plan.sweeps) std::sort(s.writes.begin(), s.writes.end());
+  plan.nodes = static_cast<int32_t>(numbering.ids.size()) + 1;
+  return plan;
+}
+
+}  // namespace
+
+SortedHaps SortedHaps::make(const std::vector<HapView>& haps, bool share_suffixes) {
+  SortedHaps s;
+  const size_t n = haps.size();
+  s.order.resize(n);
+  for (size_t i = 0; i < n; ++i) s.order[i] = static_cast<int32_t>(i);
+  std::stable_sort(s.order.begin(), s.order.end(), [&](int32_t a, int32_t b) { return lex_less(haps[a], haps[b]); });
+  s.bases.reserve(n);
+  for (int32_t i : s.order) s.bases.push_back(haps[i]);
+  for (const auto& h : s.bases)
+    for (int32_t j = 0; j < h.len; ++j) {
+      const uint8_t b = h.bases[j];
+      if (standard_code(b) < 0 && std::find(s.extra_bases.begin(), s.extra_bases.end(), b) == s.extra_bases.end())
+        s.extra_bases.push_back(b);
+    }
+  if (s.extra_bases.size() > 250) throw std::invalid_argument("more than 250 distinct non-ACGTN haplotype bytes");
+  s.codes.resize(n);
+  for (size_t k = 0; k < n; ++k) {
+    const HapView& h = s.bases[k];
+    s.codes[k].resize(h.len);
+    for (int32_t j = 0; j < h.len; ++j) {
+      const uint8_t b = h.bases[j];
+      const int c = standard_code(b);
+      s.codes[k][j] = c >= 0 ? static_cast<uint8_t>(c)
+                             : static_cast<uint8_t>(5 + (std::find(s.extra_bases.begin(), s.extra_bases.end(), b) -
+                                                         s.extra_bases.begin()));
+    }
+  }
+  s.lcp.assign(n, 0);
+  s.dup.assign(n, 0);
+  for (size_t k = 1; k < n; ++k) {
+    s.lcp[k] = common_prefix(s.bases[k - 1], s.bases[k]);
+    s.dup[k] = same(s.bases[k - 1], s.bases[k]) ? 1 : 0;
+  }
+  for (const auto& h : s.bases) s.max_len = std::max(s.max_len, h.len);
+  s.plan = share_suffixes ? suffix_plan(s.bases, s.lcp, s.dup) : forward_only(n);
+  return s;
+}
+
+uint8_t SortedHaps::byte_of_code(int code) const {
+  return code < 5 ? kStandard[code] : extra_bases[code - 5];
+}
+
+SharedColumns SortedHaps::columns() const {
+  SharedColumns c;
+  for (size_t k = 0; k < bases.size(); ++k) {
+    if (dup[k]) continue;
+    const int32_t len = bases[k].len;
+    const int32_t stop = plan.cuts[k].column >= 0 ? plan.cuts[k].column - 1 : len;
+    c.prefix_only += static_cast<uint64_t>(len - lcp[k]);
+    c.forward += static_cast<uint64_t>(stop - lcp[k]);
+  }
+  for (const auto& s : plan.sweeps) c.backward += static_cast<uint64_t>(s.need - s.resume);
+  return c;
+}
+
+void code_table(const SortedHaps& s, uint8_t out[256]) {
+  std::memset(out, kNoCode, 256);
+  for (int c = 0; c < s.num_codes(); ++c) out[s.byte_of_code(c)] = static_cast<uint8_t>(c);
+}
+
+void emit_program(const SortedHaps& s, bool with_suffix, ProgramBuild& out) {
+  const size_t n = s.bases.size();
+  const double init_f64 = std::ldexp(1.0, 1020);
+  const double init_f32 = std::ldexp(1.0, 120);
+
+  // Per column, how many haplotypes still to come start from it (kernel.rs:556-562).
+  std::vector<int32_t> lcp_counts(static_cast<size_t>(s.max_len) + 1, 0);
+  for (size_t k = 1; k < n; ++k)
+    if (!s.dup[k]) lcp_counts[s.lcp[k]]++;
+  std::vector<int32_t> slot_of_col(static_cast<size_t>(s.max_len) + 1, -1);
+  int32_t n_slots = 0;
+  for (int32_t c = 1; c <= s.max_len; ++c)
+    if (lcp_counts[c] > 0) slot_of_col[c] = n_slots++;
+  std::vector<int32_t> slot_len(n_slots, 0);  // haplotype length of the last writer, 0 = unwritten
+
+  for (size_t k = 0; k < n; ++k) {
+    if (s.dup[k]) continue;
+    const int32_t start = s.lcp[k];
+    if (k > 0) lcp_counts[start]--;
+    const int32_t len = s.bases[k].len;
+    const Cut cut = with_suffix ? s.plan.cuts[k] : Cut{-1, -1};
+    const int32_t stop = cut.column >= 0 ? cut.column - 1 : len;
+    if (stop < start) throw std::logic_error("cut before the shared prefix");
+    Segment seg{};
+    seg.hap = static_cast<int32_t>(k);
+    seg.node = cut.column >= 0 ? cut.node : -1;
+    seg.cut_code = cut.column >= 0 ? s.codes[k][cut.column - 1] : 0;
+    int32_t src_len = 1;
+    seg.slot_in = -1;
+    if (start > 0) {
+      seg.slot_in = slot_of_col[start];
+      if (seg.slot_in < 0 || slot_len[seg.slot_in] == 0) throw std::logic_error("snapshot read before written");
+      src_len = slot_len[seg.slot_in];
+    }
+    seg.scale_d = static_cast<double>(src_len) / static_cast<double>(len);
+    seg.scale_f = static_cast<float>(seg.scale_d);
+    seg.init_d = init_f64 / static_cast<double>(len);
+    seg.init_f = static_cast<float>(init_f32 / static_cast<double>(len));
+    out.segs.push_back(seg);
+    if (stop > start) {
+      for (int32_t j = start + 1; j <= stop; ++j) {
+        uint16_t e = s.codes[k][j - 1];
+        if (j == start + 1) e |= EV_BEGIN;
+        if (j == stop) e |= EV_END;
+        if (lcp_counts[j] > 0) {
+          e |= EV_SNAP;
+          out.snap_slots.push_back(slot_of_col[j]);
+          slot_len[slot_of_col[j]] = len;
+        }
+        out.fwd.push_back(e);
+      }
+    } else {
+      out.fwd.push_back(EV_BEGIN | EV_END | EV_NOCOMP);
+    }
+    out.fwd_columns += static_cast<uint64_t>(stop - start);
+  }
+  out.n_slots = n_slots;
+
+  out.n_nodes = 0;
+  if (with_suffix && !s.plan.sweeps.empty()) {
+    // Node 0: the last column of every haplotype, computed from the all-zero column beyond it.
+    out.bwd.push_back(EV_SWEEP | EV_NODE);
+    out.sweep_starts.push_back(-1);
+    out.node_writes.push_back(0);
+    for (const auto& sw : s.plan.sweeps) {
+      const int32_t len = s.bases[sw.hap].len;
+      const int32_t right = len - sw.resume, left = len - sw.need;
+      out.sweep_starts.push_back(sw.start);
+      size_t w = 0;
+      for (int32_t j = right - 1; j >= left; --j) {
+        uint16_t e = s.codes[sw.hap][j];  // base at column j + 1, emitted moving down-right from column j
+        if (j == right - 1) e |= EV_SWEEP;
+        if (w < sw.writes.size() && len - sw.writes[w].first == j) {
+          e |= EV_NODE;
+          out.node_writes.push_back(sw.writes[w].second);
+          ++w;
+        }
+        out.bwd.push_back(e);
+      }
+      if (w != sw.writes.size()) throw std::logic_error("backward write outside its sweep");
+      out.bwd_columns += static_cast<uint64_t>(sw.need - sw.resume);
+    }
+    out.n_nodes = s.plan.nodes;
+  }
+}
+
+}  // namespace fgkl

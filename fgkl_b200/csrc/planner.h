@@ -1,0 +1,80 @@
+// Host-side haplotype sorter and sharing planner.
+//
+// Restates, bit for bit, fgkl's plain-kernel planning:
+//   SortedHaps::new        crates/pairhmm/src/kernel.rs:53-81   (stable lexicographic sort, LCP,
+//                                                                duplicate flags, prior codes)
+//   SuffixPlan::new        crates/pairhmm/src/plan.rs:61-89     (cut depths, backward sweeps, node
+//                                                                numbering; MIN_SAVING = 4)
+//   SharedColumns          crates/pairhmm/src/plan.rs:93-113
+// and turns the result into the column stream the sm_100a kernels walk (program.h).
+#pragma once
+#include <cstdint>
+#include <utility>
+#include <vector>
+
+#include "program.h"
+
+namespace fgkl {
+
+struct HapView {
+  const uint8_t* bases;
+  int32_t len;
+};
+
+struct Cut {
+  int32_t column;  // forward sweep stops at column - 1 and joins backward node `node` at `column`
+  int32_t node;
+};
+
+struct BackwardSweep {
+  int32_t hap;     // sorted index of the haplotype whose bases the sweep follows
+  int32_t resume;  // depth of the start node
+  int32_t need;    // deepest depth computed
+  int32_t start;   // node holding depth `resume`
+  std::vector<std::pair<int32_t, int32_t>> writes;  // (depth, node), ascending
+};
+
+struct SuffixPlan {
+  std::vector<Cut> cuts;  // per sorted haplotype; column == -1 means no cut
+  std::vector<BackwardSweep> sweeps;
+  int32_t nodes = 1;
+};
+
+struct SharedColumns {
+  uint64_t prefix_only = 0, forward = 0, backward = 0;
+};
+
+struct SortedHaps {
+  std::vector<int32_t> order;  // order[k] = caller index of sorted haplotype k
+  std::vector<HapView> bases;  // sorted
+  std::vector<std::vector<uint8_t>> codes;
+  std::vector<int32_t> lcp;
+  std::vector<uint8_t> dup;
+  std::vector<uint8_t> extra_bases;  // bytes outside ACGTN, first-seen order over sorted haplotypes
+  int32_t max_len = 0;
+  SuffixPlan plan;
+
+  static SortedHaps make(const std::vector<HapView>& haps, bool share_suffixes);
+  int num_codes() const { return 5 + static_cast<int>(extra_bases.size()); }
+  uint8_t byte_of_code(int code) const;
+  SharedColumns columns() const;
+};
+
+// Host copy of one program (program.h), before it is concatenated into a batch.
+struct ProgramBuild {
+  std::vector<uint16_t> fwd, bwd;
+  std::vector<Segment> segs;
+  std::vector<int32_t> snap_slots, node_writes, sweep_starts;
+  int32_t n_slots = 0, n_nodes = 0;
+  // Σ(forward columns) and Σ(backward columns) per read row, for the computed-cell count.
+  uint64_t fwd_columns = 0, bwd_columns = 0;
+};
+
+// The forward (and, with `with_suffix`, backward) column stream of a sorted haplotype set.
+void emit_program(const SortedHaps& s, bool with_suffix, ProgramBuild& out);
+
+// 256-entry byte -> prior code table of a sorted set (kNoCode for bytes no haplotype holds that
+// are not A, C, G, T or N).
+void code_table(const SortedHaps& s, uint8_t out[256]);
+
+}  // namespace fgkl

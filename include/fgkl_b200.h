@@ -1,0 +1,171 @@
+/*
+ * fgkl_b200: the PairHMM / PD-HMM read-versus-haplotype likelihood path of fulcrumgenomics/fgkl,
+ * rebuilt for NVIDIA B200 (sm_100a), behind a plain C ABI.
+ *
+ * Every entry point takes plain pointers and sizes, returns 0 (FGKL_OK) or a negative FGKL_E_*
+ * code, and never aborts; fgkl_last_error() gives the calling thread's last message. Likelihoods
+ * are log10 values written row-major, out[read * num_haplotypes + haplotype], in the caller's
+ * read and haplotype order, exactly as fgkl's PairHmm::compute_log10_likelihoods
+ * (crates/pairhmm/src/lib.rs:270-293) and its JNI entry points (crates/jni/src/lib.rs:159-254).
+ *
+ * Threading: any number of threads may call concurrently. The per-call entry points use a
+ * context private to the calling thread (created on first use), mirroring fgkl's thread-local
+ * workspaces (crates/pairhmm/src/kernel.rs:144-163). Explicit contexts must not be shared between
+ * threads without external locking.
+ */
+#ifndef FGKL_B200_H
+#define FGKL_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes; the first five mirror fgkl's Error enum (crates/pairhmm/src/lib.rs:303-323) ---- */
+#define FGKL_OK 0
+#define FGKL_E_EMPTY_READ (-1)                  /* Error::EmptyRead */
+#define FGKL_E_MISMATCHED_READ_ARRAYS (-2)      /* Error::MismatchedReadArrays */
+#define FGKL_E_EMPTY_HAPLOTYPE (-3)             /* Error::EmptyHaplotype */
+#define FGKL_E_MISMATCHED_HAPLOTYPE_ARRAYS (-4) /* Error::MismatchedHaplotypeArrays */
+#define FGKL_E_OUTPUT_LENGTH (-5)               /* Error::OutputLength */
+#define FGKL_E_BAD_OFFSETS (-6)                 /* offset table checks of crates/jni/src/lib.rs:343-363 */
+#define FGKL_E_INVALID_ARGUMENT (-7)            /* NULL pointer or negative size */
+#define FGKL_E_UNSUPPORTED (-8)                 /* a read of 512 or more bases */
+#define FGKL_E_NO_DEVICE (-9)                   /* no CUDA device, or not an sm_100 part */
+#define FGKL_E_CUDA (-10)                       /* CUDA runtime error (message in fgkl_last_error) */
+
+/* How to compute (crates/pairhmm/src/lib.rs:211-238). */
+typedef struct fgkl_config {
+  int32_t double_precision; /* 0: FP32 with FP64 recomputation of lost pairs (Precision::Float) */
+  int32_t double_fallback;  /* recompute lost pairs; 0 leaves them NaN (lib.rs:218-222) */
+  int32_t share_suffixes;   /* suffix sharing for the plain PairHMM (lib.rs:223-226) */
+} fgkl_config;
+
+/* Counters of one call. */
+typedef struct fgkl_stats {
+  uint64_t fallback_pairs;    /* pairs lost by the first pass (PairHmm::fallback_pairs, lib.rs:263-268) */
+  uint64_t rescue_reads;      /* reads recomputed in FP64 */
+  uint64_t nominal_cells;     /* Σ over regions of Σ read lengths x Σ haplotype lengths */
+  uint64_t computed_cells;    /* forward + backward DP cells the first pass computed */
+  uint64_t forward_cells;
+  uint64_t backward_cells;
+  uint64_t prefix_only_cells; /* forward cells with prefix sharing alone */
+  uint64_t kernel_launches;   /* kernels launched by the call's run phase */
+} fgkl_stats;
+
+/* The five read arrays of one call, concatenated, delimited by `offsets` (num_reads + 1 entries,
+ * starting at 0, non-decreasing, ending at the array length), as the JNI boundary passes them. */
+typedef struct fgkl_reads {
+  const uint8_t* bases;   int64_t bases_len;
+  const uint8_t* quals;   int64_t quals_len;
+  const uint8_t* ins_gop; int64_t ins_gop_len;
+  const uint8_t* del_gop; int64_t del_gop_len;
+  const uint8_t* gcp;     int64_t gcp_len;
+  const int32_t* offsets; int64_t offsets_len;
+} fgkl_reads;
+
+/* Concatenated haplotypes; `flags` (same length as `bases`) only for the PD-HMM. */
+typedef struct fgkl_haplotypes {
+  const uint8_t* bases;   int64_t bases_len;
+  const uint8_t* flags;   int64_t flags_len;
+  const int32_t* offsets; int64_t offsets_len;
+} fgkl_haplotypes;
+
+/*
+ * Per-call PairHMM: the drop-in for
+ *   Java_com_fulcrumgenomics_fgkl_pairhmm_FgklPairHmm_computeNative  (crates/jni/src/lib.rs:159-195)
+ * which builds PairHmm::new(&config(double)) (lib.rs:247-251) and calls
+ * compute_log10_likelihoods (lib.rs:270-293). `out_len` must be num_reads * num_haplotypes.
+ */
+int fgkl_pairhmm_compute(const fgkl_reads* reads, const fgkl_haplotypes* haps, int32_t double_precision,
+                         double* out, int64_t out_len);
+
+/* As fgkl_pairhmm_compute with an explicit Config (lib.rs:211-238) and call counters. */
+int fgkl_pairhmm_compute_config(const fgkl_reads* reads, const fgkl_haplotypes* haps, const fgkl_config* config,
+                                double* out, int64_t out_len, fgkl_stats* stats);
+
+/*
+ * Per-call PD-HMM: the drop-in for
+ *   Java_com_fulcrumgenomics_fgkl_pdhmm_FgklPdHmm_computeNative  (crates/jni/src/lib.rs:206-254)
+ * (PdPairHmm::compute_log10_likelihoods, crates/pairhmm/src/pd.rs:251-279).
+ */
+int fgkl_pdhmm_compute(const fgkl_reads* reads, const fgkl_haplotypes* haps, int32_t double_precision,
+                       double* out, int64_t out_len);
+int fgkl_pdhmm_compute_config(const fgkl_reads* reads, const fgkl_haplotypes* haps, const fgkl_config* config,
+                              double* out, int64_t out_len, fgkl_stats* stats);
+
+/* Name of the backend, the analogue of backendNative (crates/jni/src/lib.rs:149-156). */
+const char* fgkl_backend(void);
+
+/* The calling thread's last error message ("" when none). */
+const char* fgkl_last_error(void);
+
+/* ---- batched form: many regions, one planned upload, persistent launches ---- */
+
+typedef struct fgkl_context fgkl_context;
+
+/* Regions concatenated: region g owns region_reads[g] consecutive reads and region_haps[g]
+ * consecutive haplotypes; its output block of region_reads[g] x region_haps[g] likelihoods
+ * follows the previous region's. Offsets are byte offsets (total + 1 entries, starting at 0). */
+typedef struct fgkl_batch {
+  int32_t num_regions;
+  const int32_t* region_reads;
+  const int32_t* region_haps;
+  const uint8_t* bases;
+  const uint8_t* quals;
+  const uint8_t* ins_gop;
+  const uint8_t* del_gop;
+  const uint8_t* gcp;
+  const int64_t* read_offsets;
+  const uint8_t* hap_bases;
+  const uint8_t* hap_flags; /* NULL for the plain PairHMM; else per-base PD flags */
+  const int64_t* hap_offsets;
+} fgkl_batch;
+
+/* A context on `device`; `stream` is a cudaStream_t to run on, or NULL for a private stream. */
+fgkl_context* fgkl_context_create(int32_t device, void* stream);
+void fgkl_context_destroy(fgkl_context* ctx);
+
+/* Validates and plans the batch on the host and uploads it. */
+int fgkl_batch_prepare(fgkl_context* ctx, const fgkl_batch* batch, const fgkl_config* config);
+/* Enqueues the kernels of the prepared batch on the context's stream, without waiting. The launch
+ * sequence is captured into a CUDA graph on the first call and replayed afterwards. */
+int fgkl_batch_run(fgkl_context* ctx);
+/* Waits for the stream and copies the likelihoods (Σ reads x haplotypes) and counters back. */
+int fgkl_batch_fetch(fgkl_context* ctx, double* out, int64_t out_len, fgkl_stats* stats);
+/* prepare + run + fetch. */
+int fgkl_batch_compute(fgkl_context* ctx, const fgkl_batch* batch, const fgkl_config* config, double* out,
+                       int64_t out_len, fgkl_stats* stats);
+/* Number of likelihoods the prepared batch produces. */
+int64_t fgkl_batch_output_len(const fgkl_context* ctx);
+
+/* ---- synthetic workloads (the analogue of fgkl's crates/pairhmm/src/synthetic.rs) ---- */
+
+typedef struct fgkl_synth fgkl_synth;
+/* A benchmark workload (0-4, see synthetic.h); `regions` 0 keeps its default region count. */
+fgkl_synth* fgkl_synth_config(int32_t which, uint64_t seed, int32_t regions, int32_t threads);
+/* One region drawn exactly as fgkl's Region::generate (pd = 0) or PdRegion::generate (pd = 1). */
+fgkl_synth* fgkl_synth_reference_region(uint64_t seed, int64_t reads, int64_t read_len, int64_t haps, int64_t hap_len,
+                                        int32_t pd);
+/* Points `out` into the workload; sizes = {total reads, read bases, total haplotypes, haplotype bases}. */
+void fgkl_synth_view(const fgkl_synth* s, fgkl_batch* out, int64_t sizes[4]);
+void fgkl_synth_free(fgkl_synth* s);
+
+/* ---- planner diagnostics (SortedHaps::new, kernel.rs:53-81; SuffixPlan::new, plan.rs:61-89) ---- */
+
+/* Sorted order, LCP, duplicate flags, cuts (column -1: none), sweep and node counts and the
+ * SharedColumns {prefix_only, forward, backward} of one haplotype set. */
+int fgkl_plan_describe(const uint8_t* hap_bases, const int32_t* hap_offsets, int32_t num_haps, int32_t share_suffixes,
+                       int32_t* order, int32_t* lcp, uint8_t* dup, int32_t* cut_column, int32_t* cut_node,
+                       int32_t* num_sweeps, int32_t* num_nodes, uint64_t columns[3]);
+/* Backward sweeps: 6 ints each (hap, resume, need, start, first write, write count) and the
+ * (depth, node) writes, 2 ints each. */
+int fgkl_plan_sweeps(const uint8_t* hap_bases, const int32_t* hap_offsets, int32_t num_haps, int32_t* sweeps,
+                     int32_t max_sweeps, int32_t* writes, int32_t max_writes);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FGKL_B200_H */

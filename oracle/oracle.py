@@ -1,0 +1,156 @@
+"""ctypes binding of the CPU oracle (``oracle/liboracle.so``) -- TEST INFRASTRUCTURE ONLY.
+
+Only the tests, the smoke check and the CPU-baseline leg of the benchmark use this module, and only
+as the checker (or the timed CPU reference). The product never imports it.
+
+The oracle restates fgkl's scalar FP64 reference (crates/pairhmm/src/model.rs:37-106,
+reference.rs:20-64, pd_reference.rs:29-118) in C; see pairhmm_oracle.c.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "liboracle.so"
+
+_u8p = C.POINTER(C.c_uint8)
+_i32p = C.POINTER(C.c_int32)
+_f64p = C.POINTER(C.c_double)
+_lib = None
+
+
+def build() -> Path:
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists() or LIB_PATH.stat().st_mtime < (HERE / "pairhmm_oracle.c").stat().st_mtime:
+            build()
+        L = C.CDLL(str(LIB_PATH))
+        L.or_error_prob.restype = C.c_double
+        L.or_error_prob.argtypes = [C.c_int]
+        L.or_match_to_match.restype = C.c_double
+        L.or_match_to_match.argtypes = [C.c_int, C.c_int]
+        L.or_transitions.argtypes = [C.c_int, C.c_int, C.c_int, _f64p]
+        L.or_priors.argtypes = [C.c_int, _f64p]
+        L.or_initial_condition.restype = C.c_double
+        L.or_approximate_log10_sum_log10.restype = C.c_double
+        L.or_approximate_log10_sum_log10.argtypes = [C.c_double, C.c_double]
+        L.or_base_matches_pd.restype = C.c_int
+        L.or_base_matches_pd.argtypes = [C.c_uint8, C.c_uint8]
+        L.or_log10_likelihood.restype = C.c_double
+        L.or_log10_likelihood.argtypes = [_u8p, C.c_int, _u8p, _u8p, _u8p, _u8p, _u8p, C.c_int]
+        L.or_pd_log10_likelihood.restype = C.c_double
+        L.or_pd_log10_likelihood.argtypes = [_u8p, _u8p, C.c_int, _u8p, _u8p, _u8p, _u8p, _u8p, C.c_int]
+        L.or_compute_matrix.argtypes = [_u8p, _u8p, _u8p, _u8p, _u8p, _i32p, C.c_int, _u8p, _u8p, _i32p, C.c_int, _f64p, C.c_int]
+        L.or_adj_log10_likelihood.restype = C.c_double
+        L.or_adj_log10_likelihood.argtypes = [_u8p, C.c_int, _u8p, C.c_int, _f64p, _f64p, _f64p, _f64p]
+        L.or_adj_gradient.restype = C.c_double
+        L.or_adj_gradient.argtypes = [_u8p, C.c_int, _u8p, C.c_int, _f64p, _f64p, _f64p, _f64p, _f64p, _f64p, _f64p, _f64p]
+        _lib = L
+    return _lib
+
+
+def _u8(b) -> np.ndarray:
+    return np.ascontiguousarray(np.frombuffer(bytes(b), np.uint8) if not isinstance(b, np.ndarray) else b, dtype=np.uint8)
+
+
+def _p(a, t):
+    return a.ctypes.data_as(t)
+
+
+def error_prob(q: int) -> float:
+    return lib().or_error_prob(q)
+
+
+def match_to_match(a: int, b: int) -> float:
+    return lib().or_match_to_match(a, b)
+
+
+def transitions(ins: int, dele: int, gcp: int) -> list[float]:
+    t = (C.c_double * 6)()
+    lib().or_transitions(ins, dele, gcp, t)
+    return list(t)
+
+
+def priors(q: int) -> tuple[float, float]:
+    t = (C.c_double * 2)()
+    lib().or_priors(q, t)
+    return t[0], t[1]
+
+
+def initial_condition() -> float:
+    return lib().or_initial_condition()
+
+
+def approximate_log10_sum_log10(a: float, b: float) -> float:
+    return lib().or_approximate_log10_sum_log10(a, b)
+
+
+def base_matches_pd(read_base: int, flags: int) -> bool:
+    return bool(lib().or_base_matches_pd(read_base, flags))
+
+
+def log10_likelihood(hap: bytes, read) -> float:
+    """reference::log10_likelihood (reference.rs:20-64)."""
+    h = _u8(hap)
+    a = [_u8(getattr(read, f)) for f in ("bases", "quals", "ins_gop", "del_gop", "gcp")]
+    return lib().or_log10_likelihood(_p(h, _u8p), h.size, *[_p(x, _u8p) for x in a], a[0].size)
+
+
+def pd_log10_likelihood(bases: bytes, flags: bytes, read) -> float:
+    """pd_reference::log10_likelihood (pd_reference.rs:29-118)."""
+    h, f = _u8(bases), _u8(flags)
+    a = [_u8(getattr(read, x)) for x in ("bases", "quals", "ins_gop", "del_gop", "gcp")]
+    return lib().or_pd_log10_likelihood(_p(h, _u8p), _p(f, _u8p), h.size, *[_p(x, _u8p) for x in a], a[0].size)
+
+
+def compute_matrix(reads, haps, threads: int | None = None) -> np.ndarray:
+    """Every read against every haplotype, ``out[r * len(haps) + h]``; PD when haps carry flags."""
+    threads = threads or os.cpu_count() or 1
+    cols = [np.concatenate([_u8(getattr(r, f)) for r in reads]) for f in ("bases", "quals", "ins_gop", "del_gop", "gcp")]
+    roff = np.zeros(len(reads) + 1, np.int32)
+    np.cumsum([len(r.bases) for r in reads], out=roff[1:])
+    pd = len(haps) > 0 and hasattr(haps[0], "flags")
+    hb = np.concatenate([_u8(h.bases if pd else h) for h in haps])
+    hf = np.concatenate([_u8(h.flags) for h in haps]) if pd else None
+    hoff = np.zeros(len(haps) + 1, np.int32)
+    np.cumsum([len(h.bases if pd else h) for h in haps], out=hoff[1:])
+    out = np.empty(len(reads) * len(haps), np.float64)
+    lib().or_compute_matrix(*[_p(c, _u8p) for c in cols], _p(roff, _i32p), len(reads), _p(hb, _u8p),
+                            _p(hf, _u8p) if hf is not None else None, _p(hoff, _i32p), len(haps), _p(out, _f64p), threads)
+    return out
+
+
+def workload_matrix(workload, regions=None, threads: int | None = None) -> np.ndarray:
+    """Oracle results of a synthetic workload's regions, concatenated in output order."""
+    parts = []
+    for g in (regions if regions is not None else range(workload.num_regions)):
+        reads, haps = workload.region(g)
+        parts.append(compute_matrix(reads, haps, threads) if reads and haps else np.zeros(0))
+    return np.concatenate(parts) if parts else np.zeros(0)
+
+
+def adj_log10_likelihood(hap: bytes, read_bases: bytes, d_ins, d_del, eps, err) -> float:
+    """log10 L under the continuous parameterisation (dI, dD, eps, e per read position)."""
+    h, b = _u8(hap), _u8(read_bases)
+    arrs = [np.ascontiguousarray(x, np.float64) for x in (d_ins, d_del, eps, err)]
+    return lib().or_adj_log10_likelihood(_p(h, _u8p), h.size, _p(b, _u8p), b.size, *[_p(a, _f64p) for a in arrs])
+
+
+def adj_gradient(hap: bytes, read_bases: bytes, d_ins, d_del, eps, err):
+    """(log10 L, d/d dI, d/d dD, d/d eps, d/d e) per read position, FP64 forward-backward."""
+    h, b = _u8(hap), _u8(read_bases)
+    arrs = [np.ascontiguousarray(x, np.float64) for x in (d_ins, d_del, eps, err)]
+    g = [np.zeros(b.size, np.float64) for _ in range(4)]
+    ll = lib().or_adj_gradient(_p(h, _u8p), h.size, _p(b, _u8p), b.size, *[_p(a, _f64p) for a in arrs],
+                               *[_p(x, _f64p) for x in g])
+    return (ll, *g)

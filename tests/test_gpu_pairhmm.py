@@ -1,0 +1,309 @@
+"""GPU parity of the plain PairHMM against the FP64 oracle, through the C ABI.
+
+Restates the reference's own tests (crates/pairhmm/src/lib.rs:583-1097) with its regions (rebuilt
+draw for draw from their seeds), tolerances (1e-9 log10 in double, 1e-4 in float) and bit-identity
+invariants. The "every backend" loops collapse to the one sm_100a backend.
+"""
+import numpy as np
+import pytest
+
+from fgkl_b200 import Config, PairHmm, Precision, Read, plan, synthetic
+from oracle import oracle as O
+from refgen import Rng, edited
+
+pytestmark = pytest.mark.gpu
+
+FLOAT = Config(precision=Precision.FLOAT)
+DOUBLE = Config(precision=Precision.DOUBLE)
+
+
+def region(seed, num_reads, read_len, num_haps, hap_len):
+    return synthetic.reference_region(seed, num_reads, read_len, num_haps, hap_len).region(0)
+
+
+def reference_all(reads, haps):
+    return O.compute_matrix(reads, haps)
+
+
+def compute(config, reads, haps):
+    return PairHmm(config).compute_log10_likelihoods(reads, haps)
+
+
+def compute_counting(config, reads, haps):
+    hmm = PairHmm(config)
+    out = hmm.compute_log10_likelihoods(reads, haps)
+    return out, hmm.fallback_pairs()
+
+
+def assert_close(actual, expected, tol, what=""):
+    assert actual.shape == expected.shape
+    d = np.abs(actual - expected)
+    worst = int(np.argmax(d))
+    assert np.all(d <= tol), f"{what}: pair {worst}: got {actual[worst]}, expected {expected[worst]} (diff {d[worst]})"
+    assert np.isfinite(d).all()
+
+
+def cfg(precision, share):
+    return Config(precision=precision, double_fallback=True, share_suffixes=share)
+
+
+def simple_read(bases: bytes, q=30):
+    n = len(bases)
+    return Read(bases, bytes([q] * n), bytes([45] * n), bytes([45] * n), bytes([10] * n))
+
+
+def test_double_precision_matches_reference(gpu):
+    reads, haps = region(11, 70, 120, 24, 300)
+    assert_close(compute(DOUBLE, reads, haps), reference_all(reads, haps), 1e-9, "double")
+
+
+def test_single_precision_matches_reference_within_float_tolerance(gpu):
+    reads, haps = region(11, 70, 120, 24, 300)
+    assert_close(compute(FLOAT, reads, haps), reference_all(reads, haps), 1e-4, "float")
+
+
+def test_haplotype_order_does_not_change_results(gpu):
+    reads, haps = region(11, 70, 120, 24, 300)
+    fwd = compute(DOUBLE, reads, haps)
+    rev = compute(DOUBLE, reads, haps[::-1])
+    n = len(haps)
+    for r in range(len(reads)):
+        for h in range(n):
+            assert abs(fwd[r * n + h] - rev[r * n + (n - 1 - h)]) < 1e-11
+
+
+def test_prefix_sharing_handles_nested_and_repeated_prefixes(gpu):
+    haps = [b"ABBC", b"AAAC", b"AC", b"AAAB", b"ABBB", b"AAAC", b"ABBCC"]
+    reads, _ = region(3, 20, 6, 1, 8)
+    assert_close(compute(DOUBLE, reads, haps), reference_all(reads, haps), 1e-9)
+
+
+def test_haplotypes_of_different_lengths_share_prefixes_correctly(gpu):
+    haps = [b"ACGTACGTAC", b"ACGTACGT", b"ACGTACGTACGTACGT", b"ACGT", b"A"]
+    reads, _ = region(9, 40, 12, 1, 16)
+    assert_close(compute(DOUBLE, reads, haps), reference_all(reads, haps), 1e-9)
+
+
+def test_non_acgtn_bases_match_only_themselves(gpu):
+    reads = [Read(b"ACRTN", bytes([30] * 5), bytes([45] * 5), bytes([45] * 5), bytes([10] * 5))]
+    haps = [b"ACRTG", b"ACGTG", b"ACNTG", b"RRRRR"]
+    expected = reference_all(reads, haps)
+    assert_close(compute(DOUBLE, reads, haps), expected, 1e-9)
+    assert expected[0] > expected[1]
+    assert expected[2] >= expected[0]
+
+
+def test_float_underflow_falls_back_to_double(gpu):
+    reads = [Read(b"A" * 80, bytes([40] * 80), bytes([45] * 80), bytes([45] * 80), bytes([10] * 80))]
+    haps = [b"C" * 80]
+    expected = reference_all(reads, haps)
+    assert np.isfinite(expected[0]) and expected[0] < -50.0
+    assert_close(compute(FLOAT, reads, haps), expected, 1e-9)
+
+
+def suffix_sharing_region():
+    return region(21, 90, 150, 40, 260)
+
+
+def test_suffix_sharing_matches_reference_in_double(gpu):
+    reads, haps = suffix_sharing_region()
+    assert sum(c is not None for c in plan(haps).cuts) > 20
+    assert_close(compute(cfg(Precision.DOUBLE, True), reads, haps), reference_all(reads, haps), 1e-9)
+
+
+def test_suffix_sharing_matches_reference_in_float_within_tolerance(gpu):
+    reads, haps = suffix_sharing_region()
+    assert_close(compute(cfg(Precision.FLOAT, True), reads, haps), reference_all(reads, haps), 1e-4)
+
+
+def test_random_small_haplotype_sets_match_reference_with_suffix_sharing(gpu):
+    rng = Rng(31)
+
+    def letter():
+        return ord("A") if rng.chance(0.5) else ord("C")
+
+    for _ in range(60):
+        haps = [bytes(letter() for _ in range(6 + rng.below(30)))]
+        for _ in range(rng.below(12)):
+            haps.append(edited(rng, b"AC", haps[rng.below(len(haps))]))
+        reads = []
+        for _ in range(1 + rng.below(20)):
+            n = 1 + rng.below(25)
+            reads.append(Read(bytes(letter() for _ in range(n)), bytes(10 + rng.below(31) for _ in range(n)),
+                              bytes(20 + rng.below(26) for _ in range(n)), bytes(20 + rng.below(26) for _ in range(n)),
+                              bytes(1 + rng.below(10) for _ in range(n))))
+        assert_close(compute(cfg(Precision.DOUBLE, True), reads, haps), reference_all(reads, haps), 1e-9)
+
+
+def test_haplotypes_without_a_cut_keep_their_prefix_only_bits(gpu):
+    reads, haps = region(23, 20, 90, 24, 160)
+    p = plan(haps)
+    uncut = [p.order[k] for k in range(len(haps)) if p.cuts[k] is None and not p.dup[k]]
+    assert uncut
+    for precision in (Precision.FLOAT, Precision.DOUBLE):
+        shared = compute(cfg(precision, True), reads, haps)
+        prefix = compute(cfg(precision, False), reads, haps)
+        for r in range(len(reads)):
+            for h in uncut:
+                i = r * len(haps) + h
+                assert shared[i].tobytes() == prefix[i].tobytes(), (precision, r, h)
+
+
+def test_deep_pairs_fall_back_to_double_with_suffix_sharing(gpu):
+    base = bytearray(b"A" * 90)
+    haps = [bytes(base)]
+    for pos in (20, 45, 70):
+        h = bytearray(base)
+        h[pos] = ord("G")
+        haps.append(bytes(h))
+    assert any(c is not None for c in plan(haps).cuts)
+    reads = [Read(b"C" * 70, bytes([40] * 70), bytes([45] * 70), bytes([45] * 70), bytes([10] * 70))]
+    expected = reference_all(reads, haps)
+    assert (expected < -50.0).all()
+    out, fallbacks = compute_counting(cfg(Precision.FLOAT, True), reads, haps)
+    assert fallbacks == len(haps)
+    assert_close(out, expected, 1e-9)
+
+
+def test_likelihoods_below_the_backward_range_are_recomputed_without_suffix_sharing(gpu):
+    rng = Rng(99)
+    reference = bytes(rng.base() for _ in range(700))
+    haps = [reference]
+    for pos in (20, 40, 60):
+        h = bytearray(reference)
+        h[pos] = ord("C") if h[pos] == ord("A") else ord("A")
+        haps.append(bytes(h))
+    assert any(c is not None for c in plan(haps).cuts)
+    reads = []
+    for n in (290, 360, 500):
+        reads.append(Read(bytes(rng.base() for _ in range(n)), bytes([40] * n), bytes([45] * n), bytes([45] * n), bytes([10] * n)))
+    expected = reference_all(reads, haps)
+    assert (expected < -400.0).any()
+    for precision in (Precision.DOUBLE, Precision.FLOAT):
+        assert_close(compute(cfg(precision, True), reads, haps), expected, 1e-9, str(precision))
+
+
+def foreign_reads(seed, n, length):
+    rng = Rng(seed)
+    out = []
+    for _ in range(n):
+        out.append(Read(bytes(rng.base() for _ in range(length)), bytes(20 + rng.below(21) for _ in range(length)),
+                        bytes([45] * length), bytes([45] * length), bytes([10] * length)))
+    return out
+
+
+def test_reads_unrelated_to_every_haplotype_are_recomputed_in_double(gpu):
+    _, haps = region(11, 70, 120, 24, 300)
+    reads = foreign_reads(5, 40, 120)
+    expected = reference_all(reads, haps)
+    assert (expected < -64.0).all()
+    out, fallbacks = compute_counting(FLOAT, reads, haps)
+    assert_close(out, expected, 1e-9)
+    assert fallbacks == expected.size
+
+
+def test_matching_and_mismatching_reads_of_varied_lengths_share_a_batch(gpu):
+    all_reads, haps = region(11, 70, 120, 24, 300)
+    owned = all_reads[:20] + foreign_reads(6, 20, 120)
+    reads = []
+    for i, r in enumerate(owned):
+        n = 30 + (i * 7) % 90
+        reads.append(Read(r.bases[:n], r.quals[:n], r.ins_gop[:n], r.del_gop[:n], r.gcp[:n]))
+    expected = reference_all(reads, haps)
+    out, fallbacks = compute_counting(FLOAT, reads, haps)
+    assert_close(out, expected, 1e-4)
+    assert fallbacks > 0
+
+
+def test_a_read_gets_the_same_bits_whatever_shares_its_batch(gpu):
+    all_reads, haps = region(11, 70, 120, 24, 300)
+    alone = all_reads[:3]
+    batched = all_reads[:3] + foreign_reads(7, 29, 120)
+    for precision in (Precision.FLOAT, Precision.DOUBLE):
+        solo = compute(Config(precision=precision), alone, haps)
+        with_others = compute(Config(precision=precision), batched, haps)
+        assert solo.tobytes() == with_others[: solo.size].tobytes(), precision
+
+
+def test_a_read_gets_the_same_bits_in_a_full_batch_and_in_a_remainder(gpu):
+    reads, haps = region(5, 40, 60, 4, 100)
+    for precision in (Precision.FLOAT, Precision.DOUBLE):
+        config = Config(precision=precision)
+        solo = [compute(config, [r], haps) for r in reads]
+        for n in (1, 2, 3, 16, 17, 31, 33, 40):
+            got = compute(config, reads[:n], haps)
+            for r in range(n):
+                assert got[r * len(haps):(r + 1) * len(haps)].tobytes() == solo[r].tobytes(), (precision, n, r)
+
+
+def test_a_read_matching_only_the_previous_haplotype_is_recomputed_in_double(gpu):
+    rng = Rng(8)
+    reference = bytes(rng.base() for _ in range(300))
+    tail = bytes(rng.base() for _ in range(150))
+    h1 = reference
+    h2 = reference[:150] + tail
+    h3 = bytearray(reference)
+    h3[200] = ord("C") if h3[200] == ord("A") else ord("A")
+    haps = [h1, h2, bytes(h3)]
+    reads = []
+    for k in range(12):
+        source = reference if k % 2 == 0 else h2
+        start = 100 + (k * 13) % 80
+        reads.append(Read(source[start:start + 100], bytes([35] * 100), bytes([45] * 100), bytes([45] * 100), bytes([10] * 100)))
+    expected = reference_all(reads, haps)
+    assert (expected < -64.0).any() and (expected > -10.0).any()
+    out, fallbacks = compute_counting(FLOAT, reads, haps)
+    assert_close(out, expected, 1e-4)
+    assert 0 < fallbacks <= 24
+
+
+def test_more_reads_than_lanes_and_single_read_both_work(gpu):
+    reads, haps = region(21, 1, 50, 3, 60)
+    assert_close(compute(Config(), reads, haps), reference_all(reads, haps), 1e-4, "single")
+    reads, haps = region(22, 37, 50, 3, 60)
+    assert_close(compute(Config(), reads, haps), reference_all(reads, haps), 1e-4, "many")
+
+
+def test_empty_inputs_produce_no_output(gpu):
+    _, haps = region(3, 5, 50, 4, 80)
+    assert compute(FLOAT, [], haps).size == 0
+    reads, _ = region(3, 5, 50, 4, 80)
+    assert compute(FLOAT, reads, []).size == 0
+
+
+# ---- the benchmark workloads at test size ----
+
+def test_single_region_workload_double_and_float(gpu):
+    w = synthetic.workload(0, seed=0)
+    reads, haps = w.region(0)
+    expected = reference_all(reads, haps)
+    assert_close(compute(DOUBLE, reads, haps), expected, 1e-9, "double")
+    assert_close(compute(FLOAT, reads, haps), expected, 1e-4, "float")
+
+
+def test_batched_uneven_regions_match_oracle_and_per_call(gpu):
+    from fgkl_b200 import BatchContext
+
+    w = synthetic.workload(1, seed=3, regions=24)
+    ctx = BatchContext()
+    out, stats = ctx.compute(w, FLOAT)
+    expected = O.workload_matrix(w)
+    assert_close(out, expected, 1e-3, "batched float")
+    assert stats.computed_cells < stats.nominal_cells
+    # The batched form gives every pair the bits the per-call form gives it.
+    offs = w.output_offsets()
+    for g in (0, 5, 23):
+        reads, haps = w.region(g)
+        assert compute(FLOAT, reads, haps).tobytes() == out[offs[g]:offs[g + 1]].tobytes()
+
+
+def test_shared_prefix_and_suffix_workload_against_unshared_oracle(gpu):
+    from fgkl_b200 import BatchContext
+
+    w = synthetic.workload(2, seed=5, regions=2)
+    ctx = BatchContext()
+    out, stats = ctx.compute(w, FLOAT)
+    expected = O.workload_matrix(w)
+    assert_close(out, expected, 1e-3, "c2 float")
+    assert stats.backward_cells > 0
+    assert stats.forward_cells < 0.5 * stats.prefix_only_cells + stats.forward_cells
