@@ -1,0 +1,367 @@
+"""PairHMM throughput benchmark (GCUPS) on B200, batched vs per-call, with accuracy vs the FP64 oracle.
+
+Workload (one step = one pass of the hot path over the batch): 4096 uneven regions of 8-256 reads
+(75% of length 151, else 50-250) against 2-32 haplotypes whose reference window is the region's
+longest read plus 50-400 bases, FP32 with FP64 recomputation of lost pairs, prefix and suffix
+sharing. GCUPS counts nominal cells (Σ read lengths x Σ haplotype lengths per region), as fgkl's
+pairhmm-bench does (crates/pairhmm/src/bin/bench.rs:59, :102).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank runs its own batch (seed + rank) on its own GPU: regions are independent,
+so there is no data-path collective (weak scaling); the step time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "PairHMM GCUPS, batched vs per-call on one B200, at max |dlog10L| vs FP64 oracle"
+WORKLOAD = ("batched uneven PairHMM: 4096 regions, 8-256 reads (75% of length 151, else 50-250) x 2-32 "
+            "haplotypes (longest read + 50-400 bases), FP32 + FP64 recomputation, prefix+suffix sharing")
+FLOP_FORWARD = 12  # 4 FMUL + 4 FFMA per forward cell (fgkl kernel.rs:1011-1013)
+FLOP_BACKWARD = 11  # 3 FMUL + 4 FFMA per backward cell (kernel.rs:1080-1088)
+L2_BYTES = 126 * 1024 * 1024
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--regions", type=int, default=4096)
+    p.add_argument("--seed", type=int, default=1)
+    p.add_argument("--per-call-regions", type=int, default=128)
+    p.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU work of the oracle sample")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+# ---------------------------------------------------------------------------------------------
+# distributed plumbing
+# ---------------------------------------------------------------------------------------------
+
+def dist_init(n_gpus):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return rank, world, local, pg
+
+
+def barrier(pg, device):
+    if pg is not None:
+        import torch
+
+        t = torch.zeros(1, device=f"cuda:{device}")
+        pg.all_reduce(t)
+        torch.cuda.synchronize(device)
+
+
+def max_over_ranks(pg, value, device):
+    if pg is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{device}")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------------------------
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        cmd = ["nvidia-smi", f"--id={self.device}", "--query-gpu=clocks.sm,clocks.max.sm,power.draw,"
+               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+               "--format=csv,noheader,nounits", "-lms", "200"]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                rows.append((float(parts[0]), float(parts[1]), parts[3:7]))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, flags in rows for i, f in enumerate(flags) if f.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows), "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------------------------
+# CPU baseline: the FP64 oracle on a bounded sample of the same workload (the checker, timed)
+# ---------------------------------------------------------------------------------------------
+
+def cpu_sample_regions(w, target_cells):
+    cells = w.region_nominal_cells()
+    picked, acc = [], 0
+    for g in range(w.num_regions):
+        if acc >= target_cells and picked:
+            break
+        picked.append(g)
+        acc += int(cells[g])
+    return picked, acc
+
+
+def run_oracle(w, regions, threads):
+    from oracle import oracle
+
+    t0 = time.perf_counter()
+    res = oracle.workload_matrix(w, regions, threads)
+    return res, time.perf_counter() - t0
+
+
+# ---------------------------------------------------------------------------------------------
+# the reference arm
+# ---------------------------------------------------------------------------------------------
+
+def reference_arm(args, rank, world, pg):
+    if rank != 0:
+        return
+    from fgkl_b200 import synthetic
+
+    threads = os.cpu_count() or 1
+    w = synthetic.workload(1, seed=args.seed, regions=args.regions, threads=threads)
+    # Calibrate the per-step sample to a few seconds of oracle work on this host.
+    regions, cells = cpu_sample_regions(w, 2e8)
+    _, secs = run_oracle(w, regions, threads)
+    rate = cells / secs
+    per_step_cells = rate * 3.0
+    regions, cells = cpu_sample_regions(w, per_step_cells)
+    for _ in range(args.warmup):
+        run_oracle(w, regions[:1], threads)
+    times = []
+    for _ in range(args.steps):
+        _, s = run_oracle(w, regions, threads)
+        times.append(s)
+    total = sum(times)
+    value = cells * args.steps / total / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "GCUPS", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "regions": args.regions, "seed": args.seed, "sample_regions": len(regions),
+                   "sample_nominal_cells": cells},
+        "cpu_baseline": {"value": value, "unit": "GCUPS", "cores": threads, "kind": "port",
+                         "sample": f"{len(regions)} regions ({cells:.3g} nominal cells) of the workload per step; fgkl's "
+                                   "Rust crate cannot be built here (no cargo), so the scalar FP64 oracle restating "
+                                   "reference.rs runs, one region row per thread"},
+        "e2e": {"value": value, "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------------------------
+
+def ours(args, rank, world, local, pg):
+    import torch
+
+    from fgkl_b200 import BatchContext, Config, PairHmm, Precision, _lib, synthetic
+
+    device = local
+    torch.cuda.set_device(device)
+    threads = os.cpu_count() or 1
+    w = synthetic.workload(1, seed=args.seed + rank, regions=args.regions, threads=threads)
+    nominal = w.nominal_cells()
+    stream = torch.cuda.Stream(device=device)
+    ctx = BatchContext(device=device, stream=stream.cuda_stream)
+    cfg = Config(precision=Precision.FLOAT)
+    n_out = ctx.prepare(w, cfg)
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=f"cuda:{device}")
+
+    # Warm-up (first run also captures the CUDA graph).
+    for _ in range(args.warmup):
+        ctx.run()
+    torch.cuda.synchronize(device)
+    out, stats = ctx.fetch()
+    planned_launches = int(stats.kernel_launches)
+
+    # Timed steps: device-resident inputs, L2 flushed between steps (untimed), events on our stream.
+    times = []
+    barrier(pg, device)
+    torch.cuda.synchronize(device)
+    with ClockSampler(device) as clocks:
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                ev0 = torch.cuda.Event(enable_timing=True)
+                ev1 = torch.cuda.Event(enable_timing=True)
+                ev0.record(stream)
+                ctx.run()
+                ev1.record(stream)
+            ev1.synchronize()
+            times.append(ev0.elapsed_time(ev1) / 1e3)
+    torch.cuda.synchronize(device)
+    barrier(pg, device)
+    step = statistics.mean(times)
+    step_max = max_over_ranks(pg, step, device)
+    out, stats = ctx.fetch()
+    value = nominal * world / step_max / 1e9
+
+    # Roofline of the first-pass kernels: algorithmic FP32 FLOPs over the measured step time.
+    flops = FLOP_FORWARD * stats.forward_cells + FLOP_BACKWARD * stats.backward_cells
+    s_tf, p_tf, clk = C.c_double(), C.c_double(), C.c_double()
+    _lib.lib().fgkl_probe_fp32_tflops(device, C.byref(s_tf), C.byref(p_tf), C.byref(clk))
+    peak = max(s_tf.value, p_tf.value)
+    achieved = flops / step / 1e12
+
+    # End to end: the C-ABI batch call from host buffers (planning, H2D, kernels, D2H).
+    h2d = int(w.bases.size * 5 + w.read_offsets.nbytes)
+    d2h = int(n_out * 8)
+    e2e_times = []
+    ctx2 = BatchContext(device=device)
+    out2 = np.empty(n_out, np.float64)
+    for i in range(max(1, min(3, args.steps))):
+        barrier(pg, device)
+        t0 = time.perf_counter()
+        from fgkl_b200.pairhmm import _check, _ptr
+        b = w.as_batch()
+        c = cfg._c()
+        st = _lib.Stats()
+        _check(_lib.lib().fgkl_batch_compute(ctx2._ctx, C.byref(b), C.byref(c), _ptr(out2, _lib.f64p), n_out, C.byref(st)))
+        e2e_times.append(time.perf_counter() - t0)
+    e2e_step = max_over_ranks(pg, statistics.mean(e2e_times), device)
+    e2e_value = nominal * world / e2e_step / 1e9
+    identical = out2.tobytes() == out.tobytes()
+
+    if rank != 0:
+        barrier(pg, device)
+        return
+
+    # Per-call form: one C-ABI call per region, host buffers, as GATK calls the binding.
+    hmm = PairHmm(cfg)
+    pc_regions = [w.region(g) for g in range(min(args.per_call_regions, w.num_regions))]
+    for reads, haps in pc_regions[:4]:
+        hmm.compute_log10_likelihoods(reads, haps)
+    pc_cells = sum(sum(len(r.bases) for r in reads) * sum(len(h) for h in haps) for reads, haps in pc_regions)
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    for reads, haps in pc_regions:
+        hmm.compute_log10_likelihoods(reads, haps)
+    pc_secs = time.perf_counter() - t0
+    per_call = pc_cells / pc_secs / 1e9
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "GCUPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * step_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "regions": args.regions, "seed": args.seed, "pairs": n_out,
+                   "nominal_cells": nominal, "computed_cells": int(stats.computed_cells),
+                   "forward_cells": int(stats.forward_cells), "backward_cells": int(stats.backward_cells),
+                   "prefix_only_cells": int(stats.prefix_only_cells),
+                   "l2": f"inputs {w.bases.size * 5 / 2**20:.0f} MiB > L2 126 MiB; L2 also flushed (untimed) between steps",
+                   "parallelism": f"region sharding x{world}, no collective"},
+        "computed_gcups": stats.computed_cells / step / 1e9,
+        "fallback_pairs": int(stats.fallback_pairs), "rescue_reads": int(stats.rescue_reads),
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                     "traffic": None,
+                     "peak_source": f"measured FP32 FMA probe on this GPU (scalar {s_tf.value:.1f}, packed {p_tf.value:.1f} "
+                                    "TFLOP/s); MEASURED_PEAKS.json holds no FP32 figure",
+                     "flop_per_cell": {"forward": FLOP_FORWARD, "backward": FLOP_BACKWARD}},
+        "e2e": {"value": e2e_value, "unit": "GCUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "includes": "host planning + pinned staging + H2D + kernels + D2H", "bit_identical_to_device_run": identical},
+        "per_call": {"value": per_call, "unit": "GCUPS", "regions": len(pc_regions),
+                     "form": "one fgkl_pairhmm_compute_config call per region from host buffers"},
+        "batched_over_per_call": value / world / per_call,
+        "gpu_launches": planned_launches * args.steps,
+        "clocks": clocks.summary(),
+    }
+
+    if not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        regions, cells = cpu_sample_regions(w, 1e9)
+        ref, secs = run_oracle(w, regions, threads)
+        rate = cells / secs
+        target = args.cpu_seconds * rate
+        if target > cells * 1.5:
+            regions, cells = cpu_sample_regions(w, target)
+            ref, secs = run_oracle(w, regions, threads)
+        offs = w.output_offsets()
+        got = np.concatenate([out[offs[g]:offs[g + 1]] for g in regions])
+        line["max_abs_dlog10"] = float(np.max(np.abs(got - ref)))
+        line["accuracy_sample"] = {"regions": len(regions), "pairs": int(got.size)}
+        line["cpu_baseline"] = {"value": cells / secs / 1e9, "unit": "GCUPS", "cores": threads, "kind": "port",
+                                "sample": f"first {len(regions)} regions ({cells:.3g} nominal cells) of the same batch; "
+                                          "scalar FP64 oracle restating fgkl reference.rs (the Rust crate cannot be "
+                                          "built here)"}
+    print(json.dumps(line), flush=True)
+    barrier(pg, device)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        # The reference arm is host-only: rank 0 times it, other ranks exit without work.
+        reference_arm(args, int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), None)
+        return
+    rank, world, local, pg = dist_init(args.gpus)
+    if False:
+        pass
+    else:
+        ours(args, rank, world, local, pg)
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -122,6 +122,7 @@ def lib() -> C.CDLL:
     L.fgkl_plan_describe.argtypes = [u8p, i32p, C.c_int32, C.c_int32, i32p, i32p, u8p, i32p, i32p, i32p, i32p,
                                      C.POINTER(C.c_uint64)]
     L.fgkl_plan_sweeps.argtypes = [u8p, i32p, C.c_int32, i32p, C.c_int32, i32p, C.c_int32]
+    L.fgkl_probe_fp32_tflops.argtypes = [C.c_int32, f64p, f64p, f64p]
     _lib = L
     return L
 
@@ -135,5 +136,5 @@ EXPORTED = [
     "fgkl_pairhmm_compute", "fgkl_pairhmm_compute_config", "fgkl_pdhmm_compute", "fgkl_pdhmm_compute_config",
     "fgkl_backend", "fgkl_last_error", "fgkl_context_create", "fgkl_context_destroy", "fgkl_batch_prepare",
     "fgkl_batch_run", "fgkl_batch_fetch", "fgkl_batch_compute", "fgkl_batch_output_len", "fgkl_synth_config",
-    "fgkl_synth_reference_region", "fgkl_synth_view", "fgkl_synth_free", "fgkl_plan_describe", "fgkl_plan_sweeps",
+    "fgkl_synth_reference_region", "fgkl_synth_view", "fgkl_synth_free", "fgkl_plan_describe", "fgkl_plan_sweeps", "fgkl_probe_fp32_tflops",
 ]

@@ -41,11 +41,15 @@ class Workload:
 
     def nominal_cells(self) -> int:
         """Σ over regions of Σ read lengths x Σ haplotype lengths (fgkl synthetic.rs:166-170)."""
+        return int(self.region_nominal_cells().sum())
+
+    def region_nominal_cells(self) -> np.ndarray:
+        """Per region: Σ read lengths x Σ haplotype lengths."""
         rl = np.diff(self.read_offsets)
         hl = np.diff(self.hap_offsets)
-        rs = np.add.reduceat(rl, np.r_[0, np.cumsum(self.region_reads)[:-1]]) if rl.size else np.zeros(0)
-        hs = np.add.reduceat(hl, np.r_[0, np.cumsum(self.region_haps)[:-1]]) if hl.size else np.zeros(0)
-        return int(np.dot(rs.astype(np.int64), hs.astype(np.int64)))
+        rs = np.add.reduceat(rl, np.r_[0, np.cumsum(self.region_reads)[:-1]]) if rl.size else np.zeros(0, np.int64)
+        hs = np.add.reduceat(hl, np.r_[0, np.cumsum(self.region_haps)[:-1]]) if hl.size else np.zeros(0, np.int64)
+        return rs.astype(np.int64) * hs.astype(np.int64)
 
     def as_batch(self) -> _lib.Batch:
         u8 = _lib.u8p

@@ -140,6 +140,12 @@ int fgkl_batch_compute(fgkl_context* ctx, const fgkl_batch* batch, const fgkl_co
 /* Number of likelihoods the prepared batch produces. */
 int64_t fgkl_batch_output_len(const fgkl_context* ctx);
 
+/* ---- measurement support ---- */
+
+/* Measured FP32 FMA throughput of `device` (TFLOP/s) with scalar FFMA and packed FP32x2 FFMA chains:
+ * the denominator of the kernels' FP32 roofline. */
+int fgkl_probe_fp32_tflops(int32_t device, double* scalar_tflops, double* packed_tflops, double* sm_clock_mhz);
+
 /* ---- synthetic workloads (the analogue of fgkl's crates/pairhmm/src/synthetic.rs) ---- */
 
 typedef struct fgkl_synth fgkl_synth;
