@@ -14,14 +14,17 @@ namespace fgkl {
 namespace {
 
 constexpr int kWarpsPerBlock = 4;
-constexpr int kRowBins = 17;  // rows-per-lane values 1..16 index the recomputation queues
-constexpr int64_t kMaxReadLen = 511;
+constexpr int kRowBins = 21;  // rows-per-lane values 1..20 index the recomputation queues
+constexpr int64_t kMaxReadLen = 620;  // 31 rows per lane x 20 rows
+
+// Rows per lane: lane 0 holds only padding rows, so 31 * rows >= len.
+int packed_rows(int len) { return (len + 30) / 31; }
 
 size_t align_up(size_t x, size_t a = 256) { return (x + a - 1) / a * a; }
 
-// Rows per lane for one read on the single-read kinds: 32 * rows > len, even above 8.
+// Rows per lane for one read on the single-read kinds: 31 * rows >= len, even above 8.
 int single_rows(int len) {
-  int rows = len / 32 + 1;
+  int rows = packed_rows(len);
   if (rows > 8) rows = (rows + 1) & ~1;
   return rows;
 }
@@ -82,6 +85,11 @@ Engine::Engine(int device, cudaStream_t stream) : device_(device), stream_(strea
   cudaMemcpy(d_err_, t.error_prob.data(), sizeof(double) * t.error_prob.size(), cudaMemcpyHostToDevice);
   cudaMemcpy(d_m2m_, t.m2m.data(), sizeof(double) * t.m2m.size(), cudaMemcpyHostToDevice);
   cudaMalloc(&d_counters_, sizeof(Counters));
+  for (int i = 0; i < kAuxStreams; ++i) {
+    cudaStreamCreateWithFlags(&aux_[i], cudaStreamNonBlocking);
+    cudaEventCreateWithFlags(&join_[i], cudaEventDisableTiming);
+  }
+  cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming);
 }
 
 Engine::~Engine() {
@@ -99,6 +107,11 @@ Engine::~Engine() {
   cudaFree(d_err_);
   cudaFree(d_m2m_);
   if (h_stage_) cudaFreeHost(h_stage_);
+  for (int i = 0; i < kAuxStreams; ++i) {
+    cudaStreamDestroy(aux_[i]);
+    cudaEventDestroy(join_[i]);
+  }
+  cudaEventDestroy(fork_);
   if (own_stream_) cudaStreamDestroy(stream_);
 }
 
@@ -154,7 +167,7 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
       if (len <= 0) return fail(FGKL_E_EMPTY_READ, "read " + std::to_string(r - first_read[g]) + " has no bases");
       if (len > kMaxReadLen)
         return fail(FGKL_E_UNSUPPORTED, "read " + std::to_string(r - first_read[g]) + " has " + std::to_string(len) +
-                                            " bases; reads of at most 511 bases are supported");
+                                            " bases; reads of at most 620 bases are supported");
     }
     for (int64_t h = first_hap[g]; h < first_hap[g + 1]; ++h)
       if (in.hap_off[h + 1] - in.hap_off[h] <= 0)
@@ -174,33 +187,29 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
     for (auto& th : pool) th.join();
   }
 
-  // Concatenate the programs.
+  // Concatenate the programs; each stream gets kStreamPad zero entries on both sides.
   std::vector<Region> regions(static_cast<size_t>(N));
   std::vector<HapInfo> haps;
-  std::vector<uint16_t> stream;
+  std::vector<uint32_t> stream(kStreamPad, 0u);
   std::vector<Segment> segs;
-  std::vector<int32_t> snaps, nodew, sweeps;
+  std::vector<Sweep> sweeps;
   std::vector<uint8_t> codes(static_cast<size_t>(N) * 256);
   int max_slots = 1, max_nodes = 1, max_segs = 1;
+  auto put_stream = [&](const std::vector<uint32_t>& v, int32_t& off, int32_t& len) {
+    off = static_cast<int32_t>(stream.size());
+    len = v.empty() ? 0 : static_cast<int32_t>(v.size()) - 1;  // the last entry only carries post events
+    stream.insert(stream.end(), v.begin(), v.end());
+    stream.insert(stream.end(), kStreamPad, 0u);
+  };
   auto put_program = [&](const ProgramBuild& b, Program& p) {
-    p.fwd_off = static_cast<int32_t>(stream.size());
-    p.fwd_len = static_cast<int32_t>(b.fwd.size());
-    stream.insert(stream.end(), b.fwd.begin(), b.fwd.end());
-    p.bwd_off = static_cast<int32_t>(stream.size());
-    p.bwd_len = static_cast<int32_t>(b.bwd.size());
-    stream.insert(stream.end(), b.bwd.begin(), b.bwd.end());
+    put_stream(b.fwd, p.fwd_off, p.fwd_len);
+    put_stream(b.bwd, p.bwd_off, p.bwd_len);
     p.seg_off = static_cast<int32_t>(segs.size());
     p.n_segs = static_cast<int32_t>(b.segs.size());
     segs.insert(segs.end(), b.segs.begin(), b.segs.end());
-    p.snap_off = static_cast<int32_t>(snaps.size());
-    p.n_snaps = static_cast<int32_t>(b.snap_slots.size());
-    snaps.insert(snaps.end(), b.snap_slots.begin(), b.snap_slots.end());
-    p.nodew_off = static_cast<int32_t>(nodew.size());
-    p.n_nodew = static_cast<int32_t>(b.node_writes.size());
-    nodew.insert(nodew.end(), b.node_writes.begin(), b.node_writes.end());
     p.sweep_off = static_cast<int32_t>(sweeps.size());
-    p.n_sweeps = static_cast<int32_t>(b.sweep_starts.size());
-    sweeps.insert(sweeps.end(), b.sweep_starts.begin(), b.sweep_starts.end());
+    p.n_sweeps = static_cast<int32_t>(b.sweeps.size());
+    sweeps.insert(sweeps.end(), b.sweeps.begin(), b.sweeps.end());
     p.n_slots = b.n_slots;
     p.n_nodes = b.n_nodes;
     max_slots = std::max(max_slots, b.n_slots);
@@ -253,14 +262,14 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
             {cost_cols * rows, Task{g, {static_cast<int32_t>(first_read[g] + order[i]), -1}, rows}});
       }
     } else {
-      while (i < order.size() && len_of(order[i]) >= 256) {
+      while (i < order.size() && packed_rows(len_of(order[i])) > 8) {
         const int rows = single_rows(len_of(order[i]));
         by_bin[{Kind::kOneF32, rows}].push_back(
             {cost_cols * rows, Task{g, {static_cast<int32_t>(first_read[g] + order[i]), -1}, rows}});
         ++i;
       }
       for (; i < order.size(); i += 2) {
-        const int rows = len_of(order[i]) / 32 + 1;
+        const int rows = packed_rows(len_of(order[i]));
         const int32_t a = static_cast<int32_t>(first_read[g] + order[i]);
         const int32_t b = i + 1 < order.size() ? static_cast<int32_t>(first_read[g] + order[i + 1]) : -1;
         by_bin[{Kind::kPackedF32, rows}].push_back({cost_cols * rows, Task{g, {a, b}, rows}});
@@ -268,17 +277,24 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
     }
   }
   std::vector<Task> tasks;
-  size_t scratch_total = 256;
+  std::vector<std::pair<uint64_t, Bin>> first;
   for (auto& [key, list] : by_bin) {
     std::stable_sort(list.begin(), list.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
-    Bin b{key.kind, key.rows, static_cast<int>(tasks.size()), static_cast<int>(list.size()), 0};
-    for (auto& e : list) tasks.push_back(e.second);
+    Bin b{key.kind, key.rows, static_cast<int>(tasks.size()), static_cast<int>(list.size()), 0, 0, 0};
+    uint64_t cost = 0;
+    for (auto& e : list) {
+      tasks.push_back(e.second);
+      cost += e.first;
+    }
     int per_sm = 0, threads = 0;
     occupancy(b.kind, b.rows, &per_sm, &threads);
     if (per_sm <= 0) return fail(FGKL_E_CUDA, "kernel instantiation unavailable on this device");
     b.blocks = std::max(1, std::min((b.n_tasks + kWarpsPerBlock - 1) / kWarpsPerBlock, per_sm * sms_));
-    bins_.push_back(b);
+    first.push_back({cost, b});
   }
+  // The bin with the most work launches first; the others fill the SMs its tail frees.
+  std::stable_sort(first.begin(), first.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+  for (auto& f : first) bins_.push_back(f.second);
   std::vector<int> queue_off(kRowBins, 0);
   {
     int acc = 0;
@@ -293,29 +309,30 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
       int per_sm = 0, threads = 0;
       occupancy(Kind::kOneF64, r, &per_sm, &threads);
       if (per_sm <= 0) return fail(FGKL_E_CUDA, "recomputation kernel unavailable on this device");
-      Bin b{Kind::kOneF64, r, queue_off[r], rescue_count[r], 0};
+      Bin b{Kind::kOneF64, r, queue_off[r], rescue_count[r], 0, 0, 0};
       b.blocks = std::max(1, std::min((b.n_tasks + kWarpsPerBlock - 1) / kWarpsPerBlock, per_sm * sms_));
       rescue_bins_.push_back(b);
     }
   }
-  scratch_stride_ = 0;
-  for (const auto* list : {&bins_, &rescue_bins_})
-    for (const Bin& b : *list) {
-      const size_t stride = align_up(scratch_bytes(b.kind, b.rows, max_slots, max_nodes, max_segs));
-      scratch_stride_ = std::max(scratch_stride_, stride);
+  // Bins of one pass run concurrently, so each owns a slice of the scratch.
+  size_t scratch_total = 256;
+  for (auto* list : {&bins_, &rescue_bins_}) {
+    size_t off = 0;
+    for (Bin& b : *list) {
+      b.stride = align_up(scratch_bytes(b.kind, b.rows, max_slots, max_nodes, max_segs));
+      b.scratch_off = off;
+      off += static_cast<size_t>(b.blocks) * kWarpsPerBlock * b.stride;
     }
-  for (const auto* list : {&bins_, &rescue_bins_})
-    for (const Bin& b : *list) scratch_total = std::max(scratch_total, static_cast<size_t>(b.blocks) * kWarpsPerBlock * scratch_stride_);
+    scratch_total = std::max(scratch_total, off);
+  }
 
-  // Plan blob: regions | haps | stream | segs | snaps | node writes | sweep starts | code tables.
+  // Plan blob: regions | haps | stream | segs | sweeps | code tables.
   std::vector<uint8_t> blob;
-  size_t o_regions, o_haps, o_stream, o_segs, o_snaps, o_nodew, o_sweeps, o_codes;
+  size_t o_regions, o_haps, o_stream, o_segs, o_sweeps, o_codes;
   append_section(blob, regions, o_regions);
   append_section(blob, haps, o_haps);
   append_section(blob, stream, o_stream);
   append_section(blob, segs, o_segs);
-  append_section(blob, snaps, o_snaps);
-  append_section(blob, nodew, o_nodew);
   append_section(blob, sweeps, o_sweeps);
   append_section(blob, codes, o_codes);
 
@@ -377,11 +394,9 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
   view_.read_off = d_read_off_;
   view_.regions = reinterpret_cast<const Region*>(d_plan_ + o_regions);
   view_.haps = reinterpret_cast<const HapInfo*>(d_plan_ + o_haps);
-  view_.stream = reinterpret_cast<const uint16_t*>(d_plan_ + o_stream);
+  view_.stream = reinterpret_cast<const uint32_t*>(d_plan_ + o_stream);
   view_.segs = reinterpret_cast<const Segment*>(d_plan_ + o_segs);
-  view_.snap_slots = reinterpret_cast<const int32_t*>(d_plan_ + o_snaps);
-  view_.node_writes = reinterpret_cast<const int32_t*>(d_plan_ + o_nodew);
-  view_.sweep_starts = reinterpret_cast<const int32_t*>(d_plan_ + o_sweeps);
+  view_.sweeps = reinterpret_cast<const Sweep*>(d_plan_ + o_sweeps);
   view_.code_of_byte = d_plan_ + o_codes;
   view_.err_prob = d_err_;
   view_.m2m = d_m2m_;
@@ -403,42 +418,39 @@ int Engine::run() {
   if ((rc = check(cudaMemsetAsync(d_counters_, 0, sizeof(Counters), stream_), "reset counters"))) return rc;
   planned_.kernel_launches = 0;
   int i = 0;
-  for (const Bin& b : bins_) {
-    LaunchArgs a{};
-    a.v = view_;
-    a.tasks = d_tasks_ + b.task_off;
-    a.n_tasks = b.n_tasks;
-    a.count = nullptr;
-    a.task_counter = counters + i++;
-    a.scratch = d_scratch_;
-    a.scratch_stride = scratch_stride_;
-    a.use_prefix = cfg_.share_suffixes ? 0 : 1;
-    a.rescue = 0;
-    a.queue = cfg_.double_fallback ? d_queue_ : nullptr;
-    a.queue_off = queue_off;
-    a.queue_tail = queue_tail;
-    a.min_accept_plain = cfg_.double_precision ? 0 : 1;
-    if ((rc = check(launch(b.kind, b.rows, b.blocks, a, stream_), "first-pass launch"))) return rc;
-    planned_.kernel_launches++;
-  }
-  for (const Bin& b : rescue_bins_) {
-    LaunchArgs a{};
-    a.v = view_;
-    a.tasks = d_queue_ + b.task_off;
-    a.n_tasks = b.n_tasks;
-    a.count = queue_tail + b.rows;
-    a.task_counter = counters + i++;
-    a.scratch = d_scratch_;
-    a.scratch_stride = scratch_stride_;
-    a.use_prefix = 1;
-    a.rescue = 1;
-    a.queue = nullptr;
-    a.queue_off = queue_off;
-    a.queue_tail = queue_tail;
-    a.min_accept_plain = 0;
-    if ((rc = check(launch(b.kind, b.rows, b.blocks, a, stream_), "recomputation launch"))) return rc;
-    planned_.kernel_launches++;
-  }
+  // Each pass forks its bins onto the auxiliary streams and joins them back.
+  auto pass = [&](const std::vector<Bin>& list, bool rescue) -> int {
+    if (list.empty()) return FGKL_OK;
+    if ((rc = check(cudaEventRecord(fork_, stream_), "fork"))) return rc;
+    for (size_t b = 0; b < list.size(); ++b) {
+      const Bin& bin = list[b];
+      cudaStream_t s = aux_[b % kAuxStreams];
+      if ((rc = check(cudaStreamWaitEvent(s, fork_, 0), "fork wait"))) return rc;
+      LaunchArgs a{};
+      a.v = view_;
+      a.tasks = (rescue ? d_queue_ : d_tasks_) + bin.task_off;
+      a.n_tasks = bin.n_tasks;
+      a.count = rescue ? queue_tail + bin.rows : nullptr;
+      a.task_counter = counters + i++;
+      a.scratch = d_scratch_ + bin.scratch_off;
+      a.scratch_stride = bin.stride;
+      a.use_prefix = rescue ? 1 : (cfg_.share_suffixes ? 0 : 1);
+      a.rescue = rescue ? 1 : 0;
+      a.queue = (!rescue && cfg_.double_fallback) ? d_queue_ : nullptr;
+      a.queue_off = queue_off;
+      a.queue_tail = queue_tail;
+      a.min_accept_plain = (!rescue && !cfg_.double_precision) ? 1 : 0;
+      if ((rc = check(launch(bin.kind, bin.rows, bin.blocks, a, s), rescue ? "recomputation launch" : "first-pass launch")))
+        return rc;
+      planned_.kernel_launches++;
+      if ((rc = check(cudaEventRecord(join_[b % kAuxStreams], s), "join"))) return rc;
+    }
+    for (size_t b = 0; b < std::min<size_t>(list.size(), kAuxStreams); ++b)
+      if ((rc = check(cudaStreamWaitEvent(stream_, join_[b], 0), "join wait"))) return rc;
+    return FGKL_OK;
+  };
+  if ((rc = pass(bins_, false))) return rc;
+  if ((rc = pass(rescue_bins_, true))) return rc;
   return FGKL_OK;
 }
 
@@ -462,8 +474,6 @@ int Engine::fetch(double* out, int64_t out_len, BatchStats* stats) {
     *stats = planned_;
     stats->fallback_pairs = h_cnt->lost_pairs;
     stats->rescue_reads = h_cnt->rescue_reads;
-    stats->device_fwd_columns = h_cnt->fwd_columns;
-    stats->device_bwd_columns = h_cnt->bwd_columns;
   }
   return FGKL_OK;
 }

@@ -39,8 +39,6 @@ struct BatchStats {
   uint64_t forward_cells = 0;
   uint64_t backward_cells = 0;
   uint64_t prefix_only_cells = 0;   // forward cells prefix sharing alone would compute
-  uint64_t device_fwd_columns = 0;  // stream positions the kernels walked (cross-check)
-  uint64_t device_bwd_columns = 0;
   uint64_t kernel_launches = 0;     // launches issued by the last run()
 };
 
@@ -75,7 +73,10 @@ class Engine {
     int task_off;  // into the device task array
     int n_tasks;
     int blocks;
+    size_t stride;       // scratch bytes per warp
+    size_t scratch_off;  // this bin's slice of the scratch
   };
+  static constexpr int kAuxStreams = 8;
   template <class T>
   T* grow(T*& ptr, size_t& cap, size_t n);
   int fail(int code, const std::string& msg);
@@ -85,6 +86,9 @@ class Engine {
   int sms_ = 0;
   cudaStream_t stream_ = nullptr;
   bool own_stream_ = false;
+  cudaStream_t aux_[kAuxStreams] = {};
+  cudaEvent_t join_[kAuxStreams] = {};
+  cudaEvent_t fork_ = nullptr;
   std::string error_;
   EngineConfig cfg_;
   BatchStats planned_;
@@ -117,7 +121,6 @@ class Engine {
   // Prepared batch.
   BatchView view_{};
   std::vector<Bin> bins_, rescue_bins_;
-  size_t scratch_stride_ = 0;
   int64_t out_len_ = 0;
   int n_small_ = 0;
 };

@@ -1,26 +1,34 @@
-// sm_100a PairHMM kernels: one warp per read task, read rows on lanes, columns streamed as an
-// anti-diagonal wavefront.
+// sm_100a PairHMM kernels: one warp per read task, read rows on lanes, the region's column stream
+// walked as an anti-diagonal wavefront.
 //
-// Lane l holds rows l*R .. l*R+R-1 of a 32*R-row block whose LAST row is the read's last row; the
-// rows above the read are padding rows whose transitions reproduce row 0 of GATK's matrix (M = X =
-// 0 and a constant deletion value of INITIAL / haplotype length), so the row just above the read
-// plays row 0 and every read ends on lane 31's last row. At loop step t lane l computes stream
-// position t - l (forward) or t - (31 - l) (backward); the row above (below) arrives from the
-// neighbouring lane by one shuffle per state value per step.
+// Rows. Lane l holds rows l*R .. l*R+R-1 of a 32*R-row block whose LAST row is the read's last row
+// and R = ceil(len / 31), so lane 0 holds only padding rows. Padding rows have zero transitions and
+// priors and a deletion chain of 1: they keep M = X = 0 and Y = INITIAL / hap_len, i.e. they
+// reproduce row 0 of GATK's matrix, the row just above the read plays row 0, and lane 0 feeds
+// itself exact row-0 values through the shuffle. At loop step t lane l is at stream position t - l
+// (forward) or t - (31 - l) (backward); the row above (below) arrives by one shuffle per value.
 //
 // Forward recurrence per cell (GATK LoglessPairHMM, fgkl kernel.rs:1011-1013):
 //   M = prior * (mm*M(i-1,j-1) + im*(X(i-1,j-1) + Y(i-1,j-1)))
 //   X = mi*M(i-1,j) + ii*X(i-1,j)          Y = md*M(i,j-1) + dd*Y(i,j-1)
-// The single-precision kernels carry X/mi and Y/md instead of X and Y (per-row constants), which
-// turns the X and Y updates into one FMA each: 6 FP32 operations per cell instead of 8. Every term
-// stays positive, so the change of variables costs no accuracy; an overflow it could cause in
-// pathological gap-open ratios surfaces as a non-finite result, which the double-precision
-// recomputation replaces. The double-precision kernels use the plain recurrence.
+// The FP32 kernels carry X/mi and Y/md (per-row constants) instead of X and Y: every term stays
+// positive, the X and Y updates become one FMA each, 6 FP32 operations per cell instead of 8. An
+// overflow this could cause for extreme gap-open ratios surfaces as a non-finite result, which is
+// recomputed in FP64 with the plain recurrence.
 //
-// Backward recurrence (suffix sharing, fgkl kernel.rs:1080-1088) per cell, row i from row i+1:
+// Backward recurrence (suffix sharing, fgkl kernel.rs:1080-1088), row i from row i+1:
 //   into = prior(i+1,j+1) * BM(i+1,j+1);  BX = ii'*BX(i+1,j) + im'*into
 //   BY = dd*BY(i,j+1) + im'*into;         BM = md*BY(i,j+1) + mi'*BX(i+1,j) + mm'*into
-// with primed transitions those of row i+1, plus BACKWARD_SCALE at the read's last row.
+// (primed: transitions of row i+1), plus BACKWARD_SCALE at the read's last row. The padding row
+// above the read accumulates fgkl's row-0 start mass `s` in its BY (dd = 1 there).
+//
+// Events. A lane handles all events of a step in one divergent branch: the stores for the previous
+// column (SNAP, END, NODE) and then the loads for its own (BEGIN, SWEEP). Start states come from a
+// per-warp ping-pong staging buffer in shared memory: the previous segment writes it directly when
+// it is the snapshot's last writer, otherwise the state is prefetched from global scratch with
+// cp.async at the previous segment's BEGIN. Joins only store their forward column; the products
+// with the backward node are summed after the sweep, warp-wide, in an order fixed by the read row.
+#include <cuda_pipeline.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -109,16 +117,29 @@ struct Consts;
 template <>
 struct Consts<false> {
   static constexpr double kBackwardScale = 1329227995784915872903807060280344576.0;  // 2^120
-  static constexpr double kLog10Initial = 36.123599479677743;                         // 120*log10(2)
+  static constexpr double kLog10Initial = 120.0 * 0.301029995663981195213738894724493027;
   static constexpr double kMinAccepted = 1e-28;
   static constexpr double kMinAcceptedJoined = 1e-28;
 };
 template <>
 struct Consts<true> {
   static constexpr double kBackwardScale = 1.0;
-  static constexpr double kLog10Initial = 307.05059557726084;  // 1020*log10(2)
-  static constexpr double kMinAccepted = 0.0;                 // never lost
+  static constexpr double kLog10Initial = 1020.0 * 0.301029995663981195213738894724493027;
+  static constexpr double kMinAccepted = 0.0;  // never lost
   static constexpr double kMinAcceptedJoined = 1e24;
+};
+
+// Per-lane field counts of the scratch records, rounded so every record starts on 16 bytes.
+template <class P, int R>
+struct Layout {
+  using V = typename P::V;
+  static constexpr int kRound = 16 / static_cast<int>(sizeof(V)) > 1 ? 16 / static_cast<int>(sizeof(V)) : 1;
+  static constexpr int up(int x) { return (x + kRound - 1) / kRound * kRound; }
+  static constexpr int kSnap = up(3 * R + 4);  // M, X, Y rows; above-row M, X, Y; accumulated result
+  static constexpr int kNode = up(2 * R + 1);  // BM, BY rows; below-row BM
+  static constexpr int kJoin = 2 * R;          // cut column M and Y rows
+  static constexpr int kStage = kSnap > kNode ? kSnap : kNode;
+  static constexpr size_t kSmemPerWarp = 2ull * 32 * kStage * sizeof(V);
 };
 
 // ---------------------------------------------------------------------------------------------
@@ -190,7 +211,8 @@ struct FwdRows {
         const RowModel m = row_model(v, rd[c], g - rd[c].pad, codes);
         double k0, k1, k2, k3, k4;
         if (P::kTransformed) {
-          // S = mm*M + (im*mi')*X^ + (im*md')*Y^ with X = mi*X^, Y = md*Y^; X^ = M_up + c3*X^_up; Y^ = M_left + gc*Y^_left.
+          // S = mm*M + (im*mi')*X^ + (im*md')*Y^ with X = mi*X^, Y = md*Y^;
+          // X^ = M_up + (gc*mi'/mi)*X^_up; Y^ = M_left + gc*Y^_left.
           if (m.read) {
             k0 = m.mm;
             k1 = m.im * m.mi_prev;
@@ -258,35 +280,47 @@ struct BwdRows {
 };
 
 // ---------------------------------------------------------------------------------------------
-// Per-warp scratch: snapshots, backward nodes, segment results.
+// Scratch: global per-warp records and the shared-memory staging buffers.
 // ---------------------------------------------------------------------------------------------
 
 template <class P, int R>
 struct Scratch {
   using V = typename P::V;
-  static constexpr int kSnapFields = 3 * R + 5;  // M, X, Y rows; above-row M, X, Y; acc M, X
-  static constexpr int kNodeFields = 2 * R + 1;  // BM, BY rows; below-row BM
-  V* snaps;
-  V* nodes;
-  double* seg_acc;   // [seg][c]
-  double* seg_prod;  // [seg][row g][c]
+  using L = Layout<P, R>;
+  V* slots;         // [slot][lane][kSnap]
+  V* nodes;         // [node][lane][kNode]
+  V* joins;         // [seg][lane][kJoin]
+  double* seg_raw;  // [seg][c]
+  V* stage;         // shared: [buf][lane][kStage]
 
-  __device__ Scratch(char* base, int max_slots, int max_nodes, int max_segs) {
-    snaps = reinterpret_cast<V*>(base);
-    nodes = snaps + static_cast<size_t>(max_slots) * kSnapFields * 32;
-    seg_acc = reinterpret_cast<double*>(nodes + static_cast<size_t>(max_nodes) * kNodeFields * 32);
-    seg_prod = seg_acc + static_cast<size_t>(max_segs) * P::NC;
+  __device__ Scratch(char* base, V* smem, int n_slots, int n_nodes, int n_segs) {
+    slots = reinterpret_cast<V*>(base);
+    nodes = slots + static_cast<size_t>(n_slots) * 32 * L::kSnap;
+    joins = nodes + static_cast<size_t>(n_nodes) * 32 * L::kNode;
+    seg_raw = reinterpret_cast<double*>(joins + static_cast<size_t>(n_segs) * 32 * L::kJoin);
+    stage = smem;
   }
-  __device__ V* snap(int slot, int f, int lane) { return snaps + (static_cast<size_t>(slot) * kSnapFields + f) * 32 + lane; }
-  __device__ V* node(int n, int f, int lane) { return nodes + (static_cast<size_t>(n) * kNodeFields + f) * 32 + lane; }
-  __device__ double* prod(int seg, int g, int c) { return seg_prod + (static_cast<size_t>(seg) * 32 * R + g) * P::NC + c; }
+  __device__ V* slot(int s, int lane) { return slots + (static_cast<size_t>(s) * 32 + lane) * L::kSnap; }
+  __device__ V* node(int n, int lane) { return nodes + (static_cast<size_t>(n) * 32 + lane) * L::kNode; }
+  __device__ V* join(int seg, int lane) { return joins + (static_cast<size_t>(seg) * 32 + lane) * L::kJoin; }
+  __device__ V* staged(int buf, int lane) { return stage + (static_cast<size_t>(buf & 1) * 32 + lane) * L::kStage; }
 };
 
 template <class P, int R>
-__host__ __device__ constexpr size_t scratch_size(int max_slots, int max_nodes, int max_segs) {
+__host__ __device__ constexpr size_t scratch_size(int n_slots, int n_nodes, int n_segs) {
   using V = typename P::V;
-  return static_cast<size_t>(max_slots) * (3 * R + 5) * 32 * sizeof(V) + static_cast<size_t>(max_nodes) * (2 * R + 1) * 32 * sizeof(V) +
-         static_cast<size_t>(max_segs) * P::NC * sizeof(double) + static_cast<size_t>(max_segs) * 32 * R * P::NC * sizeof(double);
+  using L = Layout<P, R>;
+  return (static_cast<size_t>(n_slots) * 32 * L::kSnap + static_cast<size_t>(n_nodes) * 32 * L::kNode +
+          static_cast<size_t>(n_segs) * 32 * L::kJoin) * sizeof(V) + static_cast<size_t>(n_segs) * P::NC * sizeof(double);
+}
+
+// Copies `fields` values (a multiple of 16 bytes) from global to shared memory without registers.
+template <class V>
+__device__ __forceinline__ void prefetch(V* dst_smem, const V* src, int fields) {
+  const int chunks = fields * static_cast<int>(sizeof(V)) / 16;
+  for (int i = 0; i < chunks; ++i)
+    __pipeline_memcpy_async(reinterpret_cast<char*>(dst_smem) + 16 * i, reinterpret_cast<const char*>(src) + 16 * i, 16);
+  __pipeline_commit();
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -295,8 +329,9 @@ __host__ __device__ constexpr size_t scratch_size(int max_slots, int max_nodes, 
 
 template <class P, int R>
 __device__ void backward_pass(const LaunchArgs& a, const Program& prog, const ReadRef* rd, const uint8_t* codes, int lane,
-                              Scratch<P, R>& sc, unsigned long long& columns) {
+                              Scratch<P, R>& sc) {
   using V = typename P::V;
+  using L = Layout<P, R>;
   BwdRows<P, R> bp;
   bp.load(a.v, rd, lane, codes);
   const V sink = P::splat(lane == 31 ? static_cast<typename P::S>(Consts<P::kDouble>::kBackwardScale) : 0);
@@ -304,68 +339,80 @@ __device__ void backward_pass(const LaunchArgs& a, const Program& prog, const Re
 #pragma unroll
   for (int r = 0; r < R; ++r) BM[r] = BY[r] = P::zero();
   V dBM = P::zero(), topBM = P::zero(), topBX = P::zero();
-  const uint16_t* stream = a.v.stream + prog.bwd_off;
   const int n = prog.bwd_len;
-  int sweep = prog.sweep_off - 1, nodew = prog.nodew_off;
-  for (int t = 0; t < n + 31; ++t) {
-    V rBM = P::down(topBM), rBX = P::down(topBX);
-    if (lane == 31) rBM = rBX = P::zero();
-    const int p = t - (31 - lane);
-    const bool live = p >= 0 && p < n;
-    const uint16_t ev = live ? __ldg(stream + p) : 0;
-    if (ev & EV_SWEEP) {
-      const int start = a.v.sweep_starts[++sweep];
-      if (start < 0) {
-#pragma unroll
-        for (int r = 0; r < R; ++r) BM[r] = BY[r] = P::zero();
-        dBM = P::zero();
-      } else {
+  const uint32_t* stream = a.v.stream + prog.bwd_off - (31 - lane);  // entry of this lane's position at t
+  int sweep = -1;
+  Sweep nxt = a.v.sweeps[prog.sweep_off];
+  uint32_t ev_next = __ldg(stream);
+  for (int t = 0; t < n + 32; ++t) {
+    const V rBM = P::down(topBM), rBX = P::down(topBX);
+    const uint32_t ev = ev_next;
+    ev_next = __ldg(stream + t + 1);
+    if (ev & kEvMask) {
+      if (ev & EV_NODE) {
+        const uint32_t node = ev >> kPayloadShift;
+        V* g = sc.node(static_cast<int>(node), lane);
+        V* s = (ev & EV_NSTAGE) ? sc.staged(sweep + 1, lane) : nullptr;
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-          BM[r] = *sc.node(start, r, lane);
-          BY[r] = *sc.node(start, R + r, lane);
+          g[r] = BM[r];
+          g[R + r] = BY[r];
+          if (s) {
+            s[r] = BM[r];
+            s[R + r] = BY[r];
+          }
         }
-        dBM = *sc.node(start, 2 * R, lane);
+        g[2 * R] = dBM;
+        if (s) s[2 * R] = dBM;
       }
-    }
-    if (live) {
-      const int code = ev & kCodeMask;
-      const bool isN = code == kCodeN;
-      V belowX = rBX, diagM = dBM;
+      if (ev & EV_SWEEP) {
+        ++sweep;
+        const Sweep cur = nxt;
+        if (sweep + 1 < prog.n_sweeps) nxt = a.v.sweeps[prog.sweep_off + sweep + 1];
+        if (cur.staged) {
+          __pipeline_wait_prior(0);
+          const V* s = sc.staged(sweep, lane);
 #pragma unroll
-      for (int r = R - 1; r >= 0; --r) {
-        const bool m0 = (code == bp.oc[0][r]) | isN;
-        const bool m1 = (code == bp.oc[P::NC - 1][r]) | isN;
-        const V prior = P::sel(m0, m1, bp.pm[r], bp.px[r]);
-        const V into = P::mul(prior, diagM);
-        const V itm = P::mul(into, bp.im[r]);
-        V bx = P::fma(belowX, bp.ii[r], itm);
-        const V by = P::fma(BY[r], bp.dd[r], itm);
-        V bm = P::fma(BY[r], bp.md[r], P::fma(belowX, bp.mi[r], P::mul(into, bp.mm[r])));
-        if (r == R - 1) {
-          bm = P::add(bm, sink);
-          bx = P::add(bx, sink);
+          for (int r = 0; r < R; ++r) {
+            BM[r] = s[r];
+            BY[r] = s[R + r];
+          }
+          dBM = s[2 * R];
+        } else {
+#pragma unroll
+          for (int r = 0; r < R; ++r) BM[r] = BY[r] = P::zero();
+          dBM = P::zero();
         }
-        diagM = BM[r];
-        BM[r] = bm;
-        BY[r] = by;
-        belowX = bx;
+        if (cur.next_node >= 0) prefetch(sc.staged(sweep + 1, lane), sc.node(cur.next_node, lane), L::kNode);
       }
-      topBM = BM[0];
-      topBX = belowX;
-      dBM = rBM;
-      if (lane == 0) ++columns;
     }
-    if (ev & EV_NODE) {
-      const int node = a.v.node_writes[nodew++];
+    const int code = ev & kCodeMask;
+    const bool isN = code == kCodeN;
+    V belowX = rBX, diagM = dBM;
 #pragma unroll
-      for (int r = 0; r < R; ++r) {
-        *sc.node(node, r, lane) = BM[r];
-        *sc.node(node, R + r, lane) = BY[r];
+    for (int r = R - 1; r >= 0; --r) {
+      const bool m0 = (code == bp.oc[0][r]) | isN;
+      const bool m1 = (code == bp.oc[P::NC - 1][r]) | isN;
+      const V prior = P::sel(m0, m1, bp.pm[r], bp.px[r]);
+      const V into = P::mul(prior, diagM);
+      const V itm = P::mul(into, bp.im[r]);
+      V bx = P::fma(belowX, bp.ii[r], itm);
+      const V by = P::fma(BY[r], bp.dd[r], itm);
+      V bm = P::fma(BY[r], bp.md[r], P::fma(belowX, bp.mi[r], P::mul(into, bp.mm[r])));
+      if (r == R - 1) {
+        bm = P::add(bm, sink);
+        bx = P::add(bx, sink);
       }
-      *sc.node(node, 2 * R, lane) = rBM;
+      diagM = BM[r];
+      BM[r] = bm;
+      BY[r] = by;
+      belowX = bx;
     }
+    topBM = BM[0];
+    topBX = belowX;
+    dBM = rBM;
   }
+  __pipeline_wait_prior(0);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -380,218 +427,240 @@ __device__ __forceinline__ typename P::V cell_match(const typename P::V& dM, con
   return P::fma(dY, k1, P::fma(dX, k1, P::mul(dM, k0)));
 }
 
+struct SegState {
+  float scale_f, init_f;
+  double scale_d, init_d;
+  int staged, next_slot, node, cut_code;
+};
+
+__device__ __forceinline__ SegState load_seg(const Segment* s) {
+  SegState r;
+  r.scale_f = s->scale_f;
+  r.init_f = s->init_f;
+  r.scale_d = s->scale_d;
+  r.init_d = s->init_d;
+  r.staged = s->staged;
+  r.next_slot = s->next_slot;
+  r.node = s->node;
+  r.cut_code = s->cut_code;
+  return r;
+}
+
 template <class P, int R>
 __device__ void forward_pass(const LaunchArgs& a, const Program& prog, const ReadRef* rd, const uint8_t* codes, int lane,
-                             Scratch<P, R>& sc, unsigned long long& columns) {
+                             Scratch<P, R>& sc) {
   using V = typename P::V;
   using S = typename P::S;
+  using L = Layout<P, R>;
   FwdRows<P, R> fr;
   fr.load(a.v, rd, lane, codes);
-  // Which of the lane's rows (and the row above them) are padding, per component.
-  unsigned pad_mask[P::NC];
-  bool above_pad[P::NC];
-#pragma unroll
-  for (int c = 0; c < P::NC; ++c) {
-    pad_mask[c] = 0;
-#pragma unroll
-    for (int r = 0; r < R; ++r)
-      if (lane * R + r < rd[c].pad) pad_mask[c] |= 1u << r;
-    above_pad[c] = lane * R - 1 < rd[c].pad;
-  }
-  // X factor of the read's last row (lane 31), turning the accumulated X^ back into X.
-  double last_mi[P::NC];
+  // X factor of the read's last row (lane 31): the accumulated result is Σ M + mi_n * X^.
+  V an;
 #pragma unroll
   for (int c = 0; c < P::NC; ++c)
-    last_mi[c] = (P::kTransformed && rd[c].len > 0) ? err_prob(a.v, a.v.ins[rd[c].off + rd[c].len - 1]) : 1.0;
+    P::put(an, c, static_cast<S>((P::kTransformed && rd[c].len > 0) ? err_prob(a.v, a.v.ins[rd[c].off + rd[c].len - 1]) : 1.0));
 
   V M[R], X[R], Y[R];
 #pragma unroll
   for (int r = 0; r < R; ++r) M[r] = X[r] = Y[r] = P::zero();
-  V dM = P::zero(), dX = P::zero(), dY = P::zero();
-  V aM = P::zero(), aX = P::zero(), aY = P::zero();  // row above at the segment's start column
-  V accM = P::zero(), accX = P::zero();
-  V init = P::zero();
-  Segment seg{};
-  const uint16_t* stream = a.v.stream + prog.fwd_off;
+  V dM = P::zero(), dX = P::zero(), dY = P::zero(), acc = P::zero();
   const int n = prog.fwd_len;
-  int seg_i = -1, snap_i = prog.snap_off;
-  uint16_t ev_next = (lane == 0 && n > 0) ? __ldg(stream) : 0;
-  for (int t = 0; t < n + 31; ++t) {
-    V uM = P::up(M[R - 1]), uX = P::up(X[R - 1]), uY = P::up(Y[R - 1]);
-    const int p = t - lane;
-    const bool live = p >= 0 && p < n;
-    const uint16_t ev = ev_next;
-    ev_next = (p + 1 >= 0 && p + 1 < n) ? __ldg(stream + p + 1) : 0;
-    if (ev & EV_BEGIN) {
-      ++seg_i;
-      seg = a.v.segs[prog.seg_off + seg_i];
-      const S sc_s = P::kDouble ? static_cast<S>(seg.scale_d) : static_cast<S>(seg.scale_f);
-      const S in_s = P::kDouble ? static_cast<S>(seg.init_d) : static_cast<S>(seg.init_f);
-      init = P::splat(in_s);
-      const V scale = P::splat(sc_s);
-      if (seg.slot_in < 0) {
+  const uint32_t* stream = a.v.stream + prog.fwd_off - lane;
+  int seg_i = -1;
+  SegState cur{}, nxt = load_seg(a.v.segs + prog.seg_off);
+  uint32_t ev_next = __ldg(stream);
+
+  // The cut column's match and deletion values entered from the current column, per row, stored
+  // for the join (fgkl kernel.rs:744-755); the row above the lane's top row is (dM, dX, dY).
+  auto end_segment = [&]() {
+    if (lane == 31) {
 #pragma unroll
-        for (int r = 0; r < R; ++r) {
-          M[r] = X[r] = P::zero();
-#pragma unroll
-          for (int c = 0; c < P::NC; ++c) P::put(Y[r], c, (pad_mask[c] >> r) & 1 ? in_s : S(0));
-        }
-        aM = aX = P::zero();
-#pragma unroll
-        for (int c = 0; c < P::NC; ++c) P::put(aY, c, above_pad[c] ? in_s : S(0));
-        accM = accX = P::zero();
-      } else {
-        const int s = seg.slot_in;
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-          M[r] = P::mul(*sc.snap(s, r, lane), scale);
-          X[r] = P::mul(*sc.snap(s, R + r, lane), scale);
-          Y[r] = P::mul(*sc.snap(s, 2 * R + r, lane), scale);
-#pragma unroll
-          for (int c = 0; c < P::NC; ++c)
-            if ((pad_mask[c] >> r) & 1) P::put(Y[r], c, in_s);
-        }
-        aM = P::mul(*sc.snap(s, 3 * R, lane), scale);
-        aX = P::mul(*sc.snap(s, 3 * R + 1, lane), scale);
-        aY = P::mul(*sc.snap(s, 3 * R + 2, lane), scale);
-#pragma unroll
-        for (int c = 0; c < P::NC; ++c)
-          if (above_pad[c]) P::put(aY, c, in_s);
-        accM = P::mul(*sc.snap(s, 3 * R + 3, lane), scale);
-        accX = P::mul(*sc.snap(s, 3 * R + 4, lane), scale);
-      }
-      dM = aM;
-      dX = aX;
-      dY = aY;
+      for (int c = 0; c < P::NC; ++c) sc.seg_raw[seg_i * P::NC + c] = static_cast<double>(P::get(acc, c));
     }
-    if (lane == 0) {
-      uM = uX = P::zero();
-      uY = init;
-    }
-    if (ev & EV_NOCOMP) {
-      uM = aM;
-      uX = aX;
-      uY = aY;
-    }
-    if (live && !(ev & EV_NOCOMP)) {
-      const int code = ev & kCodeMask;
+    if (cur.node >= 0) {
+      const int code = cur.cut_code;
       const bool isN = code == kCodeN;
-      V pM = dM, pX = dX, pY = dY, qM = uM, qX = uX;
+      V* j = sc.join(seg_i, lane);
+      V jM = dM, jX = dX, jY = dY;
 #pragma unroll
       for (int r = 0; r < R; ++r) {
-        const V oM = M[r], oX = X[r], oY = Y[r];
         const bool m0 = (code == fr.oc[0][r]) | isN;
         const bool m1 = (code == fr.oc[P::NC - 1][r]) | isN;
         const V prior = P::sel(m0, m1, fr.pm[r], fr.px[r]);
-        const V nM = P::mul(prior, cell_match<P>(pM, pX, pY, fr.c0[r], fr.c1[r], fr.c2[r]));
-        V nX, nY;
-        if (P::kTransformed) {
-          nX = P::fma(qX, fr.c3[r], qM);
-          nY = P::fma(oY, fr.c4[r], oM);
-        } else {
-          nX = P::fma(qX, fr.c3[r], P::mul(qM, fr.c2[r]));
-          nY = P::fma(oY, fr.c3[r], P::mul(oM, fr.c4[r]));
-        }
-        M[r] = nM;
-        X[r] = nX;
-        Y[r] = nY;
-        pM = oM;
-        pX = oX;
-        pY = oY;
-        qM = nM;
-        qX = nX;
+        j[r] = P::mul(prior, cell_match<P>(jM, jX, jY, fr.c0[r], fr.c1[r], fr.c2[r]));
+        j[R + r] = P::kTransformed ? P::fma(Y[r], fr.c4[r], M[r]) : P::fma(Y[r], fr.c3[r], P::mul(M[r], fr.c4[r]));
+        jM = M[r];
+        jX = X[r];
+        jY = Y[r];
       }
-      dM = uM;
-      dX = uX;
-      dY = uY;
-      accM = P::add(accM, M[R - 1]);
-      accX = P::add(accX, X[R - 1]);
-      if (lane == 0) ++columns;
     }
-    if (ev & EV_SNAP) {
-      const int s = a.v.snap_slots[snap_i++];
+  };
+
+  for (int t = 0; t < n + 32; ++t) {
+    const V uM = P::up(M[R - 1]), uX = P::up(X[R - 1]), uY = P::up(Y[R - 1]);
+    const uint32_t ev = ev_next;
+    ev_next = __ldg(stream + t + 1);
+    if (ev & kEvMask) {
+      if (ev & EV_SNAP) {
+        const uint32_t slot = ev >> kPayloadShift;
+        V* g = slot != kPayloadNone ? sc.slot(static_cast<int>(slot), lane) : nullptr;
+        V* s = (ev & EV_STAGE) ? sc.staged(seg_i + 1, lane) : nullptr;
+        for (int dst = 0; dst < 2; ++dst) {
+          V* o = dst ? s : g;
+          if (!o) continue;
 #pragma unroll
-      for (int r = 0; r < R; ++r) {
-        *sc.snap(s, r, lane) = M[r];
-        *sc.snap(s, R + r, lane) = X[r];
-        *sc.snap(s, 2 * R + r, lane) = Y[r];
-      }
-      *sc.snap(s, 3 * R, lane) = uM;
-      *sc.snap(s, 3 * R + 1, lane) = uX;
-      *sc.snap(s, 3 * R + 2, lane) = uY;
-      *sc.snap(s, 3 * R + 3, lane) = accM;
-      *sc.snap(s, 3 * R + 4, lane) = accX;
-    }
-    if (ev & EV_END) {
-      if (lane == 31) {
-#pragma unroll
-        for (int c = 0; c < P::NC; ++c)
-          sc.seg_acc[seg_i * P::NC + c] =
-              __dadd_rn(static_cast<double>(P::get(accM, c)), __dmul_rn(last_mi[c], static_cast<double>(P::get(accX, c))));
-      }
-      if (seg.node >= 0) {
-        // Join (fgkl kernel.rs:744-755, :767-791): the cut column's match and deletion values,
-        // entered from this column, times the backward node's values, per row in f64.
-        const int code = seg.cut_code;
-        const bool isN = code == kCodeN;
-        V jM = uM, jX = uX, jY = uY;
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-          const bool m0 = (code == fr.oc[0][r]) | isN;
-          const bool m1 = (code == fr.oc[P::NC - 1][r]) | isN;
-          const V prior = P::sel(m0, m1, fr.pm[r], fr.px[r]);
-          const V fM = P::mul(prior, cell_match<P>(jM, jX, jY, fr.c0[r], fr.c1[r], fr.c2[r]));
-          const V fY = P::kTransformed ? P::fma(Y[r], fr.c4[r], M[r]) : P::fma(Y[r], fr.c3[r], P::mul(M[r], fr.c4[r]));
-          const V bM = *sc.node(seg.node, r, lane);
-          const V bY = *sc.node(seg.node, R + r, lane);
-          const int g = lane * R + r;
-#pragma unroll
-          for (int c = 0; c < P::NC; ++c) {
-            double yfac = 1.0;
-            const int q = g - rd[c].pad;
-            if (P::kTransformed && rd[c].len > 0 && q >= 0) yfac = err_prob(a.v, a.v.del[rd[c].off + q]);
-            const double fy = __dmul_rn(yfac, static_cast<double>(P::get(fY, c)));
-            *sc.prod(seg_i, g, c) = __dadd_rn(__dmul_rn(static_cast<double>(P::get(fM, c)), static_cast<double>(P::get(bM, c))),
-                                              __dmul_rn(fy, static_cast<double>(P::get(bY, c))));
+          for (int r = 0; r < R; ++r) {
+            o[r] = M[r];
+            o[R + r] = X[r];
+            o[2 * R + r] = Y[r];
           }
-          jM = M[r];
-          jX = X[r];
-          jY = Y[r];
+          o[3 * R] = dM;
+          o[3 * R + 1] = dX;
+          o[3 * R + 2] = dY;
+          o[3 * R + 3] = acc;
         }
       }
+      if (ev & EV_END) end_segment();
+      if (ev & EV_BEGIN) {
+        ++seg_i;
+        cur = nxt;
+        if (seg_i + 1 < prog.n_segs) nxt = load_seg(a.v.segs + prog.seg_off + seg_i + 1);
+        const S in_s = P::kDouble ? static_cast<S>(cur.init_d) : static_cast<S>(cur.init_f);
+        const S sc_s = P::kDouble ? static_cast<S>(cur.scale_d) : static_cast<S>(cur.scale_f);
+        const V scale = P::splat(sc_s);
+        if (cur.staged) {
+          __pipeline_wait_prior(0);
+          const V* s = sc.staged(seg_i, lane);
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            M[r] = P::mul(s[r], scale);
+            X[r] = P::mul(s[R + r], scale);
+            Y[r] = P::mul(s[2 * R + r], scale);
+          }
+          dM = P::mul(s[3 * R], scale);
+          dX = P::mul(s[3 * R + 1], scale);
+          dY = P::mul(s[3 * R + 2], scale);
+          acc = P::mul(s[3 * R + 3], scale);
+        } else {
+#pragma unroll
+          for (int r = 0; r < R; ++r) M[r] = X[r] = Y[r] = P::zero();
+          dM = dX = dY = acc = P::zero();
+        }
+        // Padding rows (and the row above the lane when it is padding) hold exact row-0 values.
+#pragma unroll
+        for (int c = 0; c < P::NC; ++c) {
+#pragma unroll
+          for (int r = 0; r < R; ++r)
+            if (lane * R + r < rd[c].pad) P::put(Y[r], c, in_s);
+          if (lane * R - 1 < rd[c].pad) P::put(dY, c, in_s);
+        }
+        if (cur.next_slot >= 0) prefetch(sc.staged(seg_i + 1, lane), sc.slot(cur.next_slot, lane), L::kSnap);
+        if (ev & EV_NOCOMP) end_segment();
+      }
     }
+    const int code = ev & kCodeMask;
+    const bool isN = code == kCodeN;
+    V pM = dM, pX = dX, pY = dY, qM = uM, qX = uX;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const V oM = M[r], oX = X[r], oY = Y[r];
+      const bool m0 = (code == fr.oc[0][r]) | isN;
+      const bool m1 = (code == fr.oc[P::NC - 1][r]) | isN;
+      const V prior = P::sel(m0, m1, fr.pm[r], fr.px[r]);
+      const V nM = P::mul(prior, cell_match<P>(pM, pX, pY, fr.c0[r], fr.c1[r], fr.c2[r]));
+      V nX, nY;
+      if (P::kTransformed) {
+        nX = P::fma(qX, fr.c3[r], qM);
+        nY = P::fma(oY, fr.c4[r], oM);
+      } else {
+        nX = P::fma(qX, fr.c3[r], P::mul(qM, fr.c2[r]));
+        nY = P::fma(oY, fr.c3[r], P::mul(oM, fr.c4[r]));
+      }
+      M[r] = nM;
+      X[r] = nX;
+      Y[r] = nY;
+      pM = oM;
+      pX = oX;
+      pY = oY;
+      qM = nM;
+      qX = nX;
+    }
+    dM = uM;
+    dX = uX;
+    dY = uY;
+    acc = P::fma(X[R - 1], an, P::add(acc, M[R - 1]));
   }
+  __pipeline_wait_prior(0);
 }
 
 // ---------------------------------------------------------------------------------------------
-// Finalisation: raw results to log10 likelihoods in the caller's layout.
+// Finalisation: joins, thresholds, log10, and the caller's layout.
 // ---------------------------------------------------------------------------------------------
 
 template <class P, int R>
 __device__ void finalize(const LaunchArgs& a, const Task& task, const Region& region, const Program& prog, const ReadRef* rd,
                          int lane, Scratch<P, R>& sc) {
   using C = Consts<P::kDouble>;
+  double* red = reinterpret_cast<double*>(sc.stage);  // [c][row q], the staging buffers are free now
+  const int max_rows = 32 * R;
+  // Joins (fgkl kernel.rs:767-791): raw = acc + (Σ_rows F_M*B_M + F_Y*B_Y + init*s) / BACKWARD_SCALE,
+  // with the row sum taken in an order fixed by the read row so it does not depend on R.
+  for (int seg = 0; seg < prog.n_segs; ++seg) {
+    const int node = a.v.segs[prog.seg_off + seg].node;
+    if (node < 0) continue;
+    const typename P::V* f = sc.join(seg, lane);
+    const typename P::V* b = sc.node(node, lane);
+    double row0[P::NC];
+#pragma unroll
+    for (int c = 0; c < P::NC; ++c) row0[c] = 0.0;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const typename P::V fM = f[r], fY = f[R + r], bM = b[r], bY = b[R + r];
+#pragma unroll
+      for (int c = 0; c < P::NC; ++c) {
+        const int q = lane * R + r - rd[c].pad;
+        double yfac = 1.0;
+        if (P::kTransformed && rd[c].len > 0 && q >= 0) yfac = err_prob(a.v, a.v.del[rd[c].off + q]);
+        const double fy = __dmul_rn(yfac, static_cast<double>(P::get(fY, c)));
+        const double prod = __dadd_rn(__dmul_rn(static_cast<double>(P::get(fM, c)), static_cast<double>(P::get(bM, c))),
+                                      __dmul_rn(fy, static_cast<double>(P::get(bY, c))));
+        if (q >= 0) red[c * max_rows + q] = prod;
+        if (q == -1) row0[c] = prod;
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int c = 0; c < P::NC; ++c) {
+      double s = 0.0;
+      for (int q = lane; q < rd[c].len; q += 32) s = __dadd_rn(s, red[c * max_rows + q]);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s = __dadd_rn(s, __shfl_xor_sync(kFull, s, o));
+      // Row 0's start mass lives in one lane.
+      const double r0 = __shfl_sync(kFull, row0[c], (rd[c].pad - 1) / R);
+      if (lane == 0 && task.read[c] >= 0) {
+        double* raw = sc.seg_raw + seg * P::NC + c;
+        *raw = __dadd_rn(*raw, __ddiv_rn(__dadd_rn(s, r0), C::kBackwardScale));
+      }
+    }
+    __syncwarp();
+  }
+  __syncwarp();
   bool lost_any[P::NC];
   unsigned long long lost_count = 0;
 #pragma unroll
   for (int c = 0; c < P::NC; ++c) lost_any[c] = false;
   for (int k = lane; k < region.n_haps; k += 32) {
     const HapInfo info = a.v.haps[region.hap_off + k];
-    const Segment seg = a.v.segs[prog.seg_off + info.seg];
+    const bool joined = a.v.segs[prog.seg_off + info.seg].node >= 0;
 #pragma unroll
     for (int c = 0; c < P::NC; ++c) {
       if (task.read[c] < 0) continue;
-      double raw = sc.seg_acc[info.seg * P::NC + c];
+      const double raw = sc.seg_raw[info.seg * P::NC + c];
       bool lost;
-      if (seg.node >= 0) {
-        double sum = 0.0;
-        for (int g = rd[c].pad; g < 32 * R; ++g) sum = __dadd_rn(sum, *sc.prod(info.seg, g, c));
-        sum = __dadd_rn(sum, *sc.prod(info.seg, rd[c].pad - 1, c));
-        raw = __dadd_rn(raw, __ddiv_rn(sum, C::kBackwardScale));
+      if (joined)
         lost = !(raw >= C::kMinAcceptedJoined);
-      } else {
+      else
         lost = a.min_accept_plain ? !(raw >= C::kMinAccepted) : (raw != raw);
-      }
       if (!P::kDouble) lost |= isinf(raw);
       const double result = lost ? __longlong_as_double(0x7ff8000000000000ll) : log10(raw) - C::kLog10Initial;
       const int read_local = task.read[c] - region.read_off;
@@ -614,7 +683,7 @@ __device__ void finalize(const LaunchArgs& a, const Task& task, const Region& re
     const bool any = __any_sync(kFull, lost_any[c]);
     if (any && lane == 0 && a.queue != nullptr) {
       // Queue the read for double-precision recomputation in the bin of its own rows-per-lane.
-      int rows = rd[c].len / 32 + 1;
+      int rows = (rd[c].len + 30) / 31;
       if (rows > 8) rows = (rows + 1) & ~1;
       const int slot = atomicAdd(a.queue_tail + rows, 1);
       a.queue[a.queue_off[rows] + slot] = Task{task.region, {task.read[c], -1}, rows};
@@ -625,10 +694,13 @@ __device__ void finalize(const LaunchArgs& a, const Task& task, const Region& re
 
 template <class P, int R>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) pairhmm_kernel(LaunchArgs a) {
+  using V = typename P::V;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31;
-  const int warp = blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+  const int warp_in_block = threadIdx.x >> 5;
+  const int warp = blockIdx.x * kWarpsPerBlock + warp_in_block;
+  V* smem = reinterpret_cast<V*>(smem_raw + warp_in_block * Layout<P, R>::kSmemPerWarp);
   const int count = a.count ? *a.count : a.n_tasks;
-  unsigned long long fcols = 0, bcols = 0;
   for (;;) {
     int t = 0;
     if (lane == 0) t = atomicAdd(a.task_counter, 1);
@@ -651,29 +723,30 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) pairhmm_kernel(LaunchArgs
       rd[c].pad = 32 * R - rd[c].len;
     }
     const uint8_t* codes = a.v.code_of_byte + region.code_off;
-    Scratch<P, R> sc(a.scratch + static_cast<size_t>(warp) * a.scratch_stride, region.shared.n_slots > region.prefix.n_slots ? region.shared.n_slots : region.prefix.n_slots,
-                     region.shared.n_nodes, region.shared.n_segs);
-    if (prog.bwd_len > 0) backward_pass<P, R>(a, prog, rd, codes, lane, sc, bcols);
-    forward_pass<P, R>(a, prog, rd, codes, lane, sc, fcols);
+    const int n_slots = region.shared.n_slots > region.prefix.n_slots ? region.shared.n_slots : region.prefix.n_slots;
+    Scratch<P, R> sc(a.scratch + static_cast<size_t>(warp) * a.scratch_stride, smem, n_slots, region.shared.n_nodes,
+                     region.shared.n_segs);
+    if (prog.bwd_len > 0) backward_pass<P, R>(a, prog, rd, codes, lane, sc);
+    __syncwarp();
+    forward_pass<P, R>(a, prog, rd, codes, lane, sc);
     __syncwarp();
     finalize<P, R>(a, task, region, prog, rd, lane, sc);
     __syncwarp();
-  }
-  if (lane == 0 && !a.rescue) {
-    atomicAdd(&a.v.counters->fwd_columns, fcols);
-    atomicAdd(&a.v.counters->bwd_columns, bcols);
   }
 }
 
 template <class P, int R>
 void occ(int* blocks, int* threads) {
   *threads = kWarpsPerBlock * 32;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, pairhmm_kernel<P, R>, kWarpsPerBlock * 32, 0);
+  const size_t smem = kWarpsPerBlock * Layout<P, R>::kSmemPerWarp;
+  cudaFuncSetAttribute(pairhmm_kernel<P, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, pairhmm_kernel<P, R>, kWarpsPerBlock * 32, smem);
 }
 
 template <class P, int R>
 cudaError_t go(int blocks, const LaunchArgs& a, cudaStream_t s) {
-  pairhmm_kernel<P, R><<<blocks, kWarpsPerBlock * 32, 0, s>>>(a);
+  const size_t smem = kWarpsPerBlock * Layout<P, R>::kSmemPerWarp;
+  pairhmm_kernel<P, R><<<blocks, kWarpsPerBlock * 32, smem, s>>>(a);
   return cudaGetLastError();
 }
 
@@ -694,7 +767,7 @@ struct SizeF {
 };
 
 // Rows-per-lane dispatch over the instantiated values of each kind: packed FP32 covers 1..8, single
-// FP32 the long reads (10, 12, 14, 16), FP64 both.
+// FP32 the long reads (10..20 rows, even), FP64 both.
 template <template <class, int> class F, class... Args>
 auto dispatch(Kind k, int rows, Args&&... args) -> decltype(F<PackedF32, 1>::run(args...)) {
   using Ret = decltype(F<PackedF32, 1>::run(args...));
@@ -722,6 +795,8 @@ auto dispatch(Kind k, int rows, Args&&... args) -> decltype(F<PackedF32, 1>::run
         FGKL_CASE(OneF32, 12)
         FGKL_CASE(OneF32, 14)
         FGKL_CASE(OneF32, 16)
+        FGKL_CASE(OneF32, 18)
+        FGKL_CASE(OneF32, 20)
         default:
           break;
       }
@@ -740,6 +815,8 @@ auto dispatch(Kind k, int rows, Args&&... args) -> decltype(F<PackedF32, 1>::run
         FGKL_CASE(OneF64, 12)
         FGKL_CASE(OneF64, 14)
         FGKL_CASE(OneF64, 16)
+        FGKL_CASE(OneF64, 18)
+        FGKL_CASE(OneF64, 20)
         default:
           break;
       }
@@ -754,16 +831,16 @@ bool valid_rows(Kind k, int rows) {
     case Kind::kPackedF32:
       return rows >= 1 && rows <= 8;
     case Kind::kOneF32:
-      return rows == 10 || rows == 12 || rows == 14 || rows == 16;
+      return rows >= 10 && rows <= 20 && rows % 2 == 0;
     case Kind::kOneF64:
-      return (rows >= 1 && rows <= 8) || rows == 10 || rows == 12 || rows == 14 || rows == 16;
+      return (rows >= 1 && rows <= 8) || (rows >= 10 && rows <= 20 && rows % 2 == 0);
   }
   return false;
 }
 
 }  // namespace
 
-int max_rows(Kind) { return 16; }
+int max_rows(Kind) { return 20; }
 
 size_t scratch_bytes(Kind k, int rows, int max_slots, int max_nodes, int max_segs) {
   if (!valid_rows(k, rows)) return 0;

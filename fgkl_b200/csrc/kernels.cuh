@@ -9,8 +9,8 @@ namespace fgkl {
 // Arithmetic of one kernel instantiation.
 enum class Kind : int {
   kPackedF32 = 0,  // two reads per lane set, FP32x2 arithmetic, rows-per-lane 1..8
-  kOneF32 = 1,     // one read, FP32, rows-per-lane 9..16
-  kOneF64 = 2,     // one read, FP64, rows-per-lane 1..16
+  kOneF32 = 1,     // one read, FP32, rows-per-lane 10..20 (even)
+  kOneF64 = 2,     // one read, FP64, rows-per-lane 1..8 and 10..20 (even)
 };
 
 struct LaunchArgs {

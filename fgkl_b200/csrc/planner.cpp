@@ -228,85 +228,131 @@ void emit_program(const SortedHaps& s, bool with_suffix, ProgramBuild& out) {
   const double init_f64 = std::ldexp(1.0, 1020);
   const double init_f32 = std::ldexp(1.0, 120);
 
-  // Per column, how many haplotypes still to come start from it (kernel.rs:556-562).
-  std::vector<int32_t> lcp_counts(static_cast<size_t>(s.max_len) + 1, 0);
-  for (size_t k = 1; k < n; ++k)
-    if (!s.dup[k]) lcp_counts[s.lcp[k]]++;
-  std::vector<int32_t> slot_of_col(static_cast<size_t>(s.max_len) + 1, -1);
-  int32_t n_slots = 0;
-  for (int32_t c = 1; c <= s.max_len; ++c)
-    if (lcp_counts[c] > 0) slot_of_col[c] = n_slots++;
-  std::vector<int32_t> slot_len(n_slots, 0);  // haplotype length of the last writer, 0 = unwritten
-
+  // ---- forward: one segment per distinct sorted haplotype ----
+  struct Seg {
+    int32_t hap, start, stop, len;
+    Cut cut;
+  };
+  std::vector<Seg> segs;
   for (size_t k = 0; k < n; ++k) {
     if (s.dup[k]) continue;
-    const int32_t start = s.lcp[k];
-    if (k > 0) lcp_counts[start]--;
     const int32_t len = s.bases[k].len;
     const Cut cut = with_suffix ? s.plan.cuts[k] : Cut{-1, -1};
     const int32_t stop = cut.column >= 0 ? cut.column - 1 : len;
-    if (stop < start) throw std::logic_error("cut before the shared prefix");
-    Segment seg{};
-    seg.hap = static_cast<int32_t>(k);
-    seg.node = cut.column >= 0 ? cut.node : -1;
-    seg.cut_code = cut.column >= 0 ? s.codes[k][cut.column - 1] : 0;
-    int32_t src_len = 1;
-    seg.slot_in = -1;
-    if (start > 0) {
-      seg.slot_in = slot_of_col[start];
-      if (seg.slot_in < 0 || slot_len[seg.slot_in] == 0) throw std::logic_error("snapshot read before written");
-      src_len = slot_len[seg.slot_in];
-    }
-    seg.scale_d = static_cast<double>(src_len) / static_cast<double>(len);
-    seg.scale_f = static_cast<float>(seg.scale_d);
-    seg.init_d = init_f64 / static_cast<double>(len);
-    seg.init_f = static_cast<float>(init_f32 / static_cast<double>(len));
-    out.segs.push_back(seg);
-    if (stop > start) {
-      for (int32_t j = start + 1; j <= stop; ++j) {
-        uint16_t e = s.codes[k][j - 1];
-        if (j == start + 1) e |= EV_BEGIN;
-        if (j == stop) e |= EV_END;
-        if (lcp_counts[j] > 0) {
-          e |= EV_SNAP;
-          out.snap_slots.push_back(slot_of_col[j]);
-          slot_len[slot_of_col[j]] = len;
-        }
-        out.fwd.push_back(e);
-      }
-    } else {
-      out.fwd.push_back(EV_BEGIN | EV_END | EV_NOCOMP);
-    }
-    out.fwd_columns += static_cast<uint64_t>(stop - start);
+    if (stop < s.lcp[k]) throw std::logic_error("cut before the shared prefix");
+    segs.push_back(Seg{static_cast<int32_t>(k), s.lcp[k], stop, len, cut});
   }
+  const int32_t m = static_cast<int32_t>(segs.size());
+  // The last earlier segment passing each reader's start column wrote the value it resumes from.
+  std::vector<int32_t> writer(m, -1);
+  for (int32_t i = 1; i < m; ++i) {
+    const int32_t q = segs[i].start;
+    if (q == 0) continue;
+    for (int32_t j = i - 1; j >= 0; --j)
+      if (segs[j].start < q && q <= segs[j].stop) {
+        writer[i] = j;
+        break;
+      }
+    if (writer[i] < 0) throw std::logic_error("snapshot read before written");
+  }
+  // Writes keyed by (writer, column): staged for the next segment, and/or a global slot.
+  std::map<std::pair<int32_t, int32_t>, std::pair<bool, int32_t>> writes;
+  for (int32_t i = 1; i < m; ++i)
+    if (writer[i] >= 0) writes[{writer[i], segs[i].start}] = {false, -1};
+  int32_t n_slots = 0;
+  for (int32_t i = 1; i < m; ++i) {
+    if (writer[i] < 0) continue;
+    auto& w = writes[{writer[i], segs[i].start}];
+    if (writer[i] == i - 1)
+      w.first = true;
+    else if (w.second < 0)
+      w.second = n_slots++;
+  }
+  uint32_t pending = 0;  // post events of the previous column, carried by the next entry
+  auto push = [&](std::vector<uint32_t>& v, uint32_t e) {
+    v.push_back(e | pending);
+    pending = 0;
+  };
+  for (int32_t i = 0; i < m; ++i) {
+    const Seg& g = segs[i];
+    Segment rec{};
+    rec.hap = g.hap;
+    rec.node = g.cut.column >= 0 ? g.cut.node : -1;
+    rec.cut_code = g.cut.column >= 0 ? s.codes[g.hap][g.cut.column - 1] : 0;
+    rec.staged = g.start > 0 ? 1 : 0;
+    const int32_t src_len = g.start > 0 ? segs[writer[i]].len : 1;
+    rec.scale_d = static_cast<double>(src_len) / static_cast<double>(g.len);
+    rec.scale_f = static_cast<float>(rec.scale_d);
+    rec.init_d = init_f64 / static_cast<double>(g.len);
+    rec.init_f = static_cast<float>(init_f32 / static_cast<double>(g.len));
+    rec.next_slot = -1;
+    if (i + 1 < m && writer[i + 1] >= 0 && writer[i + 1] < i) rec.next_slot = writes.at({writer[i + 1], segs[i + 1].start}).second;
+    out.segs.push_back(rec);
+    if (g.stop > g.start) {
+      for (int32_t j = g.start + 1; j <= g.stop; ++j) {
+        push(out.fwd, s.codes[g.hap][j - 1] | (j == g.start + 1 ? EV_BEGIN : 0u));
+        auto it = writes.find({i, j});
+        if (it != writes.end()) {
+          const uint32_t slot = it->second.second >= 0 ? static_cast<uint32_t>(it->second.second) : kPayloadNone;
+          pending |= EV_SNAP | (it->second.first ? EV_STAGE : 0u) | (slot << kPayloadShift);
+        }
+      }
+      pending |= EV_END;
+    } else {
+      push(out.fwd, EV_BEGIN | EV_NOCOMP);
+    }
+    out.fwd_columns += static_cast<uint64_t>(g.stop - g.start);
+  }
+  push(out.fwd, 0);
   out.n_slots = n_slots;
 
+  // ---- backward: node 0 from the all-zero column beyond the end, then the plan's sweeps ----
   out.n_nodes = 0;
-  if (with_suffix && !s.plan.sweeps.empty()) {
-    // Node 0: the last column of every haplotype, computed from the all-zero column beyond it.
-    out.bwd.push_back(EV_SWEEP | EV_NODE);
-    out.sweep_starts.push_back(-1);
-    out.node_writes.push_back(0);
-    for (const auto& sw : s.plan.sweeps) {
-      const int32_t len = s.bases[sw.hap].len;
-      const int32_t right = len - sw.resume, left = len - sw.need;
-      out.sweep_starts.push_back(sw.start);
-      size_t w = 0;
-      for (int32_t j = right - 1; j >= left; --j) {
-        uint16_t e = s.codes[sw.hap][j];  // base at column j + 1, emitted moving down-right from column j
-        if (j == right - 1) e |= EV_SWEEP;
-        if (w < sw.writes.size() && len - sw.writes[w].first == j) {
-          e |= EV_NODE;
-          out.node_writes.push_back(sw.writes[w].second);
-          ++w;
-        }
-        out.bwd.push_back(e);
-      }
-      if (w != sw.writes.size()) throw std::logic_error("backward write outside its sweep");
-      out.bwd_columns += static_cast<uint64_t>(sw.need - sw.resume);
+  if (!with_suffix || s.plan.sweeps.empty()) return;
+  const auto& plan = s.plan;
+  const int32_t S = static_cast<int32_t>(plan.sweeps.size()) + 1;
+  std::vector<int32_t> node_writer(static_cast<size_t>(plan.nodes), -1);
+  node_writer[0] = 0;
+  for (int32_t t = 1; t < S; ++t)
+    for (const auto& w : plan.sweeps[t - 1].writes) node_writer[w.second] = t;
+  auto start_of = [&](int32_t t) { return t == 0 ? -1 : plan.sweeps[t - 1].start; };
+  pending = 0;
+  for (int32_t t = 0; t < S; ++t) {
+    Sweep rec{};
+    rec.staged = t > 0 ? 1 : 0;
+    rec.next_node = -1;
+    if (t + 1 < S) {
+      const int32_t nxt = start_of(t + 1);
+      if (node_writer[nxt] < 0 || node_writer[nxt] > t) throw std::logic_error("sweep starts from an unwritten node");
+      if (node_writer[nxt] < t) rec.next_node = nxt;
     }
-    out.n_nodes = s.plan.nodes;
+    out.sweeps.push_back(rec);
+    auto node_flags = [&](int32_t node) {
+      const bool stage = t + 1 < S && start_of(t + 1) == node;
+      return EV_NODE | (stage ? EV_NSTAGE : 0u) | (static_cast<uint32_t>(node) << kPayloadShift);
+    };
+    if (t == 0) {
+      push(out.bwd, EV_SWEEP);
+      pending |= node_flags(0);
+      continue;
+    }
+    const auto& sw = plan.sweeps[t - 1];
+    const int32_t len = s.bases[sw.hap].len;
+    const int32_t right = len - sw.resume, left = len - sw.need;
+    size_t w = 0;
+    for (int32_t j = right - 1; j >= left; --j) {
+      // Base at column j + 1, emitted moving down-right from column j.
+      push(out.bwd, s.codes[sw.hap][j] | (j == right - 1 ? EV_SWEEP : 0u));
+      if (w < sw.writes.size() && len - sw.writes[w].first == j) {
+        pending |= node_flags(sw.writes[w].second);
+        ++w;
+      }
+    }
+    if (w != sw.writes.size()) throw std::logic_error("backward write outside its sweep");
+    out.bwd_columns += static_cast<uint64_t>(sw.need - sw.resume);
   }
+  push(out.bwd, 0);
+  out.n_nodes = plan.nodes;
 }
 
 }  // namespace fgkl

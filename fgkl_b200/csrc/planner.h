@@ -60,17 +60,25 @@ struct SortedHaps {
   SharedColumns columns() const;
 };
 
-// Host copy of one program (program.h), before it is concatenated into a batch.
+// Host copy of one program (program.h), before it is concatenated into a batch. Streams hold only
+// the entries of positions 0..n (the last carries the post events of the final column); the
+// kStreamPad zero entries around them are added when the batch is assembled.
 struct ProgramBuild {
-  std::vector<uint16_t> fwd, bwd;
+  std::vector<uint32_t> fwd, bwd;
   std::vector<Segment> segs;
-  std::vector<int32_t> snap_slots, node_writes, sweep_starts;
+  std::vector<Sweep> sweeps;
   int32_t n_slots = 0, n_nodes = 0;
   // Σ(forward columns) and Σ(backward columns) per read row, for the computed-cell count.
   uint64_t fwd_columns = 0, bwd_columns = 0;
 };
 
 // The forward (and, with `with_suffix`, backward) column stream of a sorted haplotype set.
+//
+// Snapshot placement: a segment resuming at column q reads the value the LAST earlier segment
+// passing q wrote (the semantics of fgkl's per-column snapshot array, kernel.rs:254-259, :656-662),
+// so each snapshot is written once, by that last writer: into the staging buffer when the very next
+// segment reads it, and into a global slot when a later one does (prefetched into staging at the
+// BEGIN of the segment before its reader).
 void emit_program(const SortedHaps& s, bool with_suffix, ProgramBuild& out);
 
 // 256-entry byte -> prior code table of a sorted set (kNoCode for bytes no haplotype holds that

@@ -1,53 +1,70 @@
 // Device-program layout shared by the host planner and the sm_100a kernels.
 //
-// A region (one PairHMM call: R reads x H haplotypes) is planned on the host into a "program": a
-// column stream that every read of the region walks through, one warp per read task. Each stream
-// entry is one DP column of one sorted haplotype (forward) or one backward column of one suffix
-// sweep (backward); its low byte is the prior code of the haplotype base the column emits and its
-// high byte carries the events the lane handles at that column. Per-segment and per-sweep details
-// live in side tables consumed in stream order, so a lane only needs running counters.
+// A region (one PairHMM call: R reads x H haplotypes) is planned on the host into a program that
+// every read of the region walks, one warp per read task. The forward stream holds one 32-bit entry
+// per DP column of each distinct sorted haplotype; the backward stream one per backward column of
+// each suffix sweep. An entry's low byte is the prior code of the haplotype base the column emits;
+// its flags name the events a lane handles when it reaches the entry: events that load state
+// (BEGIN, SWEEP) for the entry's own column, events that store state (SNAP, END, NODE) for the
+// PREVIOUS column. Deferring the stores by one column lets the lane handle every event of a step
+// in one branch before computing. Each stream is padded with kStreamPad zero entries on both sides
+// so lanes ahead of or behind the wavefront read harmless entries without bounds checks.
 #pragma once
 #include <cstdint>
 
 namespace fgkl {
 
-// ---- stream entry bits (uint16_t) ----
-constexpr uint16_t kCodeMask = 0x00FF;
-constexpr uint16_t EV_BEGIN = 1u << 8;   // forward: load the segment's start column before computing
-constexpr uint16_t EV_SNAP = 1u << 9;    // forward: store the column into the next snapshot slot
-constexpr uint16_t EV_END = 1u << 10;    // forward: finish the segment (result or join) after computing
-constexpr uint16_t EV_NOCOMP = 1u << 11; // forward: zero-length segment, no column computed
-constexpr uint16_t EV_SWEEP = 1u << 12;  // backward: load the sweep's start node before computing
-constexpr uint16_t EV_NODE = 1u << 13;   // backward: store a backward node after computing
-constexpr uint16_t kEvMask = 0xFF00;
+constexpr int kStreamPad = 64;
+
+// ---- stream entry bits (uint32_t) ----
+constexpr uint32_t kCodeMask = 0xFFu;
+// forward
+constexpr uint32_t EV_BEGIN = 1u << 8;    // load the segment's start column before computing this one
+constexpr uint32_t EV_NOCOMP = 1u << 9;   // zero-length segment: finish it right after BEGIN
+constexpr uint32_t EV_SNAP = 1u << 10;    // the previous column is a snapshot (payload: slot, staging)
+constexpr uint32_t EV_END = 1u << 11;     // the previous column ended the segment (result or join)
+constexpr uint32_t EV_STAGE = 1u << 12;   // the snapshot also goes to the staging buffer of the next segment
+// backward
+constexpr uint32_t EV_SWEEP = 1u << 8;    // load the sweep's start node before computing this column
+constexpr uint32_t EV_NODE = 1u << 10;    // the previous column is a backward node (payload: node id)
+constexpr uint32_t EV_NSTAGE = 1u << 12;  // the node also goes to the staging buffer of the next sweep
+constexpr uint32_t kEvMask = 0x1F00u;
+constexpr int kPayloadShift = 13;
+constexpr uint32_t kPayloadNone = (1u << (32 - kPayloadShift)) - 1;  // no global slot / node
 
 // Prior code of haplotype 'N' (codes 0..4 are A, C, G, T, N; extra bytes follow in first-seen
-// order, kernel.rs:27-107).
+// order, fgkl kernel.rs:27-107).
 constexpr int kCodeN = 4;
 constexpr uint8_t kNoCode = 0xFF;
 
-// One forward run of a distinct sorted haplotype: columns start+1..=stop, resumed from a snapshot
-// slot (or the origin) and either finished or joined with a backward node at column stop+1.
+// One forward run of a distinct sorted haplotype: columns start+1..=stop, resumed from its start
+// column (the origin or a staged snapshot) and either finished or joined with a backward node.
 struct Segment {
-  int32_t slot_in;   // snapshot slot holding column `start`; -1 = origin (column 0)
-  int32_t node;      // backward node joined at the cut; -1 = no cut
-  int32_t hap;       // sorted haplotype index
-  int32_t cut_code;  // prior code of the haplotype base at the cut column
-  float scale_f;     // src_len / hap_len, narrowed like kernel.rs:641
-  float init_f;      // 2^120 / hap_len narrowed to f32 (kernel.rs:640)
-  double scale_d;    // src_len / hap_len in f64
-  double init_d;     // 2^1020 / hap_len
+  float scale_f;      // src_len / hap_len narrowed like fgkl kernel.rs:641
+  float init_f;       // 2^120 / hap_len narrowed to f32 (kernel.rs:640)
+  double scale_d;
+  double init_d;      // 2^1020 / hap_len
+  int32_t staged;     // 1: start from the staging buffer; 0: from the origin (column 0)
+  int32_t next_slot;  // global snapshot slot to prefetch for the NEXT segment at this BEGIN, or -1
+  int32_t node;       // backward node joined at the cut; -1 = no cut
+  int32_t cut_code;   // prior code of the haplotype base at the cut column
+  int32_t hap;        // sorted haplotype index
+  int32_t pad_;
 };
 
-// Offsets of one program inside the batch-global arrays.
+// One backward sweep (the first of a program computes node 0 from the all-zero column).
+struct Sweep {
+  int32_t staged;     // 1: start from the staging buffer; 0: all-zero start column
+  int32_t next_node;  // global node to prefetch for the NEXT sweep at this SWEEP, or -1
+};
+
+// Offsets of one program inside the batch-global arrays (stream offsets point at entry 0).
 struct Program {
-  int32_t fwd_off, fwd_len;    // forward stream entries
-  int32_t bwd_off, bwd_len;    // backward stream entries (0 = no suffix sharing)
-  int32_t seg_off, n_segs;     // segments, forward stream order
-  int32_t snap_off, n_snaps;   // snapshot slot ids written, forward stream order
-  int32_t nodew_off, n_nodew;  // backward node ids written, backward stream order
-  int32_t sweep_off, n_sweeps; // start node per sweep (-1 = the all-zero column beyond the end)
-  int32_t n_slots, n_nodes;
+  int32_t fwd_off, fwd_len;
+  int32_t bwd_off, bwd_len;  // bwd_len 0 = no suffix sharing
+  int32_t seg_off, n_segs;
+  int32_t sweep_off, n_sweeps;
+  int32_t n_slots, n_nodes;  // global snapshot slots and backward nodes one read needs
 };
 
 struct Region {
@@ -70,7 +87,7 @@ struct HapInfo {
   int32_t pad_;
 };
 
-// One warp's unit of work: one or two reads of a region, with R rows per lane (32 * R > length).
+// One warp's unit of work: one or two reads of a region, with R rows per lane (31 * R >= length).
 struct Task {
   int32_t region;
   int32_t read[2];  // global read indices; read[1] = -1 when the task holds one read
@@ -80,9 +97,8 @@ struct Task {
 // Per-pass counters written by the kernels.
 struct Counters {
   unsigned long long lost_pairs;   // pairs handed to the double-precision recomputation
-  unsigned long long fwd_columns;  // forward stream positions processed (per read)
-  unsigned long long bwd_columns;  // backward stream positions processed (per read)
   unsigned long long rescue_reads; // reads queued for recomputation
+  unsigned long long pad_[2];
 };
 
 // Flattened batch: everything a kernel needs, as device pointers.
@@ -95,11 +111,9 @@ struct BatchView {
   const int64_t* read_off;   // global read -> first byte
   const Region* regions;
   const HapInfo* haps;
-  const uint16_t* stream;
+  const uint32_t* stream;
   const Segment* segs;
-  const int32_t* snap_slots;
-  const int32_t* node_writes;
-  const int32_t* sweep_starts;
+  const Sweep* sweeps;
   const uint8_t* code_of_byte;
   const double* err_prob;     // 255 entries
   const double* m2m;          // triangular table, 32640 entries

@@ -31,7 +31,7 @@ extern "C" {
 #define FGKL_E_OUTPUT_LENGTH (-5)               /* Error::OutputLength */
 #define FGKL_E_BAD_OFFSETS (-6)                 /* offset table checks of crates/jni/src/lib.rs:343-363 */
 #define FGKL_E_INVALID_ARGUMENT (-7)            /* NULL pointer or negative size */
-#define FGKL_E_UNSUPPORTED (-8)                 /* a read of 512 or more bases */
+#define FGKL_E_UNSUPPORTED (-8)                 /* a read of more than 620 bases */
 #define FGKL_E_NO_DEVICE (-9)                   /* no CUDA device, or not an sm_100 part */
 #define FGKL_E_CUDA (-10)                       /* CUDA runtime error (message in fgkl_last_error) */
 
