@@ -35,6 +35,7 @@ struct RegionPlan {
   uint8_t codes[256];
   SharedColumns cols;
   uint64_t read_bases = 0, hap_bases = 0;
+  bool extra_codes = false;  // a haplotype byte outside ACGTN: the region runs on the FP64 kernel
 };
 
 void plan_region(const BatchInput& in, int g, int64_t first_read, int64_t first_hap, bool share, RegionPlan& out) {
@@ -52,6 +53,7 @@ void plan_region(const BatchInput& in, int g, int64_t first_read, int64_t first_
   emit_program(s, share, out.shared);
   emit_program(s, false, out.prefix);
   code_table(s, out.codes);
+  out.extra_codes = s.num_codes() > 5;
   out.cols = s.columns();
   out.haps.resize(static_cast<size_t>(n_haps));
   int seg = -1;
@@ -255,7 +257,7 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
     const uint64_t cost_cols = plans[g].shared.fwd.size() + plans[g].shared.bwd.size() + 31;
     for (int r = 0; r < n_reads; ++r) rescue_count[single_rows(len_of(r))]++;
     size_t i = 0;
-    if (cfg.double_precision) {
+    if (cfg.double_precision || plans[g].extra_codes) {
       for (; i < order.size(); ++i) {
         const int rows = single_rows(len_of(order[i]));
         by_bin[{Kind::kOneF64, rows}].push_back(

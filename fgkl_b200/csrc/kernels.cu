@@ -139,7 +139,11 @@ struct Layout {
   static constexpr int kNode = up(2 * R + 1);  // BM, BY rows; below-row BM
   static constexpr int kJoin = 2 * R;          // cut column M and Y rows
   static constexpr int kStage = kSnap > kNode ? kSnap : kNode;
-  static constexpr size_t kSmemPerWarp = 2ull * 32 * kStage * sizeof(V);
+  // FP32 kernels look priors up in a per-lane table indexed by haplotype code (A, C, G, T, N);
+  // regions holding other haplotype bytes run on the FP64 kernel, which compares codes instead.
+  static constexpr int kPriorCodes = P::kDouble ? 0 : 5;
+  static constexpr size_t kStageBytes = 2ull * 32 * kStage * sizeof(V);
+  static constexpr size_t kSmemPerWarp = kStageBytes + static_cast<size_t>(kPriorCodes) * R * 32 * sizeof(V);
 };
 
 // ---------------------------------------------------------------------------------------------
@@ -194,6 +198,16 @@ __device__ RowModel row_model(const BatchView& v, const ReadRef& r, int q, const
   return m;
 }
 
+// Priors of the lane's rows for every haplotype code, [code][row][lane] in shared memory.
+template <class P, int R>
+__device__ __forceinline__ void put_priors(typename P::V* table, int lane, int r, int c, const RowModel& m) {
+  using S = typename P::S;
+  for (int code = 0; code < Layout<P, R>::kPriorCodes; ++code) {
+    const bool match = code == m.oc || code == kCodeN;
+    P::put(table[(code * R + r) * 32 + lane], c, static_cast<S>(match ? m.pm : m.px));
+  }
+}
+
 // Forward coefficients of the lane's rows.
 template <class P, int R>
 struct FwdRows {
@@ -201,8 +215,17 @@ struct FwdRows {
   using S = typename P::S;
   V c0[R], c1[R], c2[R], c3[R], c4[R], pm[R], px[R];
   int oc[P::NC][R];
+  const V* table;  // prior table (FP32 kernels)
 
-  __device__ void load(const BatchView& v, const ReadRef* rd, int lane, const uint8_t* codes) {
+  __device__ V prior(int code, bool isN, int r, int lane) const {
+    if (Layout<P, R>::kPriorCodes) return table[(code * R + r) * 32 + lane];
+    const bool m0 = (code == oc[0][r]) | isN;
+    const bool m1 = (code == oc[P::NC - 1][r]) | isN;
+    return P::sel(m0, m1, pm[r], px[r]);
+  }
+
+  __device__ void load(const BatchView& v, const ReadRef* rd, int lane, const uint8_t* codes, V* ptable) {
+    table = ptable;
 #pragma unroll
     for (int r = 0; r < R; ++r) {
 #pragma unroll
@@ -243,6 +266,7 @@ struct FwdRows {
         P::put(pm[r], c, static_cast<S>(m.pm));
         P::put(px[r], c, static_cast<S>(m.px));
         oc[c][r] = m.oc;
+        put_priors<P, R>(ptable, lane, r, c, m);
       }
     }
   }
@@ -256,8 +280,17 @@ struct BwdRows {
   using S = typename P::S;
   V md[R], dd[R], mm[R], im[R], mi[R], ii[R], pm[R], px[R];
   int oc[P::NC][R];
+  const V* table;  // prior table of the rows below (FP32 kernels)
 
-  __device__ void load(const BatchView& v, const ReadRef* rd, int lane, const uint8_t* codes) {
+  __device__ V prior(int code, bool isN, int r, int lane) const {
+    if (Layout<P, R>::kPriorCodes) return table[(code * R + r) * 32 + lane];
+    const bool m0 = (code == oc[0][r]) | isN;
+    const bool m1 = (code == oc[P::NC - 1][r]) | isN;
+    return P::sel(m0, m1, pm[r], px[r]);
+  }
+
+  __device__ void load(const BatchView& v, const ReadRef* rd, int lane, const uint8_t* codes, V* ptable) {
+    table = ptable;
 #pragma unroll
     for (int r = 0; r < R; ++r) {
 #pragma unroll
@@ -274,6 +307,7 @@ struct BwdRows {
         P::put(pm[r], c, static_cast<S>(below.pm));
         P::put(px[r], c, static_cast<S>(below.px));
         oc[c][r] = below.oc;
+        put_priors<P, R>(ptable, lane, r, c, below);
       }
     }
   }
@@ -292,6 +326,7 @@ struct Scratch {
   V* joins;         // [seg][lane][kJoin]
   double* seg_raw;  // [seg][c]
   V* stage;         // shared: [buf][lane][kStage]
+  V* priors;        // shared: [code][row][lane]
 
   __device__ Scratch(char* base, V* smem, int n_slots, int n_nodes, int n_segs) {
     slots = reinterpret_cast<V*>(base);
@@ -299,6 +334,7 @@ struct Scratch {
     joins = nodes + static_cast<size_t>(n_nodes) * 32 * L::kNode;
     seg_raw = reinterpret_cast<double*>(joins + static_cast<size_t>(n_segs) * 32 * L::kJoin);
     stage = smem;
+    priors = reinterpret_cast<V*>(reinterpret_cast<char*>(smem) + L::kStageBytes);
   }
   __device__ V* slot(int s, int lane) { return slots + (static_cast<size_t>(s) * 32 + lane) * L::kSnap; }
   __device__ V* node(int n, int lane) { return nodes + (static_cast<size_t>(n) * 32 + lane) * L::kNode; }
@@ -323,6 +359,31 @@ __device__ __forceinline__ void prefetch(V* dst_smem, const V* src, int fields) 
   __pipeline_commit();
 }
 
+// Moves a record of N values 16 bytes at a time (records start on 16 bytes; N is a multiple of the
+// values per 16 bytes).
+template <class V, int N>
+__device__ __forceinline__ void store_record(V* dst, const V (&src)[N]) {
+  static_assert(N * sizeof(V) % 16 == 0, "record size");
+#pragma unroll
+  for (int i = 0; i < static_cast<int>(N * sizeof(V) / 16); ++i)
+    reinterpret_cast<uint4*>(dst)[i] = reinterpret_cast<const uint4*>(src)[i];
+}
+template <class V, int N>
+__device__ __forceinline__ void load_record(V (&dst)[N], const V* src) {
+#pragma unroll
+  for (int i = 0; i < static_cast<int>(N * sizeof(V) / 16); ++i)
+    reinterpret_cast<uint4*>(dst)[i] = reinterpret_cast<const uint4*>(src)[i];
+}
+
+__device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
+
+// Resident blocks per SM each instantiation is compiled for: enough registers for its rows without
+// spilling the hot loop, as many warps as that allows.
+template <class P, int R>
+struct MinBlocks {
+  static constexpr int value = P::NC == 2 ? (R <= 2 ? 4 : (R <= 6 ? 3 : 2)) : (P::kDouble ? 1 : 2);
+};
+
 // ---------------------------------------------------------------------------------------------
 // Backward pass: every suffix sweep of the program, writing backward nodes.
 // ---------------------------------------------------------------------------------------------
@@ -333,7 +394,7 @@ __device__ void backward_pass(const LaunchArgs& a, const Program& prog, const Re
   using V = typename P::V;
   using L = Layout<P, R>;
   BwdRows<P, R> bp;
-  bp.load(a.v, rd, lane, codes);
+  bp.load(a.v, rd, lane, codes, sc.priors);
   const V sink = P::splat(lane == 31 ? static_cast<typename P::S>(Consts<P::kDouble>::kBackwardScale) : 0);
   V BM[R], BY[R];
 #pragma unroll
@@ -342,7 +403,6 @@ __device__ void backward_pass(const LaunchArgs& a, const Program& prog, const Re
   const int n = prog.bwd_len;
   const uint32_t* stream = a.v.stream + prog.bwd_off - (31 - lane);  // entry of this lane's position at t
   int sweep = -1;
-  Sweep nxt = a.v.sweeps[prog.sweep_off];
   uint32_t ev_next = __ldg(stream);
   for (int t = 0; t < n + 32; ++t) {
     const V rBM = P::down(topBM), rBX = P::down(topBX);
@@ -350,34 +410,32 @@ __device__ void backward_pass(const LaunchArgs& a, const Program& prog, const Re
     ev_next = __ldg(stream + t + 1);
     if (ev & kEvMask) {
       if (ev & EV_NODE) {
-        const uint32_t node = ev >> kPayloadShift;
-        V* g = sc.node(static_cast<int>(node), lane);
-        V* s = (ev & EV_NSTAGE) ? sc.staged(sweep + 1, lane) : nullptr;
+        V rec[L::kNode];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-          g[r] = BM[r];
-          g[R + r] = BY[r];
-          if (s) {
-            s[r] = BM[r];
-            s[R + r] = BY[r];
-          }
+          rec[r] = BM[r];
+          rec[R + r] = BY[r];
         }
-        g[2 * R] = dBM;
-        if (s) s[2 * R] = dBM;
+        rec[2 * R] = dBM;
+#pragma unroll
+        for (int i = 2 * R + 1; i < L::kNode; ++i) rec[i] = P::zero();
+        store_record(sc.node(static_cast<int>(ev >> kPayloadShift), lane), rec);
+        if (ev & EV_NSTAGE) store_record(sc.staged(sweep + 1, lane), rec);
       }
       if (ev & EV_SWEEP) {
         ++sweep;
-        const Sweep cur = nxt;
-        if (sweep + 1 < prog.n_sweeps) nxt = a.v.sweeps[prog.sweep_off + sweep + 1];
+        const Sweep cur = a.v.sweeps[prog.sweep_off + sweep];
+        if (sweep + 1 < prog.n_sweeps) prefetch_l1(a.v.sweeps + prog.sweep_off + sweep + 1);
         if (cur.staged) {
           __pipeline_wait_prior(0);
-          const V* s = sc.staged(sweep, lane);
+          V rec[L::kNode];
+          load_record(rec, sc.staged(sweep, lane));
 #pragma unroll
           for (int r = 0; r < R; ++r) {
-            BM[r] = s[r];
-            BY[r] = s[R + r];
+            BM[r] = rec[r];
+            BY[r] = rec[R + r];
           }
-          dBM = s[2 * R];
+          dBM = rec[2 * R];
         } else {
 #pragma unroll
           for (int r = 0; r < R; ++r) BM[r] = BY[r] = P::zero();
@@ -391,10 +449,7 @@ __device__ void backward_pass(const LaunchArgs& a, const Program& prog, const Re
     V belowX = rBX, diagM = dBM;
 #pragma unroll
     for (int r = R - 1; r >= 0; --r) {
-      const bool m0 = (code == bp.oc[0][r]) | isN;
-      const bool m1 = (code == bp.oc[P::NC - 1][r]) | isN;
-      const V prior = P::sel(m0, m1, bp.pm[r], bp.px[r]);
-      const V into = P::mul(prior, diagM);
+      const V into = P::mul(bp.prior(code, isN, r, lane), diagM);
       const V itm = P::mul(into, bp.im[r]);
       V bx = P::fma(belowX, bp.ii[r], itm);
       const V by = P::fma(BY[r], bp.dd[r], itm);
@@ -427,23 +482,124 @@ __device__ __forceinline__ typename P::V cell_match(const typename P::V& dM, con
   return P::fma(dY, k1, P::fma(dX, k1, P::mul(dM, k0)));
 }
 
-struct SegState {
-  float scale_f, init_f;
-  double scale_d, init_d;
-  int staged, next_slot, node, cut_code;
+// Loop-carried state of the forward sweep of one lane.
+template <class P, int R>
+struct FwdState {
+  using V = typename P::V;
+  V M[R], X[R], Y[R];
+  V acc;
+  int seg_i;
 };
 
-__device__ __forceinline__ SegState load_seg(const Segment* s) {
-  SegState r;
-  r.scale_f = s->scale_f;
-  r.init_f = s->init_f;
-  r.scale_d = s->scale_d;
-  r.init_d = s->init_d;
-  r.staged = s->staged;
-  r.next_slot = s->next_slot;
-  r.node = s->node;
-  r.cut_code = s->cut_code;
-  return r;
+// One forward step: events, then the column. (uM, uX, uY) receive the bottom row of the lane above
+// for this column; (dM, dX, dY) hold it for the previous column, the top row's diagonal. The two sets
+// alternate between consecutive steps, so no copies are needed.
+template <class P, int R>
+__device__ __forceinline__ void forward_step(const LaunchArgs& a, const Program& prog, const ReadRef* rd, int lane,
+                                             const FwdRows<P, R>& fr, const typename P::V& an, int pad_hi, Scratch<P, R>& sc,
+                                             FwdState<P, R>& st, uint32_t ev, typename P::V& uM, typename P::V& uX,
+                                             typename P::V& uY, typename P::V& dM, typename P::V& dX, typename P::V& dY) {
+  using V = typename P::V;
+  using S = typename P::S;
+  using L = Layout<P, R>;
+  uM = P::up(st.M[R - 1]);
+  uX = P::up(st.X[R - 1]);
+  uY = P::up(st.Y[R - 1]);
+  if (ev & kEvMask) {
+    if (ev & EV_SNAP) {
+      const uint32_t slot = ev >> kPayloadShift;
+      V* dst[2] = {slot != kPayloadNone ? sc.slot(static_cast<int>(slot), lane) : nullptr,
+                   (ev & EV_STAGE) ? sc.staged(st.seg_i + 1, lane) : nullptr};
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        V* o = dst[k];
+        if (!o) continue;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          o[r] = st.M[r];
+          o[R + r] = st.X[r];
+          o[2 * R + r] = st.Y[r];
+        }
+        o[3 * R] = dM;
+        o[3 * R + 1] = dX;
+        o[3 * R + 2] = dY;
+        o[3 * R + 3] = st.acc;
+      }
+    }
+    if ((ev & EV_END) && lane == 31) {
+#pragma unroll
+      for (int c = 0; c < P::NC; ++c) sc.seg_raw[st.seg_i * P::NC + c] = static_cast<double>(P::get(st.acc, c));
+    }
+    if (ev & EV_JOIN) {
+      // The cut column's match and deletion rows, joined with the backward node after the sweep
+      // (fgkl kernel.rs:744-755).
+      V* j = sc.join(st.seg_i, lane);
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        j[r] = st.M[r];
+        j[R + r] = st.Y[r];
+      }
+    }
+    if (ev & EV_BEGIN) {
+      ++st.seg_i;
+      const Segment* rec = a.v.segs + prog.seg_off + st.seg_i;
+      if (st.seg_i + 1 < prog.n_segs) prefetch_l1(rec + 1);
+      const int next_slot = rec->next_slot;
+      if (rec->staged) {
+        __pipeline_wait_prior(0);
+        const V* s = sc.staged(st.seg_i, lane);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          st.M[r] = s[r];
+          st.X[r] = s[R + r];
+          st.Y[r] = s[2 * R + r];
+        }
+        dM = s[3 * R];
+        dX = s[3 * R + 1];
+        dY = s[3 * R + 2];
+        st.acc = s[3 * R + 3];
+      } else {
+        // The origin: nothing but the row-0 constant, in the padding rows (and the row above the
+        // lane when that is padding).
+        const S in_s = P::kDouble ? static_cast<S>(rec->init_d) : static_cast<S>(rec->init_f);
+#pragma unroll
+        for (int r = 0; r < R; ++r) st.M[r] = st.X[r] = st.Y[r] = P::zero();
+        dM = dX = dY = st.acc = P::zero();
+        if (lane * R <= pad_hi) {
+#pragma unroll
+          for (int c = 0; c < P::NC; ++c) {
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+              if (lane * R + r < rd[c].pad) P::put(st.Y[r], c, in_s);
+            if (lane * R - 1 < rd[c].pad) P::put(dY, c, in_s);
+          }
+        }
+      }
+      if (next_slot >= 0) prefetch(sc.staged(st.seg_i + 1, lane), sc.slot(next_slot, lane), L::kSnap);
+    }
+    if ((ev & EV_ACC) && lane == 31) {
+#pragma unroll
+      for (int c = 0; c < P::NC; ++c) sc.seg_raw[st.seg_i * P::NC + c] = static_cast<double>(P::get(st.acc, c));
+    }
+  }
+  const int code = ev & kCodeMask;
+  const bool isN = code == kCodeN;
+  // Match and deletion values from the bottom row up: each row reads the old values of the row above
+  // (its diagonal) and its own old values (left), so everything updates in place.
+#pragma unroll
+  for (int r = R - 1; r >= 0; --r) {
+    const V pM = r ? st.M[r - 1] : dM, pX = r ? st.X[r - 1] : dX, pY = r ? st.Y[r - 1] : dY;
+    const V prior = fr.prior(code, isN, r, lane);
+    st.Y[r] = P::kTransformed ? P::fma(st.Y[r], fr.c4[r], st.M[r]) : P::fma(st.Y[r], fr.c3[r], P::mul(st.M[r], fr.c4[r]));
+    st.M[r] = P::mul(prior, cell_match<P>(pM, pX, pY, fr.c0[r], fr.c1[r], fr.c2[r]));
+  }
+  // Insertion values from the top row down: each row reads the new values of the row above.
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const V qM = r ? st.M[r - 1] : uM, qX = r ? st.X[r - 1] : uX;
+    st.X[r] = P::kTransformed ? P::fma(qX, fr.c3[r], qM) : P::fma(qX, fr.c3[r], P::mul(qM, fr.c2[r]));
+  }
+  st.acc = P::fma(st.X[R - 1], an, P::add(st.acc, st.M[R - 1]));
 }
 
 template <class P, int R>
@@ -451,144 +607,32 @@ __device__ void forward_pass(const LaunchArgs& a, const Program& prog, const Rea
                              Scratch<P, R>& sc) {
   using V = typename P::V;
   using S = typename P::S;
-  using L = Layout<P, R>;
   FwdRows<P, R> fr;
-  fr.load(a.v, rd, lane, codes);
+  fr.load(a.v, rd, lane, codes, sc.priors);
   // X factor of the read's last row (lane 31): the accumulated result is Σ M + mi_n * X^.
   V an;
 #pragma unroll
   for (int c = 0; c < P::NC; ++c)
     P::put(an, c, static_cast<S>((P::kTransformed && rd[c].len > 0) ? err_prob(a.v, a.v.ins[rd[c].off + rd[c].len - 1]) : 1.0));
-
-  V M[R], X[R], Y[R];
+  int pad_hi = 0;
 #pragma unroll
-  for (int r = 0; r < R; ++r) M[r] = X[r] = Y[r] = P::zero();
-  V dM = P::zero(), dX = P::zero(), dY = P::zero(), acc = P::zero();
+  for (int c = 0; c < P::NC; ++c) pad_hi = rd[c].pad > pad_hi ? rd[c].pad : pad_hi;
+
+  FwdState<P, R> st;
+#pragma unroll
+  for (int r = 0; r < R; ++r) st.M[r] = st.X[r] = st.Y[r] = P::zero();
+  st.acc = P::zero();
+  st.seg_i = -1;
+  V aM = P::zero(), aX = P::zero(), aY = P::zero(), bM = P::zero(), bX = P::zero(), bY = P::zero();
   const int n = prog.fwd_len;
   const uint32_t* stream = a.v.stream + prog.fwd_off - lane;
-  int seg_i = -1;
-  SegState cur{}, nxt = load_seg(a.v.segs + prog.seg_off);
-  uint32_t ev_next = __ldg(stream);
-
-  // The cut column's match and deletion values entered from the current column, per row, stored
-  // for the join (fgkl kernel.rs:744-755); the row above the lane's top row is (dM, dX, dY).
-  auto end_segment = [&]() {
-    if (lane == 31) {
-#pragma unroll
-      for (int c = 0; c < P::NC; ++c) sc.seg_raw[seg_i * P::NC + c] = static_cast<double>(P::get(acc, c));
-    }
-    if (cur.node >= 0) {
-      const int code = cur.cut_code;
-      const bool isN = code == kCodeN;
-      V* j = sc.join(seg_i, lane);
-      V jM = dM, jX = dX, jY = dY;
-#pragma unroll
-      for (int r = 0; r < R; ++r) {
-        const bool m0 = (code == fr.oc[0][r]) | isN;
-        const bool m1 = (code == fr.oc[P::NC - 1][r]) | isN;
-        const V prior = P::sel(m0, m1, fr.pm[r], fr.px[r]);
-        j[r] = P::mul(prior, cell_match<P>(jM, jX, jY, fr.c0[r], fr.c1[r], fr.c2[r]));
-        j[R + r] = P::kTransformed ? P::fma(Y[r], fr.c4[r], M[r]) : P::fma(Y[r], fr.c3[r], P::mul(M[r], fr.c4[r]));
-        jM = M[r];
-        jX = X[r];
-        jY = Y[r];
-      }
-    }
-  };
-
-  for (int t = 0; t < n + 32; ++t) {
-    const V uM = P::up(M[R - 1]), uX = P::up(X[R - 1]), uY = P::up(Y[R - 1]);
-    const uint32_t ev = ev_next;
-    ev_next = __ldg(stream + t + 1);
-    if (ev & kEvMask) {
-      if (ev & EV_SNAP) {
-        const uint32_t slot = ev >> kPayloadShift;
-        V* g = slot != kPayloadNone ? sc.slot(static_cast<int>(slot), lane) : nullptr;
-        V* s = (ev & EV_STAGE) ? sc.staged(seg_i + 1, lane) : nullptr;
-        for (int dst = 0; dst < 2; ++dst) {
-          V* o = dst ? s : g;
-          if (!o) continue;
-#pragma unroll
-          for (int r = 0; r < R; ++r) {
-            o[r] = M[r];
-            o[R + r] = X[r];
-            o[2 * R + r] = Y[r];
-          }
-          o[3 * R] = dM;
-          o[3 * R + 1] = dX;
-          o[3 * R + 2] = dY;
-          o[3 * R + 3] = acc;
-        }
-      }
-      if (ev & EV_END) end_segment();
-      if (ev & EV_BEGIN) {
-        ++seg_i;
-        cur = nxt;
-        if (seg_i + 1 < prog.n_segs) nxt = load_seg(a.v.segs + prog.seg_off + seg_i + 1);
-        const S in_s = P::kDouble ? static_cast<S>(cur.init_d) : static_cast<S>(cur.init_f);
-        const S sc_s = P::kDouble ? static_cast<S>(cur.scale_d) : static_cast<S>(cur.scale_f);
-        const V scale = P::splat(sc_s);
-        if (cur.staged) {
-          __pipeline_wait_prior(0);
-          const V* s = sc.staged(seg_i, lane);
-#pragma unroll
-          for (int r = 0; r < R; ++r) {
-            M[r] = P::mul(s[r], scale);
-            X[r] = P::mul(s[R + r], scale);
-            Y[r] = P::mul(s[2 * R + r], scale);
-          }
-          dM = P::mul(s[3 * R], scale);
-          dX = P::mul(s[3 * R + 1], scale);
-          dY = P::mul(s[3 * R + 2], scale);
-          acc = P::mul(s[3 * R + 3], scale);
-        } else {
-#pragma unroll
-          for (int r = 0; r < R; ++r) M[r] = X[r] = Y[r] = P::zero();
-          dM = dX = dY = acc = P::zero();
-        }
-        // Padding rows (and the row above the lane when it is padding) hold exact row-0 values.
-#pragma unroll
-        for (int c = 0; c < P::NC; ++c) {
-#pragma unroll
-          for (int r = 0; r < R; ++r)
-            if (lane * R + r < rd[c].pad) P::put(Y[r], c, in_s);
-          if (lane * R - 1 < rd[c].pad) P::put(dY, c, in_s);
-        }
-        if (cur.next_slot >= 0) prefetch(sc.staged(seg_i + 1, lane), sc.slot(cur.next_slot, lane), L::kSnap);
-        if (ev & EV_NOCOMP) end_segment();
-      }
-    }
-    const int code = ev & kCodeMask;
-    const bool isN = code == kCodeN;
-    V pM = dM, pX = dX, pY = dY, qM = uM, qX = uX;
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const V oM = M[r], oX = X[r], oY = Y[r];
-      const bool m0 = (code == fr.oc[0][r]) | isN;
-      const bool m1 = (code == fr.oc[P::NC - 1][r]) | isN;
-      const V prior = P::sel(m0, m1, fr.pm[r], fr.px[r]);
-      const V nM = P::mul(prior, cell_match<P>(pM, pX, pY, fr.c0[r], fr.c1[r], fr.c2[r]));
-      V nX, nY;
-      if (P::kTransformed) {
-        nX = P::fma(qX, fr.c3[r], qM);
-        nY = P::fma(oY, fr.c4[r], oM);
-      } else {
-        nX = P::fma(qX, fr.c3[r], P::mul(qM, fr.c2[r]));
-        nY = P::fma(oY, fr.c3[r], P::mul(oM, fr.c4[r]));
-      }
-      M[r] = nM;
-      X[r] = nX;
-      Y[r] = nY;
-      pM = oM;
-      pX = oX;
-      pY = oY;
-      qM = nM;
-      qX = nX;
-    }
-    dM = uM;
-    dX = uX;
-    dY = uY;
-    acc = P::fma(X[R - 1], an, P::add(acc, M[R - 1]));
+  uint32_t n0 = __ldg(stream), n1 = __ldg(stream + 1);
+  for (int t = 0; t < n + 32; t += 2) {
+    const uint32_t e0 = n0, e1 = n1;
+    n0 = __ldg(stream + t + 2);
+    n1 = __ldg(stream + t + 3);
+    forward_step<P, R>(a, prog, rd, lane, fr, an, pad_hi, sc, st, e0, aM, aX, aY, bM, bX, bY);
+    forward_step<P, R>(a, prog, rd, lane, fr, an, pad_hi, sc, st, e1, bM, bX, bY, aM, aX, aY);
   }
   __pipeline_wait_prior(0);
 }
@@ -651,11 +695,13 @@ __device__ void finalize(const LaunchArgs& a, const Task& task, const Region& re
   for (int c = 0; c < P::NC; ++c) lost_any[c] = false;
   for (int k = lane; k < region.n_haps; k += 32) {
     const HapInfo info = a.v.haps[region.hap_off + k];
-    const bool joined = a.v.segs[prog.seg_off + info.seg].node >= 0;
+    const Segment* seg = a.v.segs + prog.seg_off + info.seg;
+    const bool joined = seg->node >= 0;
+    const double factor = seg->factor;
 #pragma unroll
     for (int c = 0; c < P::NC; ++c) {
       if (task.read[c] < 0) continue;
-      const double raw = sc.seg_raw[info.seg * P::NC + c];
+      const double raw = __dmul_rn(sc.seg_raw[info.seg * P::NC + c], factor);
       bool lost;
       if (joined)
         lost = !(raw >= C::kMinAcceptedJoined);
@@ -693,7 +739,7 @@ __device__ void finalize(const LaunchArgs& a, const Task& task, const Region& re
 }
 
 template <class P, int R>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32) pairhmm_kernel(LaunchArgs a) {
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, (MinBlocks<P, R>::value)) pairhmm_kernel(LaunchArgs a) {
   using V = typename P::V;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31;

@@ -273,35 +273,33 @@ void emit_program(const SortedHaps& s, bool with_suffix, ProgramBuild& out) {
     v.push_back(e | pending);
     pending = 0;
   };
+  std::vector<int32_t> eff_len(m, 0);
   for (int32_t i = 0; i < m; ++i) {
     const Seg& g = segs[i];
+    eff_len[i] = g.start > 0 ? eff_len[writer[i]] : g.len;
     Segment rec{};
     rec.hap = g.hap;
     rec.node = g.cut.column >= 0 ? g.cut.node : -1;
-    rec.cut_code = g.cut.column >= 0 ? s.codes[g.hap][g.cut.column - 1] : 0;
     rec.staged = g.start > 0 ? 1 : 0;
-    const int32_t src_len = g.start > 0 ? segs[writer[i]].len : 1;
-    rec.scale_d = static_cast<double>(src_len) / static_cast<double>(g.len);
-    rec.scale_f = static_cast<float>(rec.scale_d);
+    rec.factor = static_cast<double>(eff_len[i]) / static_cast<double>(g.len);
     rec.init_d = init_f64 / static_cast<double>(g.len);
     rec.init_f = static_cast<float>(init_f32 / static_cast<double>(g.len));
     rec.next_slot = -1;
     if (i + 1 < m && writer[i + 1] >= 0 && writer[i + 1] < i) rec.next_slot = writes.at({writer[i + 1], segs[i + 1].start}).second;
     out.segs.push_back(rec);
-    if (g.stop > g.start) {
-      for (int32_t j = g.start + 1; j <= g.stop; ++j) {
-        push(out.fwd, s.codes[g.hap][j - 1] | (j == g.start + 1 ? EV_BEGIN : 0u));
-        auto it = writes.find({i, j});
-        if (it != writes.end()) {
-          const uint32_t slot = it->second.second >= 0 ? static_cast<uint32_t>(it->second.second) : kPayloadNone;
-          pending |= EV_SNAP | (it->second.first ? EV_STAGE : 0u) | (slot << kPayloadShift);
-        }
+    // A cut segment also computes its cut column (stop + 1) as an ordinary column.
+    const int32_t last = g.cut.column >= 0 ? g.cut.column : g.stop;
+    for (int32_t j = g.start + 1; j <= last; ++j) {
+      const bool is_cut = g.cut.column >= 0 && j == g.cut.column;
+      push(out.fwd, s.codes[g.hap][j - 1] | (j == g.start + 1 ? EV_BEGIN : 0u) | (is_cut ? EV_ACC : 0u));
+      auto it = is_cut ? writes.end() : writes.find({i, j});
+      if (it != writes.end()) {
+        const uint32_t slot = it->second.second >= 0 ? static_cast<uint32_t>(it->second.second) : kPayloadNone;
+        pending |= EV_SNAP | (it->second.first ? EV_STAGE : 0u) | (slot << kPayloadShift);
       }
-      pending |= EV_END;
-    } else {
-      push(out.fwd, EV_BEGIN | EV_NOCOMP);
     }
-    out.fwd_columns += static_cast<uint64_t>(g.stop - g.start);
+    pending |= g.cut.column >= 0 ? EV_JOIN : EV_END;
+    out.fwd_columns += static_cast<uint64_t>(last - g.start);
   }
   push(out.fwd, 0);
   out.n_slots = n_slots;

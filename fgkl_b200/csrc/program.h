@@ -4,9 +4,9 @@
 // every read of the region walks, one warp per read task. The forward stream holds one 32-bit entry
 // per DP column of each distinct sorted haplotype; the backward stream one per backward column of
 // each suffix sweep. An entry's low byte is the prior code of the haplotype base the column emits;
-// its flags name the events a lane handles when it reaches the entry: events that load state
-// (BEGIN, SWEEP) for the entry's own column, events that store state (SNAP, END, NODE) for the
-// PREVIOUS column. Deferring the stores by one column lets the lane handle every event of a step
+// its flags name the events a lane handles when it reaches the entry: events that load or keep state
+// before the entry's own column is computed (BEGIN, ACC, SWEEP), and events that store the state of
+// the PREVIOUS column (SNAP, END, JOIN, NODE). Deferring the stores by one column lets the lane handle every event of a step
 // in one branch before computing. Each stream is padded with kStreamPad zero entries on both sides
 // so lanes ahead of or behind the wavefront read harmless entries without bounds checks.
 #pragma once
@@ -20,34 +20,39 @@ constexpr int kStreamPad = 64;
 constexpr uint32_t kCodeMask = 0xFFu;
 // forward
 constexpr uint32_t EV_BEGIN = 1u << 8;    // load the segment's start column before computing this one
-constexpr uint32_t EV_NOCOMP = 1u << 9;   // zero-length segment: finish it right after BEGIN
+constexpr uint32_t EV_ACC = 1u << 9;      // this column is a cut column: keep the result so far first
 constexpr uint32_t EV_SNAP = 1u << 10;    // the previous column is a snapshot (payload: slot, staging)
-constexpr uint32_t EV_END = 1u << 11;     // the previous column ended the segment (result or join)
+constexpr uint32_t EV_END = 1u << 11;     // the previous column ended the segment
 constexpr uint32_t EV_STAGE = 1u << 12;   // the snapshot also goes to the staging buffer of the next segment
+constexpr uint32_t EV_JOIN = 1u << 13;    // the previous column is a cut column: keep its M and Y rows
 // backward
 constexpr uint32_t EV_SWEEP = 1u << 8;    // load the sweep's start node before computing this column
 constexpr uint32_t EV_NODE = 1u << 10;    // the previous column is a backward node (payload: node id)
 constexpr uint32_t EV_NSTAGE = 1u << 12;  // the node also goes to the staging buffer of the next sweep
-constexpr uint32_t kEvMask = 0x1F00u;
-constexpr int kPayloadShift = 13;
-constexpr uint32_t kPayloadNone = (1u << (32 - kPayloadShift)) - 1;  // no global slot / node
+constexpr uint32_t kEvMask = 0x3F00u;
+constexpr int kPayloadShift = 14;
+constexpr uint32_t kPayloadNone = (1u << (32 - kPayloadShift)) - 1;  // no global slot
 
 // Prior code of haplotype 'N' (codes 0..4 are A, C, G, T, N; extra bytes follow in first-seen
 // order, fgkl kernel.rs:27-107).
 constexpr int kCodeN = 4;
 constexpr uint8_t kNoCode = 0xFF;
 
-// One forward run of a distinct sorted haplotype: columns start+1..=stop, resumed from its start
-// column (the origin or a staged snapshot) and either finished or joined with a backward node.
+// One forward run of a distinct sorted haplotype: columns start+1..=stop resumed from its start
+// column (the origin or a staged snapshot), then either finished or, for a cut, continued through
+// the cut column, whose match and deletion rows are joined with backward node `node`.
+//
+// Snapshots are never rescaled: the recurrence is linear in the row-0 constant INITIAL / length, so
+// a segment keeps the constant of the first segment of its snapshot chain (length eff_len) and its
+// raw result is multiplied by eff_len / hap_len at the end (fgkl rescales at every resume,
+// kernel.rs:641, :673-678; the two agree up to rounding).
 struct Segment {
-  float scale_f;      // src_len / hap_len narrowed like fgkl kernel.rs:641
-  float init_f;       // 2^120 / hap_len narrowed to f32 (kernel.rs:640)
-  double scale_d;
-  double init_d;      // 2^1020 / hap_len
+  double factor;      // eff_len / hap_len
+  float init_f;       // 2^120 / hap_len narrowed to f32 (kernel.rs:640), for origin segments
   int32_t staged;     // 1: start from the staging buffer; 0: from the origin (column 0)
+  double init_d;      // 2^1020 / hap_len
   int32_t next_slot;  // global snapshot slot to prefetch for the NEXT segment at this BEGIN, or -1
   int32_t node;       // backward node joined at the cut; -1 = no cut
-  int32_t cut_code;   // prior code of the haplotype base at the cut column
   int32_t hap;        // sorted haplotype index
   int32_t pad_;
 };
