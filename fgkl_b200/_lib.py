@@ -44,6 +44,10 @@ class Stats(C.Structure):
         ("backward_cells", C.c_uint64),
         ("prefix_only_cells", C.c_uint64),
         ("kernel_launches", C.c_uint64),
+        ("host_plan_ms", C.c_double),
+        ("host_pack_ms", C.c_double),
+        ("host_upload_ms", C.c_double),
+        ("host_fetch_ms", C.c_double),
     ]
 
 

@@ -59,6 +59,8 @@ int check_offsets(const int32_t* offsets, int64_t n, int64_t total, const char* 
   return FGKL_OK;
 }
 
+void to_stats(const fgkl::BatchStats& bs, fgkl_stats* s);
+
 int per_call(const fgkl_reads* reads, const fgkl_haplotypes* haps, const fgkl_config* cfg, bool pd, double* out, int64_t out_len,
              fgkl_stats* stats) {
   t_error.clear();
@@ -112,16 +114,7 @@ int per_call(const fgkl_reads* reads, const fgkl_haplotypes* haps, const fgkl_co
   fgkl::BatchStats bs;
   rc = e->compute(in, ec, out, out_len, &bs);
   if (rc) return set_error(rc, e->error());
-  if (stats) {
-    stats->fallback_pairs = bs.fallback_pairs;
-    stats->rescue_reads = bs.rescue_reads;
-    stats->nominal_cells = bs.nominal_cells;
-    stats->computed_cells = bs.computed_cells;
-    stats->forward_cells = bs.forward_cells;
-    stats->backward_cells = bs.backward_cells;
-    stats->prefix_only_cells = bs.prefix_only_cells;
-    stats->kernel_launches = bs.kernel_launches;
-  }
+  if (stats) to_stats(bs, stats);
   return FGKL_OK;
 }
 
@@ -142,6 +135,10 @@ void to_stats(const fgkl::BatchStats& bs, fgkl_stats* s) {
   s->backward_cells = bs.backward_cells;
   s->prefix_only_cells = bs.prefix_only_cells;
   s->kernel_launches = bs.kernel_launches;
+  s->host_plan_ms = bs.host_plan_ms;
+  s->host_pack_ms = bs.host_pack_ms;
+  s->host_upload_ms = bs.host_upload_ms;
+  s->host_fetch_ms = bs.host_fetch_ms;
 }
 
 }  // namespace

@@ -1,6 +1,7 @@
 #include "engine.h"
 
 #include <algorithm>
+#include <chrono>
 #include <cstring>
 #include <map>
 #include <thread>
@@ -30,11 +31,13 @@ int single_rows(int len) {
 }
 
 struct RegionPlan {
-  ProgramBuild shared, prefix;
+  ProgramBuild prog;
   std::vector<HapInfo> haps;
+  std::vector<uint8_t> seq;  // prior codes of the distinct sorted haplotypes, concatenated
   uint8_t codes[256];
   SharedColumns cols;
   uint64_t read_bases = 0, hap_bases = 0;
+  int n_distinct = 0;
   bool extra_codes = false;  // a haplotype byte outside ACGTN: the region runs on the FP64 kernel
 };
 
@@ -50,26 +53,58 @@ void plan_region(const BatchInput& in, int g, int64_t first_read, int64_t first_
     out.read_bases += static_cast<uint64_t>(in.read_off[first_read + r + 1] - in.read_off[first_read + r]);
   if (n_haps == 0 || n_reads == 0) return;
   const SortedHaps s = SortedHaps::make(views, share);
-  emit_program(s, share, out.shared);
-  emit_program(s, false, out.prefix);
+  emit_program(s, share, out.prog);
   code_table(s, out.codes);
   out.extra_codes = s.num_codes() > 5;
   out.cols = s.columns();
   out.haps.resize(static_cast<size_t>(n_haps));
-  int seg = -1;
+  int seg = -1, src = 0;
   for (int k = 0; k < n_haps; ++k) {
-    if (!s.dup[k]) ++seg;
-    int src = k;
-    while (src > 0 && s.dup[src]) --src;
-    out.haps[k] = HapInfo{s.order[k], seg, src, 0};
+    if (!s.dup[k]) {
+      ++seg;
+      src = k;
+      out.haps[k].seq = static_cast<int32_t>(out.seq.size());
+      out.seq.insert(out.seq.end(), s.codes[k].begin(), s.codes[k].end());
+      ++out.n_distinct;
+    } else {
+      out.haps[k].seq = out.haps[src].seq;
+    }
+    HapInfo& h = out.haps[k];
+    h.order = s.order[k];
+    h.seg = seg;
+    h.src = src;
+    h.len = s.bases[k].len;
+    h.pad_[0] = h.pad_[1] = h.pad_[2] = 0;
   }
 }
 
-template <class T>
-void append_section(std::vector<uint8_t>& blob, const std::vector<T>& v, size_t& off) {
-  off = align_up(blob.size(), 16);
-  blob.resize(off + v.size() * sizeof(T));
-  if (!v.empty()) std::memcpy(blob.data() + off, v.data(), v.size() * sizeof(T));
+// Runs fn(i) for i in [0, n) on up to `threads` threads (strided, so neighbouring items spread).
+template <class F>
+void parallel_for(int64_t n, int threads, F&& fn) {
+  threads = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(threads, n)));
+  if (threads == 1) {
+    for (int64_t i = 0; i < n; ++i) fn(i);
+    return;
+  }
+  std::vector<std::thread> pool;
+  pool.reserve(static_cast<size_t>(threads));
+  for (int t = 0; t < threads; ++t)
+    pool.emplace_back([&, t] {
+      for (int64_t i = t; i < n; i += threads) fn(i);
+    });
+  for (auto& th : pool) th.join();
+}
+
+int host_threads() { return std::max(1, static_cast<int>(std::thread::hardware_concurrency())); }
+
+// Copies `bytes` bytes in `chunks` pieces on several threads.
+void parallel_copy(uint8_t* dst, const uint8_t* src, size_t bytes) {
+  constexpr size_t kChunk = size_t{4} << 20;
+  const int64_t chunks = static_cast<int64_t>((bytes + kChunk - 1) / kChunk);
+  parallel_for(chunks, std::min(host_threads(), 16), [&](int64_t c) {
+    const size_t lo = static_cast<size_t>(c) * kChunk, n = std::min(kChunk, bytes - lo);
+    std::memcpy(dst + lo, src + lo, n);
+  });
 }
 
 }  // namespace
@@ -143,8 +178,15 @@ T* Engine::grow(T*& ptr, size_t& cap, size_t n) {
   return ptr;
 }
 
+namespace {
+double ms_since(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+}  // namespace
+
 int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
   cudaSetDevice(device_);
+  const auto t_start = std::chrono::steady_clock::now();
   cfg_ = cfg;
   error_.clear();
   planned_ = BatchStats{};
@@ -163,6 +205,7 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
   }
   const int64_t total_reads = first_read[N], total_haps = first_hap[N];
   out_len_ = out_off[N];
+  n_regions_ = N;
   for (int g = 0; g < N; ++g) {
     for (int64_t r = first_read[g]; r < first_read[g + 1]; ++r) {
       const int64_t len = in.read_off[r + 1] - in.read_off[r];
@@ -179,65 +222,59 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
   // Plan the regions in parallel.
   std::vector<RegionPlan> plans(static_cast<size_t>(N));
   const bool share = cfg.share_suffixes;
-  {
-    const int threads = std::max(1, std::min<int>(static_cast<int>(std::thread::hardware_concurrency()), (N + 7) / 8));
-    std::vector<std::thread> pool;
-    for (int t = 0; t < threads; ++t)
-      pool.emplace_back([&, t] {
-        for (int g = t; g < N; g += threads) plan_region(in, g, first_read[g], first_hap[g], share, plans[g]);
-      });
-    for (auto& th : pool) th.join();
-  }
+  parallel_for(N, std::min(host_threads(), (N + 7) / 8),
+               [&](int64_t g) { plan_region(in, static_cast<int>(g), first_read[g], first_hap[g], share, plans[g]); });
 
-  // Concatenate the programs; each stream gets kStreamPad zero entries on both sides.
+  planned_.host_plan_ms = ms_since(t_start);
+  const auto t_pack = std::chrono::steady_clock::now();
+  // Section offsets. Each stream gets kStreamPad zero entries on both sides.
   std::vector<Region> regions(static_cast<size_t>(N));
-  std::vector<HapInfo> haps;
-  std::vector<uint32_t> stream(kStreamPad, 0u);
-  std::vector<Segment> segs;
-  std::vector<Sweep> sweeps;
-  std::vector<uint8_t> codes(static_cast<size_t>(N) * 256);
+  int64_t n_haps = 0, n_stream = kStreamPad, n_segs = 0, n_sweeps = 0, n_seq = 0;
   int max_slots = 1, max_nodes = 1, max_segs = 1;
-  auto put_stream = [&](const std::vector<uint32_t>& v, int32_t& off, int32_t& len) {
-    off = static_cast<int32_t>(stream.size());
-    len = v.empty() ? 0 : static_cast<int32_t>(v.size()) - 1;  // the last entry only carries post events
-    stream.insert(stream.end(), v.begin(), v.end());
-    stream.insert(stream.end(), kStreamPad, 0u);
-  };
-  auto put_program = [&](const ProgramBuild& b, Program& p) {
-    put_stream(b.fwd, p.fwd_off, p.fwd_len);
-    put_stream(b.bwd, p.bwd_off, p.bwd_len);
-    p.seg_off = static_cast<int32_t>(segs.size());
-    p.n_segs = static_cast<int32_t>(b.segs.size());
-    segs.insert(segs.end(), b.segs.begin(), b.segs.end());
-    p.sweep_off = static_cast<int32_t>(sweeps.size());
-    p.n_sweeps = static_cast<int32_t>(b.sweeps.size());
-    sweeps.insert(sweeps.end(), b.sweeps.begin(), b.sweeps.end());
-    p.n_slots = b.n_slots;
-    p.n_nodes = b.n_nodes;
-    max_slots = std::max(max_slots, b.n_slots);
-    max_nodes = std::max(max_nodes, b.n_nodes);
-    max_segs = std::max(max_segs, static_cast<int>(b.segs.size()));
-  };
+  std::vector<int64_t> queue_cap(kRowBins, 0);
   for (int g = 0; g < N; ++g) {
-    RegionPlan& rp = plans[g];
+    const RegionPlan& rp = plans[g];
     Region& R = regions[g];
     std::memset(&R, 0, sizeof R);
-    put_program(rp.shared, R.shared);
-    put_program(rp.prefix, R.prefix);
-    R.hap_off = static_cast<int32_t>(haps.size());
+    Program& p = R.prog;
+    auto put_stream = [&](const std::vector<uint32_t>& v, int32_t& off, int32_t& len) {
+      off = static_cast<int32_t>(n_stream);
+      len = v.empty() ? 0 : static_cast<int32_t>(v.size()) - 1;  // the last entry only carries post events
+      n_stream += static_cast<int64_t>(v.size()) + kStreamPad;
+    };
+    put_stream(rp.prog.fwd, p.fwd_off, p.fwd_len);
+    put_stream(rp.prog.bwd, p.bwd_off, p.bwd_len);
+    p.seg_off = static_cast<int32_t>(n_segs);
+    p.n_segs = static_cast<int32_t>(rp.prog.segs.size());
+    n_segs += p.n_segs;
+    p.sweep_off = static_cast<int32_t>(n_sweeps);
+    p.n_sweeps = static_cast<int32_t>(rp.prog.sweeps.size());
+    n_sweeps += p.n_sweeps;
+    p.n_slots = rp.prog.n_slots;
+    p.n_nodes = rp.prog.n_nodes;
+    max_slots = std::max(max_slots, rp.prog.n_slots);
+    max_nodes = std::max(max_nodes, rp.prog.n_nodes);
+    max_segs = std::max(max_segs, p.n_segs);
+    R.hap_off = static_cast<int32_t>(n_haps);
     R.n_haps = in.region_haps[g];
+    n_haps += static_cast<int64_t>(rp.haps.size());
     R.read_off = static_cast<int32_t>(first_read[g]);
     R.n_reads = in.region_reads[g];
     R.out_off = out_off[g];
     R.code_off = g * 256;
-    haps.insert(haps.end(), rp.haps.begin(), rp.haps.end());
-    if (!rp.haps.empty()) std::memcpy(codes.data() + static_cast<size_t>(g) * 256, rp.codes, 256);
+    R.seq_off = static_cast<int32_t>(n_seq);
+    n_seq += static_cast<int64_t>(rp.seq.size());
     planned_.nominal_cells += rp.read_bases * rp.hap_bases;
-    planned_.forward_cells += rp.read_bases * rp.shared.fwd_columns;
-    planned_.backward_cells += rp.read_bases * rp.shared.bwd_columns;
+    planned_.forward_cells += rp.read_bases * rp.prog.fwd_columns;
+    planned_.backward_cells += rp.read_bases * rp.prog.bwd_columns;
     planned_.prefix_only_cells += rp.read_bases * rp.cols.prefix_only;
+    if (rp.n_distinct > 0)
+      for (int64_t r = first_read[g]; r < first_read[g + 1]; ++r)
+        queue_cap[single_rows(static_cast<int>(in.read_off[r + 1] - in.read_off[r]))] += rp.n_distinct;
   }
   planned_.computed_cells = planned_.forward_cells + planned_.backward_cells;
+  if (n_stream > INT32_MAX || n_seq > INT32_MAX || n_haps > INT32_MAX)
+    return fail(FGKL_E_INVALID_ARGUMENT, "batch too large for 32-bit plan offsets; split it");
 
   // Tasks: reads sorted longest first; FP32 packs consecutive pairs below 256 bases.
   struct Key {
@@ -246,35 +283,34 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
     bool operator<(const Key& o) const { return kind != o.kind ? kind < o.kind : rows < o.rows; }
   };
   std::map<Key, std::vector<std::pair<uint64_t, Task>>> by_bin;
-  std::vector<int> rescue_count(kRowBins, 0);
+  std::vector<int> order;
   for (int g = 0; g < N; ++g) {
     const int n_reads = in.region_reads[g];
     if (n_reads == 0 || in.region_haps[g] == 0) continue;
-    std::vector<int> order(static_cast<size_t>(n_reads));
+    order.resize(static_cast<size_t>(n_reads));
     for (int r = 0; r < n_reads; ++r) order[r] = r;
     auto len_of = [&](int r) { return static_cast<int>(in.read_off[first_read[g] + r + 1] - in.read_off[first_read[g] + r]); };
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return len_of(a) > len_of(b); });
-    const uint64_t cost_cols = plans[g].shared.fwd.size() + plans[g].shared.bwd.size() + 31;
-    for (int r = 0; r < n_reads; ++r) rescue_count[single_rows(len_of(r))]++;
+    const uint64_t cost_cols = plans[g].prog.fwd.size() + plans[g].prog.bwd.size() + 31;
     size_t i = 0;
     if (cfg.double_precision || plans[g].extra_codes) {
       for (; i < order.size(); ++i) {
         const int rows = single_rows(len_of(order[i]));
         by_bin[{Kind::kOneF64, rows}].push_back(
-            {cost_cols * rows, Task{g, {static_cast<int32_t>(first_read[g] + order[i]), -1}, rows}});
+            {cost_cols * rows, Task{g, {static_cast<int32_t>(first_read[g] + order[i]), -1}, rows, -1}});
       }
     } else {
       while (i < order.size() && packed_rows(len_of(order[i])) > 8) {
         const int rows = single_rows(len_of(order[i]));
         by_bin[{Kind::kOneF32, rows}].push_back(
-            {cost_cols * rows, Task{g, {static_cast<int32_t>(first_read[g] + order[i]), -1}, rows}});
+            {cost_cols * rows, Task{g, {static_cast<int32_t>(first_read[g] + order[i]), -1}, rows, -1}});
         ++i;
       }
       for (; i < order.size(); i += 2) {
         const int rows = packed_rows(len_of(order[i]));
         const int32_t a = static_cast<int32_t>(first_read[g] + order[i]);
         const int32_t b = i + 1 < order.size() ? static_cast<int32_t>(first_read[g] + order[i + 1]) : -1;
-        by_bin[{Kind::kPackedF32, rows}].push_back({cost_cols * rows, Task{g, {a, b}, rows}});
+        by_bin[{Kind::kPackedF32, rows}].push_back({cost_cols * rows, Task{g, {a, b}, rows, -1}});
       }
     }
   }
@@ -297,61 +333,77 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
   // The bin with the most work launches first; the others fill the SMs its tail frees.
   std::stable_sort(first.begin(), first.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
   for (auto& f : first) bins_.push_back(f.second);
-  std::vector<int> queue_off(kRowBins, 0);
+  // Recomputation queues: room for every (read, distinct haplotype) pair of each rows-per-lane bin.
+  // Pairs either pass loses (an FP32 underflow, or a joined FP64 result below the backward range)
+  // are recomputed in FP64 without sharing, which cannot lose a pair (lib.rs:461-487).
+  const bool queue_on = cfg.double_fallback;
+  std::vector<int> queue_off(kRowBins + 1, 0);
   {
-    int acc = 0;
+    int64_t acc = 0;
     for (int r = 0; r < kRowBins; ++r) {
-      queue_off[r] = acc;
-      acc += rescue_count[r];
+      queue_off[r] = static_cast<int>(acc);
+      if (queue_on) acc += queue_cap[r];
     }
+    if (acc > INT32_MAX) return fail(FGKL_E_INVALID_ARGUMENT, "batch too large for the recomputation queue; split it");
+    queue_off[kRowBins] = static_cast<int>(acc);
   }
-  if (cfg.double_fallback) {
+  if (queue_on) {
     for (int r = 1; r < kRowBins; ++r) {
-      if (rescue_count[r] == 0) continue;
+      const int cap = queue_off[r + 1] - queue_off[r];
+      if (cap == 0) continue;
       int per_sm = 0, threads = 0;
       occupancy(Kind::kOneF64, r, &per_sm, &threads);
       if (per_sm <= 0) return fail(FGKL_E_CUDA, "recomputation kernel unavailable on this device");
-      Bin b{Kind::kOneF64, r, queue_off[r], rescue_count[r], 0, 0, 0};
-      b.blocks = std::max(1, std::min((b.n_tasks + kWarpsPerBlock - 1) / kWarpsPerBlock, per_sm * sms_));
+      Bin b{Kind::kOneF64, r, queue_off[r], cap, 0, 0, 0};
+      b.blocks = std::max(1, std::min((cap + kWarpsPerBlock - 1) / kWarpsPerBlock, per_sm * sms_));
       rescue_bins_.push_back(b);
     }
   }
   // Bins of one pass run concurrently, so each owns a slice of the scratch.
   size_t scratch_total = 256;
   for (auto* list : {&bins_, &rescue_bins_}) {
+    const bool rescue = list == &rescue_bins_;
     size_t off = 0;
     for (Bin& b : *list) {
-      b.stride = align_up(scratch_bytes(b.kind, b.rows, max_slots, max_nodes, max_segs));
+      b.stride = align_up(rescue ? scratch_bytes(b.kind, b.rows, 0, 0, 1) : scratch_bytes(b.kind, b.rows, max_slots, max_nodes, max_segs));
       b.scratch_off = off;
       off += static_cast<size_t>(b.blocks) * kWarpsPerBlock * b.stride;
     }
     scratch_total = std::max(scratch_total, off);
   }
 
-  // Plan blob: regions | haps | stream | segs | sweeps | code tables.
-  std::vector<uint8_t> blob;
-  size_t o_regions, o_haps, o_stream, o_segs, o_sweeps, o_codes;
-  append_section(blob, regions, o_regions);
-  append_section(blob, haps, o_haps);
-  append_section(blob, stream, o_stream);
-  append_section(blob, segs, o_segs);
-  append_section(blob, sweeps, o_sweeps);
-  append_section(blob, codes, o_codes);
+  // Plan blob: regions | haps | stream | segs | sweeps | code tables | haplotype codes.
+  size_t o_regions, o_haps, o_stream, o_segs, o_sweeps, o_codes, o_seq, blob_bytes = 0;
+  auto section = [&](size_t bytes, size_t& off) {
+    off = align_up(blob_bytes, 16);
+    blob_bytes = off + bytes;
+  };
+  section(regions.size() * sizeof(Region), o_regions);
+  section(static_cast<size_t>(n_haps) * sizeof(HapInfo), o_haps);
+  section(static_cast<size_t>(n_stream) * sizeof(uint32_t), o_stream);
+  section(static_cast<size_t>(n_segs) * sizeof(Segment), o_segs);
+  section(static_cast<size_t>(n_sweeps) * sizeof(Sweep), o_sweeps);
+  section(static_cast<size_t>(N) * 256, o_codes);
+  section(static_cast<size_t>(n_seq) + 16, o_seq);
 
   // Device buffers.
   const int64_t read_bytes = total_reads > 0 ? in.read_off[total_reads] : 0;
-  n_small_ = static_cast<int>(bins_.size() + rescue_bins_.size()) + 2 * kRowBins;
+  n_small_ = static_cast<int>(bins_.size() + rescue_bins_.size()) + 2 * kRowBins + 1;
   if (!grow(d_reads_, cap_reads_, static_cast<size_t>(read_bytes) * 5 + 16) ||
-      !grow(d_read_off_, cap_read_off_, static_cast<size_t>(total_reads) + 1) || !grow(d_plan_, cap_plan_, blob.size()) ||
-      !grow(d_tasks_, cap_tasks_, tasks.size() + 1) || !grow(d_queue_, cap_queue_, static_cast<size_t>(total_reads) + 1) ||
+      !grow(d_read_off_, cap_read_off_, static_cast<size_t>(total_reads) + 1) || !grow(d_plan_, cap_plan_, blob_bytes) ||
+      !grow(d_tasks_, cap_tasks_, tasks.size() + 1) || !grow(d_queue_, cap_queue_, static_cast<size_t>(queue_off[kRowBins]) + 1) ||
       !grow(d_small_, cap_small_, static_cast<size_t>(n_small_)) || !grow(d_out_, cap_out_, static_cast<size_t>(out_len_) + 1) ||
       !grow(d_scratch_, cap_scratch_, scratch_total))
     return fail(FGKL_E_CUDA, "device allocation failed");
 
-  // Stage and upload: reads (five arrays), read offsets, plan, tasks, queue offsets.
-  const size_t stage_bytes = align_up(static_cast<size_t>(read_bytes) * 5) + align_up((total_reads + 1) * sizeof(int64_t)) +
-                             align_up(blob.size()) + align_up(tasks.size() * sizeof(Task)) + align_up(kRowBins * sizeof(int)) +
-                             align_up(static_cast<size_t>(out_len_) * sizeof(double)) + align_up(sizeof(Counters));
+  // Pinned staging: reads (five arrays) | read offsets | plan | tasks | queue offsets | results | counters.
+  const size_t s_reads = 0, s_read_off = s_reads + align_up(static_cast<size_t>(read_bytes) * 5);
+  const size_t s_blob = s_read_off + align_up((total_reads + 1) * sizeof(int64_t));
+  const size_t s_tasks = s_blob + align_up(blob_bytes);
+  const size_t s_qoff = s_tasks + align_up(tasks.size() * sizeof(Task));
+  const size_t s_out = s_qoff + align_up((kRowBins + 1) * sizeof(int));
+  const size_t stage_bytes = s_out + align_up(static_cast<size_t>(out_len_) * sizeof(double)) + align_up(sizeof(Counters));
+  cudaStreamSynchronize(stream_);  // the staging buffer may still feed an earlier copy
   if (stage_bytes > cap_stage_) {
     if (h_stage_) cudaFreeHost(h_stage_);
     h_stage_ = nullptr;
@@ -361,33 +413,58 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
     }
     cap_stage_ = stage_bytes;
   }
-  cudaStreamSynchronize(stream_);  // the staging buffer may still feed an earlier copy
-  uint8_t* p = h_stage_;
+  out_stage_ = s_out;
+  uint8_t* const st = h_stage_;
   const uint8_t* srcs[5] = {in.bases, in.quals, in.ins, in.del, in.gcp};
   for (int a = 0; a < 5; ++a)
-    if (read_bytes) std::memcpy(p + static_cast<size_t>(a) * read_bytes, srcs[a], static_cast<size_t>(read_bytes));
-  int rc;
-  if ((rc = check(cudaMemcpyAsync(d_reads_, p, static_cast<size_t>(read_bytes) * 5, cudaMemcpyHostToDevice, stream_), "upload reads")))
-    return rc;
-  p += align_up(static_cast<size_t>(read_bytes) * 5);
-  std::memcpy(p, in.read_off, (total_reads + 1) * sizeof(int64_t));
-  if ((rc = check(cudaMemcpyAsync(d_read_off_, p, (total_reads + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, stream_), "upload offsets")))
-    return rc;
-  p += align_up((total_reads + 1) * sizeof(int64_t));
-  std::memcpy(p, blob.data(), blob.size());
-  if ((rc = check(cudaMemcpyAsync(d_plan_, p, blob.size(), cudaMemcpyHostToDevice, stream_), "upload plan"))) return rc;
-  p += align_up(blob.size());
-  if (!tasks.empty()) {
-    std::memcpy(p, tasks.data(), tasks.size() * sizeof(Task));
-    if ((rc = check(cudaMemcpyAsync(d_tasks_, p, tasks.size() * sizeof(Task), cudaMemcpyHostToDevice, stream_), "upload tasks")))
-      return rc;
+    if (read_bytes) parallel_copy(st + s_reads + static_cast<size_t>(a) * read_bytes, srcs[a], static_cast<size_t>(read_bytes));
+  std::memcpy(st + s_read_off, in.read_off, (total_reads + 1) * sizeof(int64_t));
+  {
+    uint8_t* blob = st + s_blob;
+    std::memcpy(blob + o_regions, regions.data(), regions.size() * sizeof(Region));
+    uint32_t* stream = reinterpret_cast<uint32_t*>(blob + o_stream);
+    std::memset(stream, 0, kStreamPad * sizeof(uint32_t));
+    std::memset(blob + o_seq + n_seq, 0, 16);
+    parallel_for(N, std::min(host_threads(), (N + 31) / 32), [&](int64_t g) {
+      const RegionPlan& rp = plans[g];
+      const Region& R = regions[g];
+      if (!rp.haps.empty()) std::memcpy(blob + o_haps + static_cast<size_t>(R.hap_off) * sizeof(HapInfo), rp.haps.data(), rp.haps.size() * sizeof(HapInfo));
+      auto put = [&](const std::vector<uint32_t>& v, int32_t off) {
+        if (!v.empty()) std::memcpy(stream + off, v.data(), v.size() * sizeof(uint32_t));
+        std::memset(stream + off + v.size(), 0, kStreamPad * sizeof(uint32_t));
+      };
+      put(rp.prog.fwd, R.prog.fwd_off);
+      put(rp.prog.bwd, R.prog.bwd_off);
+      if (!rp.prog.segs.empty())
+        std::memcpy(blob + o_segs + static_cast<size_t>(R.prog.seg_off) * sizeof(Segment), rp.prog.segs.data(), rp.prog.segs.size() * sizeof(Segment));
+      if (!rp.prog.sweeps.empty())
+        std::memcpy(blob + o_sweeps + static_cast<size_t>(R.prog.sweep_off) * sizeof(Sweep), rp.prog.sweeps.data(), rp.prog.sweeps.size() * sizeof(Sweep));
+      if (!rp.haps.empty()) std::memcpy(blob + o_codes + static_cast<size_t>(g) * 256, rp.codes, 256);
+      else std::memset(blob + o_codes + static_cast<size_t>(g) * 256, 0, 256);
+      if (!rp.seq.empty()) std::memcpy(blob + o_seq + R.seq_off, rp.seq.data(), rp.seq.size());
+    });
   }
-  p += align_up(tasks.size() * sizeof(Task));
-  std::memcpy(p, queue_off.data(), kRowBins * sizeof(int));
-  if ((rc = check(cudaMemcpyAsync(d_small_ + (n_small_ - 2 * kRowBins), p, kRowBins * sizeof(int), cudaMemcpyHostToDevice, stream_),
+  if (!tasks.empty()) std::memcpy(st + s_tasks, tasks.data(), tasks.size() * sizeof(Task));
+  std::memcpy(st + s_qoff, queue_off.data(), (kRowBins + 1) * sizeof(int));
+
+  planned_.host_pack_ms = ms_since(t_pack);
+  const auto t_up = std::chrono::steady_clock::now();
+  int rc;
+  if ((rc = check(cudaMemcpyAsync(d_reads_, st + s_reads, static_cast<size_t>(read_bytes) * 5, cudaMemcpyHostToDevice, stream_), "upload reads")))
+    return rc;
+  if ((rc = check(cudaMemcpyAsync(d_read_off_, st + s_read_off, (total_reads + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, stream_),
+                  "upload offsets")))
+    return rc;
+  if ((rc = check(cudaMemcpyAsync(d_plan_, st + s_blob, blob_bytes, cudaMemcpyHostToDevice, stream_), "upload plan"))) return rc;
+  if (!tasks.empty() &&
+      (rc = check(cudaMemcpyAsync(d_tasks_, st + s_tasks, tasks.size() * sizeof(Task), cudaMemcpyHostToDevice, stream_), "upload tasks")))
+    return rc;
+  if ((rc = check(cudaMemcpyAsync(d_small_ + (n_small_ - 2 * kRowBins - 1), st + s_qoff, (kRowBins + 1) * sizeof(int),
+                                  cudaMemcpyHostToDevice, stream_),
                   "upload queue offsets")))
     return rc;
 
+  planned_.host_upload_ms = ms_since(t_up);
   view_.bases = d_reads_;
   view_.quals = d_reads_ + read_bytes;
   view_.ins = d_reads_ + 2 * read_bytes;
@@ -400,6 +477,7 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
   view_.segs = reinterpret_cast<const Segment*>(d_plan_ + o_segs);
   view_.sweeps = reinterpret_cast<const Sweep*>(d_plan_ + o_sweeps);
   view_.code_of_byte = d_plan_ + o_codes;
+  view_.hap_codes = d_plan_ + o_seq;
   view_.err_prob = d_err_;
   view_.m2m = d_m2m_;
   view_.out = d_out_;
@@ -412,7 +490,7 @@ int Engine::run() {
   cudaSetDevice(device_);
   int rc;
   int* counters = d_small_;                                // one per launch
-  int* queue_off = d_small_ + (n_small_ - 2 * kRowBins);  // uploaded by prepare
+  int* queue_off = d_small_ + (n_small_ - 2 * kRowBins - 1);  // kRowBins + 1 entries, uploaded by prepare
   int* queue_tail = d_small_ + (n_small_ - kRowBins);
   const size_t n_launch = bins_.size() + rescue_bins_.size();
   if ((rc = check(cudaMemsetAsync(counters, 0, n_launch * sizeof(int), stream_), "reset task counters"))) return rc;
@@ -436,11 +514,6 @@ int Engine::run() {
       a.task_counter = counters + i++;
       a.scratch = d_scratch_ + bin.scratch_off;
       a.scratch_stride = bin.stride;
-      a.use_prefix = rescue ? 1 : (cfg_.share_suffixes ? 0 : 1);
-      a.rescue = rescue ? 1 : 0;
-      a.queue = (!rescue && cfg_.double_fallback) ? d_queue_ : nullptr;
-      a.queue_off = queue_off;
-      a.queue_tail = queue_tail;
       a.min_accept_plain = (!rescue && !cfg_.double_precision) ? 1 : 0;
       if ((rc = check(launch(bin.kind, bin.rows, bin.blocks, a, s), rescue ? "recomputation launch" : "first-pass launch")))
         return rc;
@@ -452,18 +525,24 @@ int Engine::run() {
     return FGKL_OK;
   };
   if ((rc = pass(bins_, false))) return rc;
+  if (!rescue_bins_.empty()) {
+    CollectArgs c{view_, d_queue_, queue_off, queue_tail};
+    if ((rc = check(launch_collect(c, n_regions_, stream_), "lost-pair collection"))) return rc;
+    planned_.kernel_launches++;
+  }
   if ((rc = pass(rescue_bins_, true))) return rc;
   return FGKL_OK;
 }
 
 int Engine::fetch(double* out, int64_t out_len, BatchStats* stats) {
   cudaSetDevice(device_);
+  const auto t_fetch = std::chrono::steady_clock::now();
   if (out_len != out_len_)
     return fail(FGKL_E_OUTPUT_LENGTH, "output has " + std::to_string(out_len) + " elements but reads x haplotypes is " +
                                           std::to_string(out_len_));
   int rc;
-  double* h_out = reinterpret_cast<double*>(h_stage_);
-  Counters* h_cnt = reinterpret_cast<Counters*>(h_stage_ + align_up(static_cast<size_t>(out_len_) * sizeof(double)));
+  double* h_out = reinterpret_cast<double*>(h_stage_ + out_stage_);
+  Counters* h_cnt = reinterpret_cast<Counters*>(h_stage_ + out_stage_ + align_up(static_cast<size_t>(out_len_) * sizeof(double)));
   if (out_len_ > 0 &&
       (rc = check(cudaMemcpyAsync(h_out, d_out_, static_cast<size_t>(out_len_) * sizeof(double), cudaMemcpyDeviceToHost, stream_),
                   "download results")))
@@ -471,7 +550,8 @@ int Engine::fetch(double* out, int64_t out_len, BatchStats* stats) {
   if ((rc = check(cudaMemcpyAsync(h_cnt, d_counters_, sizeof(Counters), cudaMemcpyDeviceToHost, stream_), "download counters")))
     return rc;
   if ((rc = check(cudaStreamSynchronize(stream_), "kernel execution"))) return rc;
-  if (out_len_ > 0) std::memcpy(out, h_out, static_cast<size_t>(out_len_) * sizeof(double));
+  if (out_len_ > 0) parallel_copy(reinterpret_cast<uint8_t*>(out), reinterpret_cast<const uint8_t*>(h_out), static_cast<size_t>(out_len_) * sizeof(double));
+  planned_.host_fetch_ms = ms_since(t_fetch);
   if (stats) {
     *stats = planned_;
     stats->fallback_pairs = h_cnt->lost_pairs;

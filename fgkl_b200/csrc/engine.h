@@ -40,6 +40,10 @@ struct BatchStats {
   uint64_t backward_cells = 0;
   uint64_t prefix_only_cells = 0;   // forward cells prefix sharing alone would compute
   uint64_t kernel_launches = 0;     // launches issued by the last run()
+  double host_plan_ms = 0;          // sorting, planning and program emission
+  double host_pack_ms = 0;          // concatenation into pinned staging
+  double host_upload_ms = 0;        // enqueueing the uploads
+  double host_fetch_ms = 0;         // waiting for the kernels and copying results out
 };
 
 class Engine {
@@ -117,11 +121,13 @@ class Engine {
   // Pinned host staging.
   uint8_t* h_stage_ = nullptr;
   size_t cap_stage_ = 0;
+  size_t out_stage_ = 0;  // results and counters come back here
 
   // Prepared batch.
   BatchView view_{};
   std::vector<Bin> bins_, rescue_bins_;
   int64_t out_len_ = 0;
+  int n_regions_ = 0;
   int n_small_ = 0;
 };
 

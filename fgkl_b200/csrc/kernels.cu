@@ -116,6 +116,7 @@ template <bool D>
 struct Consts;
 template <>
 struct Consts<false> {
+  static constexpr double kInitial = 0x1p120;
   static constexpr double kBackwardScale = 1329227995784915872903807060280344576.0;  // 2^120
   static constexpr double kLog10Initial = 120.0 * 0.301029995663981195213738894724493027;
   static constexpr double kMinAccepted = 1e-28;
@@ -123,6 +124,7 @@ struct Consts<false> {
 };
 template <>
 struct Consts<true> {
+  static constexpr double kInitial = 0x1p1020;
   static constexpr double kBackwardScale = 1.0;
   static constexpr double kLog10Initial = 1020.0 * 0.301029995663981195213738894724493027;
   static constexpr double kMinAccepted = 0.0;  // never lost
@@ -497,7 +499,7 @@ struct FwdState {
 template <class P, int R>
 __device__ __forceinline__ void forward_step(const LaunchArgs& a, const Program& prog, const ReadRef* rd, int lane,
                                              const FwdRows<P, R>& fr, const typename P::V& an, int pad_hi, Scratch<P, R>& sc,
-                                             FwdState<P, R>& st, uint32_t ev, typename P::V& uM, typename P::V& uX,
+                                             FwdState<P, R>& st, int synth_len, uint32_t ev, typename P::V& uM, typename P::V& uX,
                                              typename P::V& uY, typename P::V& dM, typename P::V& dX, typename P::V& dY) {
   using V = typename P::V;
   using S = typename P::S;
@@ -542,10 +544,12 @@ __device__ __forceinline__ void forward_step(const LaunchArgs& a, const Program&
     }
     if (ev & EV_BEGIN) {
       ++st.seg_i;
+      // A recomputation stream (FP64 only) has one unshared segment from the origin and no record.
+      const bool synth = synth_len > 0;
       const Segment* rec = a.v.segs + prog.seg_off + st.seg_i;
-      if (st.seg_i + 1 < prog.n_segs) prefetch_l1(rec + 1);
-      const int next_slot = rec->next_slot;
-      if (rec->staged) {
+      if (!synth && st.seg_i + 1 < prog.n_segs) prefetch_l1(rec + 1);
+      const int next_slot = synth ? -1 : rec->next_slot;
+      if (!synth && rec->staged) {
         __pipeline_wait_prior(0);
         const V* s = sc.staged(st.seg_i, lane);
 #pragma unroll
@@ -561,7 +565,8 @@ __device__ __forceinline__ void forward_step(const LaunchArgs& a, const Program&
       } else {
         // The origin: nothing but the row-0 constant, in the padding rows (and the row above the
         // lane when that is padding).
-        const S in_s = P::kDouble ? static_cast<S>(rec->init_d) : static_cast<S>(rec->init_f);
+        const S in_s = synth ? static_cast<S>(Consts<P::kDouble>::kInitial / synth_len)
+                             : (P::kDouble ? static_cast<S>(rec->init_d) : static_cast<S>(rec->init_f));
 #pragma unroll
         for (int r = 0; r < R; ++r) st.M[r] = st.X[r] = st.Y[r] = P::zero();
         dM = dX = dY = st.acc = P::zero();
@@ -602,9 +607,19 @@ __device__ __forceinline__ void forward_step(const LaunchArgs& a, const Program&
   st.acc = P::fma(st.X[R - 1], an, P::add(st.acc, st.M[R - 1]));
 }
 
+// Entry p of a recomputation stream: the haplotype's codes, BEGIN on the first column and END after
+// the last.
+__device__ __forceinline__ uint32_t synth_entry(const uint8_t* seq, int len, int p) {
+  if (p < 0 || p > len) return 0u;
+  uint32_t e = p < len ? __ldg(seq + p) : 0u;
+  if (p == 0) e |= EV_BEGIN;
+  if (p == len) e |= EV_END;
+  return e;
+}
+
 template <class P, int R>
 __device__ void forward_pass(const LaunchArgs& a, const Program& prog, const ReadRef* rd, const uint8_t* codes, int lane,
-                             Scratch<P, R>& sc) {
+                             Scratch<P, R>& sc, const uint8_t* synth_seq, int synth_len) {
   using V = typename P::V;
   using S = typename P::S;
   FwdRows<P, R> fr;
@@ -624,15 +639,24 @@ __device__ void forward_pass(const LaunchArgs& a, const Program& prog, const Rea
   st.acc = P::zero();
   st.seg_i = -1;
   V aM = P::zero(), aX = P::zero(), aY = P::zero(), bM = P::zero(), bX = P::zero(), bY = P::zero();
-  const int n = prog.fwd_len;
-  const uint32_t* stream = a.v.stream + prog.fwd_off - lane;
-  uint32_t n0 = __ldg(stream), n1 = __ldg(stream + 1);
-  for (int t = 0; t < n + 32; t += 2) {
-    const uint32_t e0 = n0, e1 = n1;
-    n0 = __ldg(stream + t + 2);
-    n1 = __ldg(stream + t + 3);
-    forward_step<P, R>(a, prog, rd, lane, fr, an, pad_hi, sc, st, e0, aM, aX, aY, bM, bX, bY);
-    forward_step<P, R>(a, prog, rd, lane, fr, an, pad_hi, sc, st, e1, bM, bX, bY, aM, aX, aY);
+  if (P::kDouble && synth_len > 0) {
+    const int n = synth_len;
+    for (int t = 0; t < n + 32; t += 2) {
+      const uint32_t e0 = synth_entry(synth_seq, n, t - lane), e1 = synth_entry(synth_seq, n, t + 1 - lane);
+      forward_step<P, R>(a, prog, rd, lane, fr, an, pad_hi, sc, st, synth_len, e0, aM, aX, aY, bM, bX, bY);
+      forward_step<P, R>(a, prog, rd, lane, fr, an, pad_hi, sc, st, synth_len, e1, bM, bX, bY, aM, aX, aY);
+    }
+  } else {
+    const int n = prog.fwd_len;
+    const uint32_t* stream = a.v.stream + prog.fwd_off - lane;
+    uint32_t n0 = __ldg(stream), n1 = __ldg(stream + 1);
+    for (int t = 0; t < n + 32; t += 2) {
+      const uint32_t e0 = n0, e1 = n1;
+      n0 = __ldg(stream + t + 2);
+      n1 = __ldg(stream + t + 3);
+      forward_step<P, R>(a, prog, rd, lane, fr, an, pad_hi, sc, st, 0, e0, aM, aX, aY, bM, bX, bY);
+      forward_step<P, R>(a, prog, rd, lane, fr, an, pad_hi, sc, st, 0, e1, bM, bX, bY, aM, aX, aY);
+    }
   }
   __pipeline_wait_prior(0);
 }
@@ -647,9 +671,10 @@ __device__ void finalize(const LaunchArgs& a, const Task& task, const Region& re
   using C = Consts<P::kDouble>;
   double* red = reinterpret_cast<double*>(sc.stage);  // [c][row q], the staging buffers are free now
   const int max_rows = 32 * R;
+  const int n_join_segs = (P::kDouble && task.hap >= 0) ? 0 : prog.n_segs;
   // Joins (fgkl kernel.rs:767-791): raw = acc + (Σ_rows F_M*B_M + F_Y*B_Y + init*s) / BACKWARD_SCALE,
   // with the row sum taken in an order fixed by the read row so it does not depend on R.
-  for (int seg = 0; seg < prog.n_segs; ++seg) {
+  for (int seg = 0; seg < n_join_segs; ++seg) {
     const int node = a.v.segs[prog.seg_off + seg].node;
     if (node < 0) continue;
     const typename P::V* f = sc.join(seg, lane);
@@ -689,10 +714,19 @@ __device__ void finalize(const LaunchArgs& a, const Task& task, const Region& re
     __syncwarp();
   }
   __syncwarp();
-  bool lost_any[P::NC];
+  if (P::kDouble && task.hap >= 0) {
+    // A recomputation task: its one segment's result goes to the haplotype and its duplicates.
+    const double raw = sc.seg_raw[0];
+    const bool lost = raw != raw;
+    const double result = lost ? __longlong_as_double(0x7ff8000000000000ll) : log10(raw) - C::kLog10Initial;
+    const int read_local = task.read[0] - region.read_off;
+    for (int k = lane; k < region.n_haps; k += 32) {
+      const HapInfo info = a.v.haps[region.hap_off + k];
+      if (info.src == task.hap) a.v.out[region.out_off + static_cast<int64_t>(read_local) * region.n_haps + info.order] = result;
+    }
+    return;
+  }
   unsigned long long lost_count = 0;
-#pragma unroll
-  for (int c = 0; c < P::NC; ++c) lost_any[c] = false;
   for (int k = lane; k < region.n_haps; k += 32) {
     const HapInfo info = a.v.haps[region.hap_off + k];
     const Segment* seg = a.v.segs + prog.seg_off + info.seg;
@@ -710,32 +744,11 @@ __device__ void finalize(const LaunchArgs& a, const Task& task, const Region& re
       if (!P::kDouble) lost |= isinf(raw);
       const double result = lost ? __longlong_as_double(0x7ff8000000000000ll) : log10(raw) - C::kLog10Initial;
       const int read_local = task.read[c] - region.read_off;
-      double* dst = a.v.out + region.out_off + static_cast<int64_t>(read_local) * region.n_haps + info.order;
-      if (a.rescue) {
-        if (isnan(*dst) && !lost) *dst = result;
-      } else {
-        *dst = result;
-        if (lost) {
-          lost_any[c] = true;
-          ++lost_count;
-        }
-      }
+      a.v.out[region.out_off + static_cast<int64_t>(read_local) * region.n_haps + info.order] = result;
+      lost_count += lost;
     }
   }
-  if (a.rescue) return;
   if (lost_count) atomicAdd(&a.v.counters->lost_pairs, lost_count);
-#pragma unroll
-  for (int c = 0; c < P::NC; ++c) {
-    const bool any = __any_sync(kFull, lost_any[c]);
-    if (any && lane == 0 && a.queue != nullptr) {
-      // Queue the read for double-precision recomputation in the bin of its own rows-per-lane.
-      int rows = (rd[c].len + 30) / 31;
-      if (rows > 8) rows = (rows + 1) & ~1;
-      const int slot = atomicAdd(a.queue_tail + rows, 1);
-      a.queue[a.queue_off[rows] + slot] = Task{task.region, {task.read[c], -1}, rows};
-      atomicAdd(&a.v.counters->rescue_reads, 1ull);
-    }
-  }
 }
 
 template <class P, int R>
@@ -746,7 +759,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, (MinBlocks<P, R>::value))
   const int warp_in_block = threadIdx.x >> 5;
   const int warp = blockIdx.x * kWarpsPerBlock + warp_in_block;
   V* smem = reinterpret_cast<V*>(smem_raw + warp_in_block * Layout<P, R>::kSmemPerWarp);
-  const int count = a.count ? *a.count : a.n_tasks;
+  const int count = a.count ? min(*a.count, a.n_tasks) : a.n_tasks;
   for (;;) {
     int t = 0;
     if (lane == 0) t = atomicAdd(a.task_counter, 1);
@@ -754,7 +767,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, (MinBlocks<P, R>::value))
     if (t >= count) break;
     const Task task = a.tasks[t];
     const Region region = a.v.regions[task.region];
-    const Program prog = a.use_prefix ? region.prefix : region.shared;
+    const Program prog = region.prog;
     ReadRef rd[P::NC];
 #pragma unroll
     for (int c = 0; c < P::NC; ++c) {
@@ -769,15 +782,45 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, (MinBlocks<P, R>::value))
       rd[c].pad = 32 * R - rd[c].len;
     }
     const uint8_t* codes = a.v.code_of_byte + region.code_off;
-    const int n_slots = region.shared.n_slots > region.prefix.n_slots ? region.shared.n_slots : region.prefix.n_slots;
-    Scratch<P, R> sc(a.scratch + static_cast<size_t>(warp) * a.scratch_stride, smem, n_slots, region.shared.n_nodes,
-                     region.shared.n_segs);
-    if (prog.bwd_len > 0) backward_pass<P, R>(a, prog, rd, codes, lane, sc);
+    char* scratch = a.scratch + static_cast<size_t>(warp) * a.scratch_stride;
+    if (P::kDouble && task.hap >= 0) {
+      const HapInfo info = a.v.haps[region.hap_off + task.hap];
+      Scratch<P, R> sc(scratch, smem, 0, 0, 1);
+      forward_pass<P, R>(a, prog, rd, codes, lane, sc, a.v.hap_codes + region.seq_off + info.seq, info.len);
+      __syncwarp();
+      finalize<P, R>(a, task, region, prog, rd, lane, sc);
+    } else {
+      Scratch<P, R> sc(scratch, smem, prog.n_slots, prog.n_nodes, prog.n_segs);
+      if (prog.bwd_len > 0) backward_pass<P, R>(a, prog, rd, codes, lane, sc);
+      __syncwarp();
+      forward_pass<P, R>(a, prog, rd, codes, lane, sc, nullptr, 0);
+      __syncwarp();
+      finalize<P, R>(a, task, region, prog, rd, lane, sc);
+    }
     __syncwarp();
-    forward_pass<P, R>(a, prog, rd, codes, lane, sc);
-    __syncwarp();
-    finalize<P, R>(a, task, region, prog, rd, lane, sc);
-    __syncwarp();
+  }
+}
+
+// Queues every pair the first pass lost -- its output is NaN -- as an FP64 recomputation task, one
+// per (read, distinct sorted haplotype), in the bin of the read's rows-per-lane. One block per
+// region; nothing to do (one load per block) when no pair was lost.
+__global__ void __launch_bounds__(256) collect_kernel(CollectArgs a) {
+  if (a.v.counters->lost_pairs == 0) return;
+  const Region region = a.v.regions[blockIdx.x];
+  const int64_t pairs = static_cast<int64_t>(region.n_reads) * region.n_haps;
+  for (int64_t e = threadIdx.x; e < pairs; e += blockDim.x) {
+    const int r = static_cast<int>(e / region.n_haps), k = static_cast<int>(e % region.n_haps);
+    const HapInfo info = a.v.haps[region.hap_off + k];
+    if (info.src != k) continue;
+    if (!isnan(a.v.out[region.out_off + static_cast<int64_t>(r) * region.n_haps + info.order])) continue;
+    const int read = region.read_off + r;
+    int rows = static_cast<int>((a.v.read_off[read + 1] - a.v.read_off[read] + 30) / 31);
+    if (rows > 8) rows = (rows + 1) & ~1;
+    const int slot = atomicAdd(a.queue_tail + rows, 1);
+    if (slot < a.queue_off[rows + 1] - a.queue_off[rows]) {
+      a.queue[a.queue_off[rows] + slot] = Task{static_cast<int32_t>(blockIdx.x), {read, -1}, rows, k};
+      atomicAdd(&a.v.counters->rescue_reads, 1ull);
+    }
   }
 }
 
@@ -898,6 +941,12 @@ void occupancy(Kind k, int rows, int* blocks, int* threads) {
   *threads = kWarpsPerBlock * 32;
   if (!valid_rows(k, rows)) return;
   dispatch<OccF>(k, rows, blocks, threads);
+}
+
+cudaError_t launch_collect(const CollectArgs& args, int n_regions, cudaStream_t stream) {
+  if (n_regions <= 0) return cudaSuccess;
+  collect_kernel<<<n_regions, 256, 0, stream>>>(args);
+  return cudaGetLastError();
 }
 
 cudaError_t launch(Kind k, int rows, int blocks, const LaunchArgs& args, cudaStream_t stream) {

@@ -21,12 +21,15 @@ struct LaunchArgs {
   int* task_counter;     // zeroed before the launch
   char* scratch;
   size_t scratch_stride; // bytes per warp
-  int use_prefix;        // 1: run the prefix-only program
-  int rescue;            // 1: write only pairs whose output is NaN
-  Task* queue;           // recomputation queue (single-read double-precision tasks), or nullptr
-  const int* queue_off;  // per rows-per-lane bin: first queue index
-  int* queue_tail;       // per bin: tasks queued
   int min_accept_plain;  // 1: results below the single-precision threshold are lost
+};
+
+// The pass between the first pass and the recomputation: queues lost pairs.
+struct CollectArgs {
+  BatchView v;
+  Task* queue;           // recomputation queue: (read, distinct haplotype) FP64 tasks
+  const int* queue_off;  // per rows-per-lane bin: first queue index (one past the last bin at the end)
+  int* queue_tail;       // per bin: tasks queued
 };
 
 // Rows per lane the instantiations cover.
@@ -37,5 +40,7 @@ size_t scratch_bytes(Kind k, int rows, int max_slots, int max_nodes, int max_seg
 void occupancy(Kind k, int rows, int* blocks_per_sm, int* threads_per_block);
 // Launches one persistent grid of `blocks` blocks.
 cudaError_t launch(Kind k, int rows, int blocks, const LaunchArgs& args, cudaStream_t stream);
+// Launches the lost-pair collection over `n_regions` regions.
+cudaError_t launch_collect(const CollectArgs& args, int n_regions, cudaStream_t stream);
 
 }  // namespace fgkl

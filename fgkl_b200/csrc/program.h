@@ -73,15 +73,14 @@ struct Program {
 };
 
 struct Region {
-  Program shared;   // prefix + suffix sharing (first pass)
-  Program prefix;   // prefix sharing only (double-precision recomputation)
+  Program prog;     // the first pass: prefix (and, when enabled, suffix) sharing
   int32_t hap_off;  // into the HapInfo array
   int32_t n_haps;
   int32_t read_off; // first global read index
   int32_t n_reads;
   int64_t out_off;  // first output element (row-major n_reads x n_haps, caller order)
   int32_t code_off; // 256-entry byte -> prior code table
-  int32_t pad_;
+  int32_t seq_off;  // sorted haplotypes' prior codes, concatenated (recomputation streams)
 };
 
 // Per sorted haplotype: where its result goes and where it comes from.
@@ -89,20 +88,25 @@ struct HapInfo {
   int32_t order;  // caller's index of the sorted haplotype
   int32_t seg;    // segment of the first copy (duplicates share it)
   int32_t src;    // sorted index of the first copy
-  int32_t pad_;
+  int32_t len;    // bases; its codes start at region.seq_off + seq
+  int32_t seq;
+  int32_t pad_[3];
 };
 
 // One warp's unit of work: one or two reads of a region, with R rows per lane (31 * R >= length).
+// A recomputation task (hap >= 0) runs one read against one distinct haplotype from the origin,
+// without sharing, from a stream synthesised from the haplotype's codes.
 struct Task {
   int32_t region;
   int32_t read[2];  // global read indices; read[1] = -1 when the task holds one read
   int32_t rows;     // R
+  int32_t hap;      // sorted haplotype of a recomputation task, else -1
 };
 
 // Per-pass counters written by the kernels.
 struct Counters {
   unsigned long long lost_pairs;   // pairs handed to the double-precision recomputation
-  unsigned long long rescue_reads; // reads queued for recomputation
+  unsigned long long rescue_reads; // (read, distinct haplotype) pairs queued for recomputation
   unsigned long long pad_[2];
 };
 
@@ -120,6 +124,7 @@ struct BatchView {
   const Segment* segs;
   const Sweep* sweeps;
   const uint8_t* code_of_byte;
+  const uint8_t* hap_codes;  // sorted haplotypes' codes per region
   const double* err_prob;     // 255 entries
   const double* m2m;          // triangular table, 32640 entries
   double* out;

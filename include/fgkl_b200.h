@@ -52,6 +52,10 @@ typedef struct fgkl_stats {
   uint64_t backward_cells;
   uint64_t prefix_only_cells; /* forward cells with prefix sharing alone */
   uint64_t kernel_launches;   /* kernels launched by the call's run phase */
+  double host_plan_ms;        /* host time: sorting, planning, program emission */
+  double host_pack_ms;        /* host time: packing the batch into pinned staging */
+  double host_upload_ms;      /* host time: enqueueing the uploads */
+  double host_fetch_ms;       /* host time: waiting for the kernels and copying results out */
 } fgkl_stats;
 
 /* The five read arrays of one call, concatenated, delimited by `offsets` (num_reads + 1 entries,
