@@ -87,6 +87,27 @@ class Batch(C.Structure):
     ]
 
 
+class DeviceRegion(C.Structure):
+    """``fgkl_device_region``: caller-owned device arrays of one region (allocation-free entry)."""
+    _fields_ = [
+        ("num_reads", C.c_int32),
+        ("num_haplotypes", C.c_int32),
+        ("bases", C.c_void_p),
+        ("quals", C.c_void_p),
+        ("ins_quals", C.c_void_p),
+        ("del_quals", C.c_void_p),
+        ("gcp", C.c_void_p),
+        ("read_offsets", C.c_void_p),
+        ("hap_bases", C.c_void_p),
+        ("hap_offsets", C.c_void_p),
+        ("max_read_len", C.c_int32),
+    ]
+
+
+NOALLOC_SCRATCH_BYTES = 2 * 1024 * 1024
+NOALLOC_MAX_READ_LEN = 620
+
+
 _lib: C.CDLL | None = None
 
 
@@ -127,6 +148,8 @@ def lib() -> C.CDLL:
                                      C.POINTER(C.c_uint64)]
     L.fgkl_plan_sweeps.argtypes = [u8p, i32p, C.c_int32, i32p, C.c_int32, i32p, C.c_int32]
     L.fgkl_probe_fp32_tflops.argtypes = [C.c_int32, f64p, f64p, f64p]
+    L.fgkl_pairhmm_compute_device_noalloc.argtypes = [C.POINTER(DeviceRegion), C.c_void_p, C.c_void_p]
+    L.fgkl_pairhmm_compute_device_noalloc.restype = C.c_int
     _lib = L
     return L
 
@@ -141,4 +164,5 @@ EXPORTED = [
     "fgkl_backend", "fgkl_last_error", "fgkl_context_create", "fgkl_context_destroy", "fgkl_batch_prepare",
     "fgkl_batch_run", "fgkl_batch_fetch", "fgkl_batch_compute", "fgkl_batch_output_len", "fgkl_synth_config",
     "fgkl_synth_reference_region", "fgkl_synth_view", "fgkl_synth_free", "fgkl_plan_describe", "fgkl_plan_sweeps", "fgkl_probe_fp32_tflops",
+    "fgkl_pairhmm_compute_device_noalloc",
 ]

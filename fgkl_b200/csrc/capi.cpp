@@ -1,8 +1,10 @@
 // The extern "C" boundary (include/fgkl_b200.h).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -10,6 +12,7 @@
 #include "engine.h"
 #include "planner.h"
 #include "synthetic.h"
+#include "tables.h"
 
 namespace {
 
@@ -139,6 +142,37 @@ void to_stats(const fgkl::BatchStats& bs, fgkl_stats* s) {
   s->host_pack_ms = bs.host_pack_ms;
   s->host_upload_ms = bs.host_upload_ms;
   s->host_fetch_ms = bs.host_fetch_ms;
+}
+
+
+// Allocation-free entry: per-device state, set up by the first call on each device.
+constexpr int kNoAllocMaxDevices = 64;
+fgkl::NoAllocDevice g_noalloc[kNoAllocMaxDevices];
+std::mutex g_noalloc_mutex;
+
+int noalloc_device(fgkl::NoAllocDevice** out) {
+  int d = -1;
+  if (cudaGetDevice(&d) != cudaSuccess || d < 0) return set_error(FGKL_E_NO_DEVICE, "no current CUDA device");
+  if (d >= kNoAllocMaxDevices) return set_error(FGKL_E_NO_DEVICE, "device ordinal beyond the 64 the entry tracks");
+  fgkl::NoAllocDevice& dev = g_noalloc[d];
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!dev.ready) {
+    int major = 0, minor = 0, sms = 0;
+    if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, d) != cudaSuccess ||
+        cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, d) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d) != cudaSuccess)
+      return set_error(FGKL_E_NO_DEVICE, "cannot query the current CUDA device");
+    if (major != 10 || minor != 0) return set_error(FGKL_E_NO_DEVICE, "the kernels are built for sm_100a");
+    uint8_t codes[256];
+    for (int b = 0; b < 256; ++b) codes[b] = static_cast<uint8_t>(b == 'N' ? fgkl::kCodeN : (b == fgkl::kCodeN ? 'N' : b));
+    const fgkl::Tables& t = fgkl::tables();
+    const cudaError_t e = fgkl::noalloc_setup(&dev, t.error_prob.data(), t.error_prob.size(), t.m2m.data(), t.m2m.size(), codes);
+    if (e != cudaSuccess) return set_error(FGKL_E_CUDA, std::string("allocation-free setup: ") + cudaGetErrorString(e));
+    dev.sms = sms;
+    dev.ready = true;
+  }
+  *out = &dev;
+  return FGKL_OK;
 }
 
 }  // namespace
@@ -384,6 +418,37 @@ int fgkl_plan_sweeps(const uint8_t* hap_bases, const int32_t* hap_offsets, int32
   } catch (const std::exception& e) {
     return set_error(FGKL_E_INVALID_ARGUMENT, e.what());
   }
+}
+
+int fgkl_pairhmm_compute_device_noalloc(const fgkl_device_region* region, double* out, void* stream) {
+  t_error.clear();
+  if (!region) return set_error(FGKL_E_INVALID_ARGUMENT, "null region");
+  const int64_t n_reads = region->num_reads, n_haps = region->num_haplotypes;
+  if (n_reads < 0 || n_haps < 0) return set_error(FGKL_E_INVALID_ARGUMENT, "negative read or haplotype count");
+  const int64_t pairs = n_reads * n_haps;
+  if (pairs > FGKL_NOALLOC_MAX_PAIRS)
+    return set_error(FGKL_E_INVALID_ARGUMENT, "the allocation-free entry takes at most 2^31 - 1 pairs per call; split the region");
+  if (region->max_read_len < 1 || region->max_read_len > FGKL_NOALLOC_MAX_READ_LEN)
+    return set_error(FGKL_E_UNSUPPORTED, "max_read_len must lie in 1..620 for the allocation-free entry");
+  if (pairs == 0) return FGKL_OK;
+  if (!out || !region->bases || !region->quals || !region->ins_quals || !region->del_quals || !region->gcp ||
+      !region->read_offsets || !region->hap_bases || !region->hap_offsets)
+    return set_error(FGKL_E_INVALID_ARGUMENT, "null device array");
+  fgkl::NoAllocDevice* dev = nullptr;
+  int rc;
+  if ((rc = noalloc_device(&dev)) != FGKL_OK) return rc;
+  const int rows = fgkl::noalloc_rows(region->max_read_len);
+  // A persistent grid: the device's resident blocks, or fewer when the pairs do not fill it, and
+  // never more warps than the file-scope scratch holds.
+  const int64_t warps_fit = static_cast<int64_t>((dev->scratch_bytes - dev->header_bytes) / dev->per_warp_bytes);
+  int64_t blocks = static_cast<int64_t>(dev->blocks_per_sm[rows]) * dev->sms;
+  blocks = std::min<int64_t>(blocks, (pairs + 3) / 4);
+  blocks = std::min<int64_t>(blocks, warps_fit / 4);
+  fgkl::NoAllocCall c{region->bases, region->quals, region->ins_quals, region->del_quals, region->gcp, region->read_offsets,
+                      region->hap_bases, region->hap_offsets, static_cast<int>(n_reads), static_cast<int>(n_haps), out};
+  const cudaError_t e = fgkl::noalloc_launch(*dev, c, rows, static_cast<int>(blocks), static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return set_error(FGKL_E_CUDA, std::string("allocation-free launch: ") + cudaGetErrorString(e));
+  return FGKL_OK;
 }
 
 }  // extern "C"

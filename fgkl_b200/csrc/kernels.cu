@@ -32,6 +32,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <type_traits>
 
 #include "kernels.cuh"
 
@@ -952,6 +953,190 @@ cudaError_t launch_collect(const CollectArgs& args, int n_regions, cudaStream_t 
 cudaError_t launch(Kind k, int rows, int blocks, const LaunchArgs& args, cudaStream_t stream) {
   if (!valid_rows(k, rows)) return cudaErrorInvalidValue;
   return dispatch<GoF>(k, rows, blocks, args, stream);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Allocation-free entry: one region's (read, haplotype) pairs from caller-owned device arrays, each
+// pair computed by one warp in FP64 without sharing (the recomputation form of the kernel above),
+// with the per-warp scratch -- the segment result the last lane hands to lane 0 -- in a file-scope
+// device array instead of an allocated buffer.
+// ---------------------------------------------------------------------------------------------
+
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = size_t{2} << 20;  // 2 MiB (FGKL_NOALLOC_SCRATCH_BYTES): header + 8191 warps
+constexpr size_t kNoAllocHeader = 256;                    // the pair counter (must be 0 at launch)
+constexpr size_t kNoAllocPerWarp = 256;                   // one warp's segment result, 256-aligned
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+static __device__ double g_noalloc_err[kMaxQualTable];
+static __device__ double g_noalloc_m2m[kM2MTable];
+static __device__ uint8_t g_noalloc_codes[256];
+
+struct NoAllocArgs {
+  BatchView v;  // read arrays and offsets, tables, read byte -> code table
+  const uint8_t* hap_bases;
+  const int64_t* hap_off;
+  int n_reads, n_haps;
+  int* counter;   // pairs claimed so far
+  char* scratch;  // kNoAllocPerWarp bytes per warp
+  double* out;    // n_reads x n_haps, row-major
+};
+
+// Prior code of a haplotype byte: the byte itself, with 'N' and byte kCodeN swapped so that N is
+// code kCodeN (matches every read base) and the mapping stays one-to-one. The read table holds the
+// same permutation, so a read base matches exactly the haplotype bytes equal to it.
+__device__ __forceinline__ uint32_t byte_code(uint32_t b) { return b == 'N' ? kCodeN : (b == kCodeN ? 'N' : b); }
+
+__device__ __forceinline__ uint32_t byte_entry(const uint8_t* hap, int len, int p) {
+  if (p < 0 || p > len) return 0u;
+  uint32_t e = p < len ? byte_code(__ldg(hap + p)) : 0u;
+  if (p == 0) e |= EV_BEGIN;
+  if (p == len) e |= EV_END;
+  return e;
+}
+
+template <int R>
+__device__ void forward_unshared(const LaunchArgs& a, const ReadRef* rd, int lane, Scratch<OneF64, R>& sc, const uint8_t* hap,
+                                 int n) {
+  using P = OneF64;
+  using V = typename P::V;
+  FwdRows<P, R> fr;
+  fr.load(a.v, rd, lane, a.v.code_of_byte, sc.priors);
+  const V an = 1.0;  // the plain recurrence: the result is the sum of the last row's M and X
+  const int pad_hi = rd[0].pad;
+  FwdState<P, R> st;
+#pragma unroll
+  for (int r = 0; r < R; ++r) st.M[r] = st.X[r] = st.Y[r] = 0.0;
+  st.acc = 0.0;
+  st.seg_i = -1;
+  const Program prog{};  // unused: the stream is synthesised from the haplotype bytes
+  V aM = 0.0, aX = 0.0, aY = 0.0, bM = 0.0, bX = 0.0, bY = 0.0;
+  for (int t = 0; t < n + 32; t += 2) {
+    const uint32_t e0 = byte_entry(hap, n, t - lane), e1 = byte_entry(hap, n, t + 1 - lane);
+    forward_step<P, R>(a, prog, rd, lane, fr, an, pad_hi, sc, st, n, e0, aM, aX, aY, bM, bX, bY);
+    forward_step<P, R>(a, prog, rd, lane, fr, an, pad_hi, sc, st, n, e1, bM, bX, bY, aM, aX, aY);
+  }
+}
+
+template <int R>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, 1) noalloc_kernel(NoAllocArgs na) {
+  using P = OneF64;
+  extern __shared__ __align__(16) unsigned char smem_raw[];  // none requested: nothing is staged
+  const int lane = threadIdx.x & 31;
+  const int warp = blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+  LaunchArgs a{};
+  a.v = na.v;
+  const int pairs = na.n_reads * na.n_haps;
+  for (;;) {
+    int t = 0;
+    if (lane == 0) t = atomicAdd(na.counter, 1);
+    t = __shfl_sync(kFull, t, 0);
+    if (t >= pairs) break;
+    const int r = t / na.n_haps, h = t % na.n_haps;
+    ReadRef rd[1];
+    rd[0].off = na.v.read_off[r];
+    const int64_t read_len = na.v.read_off[r + 1] - rd[0].off;
+    const int64_t hap_lo = na.hap_off[h], hap_len = na.hap_off[h + 1] - hap_lo;
+    if (read_len <= 0 || read_len > 31 * R || hap_len <= 0 || hap_len > (int64_t{1} << 30)) {
+      // Lengths the call's bounds exclude: the pair has no result.
+      if (lane == 0) na.out[t] = __longlong_as_double(0x7ff8000000000000ll);
+      continue;
+    }
+    rd[0].len = static_cast<int>(read_len);
+    rd[0].pad = 32 * R - rd[0].len;
+    Scratch<P, R> sc(na.scratch + static_cast<size_t>(warp) * kNoAllocPerWarp, reinterpret_cast<double*>(smem_raw), 0, 0, 0);
+    forward_unshared<R>(a, rd, lane, sc, na.hap_bases + hap_lo, static_cast<int>(hap_len));
+    __syncwarp();
+    if (lane == 0) na.out[t] = log10(sc.seg_raw[0]) - Consts<true>::kLog10Initial;
+    __syncwarp();
+  }
+}
+
+template <int R>
+cudaError_t noalloc_go(int blocks, const NoAllocArgs& na, cudaStream_t s) {
+  noalloc_kernel<R><<<blocks, kWarpsPerBlock * 32, 0, s>>>(na);
+  return cudaGetLastError();
+}
+
+template <int R>
+int noalloc_occupancy() {
+  int b = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, noalloc_kernel<R>, kWarpsPerBlock * 32, 0) != cudaSuccess) return 0;
+  return b;
+}
+
+template <class F>
+auto noalloc_dispatch(int rows, F&& f) {
+  switch (rows) {
+    case 1: return f(std::integral_constant<int, 1>{});
+    case 2: return f(std::integral_constant<int, 2>{});
+    case 3: return f(std::integral_constant<int, 3>{});
+    case 4: return f(std::integral_constant<int, 4>{});
+    case 5: return f(std::integral_constant<int, 5>{});
+    case 6: return f(std::integral_constant<int, 6>{});
+    case 7: return f(std::integral_constant<int, 7>{});
+    case 8: return f(std::integral_constant<int, 8>{});
+    case 10: return f(std::integral_constant<int, 10>{});
+    case 12: return f(std::integral_constant<int, 12>{});
+    case 14: return f(std::integral_constant<int, 14>{});
+    case 16: return f(std::integral_constant<int, 16>{});
+    case 18: return f(std::integral_constant<int, 18>{});
+    default: return f(std::integral_constant<int, 20>{});
+  }
+}
+
+}  // namespace
+
+int noalloc_rows(int max_read_len) {
+  int rows = (max_read_len + 30) / 31;
+  if (rows > 8) rows = (rows + 1) & ~1;
+  return rows;
+}
+
+cudaError_t noalloc_setup(NoAllocDevice* d, const double* err, size_t n_err, const double* m2m, size_t n_m2m,
+                          const uint8_t codes[256]) {
+  cudaError_t e;
+  if (n_err != kMaxQualTable || n_m2m != kM2MTable) return cudaErrorInvalidValue;
+  if ((e = cudaGetSymbolAddress(reinterpret_cast<void**>(&d->scratch), g_noalloc_scratch)) != cudaSuccess) return e;
+  if ((e = cudaGetSymbolAddress(reinterpret_cast<void**>(&d->err), g_noalloc_err)) != cudaSuccess) return e;
+  if ((e = cudaGetSymbolAddress(reinterpret_cast<void**>(&d->m2m), g_noalloc_m2m)) != cudaSuccess) return e;
+  if ((e = cudaGetSymbolAddress(reinterpret_cast<void**>(&d->codes), g_noalloc_codes)) != cudaSuccess) return e;
+  if ((e = cudaMemcpyToSymbol(g_noalloc_err, err, n_err * sizeof(double))) != cudaSuccess) return e;
+  if ((e = cudaMemcpyToSymbol(g_noalloc_m2m, m2m, n_m2m * sizeof(double))) != cudaSuccess) return e;
+  if ((e = cudaMemcpyToSymbol(g_noalloc_codes, codes, 256)) != cudaSuccess) return e;
+  for (int rows = 1; rows <= 20; ++rows) {
+    if (rows > 8 && rows % 2) continue;
+    d->blocks_per_sm[rows] = noalloc_dispatch(rows, [](auto r) { return noalloc_occupancy<decltype(r)::value>(); });
+    if (d->blocks_per_sm[rows] <= 0) return cudaErrorInvalidDeviceFunction;
+  }
+  d->scratch_bytes = kNoAllocScratchBytes;
+  d->header_bytes = kNoAllocHeader;
+  d->per_warp_bytes = kNoAllocPerWarp;
+  return cudaSuccess;
+}
+
+cudaError_t noalloc_launch(const NoAllocDevice& d, const NoAllocCall& c, int rows, int blocks, cudaStream_t stream) {
+  NoAllocArgs na{};
+  na.v.bases = c.bases;
+  na.v.quals = c.quals;
+  na.v.ins = c.ins;
+  na.v.del = c.del;
+  na.v.gcp = c.gcp;
+  na.v.read_off = c.read_off;
+  na.v.code_of_byte = d.codes;
+  na.v.err_prob = d.err;
+  na.v.m2m = d.m2m;
+  na.hap_bases = c.hap_bases;
+  na.hap_off = c.hap_off;
+  na.n_reads = c.n_reads;
+  na.n_haps = c.n_haps;
+  na.counter = reinterpret_cast<int*>(d.scratch);
+  na.scratch = d.scratch + d.header_bytes;
+  na.out = c.out;
+  cudaError_t e = cudaMemsetAsync(d.scratch, 0, sizeof(int), stream);  // the pair counter starts at zero
+  if (e != cudaSuccess) return e;
+  return noalloc_dispatch(rows, [&](auto r) { return noalloc_go<decltype(r)::value>(blocks, na, stream); });
 }
 
 }  // namespace fgkl

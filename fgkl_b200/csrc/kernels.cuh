@@ -43,4 +43,38 @@ cudaError_t launch(Kind k, int rows, int blocks, const LaunchArgs& args, cudaStr
 // Launches the lost-pair collection over `n_regions` regions.
 cudaError_t launch_collect(const CollectArgs& args, int n_regions, cudaStream_t stream);
 
+// ---- allocation-free entry (file-scope device scratch; see capi.cpp) ----
+constexpr size_t kMaxQualTable = 255;  // error-probability entries
+constexpr size_t kM2MTable = 32640;    // match-to-match entries
+
+// Per-device state of the allocation-free entry, filled once by noalloc_setup.
+struct NoAllocDevice {
+  bool ready = false;
+  char* scratch = nullptr;  // the file-scope scratch array: header (pair counter), then per-warp slots
+  double* err = nullptr;
+  double* m2m = nullptr;
+  uint8_t* codes = nullptr;
+  size_t scratch_bytes = 0, header_bytes = 0, per_warp_bytes = 0;
+  int blocks_per_sm[21] = {};
+  int sms = 0;
+};
+
+// One call's caller-owned device arrays.
+struct NoAllocCall {
+  const uint8_t *bases, *quals, *ins, *del, *gcp;
+  const int64_t* read_off;
+  const uint8_t* hap_bases;
+  const int64_t* hap_off;
+  int n_reads, n_haps;
+  double* out;
+};
+
+// Rows per lane for reads of at most `max_read_len` bases.
+int noalloc_rows(int max_read_len);
+// Resolves the file-scope arrays of the current device and uploads the tables (synchronous).
+cudaError_t noalloc_setup(NoAllocDevice* d, const double* err, size_t n_err, const double* m2m, size_t n_m2m,
+                          const uint8_t codes[256]);
+// Zeroes the pair counter and launches `blocks` blocks on `stream`; allocates nothing.
+cudaError_t noalloc_launch(const NoAllocDevice& d, const NoAllocCall& c, int rows, int blocks, cudaStream_t stream);
+
 }  // namespace fgkl

@@ -144,6 +144,56 @@ int fgkl_batch_compute(fgkl_context* ctx, const fgkl_batch* batch, const fgkl_co
 /* Number of likelihoods the prepared batch produces. */
 int64_t fgkl_batch_output_len(const fgkl_context* ctx);
 
+/* ---- allocation-free form (no counterpart in the reference) ----
+ *
+ * The reference has no such entry: its kernels take host slices and allocate per-thread
+ * workspaces. This one is for callers that must not allocate device memory per call: code whose
+ * device memory is held by a pool allocator that has already reserved the free memory (a further
+ * cudaMalloc fails or fragments it), and latency-bound serving loops that cannot take the
+ * device-wide synchronisation cudaFree implies while other streams run.
+ *
+ * One region's likelihoods, every pair computed in FP64 without haplotype sharing (the value
+ * Precision::Double gives, to rounding), from caller-owned arrays in the CURRENT device's memory,
+ * enqueued on `stream` (a cudaStream_t, NULL = the legacy default stream) without waiting.
+ * out[r * num_haplotypes + h] receives read r against haplotype h (device memory, not aliasing the
+ * inputs).
+ *
+ * It allocates nothing: no cudaMalloc, cudaFree, pinned or library allocation. Its scratch is a
+ * file-scope device array of FGKL_NOALLOC_SCRATCH_BYTES (2 MiB): a 256-byte header holding the
+ * pair counter, which must start at zero and which each call zeroes with cudaMemsetAsync on
+ * `stream` before its launch, then 256 bytes per resident warp (the grid is sized so they fit).
+ * The first call on each device does the setup -- resolves the array's address with
+ * cudaGetSymbolAddress and uploads the probability tables with synchronous copies -- so make it
+ * before any stream capture.
+ *
+ * Calls share the one scratch array per device: two calls whose kernels overlap (different
+ * streams, or threads, without ordering between them) race on it and give wrong results. Order
+ * them on one stream or with events.
+ *
+ * Limits: max_read_len (the caller's bound on every read length) in 1..620, else
+ * FGKL_E_UNSUPPORTED; num_reads x num_haplotypes at most FGKL_NOALLOC_MAX_PAIRS, else
+ * FGKL_E_INVALID_ARGUMENT. The arrays are not read on the host, so a read longer than
+ * max_read_len, or an empty read or haplotype, yields NaN for its pairs instead of an error. */
+#define FGKL_NOALLOC_SCRATCH_BYTES (2 * 1024 * 1024)
+#define FGKL_NOALLOC_MAX_READ_LEN 620
+#define FGKL_NOALLOC_MAX_PAIRS 2147483647LL
+
+typedef struct fgkl_device_region {
+  int32_t num_reads;
+  int32_t num_haplotypes;
+  const uint8_t* bases;        /* device; reads concatenated */
+  const uint8_t* quals;        /* device; same length */
+  const uint8_t* ins_quals;    /* device; same length */
+  const uint8_t* del_quals;    /* device; same length */
+  const uint8_t* gcp;          /* device; same length */
+  const int64_t* read_offsets; /* device; num_reads + 1 byte offsets */
+  const uint8_t* hap_bases;    /* device; haplotypes concatenated */
+  const int64_t* hap_offsets;  /* device; num_haplotypes + 1 byte offsets */
+  int32_t max_read_len;        /* host-known bound on every read's length */
+} fgkl_device_region;
+
+int fgkl_pairhmm_compute_device_noalloc(const fgkl_device_region* region, double* out, void* stream);
+
 /* ---- measurement support ---- */
 
 /* Measured FP32 FMA throughput of `device` (TFLOP/s) with scalar FFMA and packed FP32x2 FFMA chains:
