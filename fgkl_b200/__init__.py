@@ -6,5 +6,6 @@ is its host-side mirror of fgkl's Rust API (``crates/pairhmm/src/lib.rs``, ``pd.
 from .pairhmm import (  # noqa: F401
     ALT_A, ALT_C, ALT_G, ALT_T, DEL_END, DEL_START, SNP, BatchContext, Config, DeviceError, EmptyHaplotype, EmptyRead,
     MismatchedHaplotypeArrays, MismatchedReadArrays, OutputLength, PairHmm, PairHmmError, PdHaplotype, PdPairHmm, Plan,
-    Precision, Read, SharedColumns, plan, shared_columns,
+    Precision, Read, SharedColumns, plan, shared_columns, NORMAL, INSIDE_DEL, AFTER_DEL, PdPlan, pd_plan, pd_row_states,
+    pd_match_accepts,
 )

@@ -148,6 +148,9 @@ def lib() -> C.CDLL:
                                      C.POINTER(C.c_uint64)]
     L.fgkl_plan_sweeps.argtypes = [u8p, i32p, C.c_int32, i32p, C.c_int32, i32p, C.c_int32]
     L.fgkl_probe_fp32_tflops.argtypes = [C.c_int32, f64p, f64p, f64p]
+    L.fgkl_pd_row_states.argtypes = [u8p, C.c_int32, C.c_int32, u8p]
+    L.fgkl_pd_plan_describe.argtypes = [u8p, u8p, i32p, C.c_int32, i32p, i32p, u8p, u8p, i32p]
+    L.fgkl_pd_match_accepts.argtypes = [C.c_uint8, C.c_uint8, C.c_uint8]
     L.fgkl_pairhmm_compute_device_noalloc.argtypes = [C.POINTER(DeviceRegion), C.c_void_p, C.c_void_p]
     L.fgkl_pairhmm_compute_device_noalloc.restype = C.c_int
     _lib = L
@@ -164,5 +167,5 @@ EXPORTED = [
     "fgkl_backend", "fgkl_last_error", "fgkl_context_create", "fgkl_context_destroy", "fgkl_batch_prepare",
     "fgkl_batch_run", "fgkl_batch_fetch", "fgkl_batch_compute", "fgkl_batch_output_len", "fgkl_synth_config",
     "fgkl_synth_reference_region", "fgkl_synth_view", "fgkl_synth_free", "fgkl_plan_describe", "fgkl_plan_sweeps", "fgkl_probe_fp32_tflops",
-    "fgkl_pairhmm_compute_device_noalloc",
+    "fgkl_pairhmm_compute_device_noalloc", "fgkl_pd_row_states", "fgkl_pd_plan_describe", "fgkl_pd_match_accepts",
 ]

@@ -91,7 +91,6 @@ int per_call(const fgkl_reads* reads, const fgkl_haplotypes* haps, const fgkl_co
       return set_error(FGKL_E_EMPTY_HAPLOTYPE, "haplotype " + std::to_string(h) + " has no bases");
   if (stats) std::memset(stats, 0, sizeof *stats);
   if (expected == 0) return FGKL_OK;
-  if (pd) return set_error(FGKL_E_UNSUPPORTED, "the PD-HMM kernel is not available in this build");
   fgkl::Engine* e = thread_engine(&rc);
   if (!e) return rc;
   std::vector<int64_t> roff(static_cast<size_t>(n_reads) + 1), hoff(static_cast<size_t>(n_haps) + 1);
@@ -109,6 +108,7 @@ int per_call(const fgkl_reads* reads, const fgkl_haplotypes* haps, const fgkl_co
   in.gcp = reads->gcp;
   in.read_off = roff.data();
   in.hap_bases = haps->bases;
+  in.hap_flags = pd ? haps->flags : nullptr;
   in.hap_off = hoff.data();
   fgkl::EngineConfig ec;
   ec.double_precision = cfg->double_precision != 0;
@@ -232,7 +232,6 @@ void fgkl_context_destroy(fgkl_context* ctx) {
 int fgkl_batch_prepare(fgkl_context* ctx, const fgkl_batch* b, const fgkl_config* config) {
   t_error.clear();
   if (!ctx || !b || !config) return set_error(FGKL_E_INVALID_ARGUMENT, "null argument");
-  if (b->hap_flags) return set_error(FGKL_E_UNSUPPORTED, "the PD-HMM kernel is not available in this build");
   if (ctx->graph) {
     cudaGraphExecDestroy(ctx->graph);
     ctx->graph = nullptr;
@@ -248,6 +247,7 @@ int fgkl_batch_prepare(fgkl_context* ctx, const fgkl_batch* b, const fgkl_config
   in.gcp = b->gcp;
   in.read_off = b->read_offsets;
   in.hap_bases = b->hap_bases;
+  in.hap_flags = b->hap_flags;
   in.hap_off = b->hap_offsets;
   fgkl::EngineConfig ec;
   ec.double_precision = config->double_precision != 0;
@@ -418,6 +418,39 @@ int fgkl_plan_sweeps(const uint8_t* hap_bases, const int32_t* hap_offsets, int32
   } catch (const std::exception& e) {
     return set_error(FGKL_E_INVALID_ARGUMENT, e.what());
   }
+}
+
+int fgkl_pd_row_states(const uint8_t* flags, int32_t len, int32_t start_state, uint8_t* states) {
+  if (len < 0 || (len > 0 && (!flags || !states)) || start_state < 0 || start_state > 2)
+    return set_error(FGKL_E_INVALID_ARGUMENT, "bad PD row");
+  return fgkl::pd_row_states(flags, len, static_cast<uint8_t>(start_state), states);
+}
+
+int fgkl_pd_plan_describe(const uint8_t* hap_bases, const uint8_t* hap_flags, const int32_t* hap_offsets, int32_t num_haps,
+                          int32_t* order, int32_t* lcp, uint8_t* dup, uint8_t* end_state, int32_t* num_codes) {
+  try {
+    std::vector<fgkl::HapView> views(static_cast<size_t>(num_haps));
+    std::vector<const uint8_t*> flags(static_cast<size_t>(num_haps));
+    for (int h = 0; h < num_haps; ++h) {
+      views[h] = fgkl::HapView{hap_bases + hap_offsets[h], hap_offsets[h + 1] - hap_offsets[h]};
+      flags[h] = hap_flags + hap_offsets[h];
+    }
+    const auto s = fgkl::SortedHaps::make_pd(views, flags);
+    for (int k = 0; k < num_haps; ++k) {
+      order[k] = s.order[k];
+      lcp[k] = s.lcp[k];
+      dup[k] = s.dup[k];
+      end_state[k] = s.end_state[k];
+    }
+    *num_codes = s.num_codes();
+    return FGKL_OK;
+  } catch (const std::exception& e) {
+    return set_error(FGKL_E_INVALID_ARGUMENT, e.what());
+  }
+}
+
+int fgkl_pd_match_accepts(uint8_t base, uint8_t flag, uint8_t read_base) {
+  return fgkl::MatchSet::of(base, flag).accepts(read_base) ? 1 : 0;
 }
 
 int fgkl_pairhmm_compute_device_noalloc(const fgkl_device_region* region, double* out, void* stream) {

@@ -4,6 +4,7 @@
 #include <chrono>
 #include <cstring>
 #include <map>
+#include <string>
 #include <thread>
 
 #include "../../include/fgkl_b200.h"
@@ -33,7 +34,10 @@ int single_rows(int len) {
 struct RegionPlan {
   ProgramBuild prog;
   std::vector<HapInfo> haps;
-  std::vector<uint8_t> seq;  // prior codes of the distinct sorted haplotypes, concatenated
+  std::vector<uint8_t> seq;        // prior codes of the distinct sorted haplotypes, concatenated
+  std::vector<uint32_t> pd_seq;    // PD: their forward entries (code and deletion bits)
+  std::vector<uint32_t> pd_sigs;   // PD: per match-set code, the read classes it accepts
+  std::string error;               // a region the kernels cannot take
   uint8_t codes[256];
   SharedColumns cols;
   uint64_t read_bases = 0, hap_bases = 0;
@@ -41,21 +45,57 @@ struct RegionPlan {
   bool extra_codes = false;  // a haplotype byte outside ACGTN: the region runs on the FP64 kernel
 };
 
+// PD regions: the reads' distinct bytes become classes 0..30 (first-seen order) and each match-set
+// code the bit set of classes it accepts, so the kernel's prior is one bit test per row.
+bool pd_read_classes(const BatchInput& in, int64_t first_read, int n_reads, const SortedHaps& s, RegionPlan& out) {
+  std::memset(out.codes, kNoCode, 256);
+  std::vector<uint8_t> bytes;
+  for (int r = 0; r < n_reads; ++r)
+    for (int64_t o = in.read_off[first_read + r]; o < in.read_off[first_read + r + 1]; ++o) {
+      const uint8_t b = in.bases[o];
+      if (out.codes[b] != kNoCode) continue;
+      if (static_cast<int>(bytes.size()) >= kPdMaxReadClasses) return false;
+      out.codes[b] = static_cast<uint8_t>(bytes.size());
+      bytes.push_back(b);
+    }
+  out.pd_sigs.assign(s.match_sets.size(), 0u);
+  for (size_t code = 0; code < s.match_sets.size(); ++code)
+    for (size_t c = 0; c < bytes.size(); ++c)
+      if (s.match_sets[code].accepts(bytes[c])) out.pd_sigs[code] |= 1u << c;
+  return true;
+}
+
 void plan_region(const BatchInput& in, int g, int64_t first_read, int64_t first_hap, bool share, RegionPlan& out) {
   const int n_haps = in.region_haps[g], n_reads = in.region_reads[g];
   std::vector<HapView> views(static_cast<size_t>(n_haps));
+  std::vector<const uint8_t*> flags(in.hap_flags ? static_cast<size_t>(n_haps) : 0);
   for (int h = 0; h < n_haps; ++h) {
     const int64_t lo = in.hap_off[first_hap + h], hi = in.hap_off[first_hap + h + 1];
     views[h] = HapView{in.hap_bases + lo, static_cast<int32_t>(hi - lo)};
+    if (in.hap_flags) flags[h] = in.hap_flags + lo;
     out.hap_bases += static_cast<uint64_t>(hi - lo);
   }
   for (int r = 0; r < n_reads; ++r)
     out.read_bases += static_cast<uint64_t>(in.read_off[first_read + r + 1] - in.read_off[first_read + r]);
   if (n_haps == 0 || n_reads == 0) return;
-  const SortedHaps s = SortedHaps::make(views, share);
-  emit_program(s, share, out.prog);
-  code_table(s, out.codes);
-  out.extra_codes = s.num_codes() > 5;
+  const bool pd = in.hap_flags != nullptr;
+  SortedHaps s;
+  try {
+    s = pd ? SortedHaps::make_pd(views, flags) : SortedHaps::make(views, share);
+    emit_program(s, share && !pd, out.prog);
+  } catch (const std::exception& e) {
+    out.error = e.what();
+    return;
+  }
+  if (pd) {
+    if (!pd_read_classes(in, first_read, n_reads, s, out)) {
+      out.error = "a PD region's reads hold more than 31 distinct bytes";
+      return;
+    }
+  } else {
+    code_table(s, out.codes);
+    out.extra_codes = s.num_codes() > 5;
+  }
   out.cols = s.columns();
   out.haps.resize(static_cast<size_t>(n_haps));
   int seg = -1, src = 0;
@@ -63,8 +103,13 @@ void plan_region(const BatchInput& in, int g, int64_t first_read, int64_t first_
     if (!s.dup[k]) {
       ++seg;
       src = k;
-      out.haps[k].seq = static_cast<int32_t>(out.seq.size());
-      out.seq.insert(out.seq.end(), s.codes[k].begin(), s.codes[k].end());
+      if (pd) {
+        out.haps[k].seq = static_cast<int32_t>(out.pd_seq.size());
+        for (int32_t j = 0; j < s.bases[k].len; ++j) out.pd_seq.push_back(s.codes[k][j] | s.pd_bits[k][j]);
+      } else {
+        out.haps[k].seq = static_cast<int32_t>(out.seq.size());
+        out.seq.insert(out.seq.end(), s.codes[k].begin(), s.codes[k].end());
+      }
       ++out.n_distinct;
     } else {
       out.haps[k].seq = out.haps[src].seq;
@@ -225,11 +270,15 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
   parallel_for(N, std::min(host_threads(), (N + 7) / 8),
                [&](int64_t g) { plan_region(in, static_cast<int>(g), first_read[g], first_hap[g], share, plans[g]); });
 
+  for (int g = 0; g < N; ++g)
+    if (!plans[g].error.empty()) return fail(FGKL_E_UNSUPPORTED, "region " + std::to_string(g) + ": " + plans[g].error);
+  const bool pd = in.hap_flags != nullptr;
+
   planned_.host_plan_ms = ms_since(t_start);
   const auto t_pack = std::chrono::steady_clock::now();
   // Section offsets. Each stream gets kStreamPad zero entries on both sides.
   std::vector<Region> regions(static_cast<size_t>(N));
-  int64_t n_haps = 0, n_stream = kStreamPad, n_segs = 0, n_sweeps = 0, n_seq = 0;
+  int64_t n_haps = 0, n_stream = kStreamPad, n_segs = 0, n_sweeps = 0, n_seq = 0, n_pd_seq = 0, n_sigs = 0;
   int max_slots = 1, max_nodes = 1, max_segs = 1;
   std::vector<int64_t> queue_cap(kRowBins, 0);
   for (int g = 0; g < N; ++g) {
@@ -262,8 +311,11 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
     R.n_reads = in.region_reads[g];
     R.out_off = out_off[g];
     R.code_off = g * 256;
-    R.seq_off = static_cast<int32_t>(n_seq);
+    R.seq_off = static_cast<int32_t>(pd ? n_pd_seq : n_seq);
     n_seq += static_cast<int64_t>(rp.seq.size());
+    n_pd_seq += static_cast<int64_t>(rp.pd_seq.size());
+    R.sig_off = static_cast<int32_t>(n_sigs);
+    n_sigs += static_cast<int64_t>(rp.pd_sigs.size());
     planned_.nominal_cells += rp.read_bases * rp.hap_bases;
     planned_.forward_cells += rp.read_bases * rp.prog.fwd_columns;
     planned_.backward_cells += rp.read_bases * rp.prog.bwd_columns;
@@ -273,7 +325,7 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
         queue_cap[single_rows(static_cast<int>(in.read_off[r + 1] - in.read_off[r]))] += rp.n_distinct;
   }
   planned_.computed_cells = planned_.forward_cells + planned_.backward_cells;
-  if (n_stream > INT32_MAX || n_seq > INT32_MAX || n_haps > INT32_MAX)
+  if (n_stream > INT32_MAX || n_seq > INT32_MAX || n_pd_seq > INT32_MAX || n_haps > INT32_MAX)
     return fail(FGKL_E_INVALID_ARGUMENT, "batch too large for 32-bit plan offsets; split it");
 
   // Tasks: reads sorted longest first; FP32 packs consecutive pairs below 256 bases.
@@ -293,7 +345,14 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return len_of(a) > len_of(b); });
     const uint64_t cost_cols = plans[g].prog.fwd.size() + plans[g].prog.bwd.size() + 31;
     size_t i = 0;
-    if (cfg.double_precision || plans[g].extra_codes) {
+    if (pd) {
+      // PD: one read per warp, FP32 or FP64.
+      const Kind kind = cfg.double_precision ? Kind::kOneF64Pd : Kind::kOneF32Pd;
+      for (; i < order.size(); ++i) {
+        const int rows = single_rows(len_of(order[i]));
+        by_bin[{kind, rows}].push_back({cost_cols * rows, Task{g, {static_cast<int32_t>(first_read[g] + order[i]), -1}, rows, -1}});
+      }
+    } else if (cfg.double_precision || plans[g].extra_codes) {
       for (; i < order.size(); ++i) {
         const int rows = single_rows(len_of(order[i]));
         by_bin[{Kind::kOneF64, rows}].push_back(
@@ -351,10 +410,11 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
     for (int r = 1; r < kRowBins; ++r) {
       const int cap = queue_off[r + 1] - queue_off[r];
       if (cap == 0) continue;
+      const Kind kind = pd ? Kind::kOneF64Pd : Kind::kOneF64;
       int per_sm = 0, threads = 0;
-      occupancy(Kind::kOneF64, r, &per_sm, &threads);
+      occupancy(kind, r, &per_sm, &threads);
       if (per_sm <= 0) return fail(FGKL_E_CUDA, "recomputation kernel unavailable on this device");
-      Bin b{Kind::kOneF64, r, queue_off[r], cap, 0, 0, 0};
+      Bin b{kind, r, queue_off[r], cap, 0, 0, 0};
       b.blocks = std::max(1, std::min((cap + kWarpsPerBlock - 1) / kWarpsPerBlock, per_sm * sms_));
       rescue_bins_.push_back(b);
     }
@@ -372,8 +432,8 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
     scratch_total = std::max(scratch_total, off);
   }
 
-  // Plan blob: regions | haps | stream | segs | sweeps | code tables | haplotype codes.
-  size_t o_regions, o_haps, o_stream, o_segs, o_sweeps, o_codes, o_seq, blob_bytes = 0;
+  // Plan blob: regions | haps | stream | segs | sweeps | code tables | haplotype codes | PD entries | PD signatures.
+  size_t o_regions, o_haps, o_stream, o_segs, o_sweeps, o_codes, o_seq, o_pd_seq, o_sigs, blob_bytes = 0;
   auto section = [&](size_t bytes, size_t& off) {
     off = align_up(blob_bytes, 16);
     blob_bytes = off + bytes;
@@ -385,6 +445,8 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
   section(static_cast<size_t>(n_sweeps) * sizeof(Sweep), o_sweeps);
   section(static_cast<size_t>(N) * 256, o_codes);
   section(static_cast<size_t>(n_seq) + 16, o_seq);
+  section(static_cast<size_t>(n_pd_seq) * sizeof(uint32_t) + 16, o_pd_seq);
+  section(static_cast<size_t>(n_sigs) * sizeof(uint32_t) + 16, o_sigs);
 
   // Device buffers.
   const int64_t read_bytes = total_reads > 0 ? in.read_off[total_reads] : 0;
@@ -425,6 +487,8 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
     uint32_t* stream = reinterpret_cast<uint32_t*>(blob + o_stream);
     std::memset(stream, 0, kStreamPad * sizeof(uint32_t));
     std::memset(blob + o_seq + n_seq, 0, 16);
+    std::memset(blob + o_pd_seq + n_pd_seq * sizeof(uint32_t), 0, 16);
+    std::memset(blob + o_sigs + n_sigs * sizeof(uint32_t), 0, 16);
     parallel_for(N, std::min(host_threads(), (N + 31) / 32), [&](int64_t g) {
       const RegionPlan& rp = plans[g];
       const Region& R = regions[g];
@@ -442,6 +506,10 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
       if (!rp.haps.empty()) std::memcpy(blob + o_codes + static_cast<size_t>(g) * 256, rp.codes, 256);
       else std::memset(blob + o_codes + static_cast<size_t>(g) * 256, 0, 256);
       if (!rp.seq.empty()) std::memcpy(blob + o_seq + R.seq_off, rp.seq.data(), rp.seq.size());
+      if (!rp.pd_seq.empty())
+        std::memcpy(blob + o_pd_seq + static_cast<size_t>(R.seq_off) * sizeof(uint32_t), rp.pd_seq.data(), rp.pd_seq.size() * sizeof(uint32_t));
+      if (!rp.pd_sigs.empty())
+        std::memcpy(blob + o_sigs + static_cast<size_t>(R.sig_off) * sizeof(uint32_t), rp.pd_sigs.data(), rp.pd_sigs.size() * sizeof(uint32_t));
     });
   }
   if (!tasks.empty()) std::memcpy(st + s_tasks, tasks.data(), tasks.size() * sizeof(Task));
@@ -478,6 +546,8 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
   view_.sweeps = reinterpret_cast<const Sweep*>(d_plan_ + o_sweeps);
   view_.code_of_byte = d_plan_ + o_codes;
   view_.hap_codes = d_plan_ + o_seq;
+  view_.pd_entries = reinterpret_cast<const uint32_t*>(d_plan_ + o_pd_seq);
+  view_.pd_sigs = reinterpret_cast<const uint32_t*>(d_plan_ + o_sigs);
   view_.err_prob = d_err_;
   view_.m2m = d_m2m_;
   view_.out = d_out_;

@@ -28,6 +28,7 @@ struct BatchInput {
   const uint8_t *bases = nullptr, *quals = nullptr, *ins = nullptr, *del = nullptr, *gcp = nullptr;
   const int64_t* read_off = nullptr;  // total_reads + 1
   const uint8_t* hap_bases = nullptr;
+  const uint8_t* hap_flags = nullptr; // PD-HMM: per-base flags (same layout as hap_bases); nullptr = plain
   const int64_t* hap_off = nullptr;   // total_haps + 1
 };
 

@@ -1,0 +1,501 @@
+// sm_100a PD-HMM kernels (GATK LoglessPDPairHMM for DRAGEN concordance mode; fgkl pd_kernel.rs and
+// pd_reference.rs:29-118): the plain kernels' warp wavefront over a prefix-shared column stream,
+// with GATK's branch matrices.
+//
+// Per cell (row i, column j in deletion state s; left = (i, j-1), up = (i-1, j), diag = (i-1, j-1);
+// B = branch values, V = (M, X, Y)):
+//   B(i,j) = V(left)                 s = NORMAL
+//          = B(left)                 s = INSIDE_DEL
+//          = max(B(left), V(left))   s = AFTER_DEL
+//   M = prior * (mm*D.M + im*(D.X + D.Y)),  D = max(B(diag), V(diag)) after a deletion, else V(diag)
+//   Y = md*W.M + dd*W.Y,                    W = max(B(left), V(left)) after a deletion, else V(left)
+//   X = mi*U.M + ii*U.X,                    U = max(B(up), V(up)) on a DEL_END column, else V(up)
+// The state of a column depends only on the flags and on the state the row started in: NORMAL for
+// the read's first row, the state the previous row ended in for the others. The host resolves both
+// per column into the stream entry (program.h), with the column's prior code (a match set: its base
+// and, on a SNP column, the flagged alternates).
+//
+// Branch values are only ever read at a column following one that carries DEL_START or DEL_END (and
+// one row down from a DEL_END column), so a lane keeps them lazily: its per-row branch registers are
+// updated only on columns carrying either flag (B = V(left), held, or merged by the state), and
+// hold a stale value elsewhere that nothing reads. Columns with no flag and not right after a
+// deletion (the vast majority) run the plain recurrence. The branch values of the lane above arrive
+// by shuffle every step like its match, insertion and deletion values, one set for the column and
+// the previous set for the diagonal.
+//
+// Priors. A PD region maps its reads' distinct bytes to classes 0..30; each match-set code carries
+// the bit set of classes it accepts, so a row's prior is pm or px by one bit test.
+//
+// FP32 kernels carry X/mi and Y/md per row like the plain kernels; max() commutes with the positive
+// per-row scale, so the branch values are kept in the same scale.
+#include "dp_common.cuh"
+#include "kernels.cuh"
+
+namespace fgkl {
+
+namespace {
+
+template <class P, int R>
+struct PdLayout {
+  using V = typename P::V;
+  static constexpr int kRound = 16 / static_cast<int>(sizeof(V)) > 1 ? 16 / static_cast<int>(sizeof(V)) : 1;
+  static constexpr int up(int x) { return (x + kRound - 1) / kRound * kRound; }
+  // M, X, Y rows; branch M, X, Y rows; above-row M, X, Y and branch M, X, Y; accumulated result.
+  static constexpr int kSnap = up(6 * R + 7);
+  static constexpr size_t kStageBytes = 2ull * 32 * kSnap * sizeof(V);
+  static constexpr size_t kSmemPerWarp = kStageBytes;
+};
+
+template <class P, int R>
+struct PdScratch {
+  using V = typename P::V;
+  using L = PdLayout<P, R>;
+  V* slots;         // [slot][lane][kSnap]
+  double* seg_raw;  // [seg][c]
+  V* stage;         // shared: [buf][lane][kSnap]
+
+  __device__ PdScratch(char* base, V* smem, int n_slots) {
+    slots = reinterpret_cast<V*>(base);
+    seg_raw = reinterpret_cast<double*>(slots + static_cast<size_t>(n_slots) * 32 * L::kSnap);
+    stage = smem;
+  }
+  __device__ V* slot(int s, int lane) { return slots + (static_cast<size_t>(s) * 32 + lane) * L::kSnap; }
+  __device__ V* staged(int buf, int lane) { return stage + (static_cast<size_t>(buf & 1) * 32 + lane) * L::kSnap; }
+};
+
+template <class P, int R>
+constexpr size_t pd_scratch_size(int n_slots, int n_segs) {
+  return static_cast<size_t>(n_slots) * 32 * PdLayout<P, R>::kSnap * sizeof(typename P::V) +
+         static_cast<size_t>(n_segs) * P::NC * sizeof(double);
+}
+
+// Forward coefficients of the lane's rows (the plain kernels' FwdRows) and each row's read class.
+template <class P, int R>
+struct PdRows {
+  using V = typename P::V;
+  using S = typename P::S;
+  V c0[R], c1[R], c2[R], c3[R], c4[R], pm[R], px[R];
+  int cls[P::NC][R];  // read class of the row's base; 31 for a padding row (no code accepts it)
+
+  __device__ V prior(uint32_t sig, int r) const {
+    return P::sel((sig >> cls[0][r]) & 1u, (sig >> cls[P::NC - 1][r]) & 1u, pm[r], px[r]);
+  }
+
+  __device__ void load(const BatchView& v, const ReadRef* rd, int lane, const uint8_t* classes) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+#pragma unroll
+      for (int c = 0; c < P::NC; ++c) {
+        const RowModel m = row_model(v, rd[c], lane * R + r - rd[c].pad, classes);
+        double k0, k1, k2, k3, k4;
+        if (P::kTransformed) {
+          if (m.read) {
+            k0 = m.mm;
+            k1 = m.im * m.mi_prev;
+            k2 = m.im * m.md_prev;
+            k3 = m.gc * m.mi_prev / m.mi;
+            k4 = m.gc;
+          } else {
+            k0 = k1 = k2 = k3 = 0.0;
+            k4 = 1.0;
+          }
+        } else {
+          if (m.read) {
+            k0 = m.mm;
+            k1 = m.im;
+            k2 = m.mi;
+            k3 = m.gc;
+            k4 = m.md;
+          } else {
+            k0 = k1 = k2 = k4 = 0.0;
+            k3 = 1.0;
+          }
+        }
+        P::put(c0[r], c, static_cast<S>(k0));
+        P::put(c1[r], c, static_cast<S>(k1));
+        P::put(c2[r], c, static_cast<S>(k2));
+        P::put(c3[r], c, static_cast<S>(k3));
+        P::put(c4[r], c, static_cast<S>(k4));
+        P::put(pm[r], c, static_cast<S>(m.pm));
+        P::put(px[r], c, static_cast<S>(m.px));
+        cls[c][r] = m.read ? (m.oc & 31) : 31;
+      }
+    }
+  }
+};
+
+template <class P, int R>
+struct PdState {
+  using V = typename P::V;
+  V M[R], X[R], Y[R];
+  V BM[R], BX[R], BY[R];
+  V acc;
+  int seg_i;
+};
+
+// The lane above's bottom row: values and branch values.
+template <class P>
+struct PdEdge {
+  using V = typename P::V;
+  V M, X, Y, BM, BX, BY;
+};
+
+// One PD forward step: events, then the column. `u` receives the lane above's bottom row for this
+// column, `d` holds it for the previous column (the top row's diagonal); the two alternate.
+template <class P, int R>
+__device__ __forceinline__ void pd_step(const LaunchArgs& a, const Program& prog, const ReadRef* rd, int lane,
+                                        const PdRows<P, R>& pr, const typename P::V& an, int pad_hi, PdScratch<P, R>& sc,
+                                        PdState<P, R>& st, int synth_len, uint32_t ev, uint32_t sig, PdEdge<P>& u,
+                                        PdEdge<P>& d) {
+  using V = typename P::V;
+  using S = typename P::S;
+  using L = PdLayout<P, R>;
+  u.M = P::up(st.M[R - 1]);
+  u.X = P::up(st.X[R - 1]);
+  u.Y = P::up(st.Y[R - 1]);
+  u.BM = P::up(st.BM[R - 1]);
+  u.BX = P::up(st.BX[R - 1]);
+  u.BY = P::up(st.BY[R - 1]);
+  if (ev & kEvMask) {
+    if (ev & EV_SNAP) {
+      const uint32_t slot = ev >> kPdPayloadShift;
+      V* dst[2] = {slot != kPdPayloadNone ? sc.slot(static_cast<int>(slot), lane) : nullptr,
+                   (ev & EV_STAGE) ? sc.staged(st.seg_i + 1, lane) : nullptr};
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        V* o = dst[k];
+        if (!o) continue;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          o[r] = st.M[r];
+          o[R + r] = st.X[r];
+          o[2 * R + r] = st.Y[r];
+          o[3 * R + r] = st.BM[r];
+          o[4 * R + r] = st.BX[r];
+          o[5 * R + r] = st.BY[r];
+        }
+        o[6 * R] = d.M;
+        o[6 * R + 1] = d.X;
+        o[6 * R + 2] = d.Y;
+        o[6 * R + 3] = d.BM;
+        o[6 * R + 4] = d.BX;
+        o[6 * R + 5] = d.BY;
+        o[6 * R + 6] = st.acc;
+      }
+    }
+    if ((ev & EV_END) && lane == 31) {
+#pragma unroll
+      for (int c = 0; c < P::NC; ++c) sc.seg_raw[st.seg_i * P::NC + c] = static_cast<double>(P::get(st.acc, c));
+    }
+    if (ev & EV_BEGIN) {
+      ++st.seg_i;
+      // A recomputation stream (FP64 only) has one unshared segment from the origin and no record.
+      const bool synth = synth_len > 0;
+      const Segment* rec = a.v.segs + prog.seg_off + st.seg_i;
+      if (!synth && st.seg_i + 1 < prog.n_segs) prefetch_l1(rec + 1);
+      const int next_slot = synth ? -1 : rec->next_slot;
+      if (!synth && rec->staged) {
+        __pipeline_wait_prior(0);
+        const V* s = sc.staged(st.seg_i, lane);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          st.M[r] = s[r];
+          st.X[r] = s[R + r];
+          st.Y[r] = s[2 * R + r];
+          st.BM[r] = s[3 * R + r];
+          st.BX[r] = s[4 * R + r];
+          st.BY[r] = s[5 * R + r];
+        }
+        d.M = s[6 * R];
+        d.X = s[6 * R + 1];
+        d.Y = s[6 * R + 2];
+        d.BM = s[6 * R + 3];
+        d.BX = s[6 * R + 4];
+        d.BY = s[6 * R + 5];
+        st.acc = s[6 * R + 6];
+      } else {
+        // The origin: the row-0 constant in the padding rows, zero branch values (GATK never writes
+        // branch column zero).
+        const S in_s = synth ? static_cast<S>(Consts<P::kDouble>::kInitial / synth_len)
+                             : (P::kDouble ? static_cast<S>(rec->init_d) : static_cast<S>(rec->init_f));
+#pragma unroll
+        for (int r = 0; r < R; ++r) st.M[r] = st.X[r] = st.Y[r] = st.BM[r] = st.BX[r] = st.BY[r] = P::zero();
+        d.M = d.X = d.Y = d.BM = d.BX = d.BY = st.acc = P::zero();
+        if (lane * R <= pad_hi) {
+#pragma unroll
+          for (int c = 0; c < P::NC; ++c) {
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+              if (lane * R + r < rd[c].pad) P::put(st.Y[r], c, in_s);
+            if (lane * R - 1 < rd[c].pad) P::put(d.Y, c, in_s);
+          }
+        }
+      }
+      if (next_slot >= 0) prefetch(sc.staged(st.seg_i + 1, lane), sc.slot(next_slot, lane), L::kSnap);
+    }
+  }
+  if (ev & kPdSlowMask) {
+    // A column carrying DEL_START or DEL_END, or right after a deletion.
+    const bool mat = (ev & PD_MAT) != 0, de = (ev & PD_DE) != 0;
+    const uint32_t s_first = (ev >> kPdFirstShift) & 3u, s_later = (ev >> kPdLaterShift) & 3u;
+#pragma unroll
+    for (int r = R - 1; r >= 0; --r) {
+      bool after[P::NC], inside[P::NC];
+#pragma unroll
+      for (int c = 0; c < P::NC; ++c) {
+        const uint32_t s = (lane * R + r == rd[c].pad) ? s_first : s_later;
+        after[c] = s == kPdAfterDel;
+        inside[c] = s == kPdInsideDel;
+      }
+      const bool a0 = after[0], a1 = after[P::NC - 1];
+      const V qBM = r ? st.BM[r - 1] : d.BM, qBX = r ? st.BX[r - 1] : d.BX, qBY = r ? st.BY[r - 1] : d.BY;
+      V pM = r ? st.M[r - 1] : d.M, pX = r ? st.X[r - 1] : d.X, pY = r ? st.Y[r - 1] : d.Y;
+      pM = P::sel(a0, a1, P::max(qBM, pM), pM);
+      pX = P::sel(a0, a1, P::max(qBX, pX), pX);
+      pY = P::sel(a0, a1, P::max(qBY, pY), pY);
+      const V lM = P::sel(a0, a1, P::max(st.BM[r], st.M[r]), st.M[r]);
+      const V lX = P::sel(a0, a1, P::max(st.BX[r], st.X[r]), st.X[r]);
+      const V lY = P::sel(a0, a1, P::max(st.BY[r], st.Y[r]), st.Y[r]);
+      if (mat) {
+        st.BM[r] = P::sel(inside[0], inside[P::NC - 1], st.BM[r], lM);
+        st.BX[r] = P::sel(inside[0], inside[P::NC - 1], st.BX[r], lX);
+        st.BY[r] = P::sel(inside[0], inside[P::NC - 1], st.BY[r], lY);
+      }
+      const V prior = pr.prior(sig, r);
+      st.Y[r] = P::kTransformed ? P::fma(lY, pr.c4[r], lM) : P::fma(lY, pr.c3[r], P::mul(lM, pr.c4[r]));
+      st.M[r] = P::mul(prior, cell_match<P>(pM, pX, pY, pr.c0[r], pr.c1[r], pr.c2[r]));
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      V qM = r ? st.M[r - 1] : u.M, qX = r ? st.X[r - 1] : u.X;
+      if (de) {
+        qM = P::max(r ? st.BM[r - 1] : u.BM, qM);
+        qX = P::max(r ? st.BX[r - 1] : u.BX, qX);
+      }
+      st.X[r] = P::kTransformed ? P::fma(qX, pr.c3[r], qM) : P::fma(qX, pr.c3[r], P::mul(qM, pr.c2[r]));
+    }
+  } else {
+#pragma unroll
+    for (int r = R - 1; r >= 0; --r) {
+      const V pM = r ? st.M[r - 1] : d.M, pX = r ? st.X[r - 1] : d.X, pY = r ? st.Y[r - 1] : d.Y;
+      const V prior = pr.prior(sig, r);
+      st.Y[r] = P::kTransformed ? P::fma(st.Y[r], pr.c4[r], st.M[r]) : P::fma(st.Y[r], pr.c3[r], P::mul(st.M[r], pr.c4[r]));
+      st.M[r] = P::mul(prior, cell_match<P>(pM, pX, pY, pr.c0[r], pr.c1[r], pr.c2[r]));
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const V qM = r ? st.M[r - 1] : u.M, qX = r ? st.X[r - 1] : u.X;
+      st.X[r] = P::kTransformed ? P::fma(qX, pr.c3[r], qM) : P::fma(qX, pr.c3[r], P::mul(qM, pr.c2[r]));
+    }
+  }
+  st.acc = P::fma(st.X[R - 1], an, P::add(st.acc, st.M[R - 1]));
+}
+
+// Entry p of a recomputation stream: the haplotype's forward entries (code and deletion bits),
+// BEGIN on the first column and END after the last.
+__device__ __forceinline__ uint32_t pd_synth_entry(const uint32_t* seq, int len, int p) {
+  if (p < 0 || p > len) return 0u;
+  uint32_t e = p < len ? __ldg(seq + p) : 0u;
+  if (p == 0) e |= EV_BEGIN;
+  if (p == len) e |= EV_END;
+  return e;
+}
+
+template <class P, int R>
+__device__ void pd_forward_pass(const LaunchArgs& a, const Program& prog, const ReadRef* rd, const uint8_t* classes,
+                                const uint32_t* sigs, int lane, PdScratch<P, R>& sc, const uint32_t* synth_seq, int synth_len) {
+  using V = typename P::V;
+  using S = typename P::S;
+  PdRows<P, R> pr;
+  pr.load(a.v, rd, lane, classes);
+  V an;
+#pragma unroll
+  for (int c = 0; c < P::NC; ++c)
+    P::put(an, c, static_cast<S>((P::kTransformed && rd[c].len > 0) ? err_prob(a.v, a.v.ins[rd[c].off + rd[c].len - 1]) : 1.0));
+  int pad_hi = 0;
+#pragma unroll
+  for (int c = 0; c < P::NC; ++c) pad_hi = rd[c].pad > pad_hi ? rd[c].pad : pad_hi;
+
+  PdState<P, R> st;
+#pragma unroll
+  for (int r = 0; r < R; ++r) st.M[r] = st.X[r] = st.Y[r] = st.BM[r] = st.BX[r] = st.BY[r] = P::zero();
+  st.acc = P::zero();
+  st.seg_i = -1;
+  PdEdge<P> ea, eb;
+  ea.M = ea.X = ea.Y = ea.BM = ea.BX = ea.BY = P::zero();
+  eb = ea;
+  if (P::kDouble && synth_len > 0) {
+    const int n = synth_len;
+    for (int t = 0; t < n + 32; t += 2) {
+      const uint32_t e0 = pd_synth_entry(synth_seq, n, t - lane), e1 = pd_synth_entry(synth_seq, n, t + 1 - lane);
+      pd_step<P, R>(a, prog, rd, lane, pr, an, pad_hi, sc, st, synth_len, e0, __ldg(sigs + (e0 & kCodeMask)), ea, eb);
+      pd_step<P, R>(a, prog, rd, lane, pr, an, pad_hi, sc, st, synth_len, e1, __ldg(sigs + (e1 & kCodeMask)), eb, ea);
+    }
+  } else {
+    const int n = prog.fwd_len;
+    const uint32_t* stream = a.v.stream + prog.fwd_off - lane;
+    uint32_t n0 = __ldg(stream), n1 = __ldg(stream + 1);
+    uint32_t g0 = __ldg(sigs + (n0 & kCodeMask)), g1 = __ldg(sigs + (n1 & kCodeMask));
+    for (int t = 0; t < n + 32; t += 2) {
+      const uint32_t e0 = n0, e1 = n1, s0 = g0, s1 = g1;
+      n0 = __ldg(stream + t + 2);
+      n1 = __ldg(stream + t + 3);
+      g0 = __ldg(sigs + (n0 & kCodeMask));
+      g1 = __ldg(sigs + (n1 & kCodeMask));
+      pd_step<P, R>(a, prog, rd, lane, pr, an, pad_hi, sc, st, 0, e0, s0, ea, eb);
+      pd_step<P, R>(a, prog, rd, lane, pr, an, pad_hi, sc, st, 0, e1, s1, eb, ea);
+    }
+  }
+  __pipeline_wait_prior(0);
+}
+
+// Thresholds, log10 and the caller's layout (fgkl kernel.rs:897-914 via pd_kernel.rs:262-270).
+template <class P, int R>
+__device__ void pd_finalize(const LaunchArgs& a, const Task& task, const Region& region, const Program& prog, int lane,
+                            PdScratch<P, R>& sc) {
+  using C = Consts<P::kDouble>;
+  __syncwarp();
+  if (P::kDouble && task.hap >= 0) {
+    const double raw = sc.seg_raw[0];
+    const double result = raw != raw ? __longlong_as_double(0x7ff8000000000000ll) : log10(raw) - C::kLog10Initial;
+    const int read_local = task.read[0] - region.read_off;
+    for (int k = lane; k < region.n_haps; k += 32) {
+      const HapInfo info = a.v.haps[region.hap_off + k];
+      if (info.src == task.hap) a.v.out[region.out_off + static_cast<int64_t>(read_local) * region.n_haps + info.order] = result;
+    }
+    return;
+  }
+  unsigned long long lost_count = 0;
+  for (int k = lane; k < region.n_haps; k += 32) {
+    const HapInfo info = a.v.haps[region.hap_off + k];
+    const double factor = a.v.segs[prog.seg_off + info.seg].factor;
+#pragma unroll
+    for (int c = 0; c < P::NC; ++c) {
+      if (task.read[c] < 0) continue;
+      const double raw = __dmul_rn(sc.seg_raw[info.seg * P::NC + c], factor);
+      bool lost = a.min_accept_plain ? !(raw >= C::kMinAccepted) : (raw != raw);
+      if (!P::kDouble) lost |= isinf(raw);
+      const double result = lost ? __longlong_as_double(0x7ff8000000000000ll) : log10(raw) - C::kLog10Initial;
+      const int read_local = task.read[c] - region.read_off;
+      a.v.out[region.out_off + static_cast<int64_t>(read_local) * region.n_haps + info.order] = result;
+      lost_count += lost;
+    }
+  }
+  if (lost_count) atomicAdd(&a.v.counters->lost_pairs, lost_count);
+}
+
+template <class P, int R>
+struct PdMinBlocks {
+  static constexpr int value = P::kDouble ? 1 : 2;
+};
+
+template <class P, int R>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, (PdMinBlocks<P, R>::value)) pd_kernel(LaunchArgs a) {
+  using V = typename P::V;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31;
+  const int warp_in_block = threadIdx.x >> 5;
+  const int warp = blockIdx.x * kWarpsPerBlock + warp_in_block;
+  V* smem = reinterpret_cast<V*>(smem_raw + warp_in_block * PdLayout<P, R>::kSmemPerWarp);
+  const int count = a.count ? min(*a.count, a.n_tasks) : a.n_tasks;
+  for (;;) {
+    int t = 0;
+    if (lane == 0) t = atomicAdd(a.task_counter, 1);
+    t = __shfl_sync(kFull, t, 0);
+    if (t >= count) break;
+    const Task task = a.tasks[t];
+    const Region region = a.v.regions[task.region];
+    const Program prog = region.prog;
+    ReadRef rd[P::NC];
+#pragma unroll
+    for (int c = 0; c < P::NC; ++c) {
+      const int id = task.read[c];
+      if (id >= 0) {
+        rd[c].off = a.v.read_off[id];
+        rd[c].len = static_cast<int>(a.v.read_off[id + 1] - rd[c].off);
+      } else {
+        rd[c].off = 0;
+        rd[c].len = 0;
+      }
+      rd[c].pad = 32 * R - rd[c].len;
+    }
+    const uint8_t* classes = a.v.code_of_byte + region.code_off;
+    const uint32_t* sigs = a.v.pd_sigs + region.sig_off;
+    char* scratch = a.scratch + static_cast<size_t>(warp) * a.scratch_stride;
+    if (P::kDouble && task.hap >= 0) {
+      const HapInfo info = a.v.haps[region.hap_off + task.hap];
+      PdScratch<P, R> sc(scratch, smem, 0);
+      pd_forward_pass<P, R>(a, prog, rd, classes, sigs, lane, sc, a.v.pd_entries + region.seq_off + info.seq, info.len);
+      pd_finalize<P, R>(a, task, region, prog, lane, sc);
+    } else {
+      PdScratch<P, R> sc(scratch, smem, prog.n_slots);
+      pd_forward_pass<P, R>(a, prog, rd, classes, sigs, lane, sc, nullptr, 0);
+      pd_finalize<P, R>(a, task, region, prog, lane, sc);
+    }
+    __syncwarp();
+  }
+}
+
+template <class P, int R>
+void pd_occ(int* blocks) {
+  const size_t smem = kWarpsPerBlock * PdLayout<P, R>::kSmemPerWarp;
+  cudaFuncSetAttribute(pd_kernel<P, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, pd_kernel<P, R>, kWarpsPerBlock * 32, smem);
+}
+
+template <class P, int R>
+cudaError_t pd_go(int blocks, const LaunchArgs& a, cudaStream_t s) {
+  const size_t smem = kWarpsPerBlock * PdLayout<P, R>::kSmemPerWarp;
+  pd_kernel<P, R><<<blocks, kWarpsPerBlock * 32, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+// Rows-per-lane dispatch over 1..8 and 10..20 (even), FP32 or FP64.
+template <class P, class F>
+auto pd_rows(int rows, F&& f) {
+  switch (rows) {
+    case 1: return f(std::integral_constant<int, 1>{});
+    case 2: return f(std::integral_constant<int, 2>{});
+    case 3: return f(std::integral_constant<int, 3>{});
+    case 4: return f(std::integral_constant<int, 4>{});
+    case 5: return f(std::integral_constant<int, 5>{});
+    case 6: return f(std::integral_constant<int, 6>{});
+    case 7: return f(std::integral_constant<int, 7>{});
+    case 8: return f(std::integral_constant<int, 8>{});
+    case 10: return f(std::integral_constant<int, 10>{});
+    case 12: return f(std::integral_constant<int, 12>{});
+    case 14: return f(std::integral_constant<int, 14>{});
+    case 16: return f(std::integral_constant<int, 16>{});
+    case 18: return f(std::integral_constant<int, 18>{});
+    default: return f(std::integral_constant<int, 20>{});
+  }
+}
+
+}  // namespace
+
+size_t pd_scratch_bytes(bool dbl, int rows, int max_slots, int max_segs) {
+  if (dbl) return pd_rows<OneF64>(rows, [&](auto r) { return pd_scratch_size<OneF64, decltype(r)::value>(max_slots, max_segs); });
+  return pd_rows<OneF32>(rows, [&](auto r) { return pd_scratch_size<OneF32, decltype(r)::value>(max_slots, max_segs); });
+}
+
+void pd_occupancy(bool dbl, int rows, int* blocks, int* threads) {
+  *threads = kWarpsPerBlock * 32;
+  *blocks = 0;
+  if (dbl)
+    pd_rows<OneF64>(rows, [&](auto r) {
+      pd_occ<OneF64, decltype(r)::value>(blocks);
+      return 0;
+    });
+  else
+    pd_rows<OneF32>(rows, [&](auto r) {
+      pd_occ<OneF32, decltype(r)::value>(blocks);
+      return 0;
+    });
+}
+
+cudaError_t pd_launch(bool dbl, int rows, int blocks, const LaunchArgs& a, cudaStream_t s) {
+  if (dbl) return pd_rows<OneF64>(rows, [&](auto r) { return pd_go<OneF64, decltype(r)::value>(blocks, a, s); });
+  return pd_rows<OneF32>(rows, [&](auto r) { return pd_go<OneF32, decltype(r)::value>(blocks, a, s); });
+}
+
+}  // namespace fgkl

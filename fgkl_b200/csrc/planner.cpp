@@ -201,6 +201,119 @@ SortedHaps SortedHaps::make(const std::vector<HapView>& haps, bool share_suffixe
   return s;
 }
 
+bool base_matches_pd(uint8_t read_base, uint8_t flags) {
+  if (!(flags & kPdSnp)) return false;
+  switch (read_base) {
+    case 'A':
+    case 'a':
+      return flags & kPdAltA;
+    case 'C':
+    case 'c':
+      return flags & kPdAltC;
+    case 'G':
+    case 'g':
+      return flags & kPdAltG;
+    case 'T':
+    case 't':
+      return flags & kPdAltT;
+    default:
+      return false;
+  }
+}
+
+MatchSet MatchSet::of(uint8_t base, uint8_t flag) {
+  const uint8_t alts = (flag & kPdSnp) ? static_cast<uint8_t>(flag & (kPdAltA | kPdAltC | kPdAltG | kPdAltT)) : 0;
+  return MatchSet{base, alts};
+}
+
+bool MatchSet::accepts(uint8_t read_base) const {
+  return read_base == base || read_base == 'N' || base == 'N' || (alts != 0 && base_matches_pd(read_base, kPdSnp | alts));
+}
+
+uint8_t pd_row_states(const uint8_t* flags, int32_t len, uint8_t state, uint8_t* out) {
+  for (int32_t j = 0; j < len; ++j) {
+    if (out) out[j] = state;
+    if (state == kPdAfterDel) state = kPdNormal;
+    if (flags[j] & kPdDelStart) state = kPdInsideDel;
+    if (flags[j] & kPdDelEnd) state = kPdAfterDel;
+  }
+  return state;
+}
+
+SortedHaps SortedHaps::make_pd(const std::vector<HapView>& haps, const std::vector<const uint8_t*>& flags) {
+  SortedHaps s;
+  s.pd = true;
+  const size_t n = haps.size();
+  std::vector<uint8_t> ends(n);
+  for (size_t i = 0; i < n; ++i) ends[i] = pd_row_states(flags[i], haps[i].len, kPdNormal, nullptr);
+  // (row-end state, interleaved (base, flag) pairs), pairs compared lexicographically, a prefix
+  // first; the sort is stable.
+  auto pairs_less = [&](int32_t a, int32_t b) {
+    const int32_t m = std::min(haps[a].len, haps[b].len);
+    for (int32_t j = 0; j < m; ++j) {
+      const uint8_t xa = haps[a].bases[j], xb = haps[b].bases[j];
+      if (xa != xb) return xa < xb;
+      const uint8_t fa = flags[a][j], fb = flags[b][j];
+      if (fa != fb) return fa < fb;
+    }
+    return haps[a].len < haps[b].len;
+  };
+  s.order.resize(n);
+  for (size_t i = 0; i < n; ++i) s.order[i] = static_cast<int32_t>(i);
+  std::stable_sort(s.order.begin(), s.order.end(), [&](int32_t a, int32_t b) {
+    if (ends[a] != ends[b]) return ends[a] < ends[b];
+    return pairs_less(a, b);
+  });
+  s.codes.resize(n);
+  s.pd_bits.resize(n);
+  std::vector<uint8_t> first, later;
+  for (size_t k = 0; k < n; ++k) {
+    const int32_t i = s.order[k];
+    const HapView& h = haps[i];
+    const uint8_t* f = flags[i];
+    s.bases.push_back(h);
+    s.flags.push_back(f);
+    s.end_state.push_back(ends[i]);
+    s.codes[k].resize(h.len);
+    for (int32_t j = 0; j < h.len; ++j) {
+      const MatchSet set = MatchSet::of(h.bases[j], f[j]);
+      auto it = std::find(s.match_sets.begin(), s.match_sets.end(), set);
+      if (it == s.match_sets.end()) {
+        if (s.match_sets.size() >= 256) throw std::invalid_argument("more than 256 distinct PD match sets");
+        s.match_sets.push_back(set);
+        it = s.match_sets.end() - 1;
+      }
+      s.codes[k][j] = static_cast<uint8_t>(it - s.match_sets.begin());
+    }
+    first.assign(static_cast<size_t>(h.len), 0);
+    later.assign(static_cast<size_t>(h.len), 0);
+    pd_row_states(f, h.len, kPdNormal, first.data());
+    const uint8_t later_end = pd_row_states(f, h.len, ends[i], later.data());
+    if (later_end != ends[i]) throw std::logic_error("row end state not fixed by the flags");
+    s.pd_bits[k].resize(h.len);
+    for (int32_t j = 0; j < h.len; ++j) {
+      uint32_t b = (static_cast<uint32_t>(first[j]) << kPdFirstShift) | (static_cast<uint32_t>(later[j]) << kPdLaterShift);
+      if (f[j] & (kPdDelStart | kPdDelEnd)) b |= PD_MAT;
+      if (f[j] & kPdDelEnd) b |= PD_DE;
+      s.pd_bits[k][j] = b;
+    }
+  }
+  s.lcp.assign(n, 0);
+  s.dup.assign(n, 0);
+  for (size_t k = 1; k < n; ++k) {
+    if (s.end_state[k] != s.end_state[k - 1]) continue;
+    const HapView &a = s.bases[k - 1], &b = s.bases[k];
+    const int32_t m = std::min(a.len, b.len);
+    int32_t j = 0;
+    while (j < m && a.bases[j] == b.bases[j] && s.flags[k - 1][j] == s.flags[k][j]) ++j;
+    s.lcp[k] = j;
+    s.dup[k] = (a.len == b.len && j == a.len) ? 1 : 0;
+  }
+  for (const auto& h : s.bases) s.max_len = std::max(s.max_len, h.len);
+  s.plan = forward_only(n);
+  return s;
+}
+
 uint8_t SortedHaps::byte_of_code(int code) const {
   return code < 5 ? kStandard[code] : extra_bases[code - 5];
 }
@@ -291,11 +404,14 @@ void emit_program(const SortedHaps& s, bool with_suffix, ProgramBuild& out) {
     const int32_t last = g.cut.column >= 0 ? g.cut.column : g.stop;
     for (int32_t j = g.start + 1; j <= last; ++j) {
       const bool is_cut = g.cut.column >= 0 && j == g.cut.column;
-      push(out.fwd, s.codes[g.hap][j - 1] | (j == g.start + 1 ? EV_BEGIN : 0u) | (is_cut ? EV_ACC : 0u));
+      const uint32_t pd_bits = s.pd ? s.pd_bits[g.hap][j - 1] : 0u;
+      push(out.fwd, s.codes[g.hap][j - 1] | pd_bits | (j == g.start + 1 ? EV_BEGIN : 0u) | (is_cut ? EV_ACC : 0u));
       auto it = is_cut ? writes.end() : writes.find({i, j});
       if (it != writes.end()) {
-        const uint32_t slot = it->second.second >= 0 ? static_cast<uint32_t>(it->second.second) : kPayloadNone;
-        pending |= EV_SNAP | (it->second.first ? EV_STAGE : 0u) | (slot << kPayloadShift);
+        const uint32_t none = s.pd ? kPdPayloadNone : kPayloadNone;
+        const uint32_t slot = it->second.second >= 0 ? static_cast<uint32_t>(it->second.second) : none;
+        if (it->second.second >= 0 && slot >= none) throw std::invalid_argument("too many snapshot slots for the stream payload");
+        pending |= EV_SNAP | (it->second.first ? EV_STAGE : 0u) | (slot << (s.pd ? kPdPayloadShift : kPayloadShift));
       }
     }
     pending |= g.cut.column >= 0 ? EV_JOIN : EV_END;

@@ -6,6 +6,11 @@
 //   SuffixPlan::new        crates/pairhmm/src/plan.rs:61-89     (cut depths, backward sweeps, node
 //                                                                numbering; MIN_SAVING = 4)
 //   SharedColumns          crates/pairhmm/src/plan.rs:93-113
+//   SortedPdHaps::new      crates/pairhmm/src/pd_kernel.rs:61-136 (sort by row-end deletion state,
+//                                                                then interleaved bases and flags; LCP
+//                                                                only between equal end states;
+//                                                                match-set codes)
+//   segments, MatchSet     crates/pairhmm/src/pd_kernel.rs:699-723, :196-214
 // and turns the result into the column stream the sm_100a kernels walk (program.h).
 #pragma once
 #include <cstdint>
@@ -44,6 +49,27 @@ struct SharedColumns {
   uint64_t prefix_only = 0, forward = 0, backward = 0;
 };
 
+// PD flag bits of a haplotype base (fgkl pd.rs:13-27).
+constexpr uint8_t kPdSnp = 1, kPdDelStart = 2, kPdDelEnd = 4, kPdAltA = 8, kPdAltC = 16, kPdAltG = 32, kPdAltT = 64;
+
+// Whether a read base matches the alternates a flag byte names (pd.rs:99-110).
+bool base_matches_pd(uint8_t read_base, uint8_t flags);
+
+// The read bases a PD column accepts: its own base and, with SNP, the flagged alternates
+// (pd_kernel.rs:196-214).
+struct MatchSet {
+  uint8_t base;
+  uint8_t alts;  // ALT bits; zero without SNP
+  static MatchSet of(uint8_t base, uint8_t flag);
+  bool accepts(uint8_t read_base) const;
+  bool operator==(const MatchSet& o) const { return base == o.base && alts == o.alts; }
+};
+
+// Deletion state of each of a row's `len` columns when the row starts in `state` (kPdNormal,
+// kPdInsideDel, kPdAfterDel); returns the state carried out of the last column
+// (pd_kernel.rs:699-723).
+uint8_t pd_row_states(const uint8_t* flags, int32_t len, uint8_t state, uint8_t* out);
+
 struct SortedHaps {
   std::vector<int32_t> order;  // order[k] = caller index of sorted haplotype k
   std::vector<HapView> bases;  // sorted
@@ -53,9 +79,18 @@ struct SortedHaps {
   std::vector<uint8_t> extra_bases;  // bytes outside ACGTN, first-seen order over sorted haplotypes
   int32_t max_len = 0;
   SuffixPlan plan;
+  // PD-HMM sets only (make_pd): codes index match_sets; pd_bits holds each column's deletion bits
+  // as forward-entry bits (program.h); end_state is the state every row after the first starts in.
+  bool pd = false;
+  std::vector<const uint8_t*> flags;
+  std::vector<MatchSet> match_sets;
+  std::vector<std::vector<uint32_t>> pd_bits;
+  std::vector<uint8_t> end_state;
 
   static SortedHaps make(const std::vector<HapView>& haps, bool share_suffixes);
-  int num_codes() const { return 5 + static_cast<int>(extra_bases.size()); }
+  // Prefix sharing only, as fgkl's PD kernel.
+  static SortedHaps make_pd(const std::vector<HapView>& haps, const std::vector<const uint8_t*>& flags);
+  int num_codes() const { return pd ? static_cast<int>(match_sets.size()) : 5 + static_cast<int>(extra_bases.size()); }
   uint8_t byte_of_code(int code) const;
   SharedColumns columns() const;
 };

@@ -33,6 +33,24 @@ constexpr uint32_t kEvMask = 0x3F00u;
 constexpr int kPayloadShift = 14;
 constexpr uint32_t kPayloadNone = (1u << (32 - kPayloadShift)) - 1;  // no global slot
 
+// PD-HMM forward entries (no suffix sharing, so ACC, JOIN and the backward events are unused) also
+// carry the column's deletion handling, which depends only on the flags (fgkl pd_kernel.rs:1-22):
+// the deletion state of the column in the read's first row and in every later row (rows after the
+// first start in the state the previous row ended in), whether the column carries DEL_END, and
+// whether it carries DEL_START or DEL_END, so its branch values must be kept. Their slot payload
+// starts higher up.
+constexpr uint32_t PD_MAT = 1u << 14;  // keep the column's branch values (DEL_START or DEL_END)
+constexpr uint32_t PD_DE = 1u << 15;   // DEL_END: insertion from the branch values above
+constexpr int kPdFirstShift = 16;      // 2 bits: deletion state in the read's first row
+constexpr int kPdLaterShift = 18;      // 2 bits: deletion state in the later rows
+constexpr uint32_t kPdNormal = 0, kPdInsideDel = 1, kPdAfterDel = 2;
+// Any column a PD lane cannot compute with the plain recurrence.
+constexpr uint32_t kPdSlowMask = PD_MAT | PD_DE | (kPdAfterDel << kPdFirstShift) | (kPdAfterDel << kPdLaterShift);
+constexpr int kPdPayloadShift = 20;
+constexpr uint32_t kPdPayloadNone = (1u << (32 - kPdPayloadShift)) - 1;
+// Read bytes a PD region distinguishes (classes 0..30; 31 marks a padding row).
+constexpr int kPdMaxReadClasses = 31;
+
 // Prior code of haplotype 'N' (codes 0..4 are A, C, G, T, N; extra bytes follow in first-seen
 // order, fgkl kernel.rs:27-107).
 constexpr int kCodeN = 4;
@@ -79,8 +97,10 @@ struct Region {
   int32_t read_off; // first global read index
   int32_t n_reads;
   int64_t out_off;  // first output element (row-major n_reads x n_haps, caller order)
-  int32_t code_off; // 256-entry byte -> prior code table
-  int32_t seq_off;  // sorted haplotypes' prior codes, concatenated (recomputation streams)
+  int32_t code_off; // 256-entry byte -> prior code table (PD: read byte -> read class)
+  int32_t seq_off;  // sorted haplotypes' prior codes (PD: forward entries), concatenated (recomputation streams)
+  int32_t sig_off;  // PD: per match-set code, the bit set of read classes it accepts
+  int32_t pad_;
 };
 
 // Per sorted haplotype: where its result goes and where it comes from.
@@ -125,6 +145,8 @@ struct BatchView {
   const Sweep* sweeps;
   const uint8_t* code_of_byte;
   const uint8_t* hap_codes;  // sorted haplotypes' codes per region
+  const uint32_t* pd_entries;  // PD: sorted haplotypes' forward entries (code and deletion bits) per region
+  const uint32_t* pd_sigs;     // PD: accepted read classes per match-set code
   const double* err_prob;     // 255 entries
   const double* m2m;          // triangular table, 32640 entries
   double* out;

@@ -274,6 +274,51 @@ def plan(haplotypes: Sequence[bytes], share_suffixes: bool = True) -> Plan:
         columns=SharedColumns(int(cols[0]), int(cols[1]), int(cols[2])))
 
 
+# PD deletion states, pd_kernel.rs:31-33.
+NORMAL, INSIDE_DEL, AFTER_DEL = 0, 1, 2
+
+
+def pd_row_states(flags: bytes, start_state: int = NORMAL) -> tuple[list[int], int]:
+    """Per-column deletion states of a row started in ``start_state``, and the state carried out of it
+    (the run boundaries of pd_kernel.rs:699-723, column by column)."""
+    f = _u8(flags) if len(flags) else np.zeros(1, np.uint8)
+    out = np.zeros(max(len(flags), 1), np.uint8)
+    end = lib().fgkl_pd_row_states(_ptr(f, _lib.u8p), len(flags), start_state, _ptr(out, _lib.u8p))
+    if end < 0:
+        _check(end)
+    return [int(x) for x in out[:len(flags)]], int(end)
+
+
+@dataclass
+class PdPlan:
+    order: list[int]
+    lcp: list[int]
+    dup: list[bool]
+    end_state: list[int]
+    num_codes: int
+
+
+def pd_plan(haplotypes: Sequence[PdHaplotype]) -> PdPlan:
+    """The PD sorter's view of a haplotype set (SortedPdHaps::new, pd_kernel.rs:61-136)."""
+    n = len(haplotypes)
+    hb = np.concatenate([_u8(h.bases) for h in haplotypes]) if n else np.zeros(1, np.uint8)
+    hf = np.concatenate([_u8(h.flags) for h in haplotypes]) if n else np.zeros(1, np.uint8)
+    off = np.zeros(n + 1, np.int32)
+    np.cumsum([len(h.bases) for h in haplotypes], out=off[1:])
+    order, lcp = (np.zeros(max(n, 1), np.int32) for _ in range(2))
+    dup, end = (np.zeros(max(n, 1), np.uint8) for _ in range(2))
+    codes = C.c_int32()
+    _check(lib().fgkl_pd_plan_describe(_ptr(hb, _lib.u8p), _ptr(hf, _lib.u8p), _ptr(off, _lib.i32p), n, _ptr(order, _lib.i32p),
+                                       _ptr(lcp, _lib.i32p), _ptr(dup, _lib.u8p), _ptr(end, _lib.u8p), C.byref(codes)))
+    return PdPlan([int(x) for x in order[:n]], [int(x) for x in lcp[:n]], [bool(x) for x in dup[:n]],
+                  [int(x) for x in end[:n]], codes.value)
+
+
+def pd_match_accepts(base: int, flag: int, read_base: int) -> bool:
+    """MatchSet::of(base, flag).accepts(read_base) (pd_kernel.rs:196-214)."""
+    return bool(lib().fgkl_pd_match_accepts(base, flag, read_base))
+
+
 def shared_columns(haplotypes: Sequence[bytes]) -> SharedColumns:
     """lib.rs:296-301."""
     return plan(haplotypes, True).columns

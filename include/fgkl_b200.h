@@ -31,7 +31,7 @@ extern "C" {
 #define FGKL_E_OUTPUT_LENGTH (-5)               /* Error::OutputLength */
 #define FGKL_E_BAD_OFFSETS (-6)                 /* offset table checks of crates/jni/src/lib.rs:343-363 */
 #define FGKL_E_INVALID_ARGUMENT (-7)            /* NULL pointer or negative size */
-#define FGKL_E_UNSUPPORTED (-8)                 /* a read of more than 620 bases */
+#define FGKL_E_UNSUPPORTED (-8)                 /* a read of more than 620 bases; a PD region whose reads hold more than 31 distinct bytes */
 #define FGKL_E_NO_DEVICE (-9)                   /* no CUDA device, or not an sm_100 part */
 #define FGKL_E_CUDA (-10)                       /* CUDA runtime error (message in fgkl_last_error) */
 
@@ -45,7 +45,7 @@ typedef struct fgkl_config {
 /* Counters of one call. */
 typedef struct fgkl_stats {
   uint64_t fallback_pairs;    /* pairs lost by the first pass (PairHmm::fallback_pairs, lib.rs:263-268) */
-  uint64_t rescue_reads;      /* reads recomputed in FP64 */
+  uint64_t rescue_reads;      /* (read, distinct haplotype) pairs recomputed in FP64 without sharing */
   uint64_t nominal_cells;     /* Σ over regions of Σ read lengths x Σ haplotype lengths */
   uint64_t computed_cells;    /* forward + backward DP cells the first pass computed */
   uint64_t forward_cells;
@@ -223,6 +223,19 @@ int fgkl_plan_describe(const uint8_t* hap_bases, const int32_t* hap_offsets, int
  * (depth, node) writes, 2 ints each. */
 int fgkl_plan_sweeps(const uint8_t* hap_bases, const int32_t* hap_offsets, int32_t num_haps, int32_t* sweeps,
                      int32_t max_sweeps, int32_t* writes, int32_t max_writes);
+
+/* ---- PD planner diagnostics (SortedPdHaps::new, segments, MatchSet: pd_kernel.rs:61-136, :196-214,
+ * :699-723) ---- */
+
+/* Deletion state (0 normal, 1 inside a deletion, 2 after one) of each of a row's `len` columns when
+ * the row starts in `start_state`; returns the state carried out of the row, or a negative code. */
+int fgkl_pd_row_states(const uint8_t* flags, int32_t len, int32_t start_state, uint8_t* states);
+/* Sorted order, LCP, duplicate flags and row-end states of a PD haplotype set, and its number of
+ * distinct match-set codes. */
+int fgkl_pd_plan_describe(const uint8_t* hap_bases, const uint8_t* hap_flags, const int32_t* hap_offsets, int32_t num_haps,
+                          int32_t* order, int32_t* lcp, uint8_t* dup, uint8_t* end_state, int32_t* num_codes);
+/* 1 when a PD column of base `base` and flags `flag` accepts `read_base` as a match, else 0. */
+int fgkl_pd_match_accepts(uint8_t base, uint8_t flag, uint8_t read_base);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,213 @@
+"""GPU parity of the PD-HMM against the FP64 PD oracle, through the C ABI.
+
+Restates the reference's own PD tests (crates/pairhmm/src/pd.rs:132-465) with its regions (rebuilt
+draw for draw from their seeds), tolerances (1e-9 log10 in double, 1e-4 in float) and invariants.
+The "every backend" loops collapse to the one sm_100a backend.
+"""
+import numpy as np
+import pytest
+
+from fgkl_b200 import (ALT_C, ALT_G, ALT_T, DEL_END, DEL_START, SNP, BatchContext, Config, PairHmm, PdHaplotype, PdPairHmm,
+                       Precision, Read, synthetic)
+from oracle import oracle as O
+from refgen import Rng
+
+pytestmark = pytest.mark.gpu
+
+FLOAT = Config(precision=Precision.FLOAT)
+DOUBLE = Config(precision=Precision.DOUBLE)
+
+
+def pd_region(seed, num_reads, read_len, num_haps, hap_len):
+    return synthetic.reference_pd_region(seed, num_reads, read_len, num_haps, hap_len).region(0)
+
+
+def reference_all(reads, haps):
+    return O.compute_matrix(reads, haps)
+
+
+def compute_counting(config, reads, haps):
+    hmm = PdPairHmm(config)
+    out = hmm.compute_log10_likelihoods(reads, haps)
+    return out, hmm.fallback_pairs()
+
+
+def compute(config, reads, haps):
+    return compute_counting(config, reads, haps)[0]
+
+
+def assert_close(actual, expected, tol, what=""):
+    assert actual.shape == expected.shape
+    d = np.abs(actual - expected)
+    worst = int(np.argmax(d))
+    assert np.all(d <= tol), f"{what}: pair {worst}: got {actual[worst]}, expected {expected[worst]} (diff {d[worst]})"
+    assert np.isfinite(d).all()
+
+
+def read(bases: bytes):
+    n = len(bases)
+    return Read(bases, bytes([30] * n), bytes([45] * n), bytes([45] * n), bytes([10] * n))
+
+
+def region():
+    return pd_region(31, 70, 120, 24, 300)
+
+
+def test_double_precision_matches_the_pd_reference(gpu):
+    reads, haps = region()
+    assert_close(compute(DOUBLE, reads, haps), reference_all(reads, haps), 1e-9, "double")
+
+
+def test_single_precision_matches_the_pd_reference_within_float_tolerance(gpu):
+    reads, haps = region()
+    assert_close(compute(FLOAT, reads, haps), reference_all(reads, haps), 1e-4, "float")
+
+
+def test_flagged_alternates_and_deletions_change_the_result(gpu):
+    reads, haps = region()
+    unflagged = [PdHaplotype(h.bases, bytes(len(h.bases))) for h in haps]
+    with_flags = compute(DOUBLE, reads, haps)
+    without = compute(DOUBLE, reads, unflagged)
+    changed = int(np.sum(np.abs(with_flags - without) > 1.0))
+    assert changed >= 20, f"{changed} of {with_flags.size} pairs changed"
+    assert np.all(with_flags >= without), "flags never lower a likelihood"
+
+
+def test_haplotypes_without_flags_agree_with_the_plain_kernel(gpu):
+    reads, plain = synthetic.reference_region(5, 40, 100, 8, 200).region(0)
+    pd = [PdHaplotype(h, bytes(len(h))) for h in plain]
+    for precision, tol in ((Precision.DOUBLE, 1e-9), (Precision.FLOAT, 1e-4)):
+        c = Config(precision=precision)
+        assert_close(compute(c, reads, pd), PairHmm(c).compute_log10_likelihoods(reads, plain), tol, str(precision))
+
+
+def test_flags_on_the_last_columns_carry_their_state_into_the_next_row(gpu):
+    hap = b"ACGTTGCAAGGCTTAGGCTTACG"
+    n = len(hap)
+    ends_del = bytearray(n)
+    ends_del[n - 3] = DEL_START
+    ends_del[n - 1] = DEL_END
+    starts_del = bytearray(n)
+    starts_del[n - 1] = DEL_START
+    single_del = bytearray(n)
+    single_del[n - 1] = DEL_START | DEL_END
+    first_del = bytearray(n)
+    first_del[0] = DEL_START | DEL_END
+    first_del[1] = SNP | ALT_G
+    snp = bytearray(n)
+    snp[n - 1] = SNP | ALT_C | ALT_T
+    haps = [PdHaplotype(hap, bytes(f)) for f in (ends_del, starts_del, single_del, first_del, snp)]
+    reads = [read(b"GTTGCAAGGCTTAG"), read(b"GGCTTAGGCTTACG"), read(b"GGCTTAGGCTTC"), read(b"GGCTTAGGCTTA"),
+             read(b"CGTTGCAAGG"), read(hap)]
+    expected = reference_all(reads, haps)
+    assert_close(compute(DOUBLE, reads, haps), expected, 1e-9, "double")
+    assert_close(compute(FLOAT, reads, haps), expected, 1e-4, "float")
+
+
+def test_adjacent_and_single_base_deletions_match_the_reference(gpu):
+    hap = b"ACGTTGCAAGGCTTAGGCTTACGATCGATTACA"
+    n = len(hap)
+    back_to_back = bytearray(n)
+    back_to_back[5] = DEL_START
+    back_to_back[7] = DEL_END
+    back_to_back[8] = DEL_START | DEL_END
+    back_to_back[9] = DEL_START
+    back_to_back[12] = DEL_END
+    singles = bytearray(n)
+    for j in range(3, n, 4):
+        singles[j] = DEL_START | DEL_END
+    snp_in_del = bytearray(n)
+    snp_in_del[10] = DEL_START
+    snp_in_del[11] = SNP | ALT_T
+    snp_in_del[13] = DEL_END | SNP | ALT_G
+    haps = [PdHaplotype(hap, bytes(f)) for f in (back_to_back, singles, snp_in_del)]
+    reads, _ = pd_region(9, 30, 25, 1, 33)
+    assert_close(compute(DOUBLE, reads, haps), reference_all(reads, haps), 1e-9, "double")
+
+
+def test_prefix_sharing_handles_nested_prefixes_lengths_and_flag_splits(gpu):
+    base = b"ACGTTGCAAGGCTTAGGCTTACGATCGATTACAGGT"
+    n = len(base)
+    plain = bytes(n)
+    snp_early = bytearray(n)
+    snp_early[5] = SNP | ALT_T
+    snp_late = bytearray(n)
+    snp_late[30] = SNP | ALT_C
+    del_mid = bytearray(n)
+    del_mid[12] = DEL_START
+    del_mid[15] = DEL_END
+    del_mid_and_snp = bytearray(del_mid)
+    del_mid_and_snp[25] = SNP | ALT_G
+    del_last = bytearray(n)
+    del_last[n - 2] = DEL_START
+    del_last[n - 1] = DEL_END
+    short = base[:20]
+    short_del = bytearray(20)
+    short_del[12] = DEL_START
+    short_del[15] = DEL_END
+    longer = base + b"ACGTAC"
+    longer_flags = bytearray(len(longer))
+    longer_flags[12] = DEL_START
+    longer_flags[15] = DEL_END
+    haps = [PdHaplotype(base, bytes(del_last)), PdHaplotype(base, bytes(snp_late)), PdHaplotype(short, bytes(short_del)),
+            PdHaplotype(base, plain), PdHaplotype(base, bytes(del_mid_and_snp)), PdHaplotype(longer, bytes(longer_flags)),
+            PdHaplotype(base, bytes(del_mid)), PdHaplotype(base, bytes(snp_early)), PdHaplotype(base, plain)]
+    reads, _ = pd_region(13, 40, 30, 1, 36)
+    expected = reference_all(reads, haps)
+    assert_close(compute(DOUBLE, reads, haps), expected, 1e-9, "double")
+    assert_close(compute(FLOAT, reads, haps), expected, 1e-4, "float")
+
+
+def test_haplotype_order_does_not_change_results(gpu):
+    reads, haps = region()
+    fwd = compute(DOUBLE, reads, haps)
+    rev = compute(DOUBLE, reads, haps[::-1])
+    n = len(haps)
+    for r in range(len(reads)):
+        for h in range(n):
+            assert abs(fwd[r * n + h] - rev[r * n + (n - 1 - h)]) < 1e-11, (r, h)
+
+
+def test_float_underflow_falls_back_to_double(gpu):
+    r = Read(b"A" * 80, bytes([40] * 80), bytes([45] * 80), bytes([45] * 80), bytes([10] * 80))
+    flags = bytearray(80)
+    flags[10] = DEL_START
+    flags[20] = DEL_END
+    haps = [PdHaplotype(b"C" * 80, bytes(flags))]
+    expected = reference_all([r], haps)
+    assert np.isfinite(expected[0]) and expected[0] < -50.0
+    out, fallbacks = compute_counting(FLOAT, [r], haps)
+    assert_close(out, expected, 1e-9)
+    assert fallbacks == 1
+
+
+def test_a_read_gets_the_same_bits_whatever_shares_its_batch(gpu):
+    reads, haps = region()
+    alone = reads[:3]
+    rng = Rng(77)
+    batched = list(alone) + [Read(bytes(rng.base() for _ in range(120)), bytes([30] * 120), bytes([45] * 120),
+                                  bytes([45] * 120), bytes([10] * 120)) for _ in range(29)]
+    for precision in (Precision.FLOAT, Precision.DOUBLE):
+        c = Config(precision=precision)
+        solo = compute(c, alone, haps)
+        with_others, fallbacks = compute_counting(c, batched, haps)
+        assert solo.tobytes() == with_others[:solo.size].tobytes(), precision
+        if precision is Precision.FLOAT:
+            assert fallbacks > 0, "the random reads must underflow"
+
+
+@pytest.mark.parametrize("seed,n_reads", [(41, 1), (42, 37), (43, 65)])
+def test_more_reads_than_lanes_and_single_read_both_work(gpu, seed, n_reads):
+    reads, haps = pd_region(seed, n_reads, 50, 3, 60)
+    assert_close(compute(Config(), reads, haps), reference_all(reads, haps), 1e-4, f"{n_reads} reads")
+
+
+def test_pd_batch_of_regions_matches_the_oracle(gpu):
+    parts = [pd_region(100 + i, 20, 90 + 30 * i, 6, 200 + 40 * i) for i in range(4)]
+    w = synthetic.from_regions(parts)
+    ctx = BatchContext()
+    ctx.prepare(w, FLOAT)
+    ctx.run()
+    out, _ = ctx.fetch()
+    expected = np.concatenate([reference_all(r, h) for r, h in parts])
+    assert_close(out, expected, 1e-4, "batched PD")
