@@ -87,6 +87,23 @@ class Batch(C.Structure):
     ]
 
 
+class AdjointBatch(C.Structure):
+    """``fgkl_adjoint_batch``."""
+    _fields_ = [
+        ("num_regions", C.c_int32),
+        ("region_reads", i32p),
+        ("region_haps", i32p),
+        ("bases", u8p),
+        ("read_offsets", i64p),
+        ("gap_open_ins", f64p),
+        ("gap_open_del", f64p),
+        ("gap_continuation", f64p),
+        ("base_error", f64p),
+        ("hap_bases", u8p),
+        ("hap_offsets", i64p),
+    ]
+
+
 class DeviceRegion(C.Structure):
     """``fgkl_device_region``: caller-owned device arrays of one region (allocation-free entry)."""
     _fields_ = [
@@ -148,6 +165,15 @@ def lib() -> C.CDLL:
                                      C.POINTER(C.c_uint64)]
     L.fgkl_plan_sweeps.argtypes = [u8p, i32p, C.c_int32, i32p, C.c_int32, i32p, C.c_int32]
     L.fgkl_probe_fp32_tflops.argtypes = [C.c_int32, f64p, f64p, f64p]
+    L.fgkl_adjoint_prepare.argtypes = [C.c_void_p, C.POINTER(AdjointBatch), C.c_int32]
+    L.fgkl_adjoint_run.argtypes = [C.c_void_p, C.POINTER(C.c_uint64)]
+    L.fgkl_adjoint_fetch.argtypes = [C.c_void_p, f64p, C.c_int64, f64p, f64p, f64p, f64p, C.c_int64, C.POINTER(C.c_uint64)]
+    L.fgkl_adjoint_compute.argtypes = [C.c_void_p, C.POINTER(AdjointBatch), C.c_int32, f64p, C.c_int64, f64p, f64p, f64p, f64p,
+                                       C.c_int64, C.POINTER(C.c_uint64)]
+    L.fgkl_adjoint_output_len.argtypes = [C.c_void_p]
+    L.fgkl_adjoint_output_len.restype = C.c_int64
+    L.fgkl_adjoint_grad_len.argtypes = [C.c_void_p]
+    L.fgkl_adjoint_grad_len.restype = C.c_int64
     L.fgkl_pd_row_states.argtypes = [u8p, C.c_int32, C.c_int32, u8p]
     L.fgkl_pd_plan_describe.argtypes = [u8p, u8p, i32p, C.c_int32, i32p, i32p, u8p, u8p, i32p]
     L.fgkl_pd_match_accepts.argtypes = [C.c_uint8, C.c_uint8, C.c_uint8]
@@ -167,5 +193,6 @@ EXPORTED = [
     "fgkl_backend", "fgkl_last_error", "fgkl_context_create", "fgkl_context_destroy", "fgkl_batch_prepare",
     "fgkl_batch_run", "fgkl_batch_fetch", "fgkl_batch_compute", "fgkl_batch_output_len", "fgkl_synth_config",
     "fgkl_synth_reference_region", "fgkl_synth_view", "fgkl_synth_free", "fgkl_plan_describe", "fgkl_plan_sweeps", "fgkl_probe_fp32_tflops",
-    "fgkl_pairhmm_compute_device_noalloc", "fgkl_pd_row_states", "fgkl_pd_plan_describe", "fgkl_pd_match_accepts",
+    "fgkl_pairhmm_compute_device_noalloc", "fgkl_adjoint_prepare", "fgkl_adjoint_run", "fgkl_adjoint_fetch",
+    "fgkl_adjoint_compute", "fgkl_adjoint_output_len", "fgkl_adjoint_grad_len", "fgkl_pd_row_states", "fgkl_pd_plan_describe", "fgkl_pd_match_accepts",
 ]

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "../../include/fgkl_b200.h"
+#include "adjoint_engine.h"
 #include "engine.h"
 #include "planner.h"
 #include "synthetic.h"
@@ -179,8 +180,12 @@ int noalloc_device(fgkl::NoAllocDevice** out) {
 
 struct fgkl_context {
   std::unique_ptr<fgkl::Engine> engine;
+  std::unique_ptr<fgkl::AdjointEngine> adjoint;  // created on the first adjoint call
   cudaGraphExec_t graph = nullptr;
   bool prepared = false;
+  bool adjoint_prepared = false;
+  int device = 0;
+  cudaStream_t stream = nullptr;
 };
 
 extern "C" {
@@ -220,6 +225,8 @@ fgkl_context* fgkl_context_create(int32_t device, void* stream) {
   }
   auto* ctx = new fgkl_context;
   ctx->engine = std::make_unique<fgkl::Engine>(device, static_cast<cudaStream_t>(stream));
+  ctx->device = device;
+  ctx->stream = ctx->engine->stream();
   return ctx;
 }
 
@@ -419,6 +426,62 @@ int fgkl_plan_sweeps(const uint8_t* hap_bases, const int32_t* hap_offsets, int32
     return set_error(FGKL_E_INVALID_ARGUMENT, e.what());
   }
 }
+
+int fgkl_adjoint_prepare(fgkl_context* ctx, const fgkl_adjoint_batch* b, int32_t double_precision) {
+  t_error.clear();
+  if (!ctx || !b) return set_error(FGKL_E_INVALID_ARGUMENT, "null argument");
+  if (!ctx->adjoint) ctx->adjoint = std::make_unique<fgkl::AdjointEngine>(ctx->device, ctx->stream);
+  fgkl::AdjointInput in;
+  in.num_regions = b->num_regions;
+  in.region_reads = b->region_reads;
+  in.region_haps = b->region_haps;
+  in.bases = b->bases;
+  in.read_off = b->read_offsets;
+  in.d_ins = b->gap_open_ins;
+  in.d_del = b->gap_open_del;
+  in.eps = b->gap_continuation;
+  in.err = b->base_error;
+  in.hap_bases = b->hap_bases;
+  in.hap_off = b->hap_offsets;
+  const int rc = ctx->adjoint->prepare(in, double_precision != 0);
+  ctx->adjoint_prepared = rc == FGKL_OK;
+  return rc ? set_error(rc, ctx->adjoint->error()) : FGKL_OK;
+}
+
+int fgkl_adjoint_run(fgkl_context* ctx, uint64_t* launches) {
+  t_error.clear();
+  if (!ctx || !ctx->adjoint || !ctx->adjoint_prepared) return set_error(FGKL_E_INVALID_ARGUMENT, "no prepared adjoint batch");
+  const int rc = ctx->adjoint->run();
+  if (launches) *launches = ctx->adjoint->launches();
+  return rc ? set_error(rc, ctx->adjoint->error()) : FGKL_OK;
+}
+
+int fgkl_adjoint_fetch(fgkl_context* ctx, double* log10_out, int64_t out_len, double* grad_gap_open_ins,
+                       double* grad_gap_open_del, double* grad_gap_continuation, double* grad_base_error, int64_t grad_len,
+                       uint64_t* fp64_reads) {
+  t_error.clear();
+  if (!ctx || !ctx->adjoint || !ctx->adjoint_prepared) return set_error(FGKL_E_INVALID_ARGUMENT, "no prepared adjoint batch");
+  if ((out_len > 0 && !log10_out) || (grad_len > 0 && (!grad_gap_open_ins || !grad_gap_open_del || !grad_gap_continuation || !grad_base_error)))
+    return set_error(FGKL_E_INVALID_ARGUMENT, "null output");
+  const int rc = ctx->adjoint->fetch(log10_out, out_len, grad_gap_open_ins, grad_gap_open_del, grad_gap_continuation, grad_base_error,
+                                     grad_len, fp64_reads);
+  return rc ? set_error(rc, ctx->adjoint->error()) : FGKL_OK;
+}
+
+int fgkl_adjoint_compute(fgkl_context* ctx, const fgkl_adjoint_batch* b, int32_t double_precision, double* log10_out,
+                         int64_t out_len, double* grad_gap_open_ins, double* grad_gap_open_del, double* grad_gap_continuation,
+                         double* grad_base_error, int64_t grad_len, uint64_t* fp64_reads) {
+  int rc = fgkl_adjoint_prepare(ctx, b, double_precision);
+  if (rc) return rc;
+  if (out_len != ctx->adjoint->output_len() || grad_len != ctx->adjoint->grad_len())
+    return set_error(FGKL_E_OUTPUT_LENGTH, "outputs must hold reads x haplotypes likelihoods and one gradient per read position");
+  if ((rc = fgkl_adjoint_run(ctx, nullptr))) return rc;
+  return fgkl_adjoint_fetch(ctx, log10_out, out_len, grad_gap_open_ins, grad_gap_open_del, grad_gap_continuation, grad_base_error,
+                            grad_len, fp64_reads);
+}
+
+int64_t fgkl_adjoint_output_len(const fgkl_context* ctx) { return ctx && ctx->adjoint ? ctx->adjoint->output_len() : 0; }
+int64_t fgkl_adjoint_grad_len(const fgkl_context* ctx) { return ctx && ctx->adjoint ? ctx->adjoint->grad_len() : 0; }
 
 int fgkl_pd_row_states(const uint8_t* flags, int32_t len, int32_t start_state, uint8_t* states) {
   if (len < 0 || (len > 0 && (!flags || !states)) || start_state < 0 || start_state > 2)

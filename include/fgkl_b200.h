@@ -144,6 +144,48 @@ int fgkl_batch_compute(fgkl_context* ctx, const fgkl_batch* batch, const fgkl_co
 /* Number of likelihoods the prepared batch produces. */
 int64_t fgkl_batch_output_len(const fgkl_context* ctx);
 
+/* ---- adjoint: gradients for fitting the indel and base-error model (no counterpart in the reference) ----
+ *
+ * d(Σ over every read x haplotype pair of log10 L)/d(parameter) for each read position's
+ * continuous parameters: insertion and deletion gap-open probabilities dI, dD (fgkl's MI, MD),
+ * gap continuation eps (II = DD = eps, IM = 1 - eps) and base error e (priors 1 - e and e / 3),
+ * with MM = 1 - dI - dD. fgkl's quantized match-to-match table (crates/pairhmm/src/model.rs:43-45)
+ * agrees with 1 - dI - dD to about 1e-6 but is not differentiable, hence this parameterisation.
+ * Haplotype bytes compare as bytes, N matching everything (reference.rs:20-64).
+ *
+ * Computed with FP32 forward and backward values and FP64 accumulation of the gradients; a read
+ * whose FP32 likelihood falls below 1e-28 against any haplotype is recomputed in FP64
+ * (`fp64_reads` counts them). double_precision = 1 runs everything in FP64. The likelihoods
+ * (log10 L per pair, row-major per region as fgkl_batch_fetch) come out too. Reads of at most 620
+ * bases. The context's stream is used. */
+typedef struct fgkl_adjoint_batch {
+  int32_t num_regions;
+  const int32_t* region_reads;
+  const int32_t* region_haps;
+  const uint8_t* bases;
+  const int64_t* read_offsets;      /* total reads + 1 */
+  const double* gap_open_ins;       /* dI per read position */
+  const double* gap_open_del;       /* dD */
+  const double* gap_continuation;   /* eps */
+  const double* base_error;         /* e */
+  const uint8_t* hap_bases;
+  const int64_t* hap_offsets;       /* total haplotypes + 1 */
+} fgkl_adjoint_batch;
+
+int fgkl_adjoint_prepare(fgkl_context* ctx, const fgkl_adjoint_batch* batch, int32_t double_precision);
+/* Enqueues the adjoint kernels on the context's stream; `launches` (may be NULL) receives their count. */
+int fgkl_adjoint_run(fgkl_context* ctx, uint64_t* launches);
+/* Waits and copies out the likelihoods and the four per-position gradient arrays. */
+int fgkl_adjoint_fetch(fgkl_context* ctx, double* log10_out, int64_t out_len, double* grad_gap_open_ins,
+                       double* grad_gap_open_del, double* grad_gap_continuation, double* grad_base_error, int64_t grad_len,
+                       uint64_t* fp64_reads);
+/* prepare + run + fetch. */
+int fgkl_adjoint_compute(fgkl_context* ctx, const fgkl_adjoint_batch* batch, int32_t double_precision, double* log10_out,
+                         int64_t out_len, double* grad_gap_open_ins, double* grad_gap_open_del, double* grad_gap_continuation,
+                         double* grad_base_error, int64_t grad_len, uint64_t* fp64_reads);
+int64_t fgkl_adjoint_output_len(const fgkl_context* ctx);
+int64_t fgkl_adjoint_grad_len(const fgkl_context* ctx);
+
 /* ---- allocation-free form (no counterpart in the reference) ----
  *
  * The reference has no such entry: its kernels take host slices and allocate per-thread
