@@ -48,6 +48,9 @@ def parse():
     p.add_argument("--per-call-regions", type=int, default=128)
     p.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU work of the oracle sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-extra-configs", action="store_true", help="skip the c2/c3/c4 lines")
+    p.add_argument("--config", default="c1", choices=["c1", "c2", "c3", "c4"],
+                   help="c2/c3/c4: time only that configuration (with --regions to shrink it), for profiling")
     return p.parse_args()
 
 
@@ -210,6 +213,119 @@ def reference_arm(args, rank, world, pg):
 
 
 # ---------------------------------------------------------------------------------------------
+# ncu-measured DRAM traffic of the dominant kernel (profiles/, committed summaries)
+# ---------------------------------------------------------------------------------------------
+
+def dominant_traffic(kernel, cells):
+    """DRAM bytes (read + write) of one launch of `kernel` computing `cells` DP cells: the bytes per
+    computed cell ncu measured for that kernel (committed summary
+    profiles/dram_traffic_pairhmm_kernel_uneven.md, a table row `| kernel | bytes per cell | ...`)
+    times the launch's cells."""
+    path = ROOT / "profiles" / "dram_traffic_pairhmm_kernel_uneven.md"
+    if not path.exists():
+        return None
+    for line in path.read_text().splitlines():
+        row = [c.strip() for c in line.strip().strip("|").split("|")]
+        if len(row) >= 2 and row[0].strip("`") == kernel:
+            try:
+                return float(row[1].replace(",", "")) * cells
+            except ValueError:
+                return None
+    return None
+
+
+# ---------------------------------------------------------------------------------------------
+# the other configurations: device-timed, with an oracle accuracy sample
+# ---------------------------------------------------------------------------------------------
+
+def time_device(stream, flush, fn, steps):
+    import torch
+
+    times = []
+    for _ in range(steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1) / 1e3)
+    return statistics.mean(times)
+
+
+def extra_configs(args, device, stream, flush, threads, which=("c2", "c3", "c4"), regions=0):
+    """c2 (shared SNP haplotypes), c3 (PD-HMM) and c4 (adjoint), one device-timed line each
+    (`regions` > 0 shrinks them, for profiling)."""
+    from fgkl_b200 import BatchContext, Config, Precision, synthetic
+    from fgkl_b200.adjoint import AdjointContext, params_from_quals
+    from oracle import oracle
+
+    steps = max(2, min(args.steps, 3))
+    res = {}
+    for cfg_id, name, note in ((2, "c2", "512 regions x 200 reads (151) x 128 SNP haplotypes (400), FP32 + FP64 recomputation, "
+                                         "prefix+suffix sharing"),
+                               (3, "c3", "PD-HMM: 1024 regions x 64 reads (151) x 16 PD haplotypes (350), 5% SNP flags, 2% "
+                                         "deletions, FP32 + FP64 recomputation, prefix sharing")):
+        if name not in which:
+            continue
+        w = synthetic.workload(cfg_id, seed=args.seed, regions=regions, threads=threads)
+        ctx = BatchContext(device=device, stream=stream.cuda_stream)
+        ctx.prepare(w, Config(precision=Precision.FLOAT))
+        for _ in range(2):
+            ctx.run()
+        t = time_device(stream, flush, ctx.run, steps)
+        out, st = ctx.fetch()
+        nominal = w.nominal_cells()
+        sample = [0]
+        ref = oracle.workload_matrix(w, sample, threads)
+        offs = w.output_offsets()
+        res[name] = {"workload": note, "regions": w.num_regions, "nominal_gcups": nominal / t / 1e9,
+                     "computed_gcups": st.computed_cells / t / 1e9, "ms_per_step": 1e3 * t, "steps": steps,
+                     "nominal_cells": nominal, "computed_cells": int(st.computed_cells),
+                     "prefix_only_cells": int(st.prefix_only_cells), "forward_cells": int(st.forward_cells),
+                     "backward_cells": int(st.backward_cells), "fallback_pairs": int(st.fallback_pairs),
+                     "max_abs_dlog10_sample": float(np.max(np.abs(out[offs[0]:offs[1]] - ref))),
+                     "accuracy_sample": "region 0 against the FP64 oracle"}
+        ctx.close()
+    if "c4" not in which:
+        return res
+    # c4: the adjoint.
+    w = synthetic.workload(4, seed=args.seed, regions=regions, threads=threads)
+    p = params_from_quals(w)
+    actx = AdjointContext(device=device, stream=stream.cuda_stream)
+    actx.prepare(w, p, False)
+    actx.run()
+    t = time_device(stream, flush, actx.run, steps)
+    r = actx.fetch()
+    nominal = w.nominal_cells()
+    # Accuracy sample: region 0's reads against the FP64 scalar adjoint, summed global gradients.
+    n0, h0 = int(w.region_reads[0]), int(w.region_haps[0])
+    lo, hi = int(w.read_offsets[0]), int(w.read_offsets[n0])
+    g_ref = np.zeros((4, hi - lo))
+    for rr in range(n0):
+        a, b = int(w.read_offsets[rr]), int(w.read_offsets[rr + 1])
+        args_ = [x[a:b] for x in (p.gap_open_ins, p.gap_open_del, p.gap_continuation, p.base_error)]
+        for h in range(h0):
+            hap = w.hap_bases[int(w.hap_offsets[h]):int(w.hap_offsets[h + 1])].tobytes()
+            _, *gr = oracle.adj_gradient(hap, w.bases[a:b].tobytes(), *args_)
+            for k in range(4):
+                g_ref[k, a - lo:b - lo] += gr[k]
+    ours_g = [r.gap_open_ins, r.gap_open_del, r.gap_continuation, r.base_error]
+    rel = [abs(ours_g[k][lo:hi].sum() - g_ref[k].sum()) / abs(g_ref[k].sum()) for k in range(4)]
+    res["c4"] = {"workload": "adjoint: 256 regions x 64 reads (151) x 8 haplotypes (350); gradients of the summed log10 "
+                             "likelihood w.r.t. gap-open (ins, del), gap continuation, base error per read position",
+                 "regions": w.num_regions, "nominal_gcups": nominal / t / 1e9, "ms_per_step": 1e3 * t, "steps": steps,
+                 "nominal_cells": nominal, "cells_per_pair_visited": "forward + backward sweep each",
+                 "fp64_reads": r.fp64_reads,
+                 "max_rel_err_global_gradients_sample": max(rel),
+                 "accuracy_sample": "region 0 against the FP64 scalar adjoint (summed gradients)"}
+    actx.close()
+    return res
+
+
+# ---------------------------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------------------------
 
@@ -258,12 +374,31 @@ def ours(args, rank, world, local, pg):
     out, stats = ctx.fetch()
     value = nominal * world / step_max / 1e9
 
-    # Roofline of the first-pass kernels: algorithmic FP32 FLOPs over the measured step time.
+    # Roofline of the dominant kernel: one extra run with the launches serialised on our stream and
+    # CUDA events around each (direct launches, no graph); the launch with the longest duration is the
+    # dominant one; its algorithmic FP32 FLOPs (12 per forward cell, 11 per backward cell) over its
+    # duration, against the FP32 FMA peak measured live on this GPU.
+    with torch.cuda.stream(stream):
+        flush.zero_()
+    ctx.set_profiling(True)
+    ctx.run()
+    launches = ctx.launch_profile()
+    ctx.set_profiling(False)
+    dom = max(launches, key=lambda x: x["ms"])
+    dom_flops = FLOP_FORWARD * dom["forward_cells"] + FLOP_BACKWARD * dom["backward_cells"]
     flops = FLOP_FORWARD * stats.forward_cells + FLOP_BACKWARD * stats.backward_cells
     s_tf, p_tf, clk = C.c_double(), C.c_double(), C.c_double()
     _lib.lib().fgkl_probe_fp32_tflops(device, C.byref(s_tf), C.byref(p_tf), C.byref(clk))
     peak = max(s_tf.value, p_tf.value)
-    achieved = flops / step / 1e12
+    achieved = dom_flops / (dom["ms"] / 1e3) / 1e12
+    step_achieved = flops / step / 1e12
+    kind_names = {0: "PackedF32", 1: "OneF32", 2: "OneF64", 3: "OneF32Pd", 4: "OneF64Pd"}
+    dominant = {"kernel": f"pairhmm_kernel<{kind_names.get(dom['kind'], dom['kind'])}, {dom['rows']}>",
+                "ms": dom["ms"], "tasks": dom["tasks"], "blocks": dom["blocks"],
+                "forward_cells": dom["forward_cells"], "backward_cells": dom["backward_cells"],
+                "share_of_serialised_time": dom["ms"] / max(1e-9, sum(x["ms"] for x in launches)),
+                "serialised_total_ms": sum(x["ms"] for x in launches)}
+    traffic = dominant_traffic(dominant["kernel"], dom["forward_cells"] + dom["backward_cells"])
 
     # End to end: the C-ABI batch call from host buffers (planning, H2D, kernels, D2H).
     h2d = int(w.bases.size * 5 + w.read_offsets.nbytes)
@@ -303,7 +438,7 @@ def ours(args, rank, world, local, pg):
     for reads, haps in pc_regions:
         hmm.compute_log10_likelihoods(reads, haps)
     pc_secs = time.perf_counter() - t0
-    per_call = pc_cells / pc_secs / 1e9
+    per_call = pc_cells / pc_secs / 1e9 if pc_cells else float("nan")
 
     line = {
         "metric": METRIC, "value": value, "unit": "GCUPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -318,10 +453,13 @@ def ours(args, rank, world, local, pg):
         "computed_gcups": stats.computed_cells / step / 1e9,
         "fallback_pairs": int(stats.fallback_pairs), "rescue_reads": int(stats.rescue_reads),
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                     "traffic": None,
+                     "traffic": traffic,
                      "peak_source": f"measured FP32 FMA probe on this GPU (scalar {s_tf.value:.1f}, packed {p_tf.value:.1f} "
                                     "TFLOP/s); MEASURED_PEAKS.json holds no FP32 figure",
-                     "flop_per_cell": {"forward": FLOP_FORWARD, "backward": FLOP_BACKWARD}},
+                     "flop_per_cell": {"forward": FLOP_FORWARD, "backward": FLOP_BACKWARD},
+                     "dominant_launch": dominant,
+                     "whole_step": {"achieved": step_achieved, "frac": step_achieved / peak,
+                                    "note": "all first-pass FLOPs over the whole step (concurrent bins, recomputation)"}},
         "e2e": {"value": e2e_value, "unit": "GCUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "includes": "host planning + pinned staging + H2D + kernels + D2H", "bit_identical_to_device_run": identical,
                 "host_phases_last_step": e2e_phases},
@@ -331,6 +469,9 @@ def ours(args, rank, world, local, pg):
         "gpu_launches": planned_launches * args.steps,
         "clocks": clocks.summary(),
     }
+
+    if not args.no_extra_configs:
+        line["configs"] = extra_configs(args, device, stream, flush, os.cpu_count() or 1)
 
     if not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -353,6 +494,18 @@ def ours(args, rank, world, local, pg):
     barrier(pg, device)
 
 
+def single_config(args, device):
+    """One of the other configurations alone (for profiling); prints its line."""
+    import torch
+
+    torch.cuda.set_device(device)
+    stream = torch.cuda.Stream(device=device)
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=f"cuda:{device}")
+    regions = args.regions if args.regions != 4096 else 0
+    res = extra_configs(args, device, stream, flush, os.cpu_count() or 1, (args.config,), regions)
+    print(json.dumps({"config": args.config, **res[args.config]}), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -360,8 +513,8 @@ def main():
         reference_arm(args, int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), None)
         return
     rank, world, local, pg = dist_init(args.gpus)
-    if False:
-        pass
+    if args.config != "c1":
+        single_config(args, local)
     else:
         ours(args, rank, world, local, pg)
     if pg is not None:

@@ -87,6 +87,11 @@ class Batch(C.Structure):
     ]
 
 
+class LaunchProfile(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("rows", C.c_int32), ("tasks", C.c_int32), ("blocks", C.c_int32),
+                ("recomputation", C.c_int32), ("forward_cells", C.c_uint64), ("backward_cells", C.c_uint64), ("ms", C.c_float)]
+
+
 class AdjointBatch(C.Structure):
     """``fgkl_adjoint_batch``."""
     _fields_ = [
@@ -165,6 +170,8 @@ def lib() -> C.CDLL:
                                      C.POINTER(C.c_uint64)]
     L.fgkl_plan_sweeps.argtypes = [u8p, i32p, C.c_int32, i32p, C.c_int32, i32p, C.c_int32]
     L.fgkl_probe_fp32_tflops.argtypes = [C.c_int32, f64p, f64p, f64p]
+    L.fgkl_context_profile.argtypes = [C.c_void_p, C.c_int32]
+    L.fgkl_batch_launch_profile.argtypes = [C.c_void_p, C.POINTER(LaunchProfile), C.c_int32, C.POINTER(C.c_int32)]
     L.fgkl_adjoint_prepare.argtypes = [C.c_void_p, C.POINTER(AdjointBatch), C.c_int32]
     L.fgkl_adjoint_run.argtypes = [C.c_void_p, C.POINTER(C.c_uint64)]
     L.fgkl_adjoint_fetch.argtypes = [C.c_void_p, f64p, C.c_int64, f64p, f64p, f64p, f64p, C.c_int64, C.POINTER(C.c_uint64)]
@@ -193,6 +200,6 @@ EXPORTED = [
     "fgkl_backend", "fgkl_last_error", "fgkl_context_create", "fgkl_context_destroy", "fgkl_batch_prepare",
     "fgkl_batch_run", "fgkl_batch_fetch", "fgkl_batch_compute", "fgkl_batch_output_len", "fgkl_synth_config",
     "fgkl_synth_reference_region", "fgkl_synth_view", "fgkl_synth_free", "fgkl_plan_describe", "fgkl_plan_sweeps", "fgkl_probe_fp32_tflops",
-    "fgkl_pairhmm_compute_device_noalloc", "fgkl_adjoint_prepare", "fgkl_adjoint_run", "fgkl_adjoint_fetch",
+    "fgkl_pairhmm_compute_device_noalloc", "fgkl_context_profile", "fgkl_batch_launch_profile", "fgkl_adjoint_prepare", "fgkl_adjoint_run", "fgkl_adjoint_fetch",
     "fgkl_adjoint_compute", "fgkl_adjoint_output_len", "fgkl_adjoint_grad_len", "fgkl_pd_row_states", "fgkl_pd_plan_describe", "fgkl_pd_match_accepts",
 ]

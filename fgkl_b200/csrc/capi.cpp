@@ -271,6 +271,11 @@ int fgkl_batch_run(fgkl_context* ctx) {
   fgkl::Engine& e = *ctx->engine;
   if (e.output_len() == 0) return FGKL_OK;
   cudaStream_t s = e.stream();
+  if (e.profiling()) {
+    // Timed launches: direct, so their events can be read back.
+    const int rc = e.run();
+    return rc ? set_error(rc, e.error()) : FGKL_OK;
+  }
   if (!ctx->graph) {
     cudaGraph_t g = nullptr;
     if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
@@ -425,6 +430,27 @@ int fgkl_plan_sweeps(const uint8_t* hap_bases, const int32_t* hap_offsets, int32
   } catch (const std::exception& e) {
     return set_error(FGKL_E_INVALID_ARGUMENT, e.what());
   }
+}
+
+int fgkl_context_profile(fgkl_context* ctx, int32_t on) {
+  t_error.clear();
+  if (!ctx) return set_error(FGKL_E_INVALID_ARGUMENT, "null context");
+  ctx->engine->set_profiling(on != 0);
+  return FGKL_OK;
+}
+
+int fgkl_batch_launch_profile(fgkl_context* ctx, fgkl_launch_profile* out, int32_t max, int32_t* count) {
+  t_error.clear();
+  if (!ctx || !count || (max > 0 && !out)) return set_error(FGKL_E_INVALID_ARGUMENT, "null argument");
+  std::vector<fgkl::Engine::BinProfile> bins;
+  const int rc = ctx->engine->bin_profile(&bins);
+  if (rc) return set_error(rc, ctx->engine->error());
+  *count = static_cast<int32_t>(bins.size());
+  for (int32_t i = 0; i < max && i < *count; ++i) {
+    const auto& b = bins[i];
+    out[i] = fgkl_launch_profile{b.kind, b.rows, b.n_tasks, b.blocks, b.rescue, b.fwd_cells, b.bwd_cells, b.ms};
+  }
+  return FGKL_OK;
 }
 
 int fgkl_adjoint_prepare(fgkl_context* ctx, const fgkl_adjoint_batch* b, int32_t double_precision) {

@@ -194,6 +194,7 @@ Engine::~Engine() {
     cudaEventDestroy(join_[i]);
   }
   cudaEventDestroy(fork_);
+  for (cudaEvent_t e : ev_) cudaEventDestroy(e);
   if (own_stream_) cudaStreamDestroy(stream_);
 }
 
@@ -335,6 +336,7 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
     bool operator<(const Key& o) const { return kind != o.kind ? kind < o.kind : rows < o.rows; }
   };
   std::map<Key, std::vector<std::pair<uint64_t, Task>>> by_bin;
+  std::map<Key, std::pair<uint64_t, uint64_t>> bin_cells;  // forward, backward DP cells per bin
   std::vector<int> order;
   for (int g = 0; g < N; ++g) {
     const int n_reads = in.region_reads[g];
@@ -344,6 +346,12 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
     auto len_of = [&](int r) { return static_cast<int>(in.read_off[first_read[g] + r + 1] - in.read_off[first_read[g] + r]); };
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return len_of(a) > len_of(b); });
     const uint64_t cost_cols = plans[g].prog.fwd.size() + plans[g].prog.bwd.size() + 31;
+    const uint64_t fcols = plans[g].prog.fwd_columns, bcols = plans[g].prog.bwd_columns;
+    auto count = [&](Kind kind, int rows, int len) {
+      auto& c = bin_cells[{kind, rows}];
+      c.first += fcols * static_cast<uint64_t>(len);
+      c.second += bcols * static_cast<uint64_t>(len);
+    };
     size_t i = 0;
     if (pd) {
       // PD: one read per warp, FP32 or FP64.
@@ -351,18 +359,21 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
       for (; i < order.size(); ++i) {
         const int rows = single_rows(len_of(order[i]));
         by_bin[{kind, rows}].push_back({cost_cols * rows, Task{g, {static_cast<int32_t>(first_read[g] + order[i]), -1}, rows, -1}});
+        count(kind, rows, len_of(order[i]));
       }
     } else if (cfg.double_precision || plans[g].extra_codes) {
       for (; i < order.size(); ++i) {
         const int rows = single_rows(len_of(order[i]));
         by_bin[{Kind::kOneF64, rows}].push_back(
             {cost_cols * rows, Task{g, {static_cast<int32_t>(first_read[g] + order[i]), -1}, rows, -1}});
+        count(Kind::kOneF64, rows, len_of(order[i]));
       }
     } else {
       while (i < order.size() && packed_rows(len_of(order[i])) > 8) {
         const int rows = single_rows(len_of(order[i]));
         by_bin[{Kind::kOneF32, rows}].push_back(
             {cost_cols * rows, Task{g, {static_cast<int32_t>(first_read[g] + order[i]), -1}, rows, -1}});
+        count(Kind::kOneF32, rows, len_of(order[i]));
         ++i;
       }
       for (; i < order.size(); i += 2) {
@@ -370,6 +381,7 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
         const int32_t a = static_cast<int32_t>(first_read[g] + order[i]);
         const int32_t b = i + 1 < order.size() ? static_cast<int32_t>(first_read[g] + order[i + 1]) : -1;
         by_bin[{Kind::kPackedF32, rows}].push_back({cost_cols * rows, Task{g, {a, b}, rows, -1}});
+        count(Kind::kPackedF32, rows, len_of(order[i]) + (i + 1 < order.size() ? len_of(order[i + 1]) : 0));
       }
     }
   }
@@ -378,6 +390,8 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
   for (auto& [key, list] : by_bin) {
     std::stable_sort(list.begin(), list.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
     Bin b{key.kind, key.rows, static_cast<int>(tasks.size()), static_cast<int>(list.size()), 0, 0, 0};
+    b.fwd_cells = bin_cells[key].first;
+    b.bwd_cells = bin_cells[key].second;
     uint64_t cost = 0;
     for (auto& e : list) {
       tasks.push_back(e.second);
@@ -568,13 +582,22 @@ int Engine::run() {
   if ((rc = check(cudaMemsetAsync(d_counters_, 0, sizeof(Counters), stream_), "reset counters"))) return rc;
   planned_.kernel_launches = 0;
   int i = 0;
+  if (profile_) {
+    const size_t need = 2 * (bins_.size() + rescue_bins_.size() + 1);
+    while (ev_.size() < need) {
+      cudaEvent_t e;
+      if ((rc = check(cudaEventCreate(&e), "profiling event"))) return rc;
+      ev_.push_back(e);
+    }
+  }
   // Each pass forks its bins onto the auxiliary streams and joins them back.
   auto pass = [&](const std::vector<Bin>& list, bool rescue) -> int {
     if (list.empty()) return FGKL_OK;
     if ((rc = check(cudaEventRecord(fork_, stream_), "fork"))) return rc;
     for (size_t b = 0; b < list.size(); ++b) {
       const Bin& bin = list[b];
-      cudaStream_t s = aux_[b % kAuxStreams];
+      // Profiled runs serialise the launches on the main stream so each one's events time it alone.
+      cudaStream_t s = profile_ ? stream_ : aux_[b % kAuxStreams];
       if ((rc = check(cudaStreamWaitEvent(s, fork_, 0), "fork wait"))) return rc;
       LaunchArgs a{};
       a.v = view_;
@@ -585,8 +608,11 @@ int Engine::run() {
       a.scratch = d_scratch_ + bin.scratch_off;
       a.scratch_stride = bin.stride;
       a.min_accept_plain = (!rescue && !cfg_.double_precision) ? 1 : 0;
+      const int li = i - 1;  // this launch's index, for profiling events
+      if (profile_ && (rc = check(cudaEventRecord(ev_[2 * li], s), "profiling event"))) return rc;
       if ((rc = check(launch(bin.kind, bin.rows, bin.blocks, a, s), rescue ? "recomputation launch" : "first-pass launch")))
         return rc;
+      if (profile_ && (rc = check(cudaEventRecord(ev_[2 * li + 1], s), "profiling event"))) return rc;
       planned_.kernel_launches++;
       if ((rc = check(cudaEventRecord(join_[b % kAuxStreams], s), "join"))) return rc;
     }
@@ -601,6 +627,23 @@ int Engine::run() {
     planned_.kernel_launches++;
   }
   if ((rc = pass(rescue_bins_, true))) return rc;
+  return FGKL_OK;
+}
+
+int Engine::bin_profile(std::vector<BinProfile>* out) {
+  cudaSetDevice(device_);
+  out->clear();
+  if (!profile_) return fail(FGKL_E_INVALID_ARGUMENT, "profiling is off");
+  int rc;
+  if ((rc = check(cudaStreamSynchronize(stream_), "profiled run"))) return rc;
+  int i = 0;
+  for (int pass = 0; pass < 2; ++pass)
+    for (const Bin& b : pass == 0 ? bins_ : rescue_bins_) {
+      float ms = 0.f;
+      if (2 * i + 1 < static_cast<int>(ev_.size())) cudaEventElapsedTime(&ms, ev_[2 * i], ev_[2 * i + 1]);
+      out->push_back(BinProfile{static_cast<int>(b.kind), b.rows, b.n_tasks, b.blocks, pass, b.fwd_cells, b.bwd_cells, ms});
+      ++i;
+    }
   return FGKL_OK;
 }
 

@@ -71,6 +71,18 @@ class Engine {
   // Device pointer to the output, for callers that keep results on the device.
   const double* device_output() const { return d_out_; }
 
+  // Per-launch timing: with profiling on, run() records CUDA events around every launch on the
+  // stream it is issued to (so run() must not be captured); bin_profile() waits and reads them.
+  struct BinProfile {
+    int kind, rows, n_tasks, blocks;
+    int rescue;
+    uint64_t fwd_cells, bwd_cells;
+    float ms;
+  };
+  void set_profiling(bool on) { profile_ = on; }
+  bool profiling() const { return profile_; }
+  int bin_profile(std::vector<BinProfile>* out);
+
  private:
   struct Bin {
     Kind kind;
@@ -80,6 +92,7 @@ class Engine {
     int blocks;
     size_t stride;       // scratch bytes per warp
     size_t scratch_off;  // this bin's slice of the scratch
+    uint64_t fwd_cells = 0, bwd_cells = 0;  // DP cells its tasks compute (first pass)
   };
   static constexpr int kAuxStreams = 8;
   template <class T>
@@ -129,6 +142,8 @@ class Engine {
   std::vector<Bin> bins_, rescue_bins_;
   int64_t out_len_ = 0;
   int n_regions_ = 0;
+  bool profile_ = false;
+  std::vector<cudaEvent_t> ev_;  // begin/end per launch of the last profiled run
   int n_small_ = 0;
 };
 

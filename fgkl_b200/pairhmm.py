@@ -353,6 +353,17 @@ class BatchContext:
         _check(lib().fgkl_batch_fetch(self._ctx, _ptr(out, _lib.f64p), out.size, C.byref(stats)))
         return out, stats
 
+    def set_profiling(self, on: bool) -> None:
+        """Direct launches timed with CUDA events (no graph); see ``launch_profile``."""
+        _check(lib().fgkl_context_profile(self._ctx, int(on)))
+
+    def launch_profile(self) -> list[dict]:
+        """Per launch of the last profiled run: kind, rows, tasks, blocks, recomputation, cells, ms."""
+        arr = (_lib.LaunchProfile * 256)()
+        n = C.c_int32()
+        _check(lib().fgkl_batch_launch_profile(self._ctx, arr, 256, C.byref(n)))
+        return [{f: getattr(arr[i], f) for f, _ in _lib.LaunchProfile._fields_} for i in range(min(n.value, 256))]
+
     def compute(self, workload, config: Config | None = None) -> tuple[np.ndarray, _lib.Stats]:
         self.prepare(workload, config)
         self.run()

@@ -144,6 +144,25 @@ int fgkl_batch_compute(fgkl_context* ctx, const fgkl_batch* batch, const fgkl_co
 /* Number of likelihoods the prepared batch produces. */
 int64_t fgkl_batch_output_len(const fgkl_context* ctx);
 
+/* Per-launch timing for measurement. With profiling on, fgkl_batch_run issues its launches directly
+ * (no CUDA graph), one after another on the context's stream instead of concurrently, with CUDA
+ * events around each, so each is timed alone; fgkl_batch_launch_profile
+ * waits and reports every first-pass and recomputation launch of the last run: kernel kind
+ * (0 packed FP32, 1 FP32, 2 FP64, 3 PD FP32, 4 PD FP64), rows per lane, tasks, blocks, whether it is
+ * a recomputation launch, the forward and backward DP cells its tasks compute, and its duration. */
+typedef struct fgkl_launch_profile {
+  int32_t kind;
+  int32_t rows;
+  int32_t tasks;
+  int32_t blocks;
+  int32_t recomputation;
+  uint64_t forward_cells;
+  uint64_t backward_cells;
+  float ms;
+} fgkl_launch_profile;
+int fgkl_context_profile(fgkl_context* ctx, int32_t on);
+int fgkl_batch_launch_profile(fgkl_context* ctx, fgkl_launch_profile* out, int32_t max, int32_t* count);
+
 /* ---- adjoint: gradients for fitting the indel and base-error model (no counterpart in the reference) ----
  *
  * d(Σ over every read x haplotype pair of log10 L)/d(parameter) for each read position's
