@@ -49,7 +49,7 @@ struct Layout {
   static constexpr int up(int x) { return (x + kRound - 1) / kRound * kRound; }
   static constexpr int kSnap = up(3 * R + 4);  // M, X, Y rows; above-row M, X, Y; accumulated result
   static constexpr int kNode = up(2 * R + 1);  // BM, BY rows; below-row BM
-  static constexpr int kJoin = 2 * R;          // cut column M and Y rows
+  static constexpr int kJoin = up(2 * R);      // cut column M and Y rows
   static constexpr int kStage = kSnap > kNode ? kSnap : kNode;
   // FP32 kernels look priors up in a per-lane table indexed by haplotype code (A, C, G, T, N);
   // regions holding other haplotype bytes run on the FP64 kernel, which compares codes instead.
@@ -335,21 +335,22 @@ __device__ __forceinline__ void forward_step(const LaunchArgs& a, const Program&
       const uint32_t slot = ev >> kPayloadShift;
       V* dst[2] = {slot != kPayloadNone ? sc.slot(static_cast<int>(slot), lane) : nullptr,
                    (ev & EV_STAGE) ? sc.staged(st.seg_i + 1, lane) : nullptr};
+      V rec[L::kSnap];
 #pragma unroll
-      for (int k = 0; k < 2; ++k) {
-        V* o = dst[k];
-        if (!o) continue;
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-          o[r] = st.M[r];
-          o[R + r] = st.X[r];
-          o[2 * R + r] = st.Y[r];
-        }
-        o[3 * R] = dM;
-        o[3 * R + 1] = dX;
-        o[3 * R + 2] = dY;
-        o[3 * R + 3] = st.acc;
+      for (int r = 0; r < R; ++r) {
+        rec[r] = st.M[r];
+        rec[R + r] = st.X[r];
+        rec[2 * R + r] = st.Y[r];
       }
+      rec[3 * R] = dM;
+      rec[3 * R + 1] = dX;
+      rec[3 * R + 2] = dY;
+      rec[3 * R + 3] = st.acc;
+#pragma unroll
+      for (int i = 3 * R + 4; i < L::kSnap; ++i) rec[i] = P::zero();
+#pragma unroll
+      for (int k = 0; k < 2; ++k)
+        if (dst[k]) store_record(dst[k], rec);
     }
     if ((ev & EV_END) && lane == 31) {
 #pragma unroll
@@ -358,12 +359,15 @@ __device__ __forceinline__ void forward_step(const LaunchArgs& a, const Program&
     if (ev & EV_JOIN) {
       // The cut column's match and deletion rows, joined with the backward node after the sweep
       // (fgkl kernel.rs:744-755).
-      V* j = sc.join(st.seg_i, lane);
+      V rec[L::kJoin];
 #pragma unroll
       for (int r = 0; r < R; ++r) {
-        j[r] = st.M[r];
-        j[R + r] = st.Y[r];
+        rec[r] = st.M[r];
+        rec[R + r] = st.Y[r];
       }
+#pragma unroll
+      for (int i = 2 * R; i < L::kJoin; ++i) rec[i] = P::zero();
+      store_record(sc.join(st.seg_i, lane), rec);
     }
     if (ev & EV_BEGIN) {
       ++st.seg_i;
@@ -374,7 +378,8 @@ __device__ __forceinline__ void forward_step(const LaunchArgs& a, const Program&
       const int next_slot = synth ? -1 : rec->next_slot;
       if (!synth && rec->staged) {
         __pipeline_wait_prior(0);
-        const V* s = sc.staged(st.seg_i, lane);
+        V s[L::kSnap];
+        load_record(s, sc.staged(st.seg_i, lane));
 #pragma unroll
         for (int r = 0; r < R; ++r) {
           st.M[r] = s[r];
