@@ -311,9 +311,26 @@ __device__ void backward_pass(const LaunchArgs& a, const Program& prog, const Re
 template <class P, int R>
 struct FwdState {
   using V = typename P::V;
+  using S = typename P::S;
   V M[R], X[R], Y[R];
   V acc;
   int seg_i;
+  // The next segment's record, loaded a segment ahead so a BEGIN never waits on memory.
+  int nx_staged, nx_slot;
+  S nx_init;
+
+  __device__ void load_next(const BatchView& v, const Program& prog, int seg) {
+    if (seg < prog.n_segs) {
+      const Segment* rec = v.segs + prog.seg_off + seg;
+      nx_staged = rec->staged;
+      nx_slot = rec->next_slot;
+      nx_init = P::kDouble ? static_cast<S>(rec->init_d) : static_cast<S>(rec->init_f);
+    } else {
+      nx_staged = 0;
+      nx_slot = -1;
+      nx_init = S(0);
+    }
+  }
 };
 
 // One forward step: events, then the column. (uM, uX, uY) receive the bottom row of the lane above
@@ -373,10 +390,11 @@ __device__ __forceinline__ void forward_step(const LaunchArgs& a, const Program&
       ++st.seg_i;
       // A recomputation stream (FP64 only) has one unshared segment from the origin and no record.
       const bool synth = synth_len > 0;
-      const Segment* rec = a.v.segs + prog.seg_off + st.seg_i;
-      if (!synth && st.seg_i + 1 < prog.n_segs) prefetch_l1(rec + 1);
-      const int next_slot = synth ? -1 : rec->next_slot;
-      if (!synth && rec->staged) {
+      const int next_slot = synth ? -1 : st.nx_slot;
+      const bool staged = !synth && st.nx_staged;
+      const S init = st.nx_init;
+      if (!synth) st.load_next(a.v, prog, st.seg_i + 1);
+      if (staged) {
         __pipeline_wait_prior(0);
         V s[L::kSnap];
         load_record(s, sc.staged(st.seg_i, lane));
@@ -393,8 +411,7 @@ __device__ __forceinline__ void forward_step(const LaunchArgs& a, const Program&
       } else {
         // The origin: nothing but the row-0 constant, in the padding rows (and the row above the
         // lane when that is padding).
-        const S in_s = synth ? static_cast<S>(Consts<P::kDouble>::kInitial / synth_len)
-                             : (P::kDouble ? static_cast<S>(rec->init_d) : static_cast<S>(rec->init_f));
+        const S in_s = synth ? static_cast<S>(Consts<P::kDouble>::kInitial / synth_len) : init;
 #pragma unroll
         for (int r = 0; r < R; ++r) st.M[r] = st.X[r] = st.Y[r] = P::zero();
         dM = dX = dY = st.acc = P::zero();
@@ -466,6 +483,7 @@ __device__ void forward_pass(const LaunchArgs& a, const Program& prog, const Rea
   for (int r = 0; r < R; ++r) st.M[r] = st.X[r] = st.Y[r] = P::zero();
   st.acc = P::zero();
   st.seg_i = -1;
+  st.load_next(a.v, prog, synth_len > 0 ? prog.n_segs : 0);
   V aM = P::zero(), aX = P::zero(), aY = P::zero(), bM = P::zero(), bX = P::zero(), bY = P::zero();
   if (P::kDouble && synth_len > 0) {
     const int n = synth_len;
@@ -842,6 +860,9 @@ __device__ void forward_unshared(const LaunchArgs& a, const ReadRef* rd, int lan
   for (int r = 0; r < R; ++r) st.M[r] = st.X[r] = st.Y[r] = 0.0;
   st.acc = 0.0;
   st.seg_i = -1;
+  st.nx_staged = 0;
+  st.nx_slot = -1;
+  st.nx_init = 0.0;
   const Program prog{};  // unused: the stream is synthesised from the haplotype bytes
   V aM = 0.0, aX = 0.0, aY = 0.0, bM = 0.0, bX = 0.0, bY = 0.0;
   for (int t = 0; t < n + 32; t += 2) {
