@@ -104,11 +104,21 @@ struct AdjBelow {
   __device__ V prior(uint32_t code, int r) const { return (static_cast<int>(code) == oc[r] || code == kCodeN) ? pm[r] : px[r]; }
 };
 
-// Column j's backward values of the warp: [k][r][lane], k = M, X, Y.
-template <class V, int R>
-__device__ __forceinline__ V* adj_column(char* scratch, int j, int lane) {
-  return reinterpret_cast<V*>(scratch) + static_cast<size_t>(j) * 3 * R * 32 + lane;
-}
+// Column j's backward values of one lane: a record of BM, BX, BY rows padded to 16 bytes,
+// [column][lane][record], so a lane stores and fetches its record with 16-byte moves.
+template <class P, int R>
+struct AdjCol {
+  using V = typename P::V;
+  static constexpr int kPer16 = 16 / static_cast<int>(sizeof(V));
+  static constexpr int kRec = (3 * R + kPer16 - 1) / kPer16 * kPer16;
+  // Columns fetched ahead of the forward sweep into a per-warp shared-memory ring (about 16 KB).
+  static constexpr int kDepthRaw = 16384 / (32 * kRec * static_cast<int>(sizeof(V)));
+  static constexpr int kDepth = kDepthRaw < 2 ? 2 : (kDepthRaw > 8 ? 8 : kDepthRaw);
+  static constexpr size_t kRingBytes = static_cast<size_t>(kDepth) * 32 * kRec * sizeof(V);
+  __device__ static V* at(char* scratch, int j, int lane) {
+    return reinterpret_cast<V*>(scratch) + (static_cast<size_t>(j) * 32 + lane) * kRec;
+  }
+};
 
 // Backward sweep of one pair; returns, in every lane, the padding row's start mass s.
 template <class P, int R>
@@ -126,6 +136,13 @@ __device__ typename P::V adj_backward(const AdjView& v, const AdjRows<P, R>& own
   const int pad_row = pad - 1;  // the padding row right above the read
   const int pad_lane = pad_row / R, pad_r = pad_row % R;
   V start_mass = P::zero();
+  // The base of column j + 1 (the diagonal successor) for position p, none beyond the haplotype;
+  // loaded one step ahead.
+  auto code_at = [&](int q) -> uint32_t {
+    const int jj = m - q;
+    return (q >= 0 && jj >= 0 && jj < m) ? adj_code(__ldg(hap + jj)) : 0u;
+  };
+  uint32_t next_code = code_at(-(31 - lane));
   for (int t = 0; t < m + 1 + 31; ++t) {
     const V rBM = P::down(topBM), rBX = P::down(topBX);
     const int p = t - (31 - lane);  // position: column m - p
@@ -136,9 +153,10 @@ __device__ typename P::V adj_backward(const AdjView& v, const AdjRows<P, R>& own
       for (int r = 0; r < R; ++r) BM[r] = BY[r] = P::zero();
       dBM = P::zero();
     }
-    // The base of column j + 1 (the diagonal successor); none beyond the haplotype.
-    const uint32_t code = (p >= 0 && j >= 0 && j < m) ? adj_code(__ldg(hap + j)) : 0u;
-    V* col = (p >= 0 && j >= 1) ? adj_column<V, R>(scratch, j, lane) : nullptr;
+    const uint32_t code = next_code;
+    next_code = code_at(p + 1);
+    using Col = AdjCol<P, R>;
+    V rec[Col::kRec];
     V belowX = rBX, diagM = dBM;
 #pragma unroll
     for (int r = R - 1; r >= 0; --r) {
@@ -155,12 +173,13 @@ __device__ typename P::V adj_backward(const AdjView& v, const AdjRows<P, R>& own
       BM[r] = bm;
       BY[r] = by;
       belowX = bx;
-      if (col) {
-        col[(0 * R + r) * 32] = bm;
-        col[(1 * R + r) * 32] = bx;
-        col[(2 * R + r) * 32] = by;
-      }
+      rec[r] = bm;
+      rec[R + r] = bx;
+      rec[2 * R + r] = by;
     }
+#pragma unroll
+    for (int i = 3 * R; i < Col::kRec; ++i) rec[i] = P::zero();
+    if (p >= 0 && j >= 1) store_record(Col::at(scratch, j, lane), rec);
     if (p == m && lane == pad_lane) {
 #pragma unroll
       for (int r = 0; r < R; ++r)
@@ -176,16 +195,35 @@ __device__ typename P::V adj_backward(const AdjView& v, const AdjRows<P, R>& own
 // Forward sweep of one pair, accumulating the pair's gradient terms scaled by `norm`; returns the
 // raw result (lane 31).
 template <class P, int R>
-__device__ typename P::V adj_forward(const AdjRows<P, R>& own, int pad, const uint8_t* hap, int m, int lane, const char* scratch,
-                                     double norm, double (&gi)[R], double (&gd)[R], double (&ge)[R], double (&gq)[R]) {
+__device__ typename P::V adj_forward(const AdjRows<P, R>& own, int pad, const uint8_t* hap, int m, int lane, char* scratch,
+                                     typename P::V* ring, double norm, double (&gi)[R], double (&gd)[R], double (&ge)[R],
+                                     double (&gq)[R]) {
   using V = typename P::V;
   using S = typename P::S;
+  using Col = AdjCol<P, R>;
+  constexpr int D = Col::kDepth;
   const S init = static_cast<S>(Consts<P::kDouble>::kInitial / m);
   V M[R], X[R], Y[R];
 #pragma unroll
   for (int r = 0; r < R; ++r) M[r] = X[r] = Y[r] = P::zero();
   V acc = P::zero();
   V dM = P::zero(), dX = P::zero(), dY = P::zero();
+  // The lane's k-th forward column (k = 0..m-1, column k + 1) sits in ring slot k % D; columns are
+  // fetched D ahead with cp.async, one commit group per column.
+  auto slot = [&](int k) { return ring + (static_cast<size_t>(k % D) * 32 + lane) * Col::kRec; };
+  auto fetch = [&](int k) {
+    if (k < m) {
+      const V* src = Col::at(scratch, k + 1, lane);
+      V* dst = slot(k);
+#pragma unroll
+      for (int i = 0; i < Col::kRec / Col::kPer16; ++i)
+        __pipeline_memcpy_async(reinterpret_cast<char*>(dst) + 16 * i, reinterpret_cast<const char*>(src) + 16 * i, 16);
+    }
+    __pipeline_commit();
+  };
+#pragma unroll
+  for (int k = 0; k < D; ++k) fetch(k);
+  uint32_t next_code = (m > 0 && lane == 0) ? adj_code(__ldg(hap)) : 0u;
   for (int t = 0; t < m + 31; ++t) {
     const V uM = P::up(M[R - 1]), uX = P::up(X[R - 1]), uY = P::up(Y[R - 1]);
     const int p = t - lane;  // column p + 1
@@ -201,14 +239,22 @@ __device__ typename P::V adj_forward(const AdjRows<P, R>& own, int pad, const ui
       acc = P::zero();
     }
     const bool live = p >= 0 && p < m;
-    const uint32_t code = live ? adj_code(__ldg(hap + p)) : 0u;
-    const V* col = live ? adj_column<V, R>(const_cast<char*>(scratch), p + 1, lane) : nullptr;
+    const uint32_t code = next_code;
+    next_code = (p + 1 >= 0 && p + 1 < m) ? adj_code(__ldg(hap + p + 1)) : 0u;
     V bM[R], bX[R], bY[R];
+    if (live) {
+      __pipeline_wait_prior(D - 1);
+      V rec[Col::kRec];
+      load_record(rec, slot(p));
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-      bM[r] = col ? col[(0 * R + r) * 32] : P::zero();
-      bX[r] = col ? col[(1 * R + r) * 32] : P::zero();
-      bY[r] = col ? col[(2 * R + r) * 32] : P::zero();
+      for (int r = 0; r < R; ++r) {
+        bM[r] = rec[r];
+        bX[r] = rec[R + r];
+        bY[r] = rec[2 * R + r];
+      }
+    } else {
+#pragma unroll
+      for (int r = 0; r < R; ++r) bM[r] = bX[r] = bY[r] = P::zero();
     }
     // Match and deletion values from the bottom row up (each row reads the old row above).
 #pragma unroll
@@ -241,11 +287,15 @@ __device__ typename P::V adj_forward(const AdjRows<P, R>& own, int pad, const ui
         ge[r] += static_cast<double>(qX) * bx_n;
       }
     }
-    if (live) acc = P::add(acc, P::add(M[R - 1], X[R - 1]));
+    if (live) {
+      acc = P::add(acc, P::add(M[R - 1], X[R - 1]));
+      fetch(p + D);  // into the slot just read (its values are consumed above)
+    }
     dM = uM;
     dX = uX;
     dY = uY;
   }
+  __pipeline_wait_prior(0);
   return __shfl_sync(kFull, acc, 31);
 }
 
@@ -257,9 +307,11 @@ struct AdjMinBlocks {
 template <class P, int R>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, (AdjMinBlocks<P, R>::value)) adjoint_kernel(AdjLaunch a) {
   using C = Consts<P::kDouble>;
+  extern __shared__ __align__(16) unsigned char adj_smem[];
   const int lane = threadIdx.x & 31;
   const int warp = blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
   char* scratch = a.scratch + static_cast<size_t>(warp) * a.scratch_stride;
+  typename P::V* ring = reinterpret_cast<typename P::V*>(adj_smem + (threadIdx.x >> 5) * AdjCol<P, R>::kRingBytes);
   const int count = a.count ? min(*a.count, a.n_tasks) : a.n_tasks;
   const double ln10 = 2.302585092994045684017991454684364208;
   for (;;) {
@@ -292,8 +344,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, (AdjMinBlocks<P, R>::valu
         break;
       }
       const double norm = 1.0 / ((C::kInitial / m) * s * ln10);
+      // The lane's backward records are fetched back by its own asynchronous copies.
+      __threadfence_block();
       __syncwarp();
-      const double fwd = static_cast<double>(adj_forward<P, R>(own, pad, hap, m, lane, scratch, norm, gi, gd, ge, gq));
+      const double fwd = static_cast<double>(adj_forward<P, R>(own, pad, hap, m, lane, scratch, ring, norm, gi, gd, ge, gq));
       if (!P::kDouble && (!(fwd >= C::kMinAccepted) || isinf(fwd))) {
         lost = true;
         break;
@@ -326,12 +380,15 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, (AdjMinBlocks<P, R>::valu
 
 template <class P, int R>
 void adj_occ(int* blocks) {
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, adjoint_kernel<P, R>, kWarpsPerBlock * 32, 0);
+  const size_t smem = kWarpsPerBlock * AdjCol<P, R>::kRingBytes;
+  cudaFuncSetAttribute(adjoint_kernel<P, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, adjoint_kernel<P, R>, kWarpsPerBlock * 32, smem);
 }
 
 template <class P, int R>
 cudaError_t adj_go(int blocks, const AdjLaunch& a, cudaStream_t s) {
-  adjoint_kernel<P, R><<<blocks, kWarpsPerBlock * 32, 0, s>>>(a);
+  const size_t smem = kWarpsPerBlock * AdjCol<P, R>::kRingBytes;
+  adjoint_kernel<P, R><<<blocks, kWarpsPerBlock * 32, smem, s>>>(a);
   return cudaGetLastError();
 }
 
@@ -358,7 +415,9 @@ auto adj_dispatch_rows(int rows, F&& f) {
 }  // namespace
 
 size_t adj_scratch_bytes(bool dbl, int rows, int max_hap_len) {
-  return static_cast<size_t>(max_hap_len + 1) * 3 * rows * 32 * (dbl ? sizeof(double) : sizeof(float));
+  const size_t rec = dbl ? adj_dispatch_rows(rows, [](auto r) { return static_cast<size_t>(AdjCol<OneF64, decltype(r)::value>::kRec); })
+                         : adj_dispatch_rows(rows, [](auto r) { return static_cast<size_t>(AdjCol<OneF32, decltype(r)::value>::kRec); });
+  return static_cast<size_t>(max_hap_len + 1) * 32 * rec * (dbl ? sizeof(double) : sizeof(float));
 }
 
 void adj_occupancy(bool dbl, int rows, int* blocks, int* threads) {
