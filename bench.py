@@ -277,6 +277,11 @@ def extra_configs(args, device, stream, flush, threads, which=("c2", "c3", "c4")
             ctx.run()
         t = time_device(stream, flush, ctx.run, steps)
         out, st = ctx.fetch()
+        # Where the step goes: one serialised run with every launch timed by CUDA events.
+        ctx.set_profiling(True)
+        ctx.run()
+        prof = ctx.launch_profile()
+        ctx.set_profiling(False)
         nominal = w.nominal_cells()
         sample = [0]
         ref = oracle.workload_matrix(w, sample, threads)
@@ -286,6 +291,8 @@ def extra_configs(args, device, stream, flush, threads, which=("c2", "c3", "c4")
                      "nominal_cells": nominal, "computed_cells": int(st.computed_cells),
                      "prefix_only_cells": int(st.prefix_only_cells), "forward_cells": int(st.forward_cells),
                      "backward_cells": int(st.backward_cells), "fallback_pairs": int(st.fallback_pairs),
+                     "serialised_ms": {"first_pass": sum(x["ms"] for x in prof if not x["recomputation"]),
+                                       "fp64_recomputation": sum(x["ms"] for x in prof if x["recomputation"])},
                      "max_abs_dlog10_sample": float(np.max(np.abs(out[offs[0]:offs[1]] - ref))),
                      "accuracy_sample": "region 0 against the FP64 oracle"}
         ctx.close()
@@ -392,7 +399,7 @@ def ours(args, rank, world, local, pg):
     peak = max(s_tf.value, p_tf.value)
     achieved = dom_flops / (dom["ms"] / 1e3) / 1e12
     step_achieved = flops / step / 1e12
-    kind_names = {0: "PackedF32", 1: "OneF32", 2: "OneF64", 3: "OneF32Pd", 4: "OneF64Pd"}
+    kind_names = {0: "PackedF32", 1: "OneF32", 2: "OneF64", 3: "OneF32Pd", 4: "OneF64Pd", 5: "PackedF32Pd"}
     dominant = {"kernel": f"pairhmm_kernel<{kind_names.get(dom['kind'], dom['kind'])}, {dom['rows']}>",
                 "ms": dom["ms"], "tasks": dom["tasks"], "blocks": dom["blocks"],
                 "forward_cells": dom["forward_cells"], "backward_cells": dom["backward_cells"],

@@ -353,13 +353,29 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
       c.second += bcols * static_cast<uint64_t>(len);
     };
     size_t i = 0;
-    if (pd) {
-      // PD: one read per warp, FP32 or FP64.
-      const Kind kind = cfg.double_precision ? Kind::kOneF64Pd : Kind::kOneF32Pd;
+    if (pd && cfg.double_precision) {
+      // PD in FP64: one read per warp.
       for (; i < order.size(); ++i) {
         const int rows = single_rows(len_of(order[i]));
-        by_bin[{kind, rows}].push_back({cost_cols * rows, Task{g, {static_cast<int32_t>(first_read[g] + order[i]), -1}, rows, -1}});
-        count(kind, rows, len_of(order[i]));
+        by_bin[{Kind::kOneF64Pd, rows}].push_back(
+            {cost_cols * rows, Task{g, {static_cast<int32_t>(first_read[g] + order[i]), -1}, rows, -1}});
+        count(Kind::kOneF64Pd, rows, len_of(order[i]));
+      }
+    } else if (pd) {
+      // PD in FP32: reads above 248 bases one per warp, the others in pairs (FP32x2).
+      while (i < order.size() && packed_rows(len_of(order[i])) > 8) {
+        const int rows = single_rows(len_of(order[i]));
+        by_bin[{Kind::kOneF32Pd, rows}].push_back(
+            {cost_cols * rows, Task{g, {static_cast<int32_t>(first_read[g] + order[i]), -1}, rows, -1}});
+        count(Kind::kOneF32Pd, rows, len_of(order[i]));
+        ++i;
+      }
+      for (; i < order.size(); i += 2) {
+        const int rows = packed_rows(len_of(order[i]));
+        const int32_t a = static_cast<int32_t>(first_read[g] + order[i]);
+        const int32_t b = i + 1 < order.size() ? static_cast<int32_t>(first_read[g] + order[i + 1]) : -1;
+        by_bin[{Kind::kPackedF32Pd, rows}].push_back({cost_cols * rows, Task{g, {a, b}, rows, -1}});
+        count(Kind::kPackedF32Pd, rows, len_of(order[i]) + (i + 1 < order.size() ? len_of(order[i + 1]) : 0));
       }
     } else if (cfg.double_precision || plans[g].extra_codes) {
       for (; i < order.size(); ++i) {

@@ -771,6 +771,8 @@ bool valid_rows(Kind k, int rows) {
     case Kind::kOneF32Pd:
     case Kind::kOneF64Pd:
       return (rows >= 1 && rows <= 8) || (rows >= 10 && rows <= 20 && rows % 2 == 0);
+    case Kind::kPackedF32Pd:
+      return rows >= 1 && rows <= 8;
   }
   return false;
 }
@@ -781,7 +783,7 @@ int max_rows(Kind) { return 20; }
 
 size_t scratch_bytes(Kind k, int rows, int max_slots, int max_nodes, int max_segs) {
   if (!valid_rows(k, rows)) return 0;
-  if (is_pd(k)) return pd_scratch_bytes(k == Kind::kOneF64Pd, rows, max_slots, max_segs);
+  if (is_pd(k)) return pd_scratch_bytes(pd_form(k), rows, max_slots, max_segs);
   return dispatch<SizeF>(k, rows, max_slots, max_nodes, max_segs);
 }
 
@@ -789,7 +791,7 @@ void occupancy(Kind k, int rows, int* blocks, int* threads) {
   *blocks = 0;
   *threads = kWarpsPerBlock * 32;
   if (!valid_rows(k, rows)) return;
-  if (is_pd(k)) return pd_occupancy(k == Kind::kOneF64Pd, rows, blocks, threads);
+  if (is_pd(k)) return pd_occupancy(pd_form(k), rows, blocks, threads);
   dispatch<OccF>(k, rows, blocks, threads);
 }
 
@@ -801,7 +803,7 @@ cudaError_t launch_collect(const CollectArgs& args, int n_regions, cudaStream_t 
 
 cudaError_t launch(Kind k, int rows, int blocks, const LaunchArgs& args, cudaStream_t stream) {
   if (!valid_rows(k, rows)) return cudaErrorInvalidValue;
-  if (is_pd(k)) return pd_launch(k == Kind::kOneF64Pd, rows, blocks, args, stream);
+  if (is_pd(k)) return pd_launch(pd_form(k), rows, blocks, args, stream);
   return dispatch<GoF>(k, rows, blocks, args, stream);
 }
 

@@ -13,9 +13,16 @@ enum class Kind : int {
   kOneF64 = 2,     // one read, FP64, rows-per-lane 1..8 and 10..20 (even)
   kOneF32Pd = 3,   // PD-HMM, one read, FP32, rows-per-lane 1..8 and 10..20 (even)
   kOneF64Pd = 4,   // PD-HMM, one read, FP64, same rows
+  kPackedF32Pd = 5,  // PD-HMM, two reads per lane set in FP32x2, rows-per-lane 1..8
 };
 
-inline bool is_pd(Kind k) { return k == Kind::kOneF32Pd || k == Kind::kOneF64Pd; }
+inline bool is_pd(Kind k) { return k == Kind::kOneF32Pd || k == Kind::kOneF64Pd || k == Kind::kPackedF32Pd; }
+
+// The PD instantiation a PD kind selects.
+enum class PdForm : int { kOneF32 = 0, kOneF64 = 1, kPackedF32 = 2 };
+inline PdForm pd_form(Kind k) {
+  return k == Kind::kOneF64Pd ? PdForm::kOneF64 : (k == Kind::kPackedF32Pd ? PdForm::kPackedF32 : PdForm::kOneF32);
+}
 
 struct LaunchArgs {
   BatchView v;
@@ -44,10 +51,10 @@ size_t scratch_bytes(Kind k, int rows, int max_slots, int max_nodes, int max_seg
 void occupancy(Kind k, int rows, int* blocks_per_sm, int* threads_per_block);
 // Launches one persistent grid of `blocks` blocks.
 cudaError_t launch(Kind k, int rows, int blocks, const LaunchArgs& args, cudaStream_t stream);
-// PD-HMM instantiations (pd_kernels.cu); `dbl` selects FP64.
-size_t pd_scratch_bytes(bool dbl, int rows, int max_slots, int max_segs);
-void pd_occupancy(bool dbl, int rows, int* blocks_per_sm, int* threads_per_block);
-cudaError_t pd_launch(bool dbl, int rows, int blocks, const LaunchArgs& args, cudaStream_t stream);
+// PD-HMM instantiations (pd_kernels.cu).
+size_t pd_scratch_bytes(PdForm form, int rows, int max_slots, int max_segs);
+void pd_occupancy(PdForm form, int rows, int* blocks_per_sm, int* threads_per_block);
+cudaError_t pd_launch(PdForm form, int rows, int blocks, const LaunchArgs& args, cudaStream_t stream);
 
 // Launches the lost-pair collection over `n_regions` regions.
 cudaError_t launch_collect(const CollectArgs& args, int n_regions, cudaStream_t stream);

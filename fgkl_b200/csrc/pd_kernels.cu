@@ -234,7 +234,10 @@ __device__ __forceinline__ void pd_step(const LaunchArgs& a, const Program& prog
       if (next_slot >= 0) prefetch(sc.staged(st.seg_i + 1, lane), sc.slot(next_slot, lane), L::kSnap);
     }
   }
-  if (ev & kPdSlowMask) {
+  // Some lane is nearly always at a column carrying DEL_START or DEL_END or right after a deletion;
+  // the general path is exact for every column, so the warp takes it whenever any lane needs it
+  // rather than running both paths divergently.
+  if (__any_sync(kFull, (ev & kPdSlowMask) != 0)) {
     // A column carrying DEL_START or DEL_END, or right after a deletion.
     const bool mat = (ev & PD_MAT) != 0, de = (ev & PD_DE) != 0;
     const uint32_t s_first = (ev >> kPdFirstShift) & 3u, s_later = (ev >> kPdLaterShift) & 3u;
@@ -386,7 +389,7 @@ __device__ void pd_finalize(const LaunchArgs& a, const Task& task, const Region&
 
 template <class P, int R>
 struct PdMinBlocks {
-  static constexpr int value = P::kDouble ? 1 : 2;
+  static constexpr int value = P::kDouble ? 1 : 2;  // the packed form (two reads) too: up to 255 registers
 };
 
 template <class P, int R>
@@ -471,31 +474,68 @@ auto pd_rows(int rows, F&& f) {
   }
 }
 
+
+// Rows 1..8 only (the packed two-read form).
+template <class F>
+auto pd_rows8(int rows, F&& f) {
+  switch (rows) {
+    case 1: return f(std::integral_constant<int, 1>{});
+    case 2: return f(std::integral_constant<int, 2>{});
+    case 3: return f(std::integral_constant<int, 3>{});
+    case 4: return f(std::integral_constant<int, 4>{});
+    case 5: return f(std::integral_constant<int, 5>{});
+    case 6: return f(std::integral_constant<int, 6>{});
+    case 7: return f(std::integral_constant<int, 7>{});
+    default: return f(std::integral_constant<int, 8>{});
+  }
+}
+
 }  // namespace
 
-size_t pd_scratch_bytes(bool dbl, int rows, int max_slots, int max_segs) {
-  if (dbl) return pd_rows<OneF64>(rows, [&](auto r) { return pd_scratch_size<OneF64, decltype(r)::value>(max_slots, max_segs); });
-  return pd_rows<OneF32>(rows, [&](auto r) { return pd_scratch_size<OneF32, decltype(r)::value>(max_slots, max_segs); });
+size_t pd_scratch_bytes(PdForm form, int rows, int max_slots, int max_segs) {
+  switch (form) {
+    case PdForm::kOneF64:
+      return pd_rows<OneF64>(rows, [&](auto r) { return pd_scratch_size<OneF64, decltype(r)::value>(max_slots, max_segs); });
+    case PdForm::kPackedF32:
+      return pd_rows8(rows, [&](auto r) { return pd_scratch_size<PackedF32, decltype(r)::value>(max_slots, max_segs); });
+    default:
+      return pd_rows<OneF32>(rows, [&](auto r) { return pd_scratch_size<OneF32, decltype(r)::value>(max_slots, max_segs); });
+  }
 }
 
-void pd_occupancy(bool dbl, int rows, int* blocks, int* threads) {
+void pd_occupancy(PdForm form, int rows, int* blocks, int* threads) {
   *threads = kWarpsPerBlock * 32;
   *blocks = 0;
-  if (dbl)
-    pd_rows<OneF64>(rows, [&](auto r) {
-      pd_occ<OneF64, decltype(r)::value>(blocks);
-      return 0;
-    });
-  else
-    pd_rows<OneF32>(rows, [&](auto r) {
-      pd_occ<OneF32, decltype(r)::value>(blocks);
-      return 0;
-    });
+  switch (form) {
+    case PdForm::kOneF64:
+      pd_rows<OneF64>(rows, [&](auto r) {
+        pd_occ<OneF64, decltype(r)::value>(blocks);
+        return 0;
+      });
+      break;
+    case PdForm::kPackedF32:
+      pd_rows8(rows, [&](auto r) {
+        pd_occ<PackedF32, decltype(r)::value>(blocks);
+        return 0;
+      });
+      break;
+    default:
+      pd_rows<OneF32>(rows, [&](auto r) {
+        pd_occ<OneF32, decltype(r)::value>(blocks);
+        return 0;
+      });
+  }
 }
 
-cudaError_t pd_launch(bool dbl, int rows, int blocks, const LaunchArgs& a, cudaStream_t s) {
-  if (dbl) return pd_rows<OneF64>(rows, [&](auto r) { return pd_go<OneF64, decltype(r)::value>(blocks, a, s); });
-  return pd_rows<OneF32>(rows, [&](auto r) { return pd_go<OneF32, decltype(r)::value>(blocks, a, s); });
+cudaError_t pd_launch(PdForm form, int rows, int blocks, const LaunchArgs& a, cudaStream_t s) {
+  switch (form) {
+    case PdForm::kOneF64:
+      return pd_rows<OneF64>(rows, [&](auto r) { return pd_go<OneF64, decltype(r)::value>(blocks, a, s); });
+    case PdForm::kPackedF32:
+      return pd_rows8(rows, [&](auto r) { return pd_go<PackedF32, decltype(r)::value>(blocks, a, s); });
+    default:
+      return pd_rows<OneF32>(rows, [&](auto r) { return pd_go<OneF32, decltype(r)::value>(blocks, a, s); });
+  }
 }
 
 }  // namespace fgkl
