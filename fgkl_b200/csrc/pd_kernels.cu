@@ -75,10 +75,10 @@ struct PdRows {
   using V = typename P::V;
   using S = typename P::S;
   V c0[R], c1[R], c2[R], c3[R], c4[R], pm[R], px[R];
-  int cls[P::NC][R];  // read class of the row's base; 31 for a padding row (no code accepts it)
+  uint32_t cls[P::NC][R];  // bit of the row's read class; 0 for a padding row (no code accepts it)
 
   __device__ V prior(uint32_t sig, int r) const {
-    return P::sel((sig >> cls[0][r]) & 1u, (sig >> cls[P::NC - 1][r]) & 1u, pm[r], px[r]);
+    return P::sel((sig & cls[0][r]) != 0u, (sig & cls[P::NC - 1][r]) != 0u, pm[r], px[r]);
   }
 
   __device__ void load(const BatchView& v, const ReadRef* rd, int lane, const uint8_t* classes) {
@@ -118,7 +118,7 @@ struct PdRows {
         P::put(c4[r], c, static_cast<S>(k4));
         P::put(pm[r], c, static_cast<S>(m.pm));
         P::put(px[r], c, static_cast<S>(m.px));
-        cls[c][r] = m.read ? (m.oc & 31) : 31;
+        cls[c][r] = m.read ? (1u << (m.oc & 31)) : 0u;
       }
     }
   }
