@@ -46,7 +46,10 @@ def parse():
     p.add_argument("--regions", type=int, default=4096)
     p.add_argument("--seed", type=int, default=1)
     p.add_argument("--per-call-regions", type=int, default=128)
-    p.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU work of the oracle sample")
+    p.add_argument("--cpu-seconds", type=float, default=15.0, help="target work of the timed CPU reference sample")
+    p.add_argument("--accuracy-seconds", type=float, default=8.0, help="target work of the FP64 oracle accuracy sample")
+    p.add_argument("--reference-step-seconds", type=float, default=4.0,
+                   help="target work of one step of the reference arm")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-extra-configs", action="store_true", help="skip the c2/c3/c4 lines")
     p.add_argument("--config", default="c1", choices=["c1", "c2", "c3", "c4"],
@@ -150,7 +153,8 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------------------------
-# CPU baseline: the FP64 oracle on a bounded sample of the same workload (the checker, timed)
+# CPU baseline: fgkl's batched CPU algorithm (oracle/fgkl_cpu.c) on a bounded sample of the same
+# workload, all host threads; the FP64 scalar oracle only measures accuracy
 # ---------------------------------------------------------------------------------------------
 
 def cpu_sample_regions(w, target_cells):
@@ -172,6 +176,24 @@ def run_oracle(w, regions, threads):
     return res, time.perf_counter() - t0
 
 
+def run_fgkl_cpu(w, regions, threads):
+    """fgkl's CPU algorithm restated (FP32 first, FP64 recomputation, prefix + suffix sharing)."""
+    from oracle import oracle
+
+    t0 = time.perf_counter()
+    res, lost = oracle.fgkl_cpu_workload(w, regions, threads)
+    return res, lost, time.perf_counter() - t0
+
+
+def fgkl_cpu_sample(threads, regions, cells, lost):
+    from oracle import oracle
+
+    return (f"{len(regions)} regions ({cells:.3g} nominal cells) of the workload; fgkl's batched CPU algorithm "
+            f"restated in C (oracle/fgkl_cpu.c: reads on SIMD lanes, FP32 first with FP64 recomputation of "
+            f"{lost} lost pairs, prefix and suffix sharing, {oracle.ISA_NAMES[oracle.cpu_isa()]}), one region per "
+            f"thread on {threads} threads; the Rust crate itself cannot be built here (no cargo)")
+
+
 # ---------------------------------------------------------------------------------------------
 # the reference arm
 # ---------------------------------------------------------------------------------------------
@@ -183,30 +205,27 @@ def reference_arm(args, rank, world, pg):
 
     threads = os.cpu_count() or 1
     w = synthetic.workload(1, seed=args.seed, regions=args.regions, threads=threads)
-    # Calibrate the per-step sample to a few seconds of oracle work on this host.
-    regions, cells = cpu_sample_regions(w, 2e8)
-    _, secs = run_oracle(w, regions, threads)
-    rate = cells / secs
-    per_step_cells = rate * 3.0
+    # Calibrate the per-step sample to a few seconds of work on this host.
+    regions, cells = cpu_sample_regions(w, 2e10)
+    _, _, secs = run_fgkl_cpu(w, regions, threads)
+    per_step_cells = cells / secs * args.reference_step_seconds
     regions, cells = cpu_sample_regions(w, per_step_cells)
     for _ in range(args.warmup):
-        run_oracle(w, regions[:1], threads)
-    times = []
+        run_fgkl_cpu(w, regions[:8], threads)
+    times, lost = [], 0
     for _ in range(args.steps):
-        _, s = run_oracle(w, regions, threads)
+        _, lost, s = run_fgkl_cpu(w, regions, threads)
         times.append(s)
     total = sum(times)
     value = cells * args.steps / total / 1e9
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "GCUPS", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "regions": args.regions, "seed": args.seed, "sample_regions": len(regions),
                    "sample_nominal_cells": cells},
         "cpu_baseline": {"value": value, "unit": "GCUPS", "cores": threads, "kind": "port",
-                         "sample": f"{len(regions)} regions ({cells:.3g} nominal cells) of the workload per step; fgkl's "
-                                   "Rust crate cannot be built here (no cargo), so the scalar FP64 oracle restating "
-                                   "reference.rs runs, one region row per thread"},
+                         "sample": fgkl_cpu_sample(threads, regions, cells, lost) + " (per step)"},
         "e2e": {"value": value, "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -482,21 +501,28 @@ def ours(args, rank, world, local, pg):
 
     if not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
+        offs = w.output_offsets()
+        # Accuracy against the FP64 scalar oracle on a sample of about args.accuracy_seconds.
         regions, cells = cpu_sample_regions(w, 1e9)
         ref, secs = run_oracle(w, regions, threads)
-        rate = cells / secs
-        target = args.cpu_seconds * rate
+        target = args.accuracy_seconds * cells / secs
         if target > cells * 1.5:
             regions, cells = cpu_sample_regions(w, target)
             ref, secs = run_oracle(w, regions, threads)
-        offs = w.output_offsets()
         got = np.concatenate([out[offs[g]:offs[g + 1]] for g in regions])
         line["max_abs_dlog10"] = float(np.max(np.abs(got - ref)))
-        line["accuracy_sample"] = {"regions": len(regions), "pairs": int(got.size)}
+        line["accuracy_sample"] = {"regions": len(regions), "pairs": int(got.size), "oracle": "scalar FP64"}
+        # The timed CPU reference: fgkl's batched algorithm on about args.cpu_seconds of work.
+        regions, cells = cpu_sample_regions(w, 2e10)
+        cpu, lost, secs = run_fgkl_cpu(w, regions, threads)
+        target = args.cpu_seconds * cells / secs
+        if target > cells * 1.5:
+            regions, cells = cpu_sample_regions(w, target)
+            cpu, lost, secs = run_fgkl_cpu(w, regions, threads)
+        mine = np.concatenate([out[offs[g]:offs[g + 1]] for g in regions])
         line["cpu_baseline"] = {"value": cells / secs / 1e9, "unit": "GCUPS", "cores": threads, "kind": "port",
-                                "sample": f"first {len(regions)} regions ({cells:.3g} nominal cells) of the same batch; "
-                                          "scalar FP64 oracle restating fgkl reference.rs (the Rust crate cannot be "
-                                          "built here)"}
+                                "sample": fgkl_cpu_sample(threads, regions, cells, lost),
+                                "max_abs_dlog10_vs_gpu": float(np.max(np.abs(mine - cpu)))}
     print(json.dumps(line), flush=True)
     barrier(pg, device)
 

@@ -32,7 +32,8 @@ def build() -> Path:
 def lib():
     global _lib
     if _lib is None:
-        if not LIB_PATH.exists() or LIB_PATH.stat().st_mtime < (HERE / "pairhmm_oracle.c").stat().st_mtime:
+        sources = ("pairhmm_oracle.c", "fgkl_cpu.c", "fgkl_cpu_kernel.h", "Makefile")
+        if not LIB_PATH.exists() or LIB_PATH.stat().st_mtime < max((HERE / f).stat().st_mtime for f in sources):
             build()
         L = C.CDLL(str(LIB_PATH))
         L.or_error_prob.restype = C.c_double
@@ -55,6 +56,11 @@ def lib():
         L.or_adj_log10_likelihood.argtypes = [_u8p, C.c_int, _u8p, C.c_int, _f64p, _f64p, _f64p, _f64p]
         L.or_adj_gradient.restype = C.c_double
         L.or_adj_gradient.argtypes = [_u8p, C.c_int, _u8p, C.c_int, _f64p, _f64p, _f64p, _f64p, _f64p, _f64p, _f64p, _f64p]
+        _i64p = C.POINTER(C.c_int64)
+        L.fc_detect_isa.restype = C.c_int
+        L.fc_compute_regions.restype = C.c_int64
+        L.fc_compute_regions.argtypes = [_u8p] * 5 + [_i64p, _u8p, _i64p, _i64p, _i32p, _i64p, _i32p, _i64p, C.c_int,
+                                                      C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _f64p]
         _lib = L
     return _lib
 
@@ -137,6 +143,48 @@ def workload_matrix(workload, regions=None, threads: int | None = None) -> np.nd
         reads, haps = workload.region(g)
         parts.append(compute_matrix(reads, haps, threads) if reads and haps else np.zeros(0))
     return np.concatenate(parts) if parts else np.zeros(0)
+
+
+ISA_NAMES = {0: "portable vectors (8 FP32 / 4 FP64 lanes)", 1: "AVX2 (8 FP32 / 4 FP64 lanes)",
+             2: "AVX-512 (16 FP32 / 8 FP64 lanes; AVX2 for a remainder of at most half a batch)"}
+
+
+def cpu_isa() -> int:
+    """The instruction set fgkl_cpu.c selects on this CPU: 2 AVX-512F, 1 AVX2, 0 portable vectors."""
+    return int(lib().fc_detect_isa())
+
+
+def fgkl_cpu_workload(workload, regions=None, threads: int | None = None, double: bool = False,
+                      share_suffixes: bool = True, double_fallback: bool = True, isa: int = -1):
+    """fgkl's batched CPU algorithm (fgkl_cpu.c) over a synthetic workload's regions.
+
+    Returns (results concatenated in output order, pairs that lost precision in the first pass)."""
+    threads = threads or os.cpu_count() or 1
+    regions = list(range(workload.num_regions)) if regions is None else list(regions)
+    nr = workload.region_reads.astype(np.int64)
+    nh = workload.region_haps.astype(np.int64)
+    read_start = np.concatenate([[0], np.cumsum(nr)[:-1]]).astype(np.int64)
+    hap_start = np.concatenate([[0], np.cumsum(nh)[:-1]]).astype(np.int64)
+    sel = np.asarray(regions, np.int64)
+    read_first = np.ascontiguousarray(read_start[sel])
+    hap_first = np.ascontiguousarray(hap_start[sel])
+    n_reads = np.ascontiguousarray(nr[sel].astype(np.int32))
+    n_haps = np.ascontiguousarray(nh[sel].astype(np.int32))
+    sizes = nr[sel] * nh[sel]
+    out_first = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.int64) if sel.size else np.zeros(0, np.int64)
+    out = np.empty(int(sizes.sum()), np.float64)
+    i64 = C.POINTER(C.c_int64)
+    cols = [np.ascontiguousarray(getattr(workload, f), np.uint8) for f in ("bases", "quals", "ins_gop", "del_gop", "gcp")]
+    ro = np.ascontiguousarray(workload.read_offsets, np.int64)
+    hb = np.ascontiguousarray(workload.hap_bases, np.uint8)
+    ho = np.ascontiguousarray(workload.hap_offsets, np.int64)
+    lost = lib().fc_compute_regions(*[_p(c, _u8p) for c in cols], _p(ro, i64), _p(hb, _u8p), _p(ho, i64),
+                                    _p(read_first, i64), _p(n_reads, _i32p), _p(hap_first, i64), _p(n_haps, _i32p),
+                                    _p(out_first, i64), int(sel.size), int(double), int(share_suffixes),
+                                    int(double_fallback), int(threads), int(isa), _p(out, _f64p))
+    if lost < 0:
+        raise ValueError("fc_compute_regions rejected its arguments")
+    return out, int(lost)
 
 
 def adj_log10_likelihood(hap: bytes, read_bases: bytes, d_ins, d_del, eps, err) -> float:

@@ -1,0 +1,107 @@
+"""fgkl's batched CPU algorithm restated in C (oracle/fgkl_cpu.c), the benchmark's timed CPU reference,
+against the scalar FP64 oracle and the golden fixtures.
+
+The tolerances are fgkl's own (crates/pairhmm/src/lib.rs:621-660): 1e-9 log10 in double, 1e-4 in
+float. Cases follow its tests: prefix sharing over nested and repeated prefixes and lengths
+(lib.rs:666-692), bytes outside ACGTN (lib.rs:694-717), float underflow falling back to double
+(lib.rs:719-739), suffix sharing with reads ending on different rows (lib.rs:746-809), and every
+instruction set this CPU has.
+"""
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from fgkl_b200 import Read, synthetic
+from oracle import oracle as O
+from refgen import Rng
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+def isas():
+    return list(range(O.cpu_isa() + 1))
+
+
+def mixed_workload():
+    rng = Rng(5)
+
+    def random_read(n):
+        return Read(bytes(rng.base() for _ in range(n)), bytes([30] * n), bytes([45] * n), bytes([45] * n),
+                    bytes([10] * n))
+
+    parts = []
+    deep = Read(b"A" * 80, bytes([40] * 80), bytes([45] * 80), bytes([45] * 80), bytes([10] * 80))
+    parts.append(([deep], [b"C" * 80, b"C" * 40 + b"A" * 40]))
+    reads, haps = synthetic.reference_region(31, 70, 120, 24, 300).region(0)
+    haps = list(haps) + [haps[3], haps[3], b"ACGTXXACGT" * 20, b"ACGTNNACGT" * 20]
+    reads = list(reads) + [random_read(120) for _ in range(29)]
+    parts.append((reads, haps))
+    for seed in range(8):
+        parts.append(synthetic.reference_region(100 + seed, 5 + 7 * seed, 50 + 10 * seed, 2 + 3 * seed,
+                                                100 + 20 * seed).region(0))
+    return synthetic.from_regions(parts)
+
+
+@pytest.fixture(scope="module")
+def mixed():
+    w = mixed_workload()
+    return w, O.workload_matrix(w, None, 8)
+
+
+@pytest.mark.parametrize("isa", isas())
+@pytest.mark.parametrize("share", [True, False])
+def test_double_matches_the_scalar_oracle(mixed, isa, share):
+    w, ref = mixed
+    out, lost = O.fgkl_cpu_workload(w, None, 4, double=True, share_suffixes=share, isa=isa)
+    assert np.abs(out - ref).max() <= 1e-9
+    assert lost == 0
+
+
+@pytest.mark.parametrize("isa", isas())
+@pytest.mark.parametrize("share", [True, False])
+def test_float_matches_the_scalar_oracle_and_recomputes_underflow(mixed, isa, share):
+    w, ref = mixed
+    out, lost = O.fgkl_cpu_workload(w, None, 4, double=False, share_suffixes=share, isa=isa)
+    assert np.isfinite(out).all()
+    assert np.abs(out - ref).max() <= 1e-4
+    assert lost > 0, "the deep pair and the random reads must underflow"
+
+
+def test_without_the_double_fallback_lost_pairs_stay_nan(mixed):
+    w, ref = mixed
+    out, lost = O.fgkl_cpu_workload(w, None, 4, double=False, double_fallback=False)
+    nan = np.isnan(out)
+    assert int(nan.sum()) == lost > 0
+    assert np.abs(out[~nan] - ref[~nan]).max() <= 1e-4
+
+
+def test_results_do_not_depend_on_threads(mixed):
+    w, _ = mixed
+    one, _ = O.fgkl_cpu_workload(w, None, 1)
+    many, _ = O.fgkl_cpu_workload(w, None, 7)
+    assert one.tobytes() == many.tobytes()
+
+
+@pytest.mark.parametrize("name", ["config0_seed0", "region_11_70x120_24x300"])
+def test_matches_the_golden_fixtures(name):
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("make_golden", GOLDEN / "make_golden.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    w = mod.build(name)
+    expected = np.array([float(x) for x in json.loads((GOLDEN / f"{name}.json").read_text())["log10"]])
+    for double, tol in ((True, 1e-9), (False, 1e-4)):
+        out, _ = O.fgkl_cpu_workload(w, None, 4, double=double)
+        assert np.abs(out - expected).max() <= tol, (name, double)
+
+
+def test_a_subset_of_regions_lands_in_output_order():
+    w = synthetic.workload(1, seed=3, regions=12, threads=4)
+    full, _ = O.fgkl_cpu_workload(w, None, 4)
+    offs = w.output_offsets()
+    picked = [2, 5, 11]
+    part, _ = O.fgkl_cpu_workload(w, picked, 4)
+    assert part.tobytes() == np.concatenate([full[offs[g]:offs[g + 1]] for g in picked]).tobytes()
