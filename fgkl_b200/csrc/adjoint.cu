@@ -380,9 +380,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, (AdjMinBlocks<P, R>::valu
 
 template <class P, int R>
 void adj_occ(int* blocks) {
-  const size_t smem = kWarpsPerBlock * AdjCol<P, R>::kRingBytes;
-  cudaFuncSetAttribute(adjoint_kernel<P, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, adjoint_kernel<P, R>, kWarpsPerBlock * 32, smem);
+  static std::atomic<int> cache[kMaxDevices];
+  *blocks = resident_blocks(adjoint_kernel<P, R>, kWarpsPerBlock * AdjCol<P, R>::kRingBytes, kWarpsPerBlock * 32, cache);
 }
 
 template <class P, int R>

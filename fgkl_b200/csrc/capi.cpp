@@ -181,7 +181,11 @@ int noalloc_device(fgkl::NoAllocDevice** out) {
 struct fgkl_context {
   std::unique_ptr<fgkl::Engine> engine;
   std::unique_ptr<fgkl::AdjointEngine> adjoint;  // created on the first adjoint call
+  // The executable graph of the last batch run. A new batch re-captures its launch sequence and
+  // updates this graph in place when the topology allows: destroying an executable graph waits for
+  // the whole device, which would stall a caller streaming batches through several contexts.
   cudaGraphExec_t graph = nullptr;
+  bool graph_current = false;  // holds the prepared batch's launches
   bool prepared = false;
   bool adjoint_prepared = false;
   int device = 0;
@@ -239,10 +243,7 @@ void fgkl_context_destroy(fgkl_context* ctx) {
 int fgkl_batch_prepare(fgkl_context* ctx, const fgkl_batch* b, const fgkl_config* config) {
   t_error.clear();
   if (!ctx || !b || !config) return set_error(FGKL_E_INVALID_ARGUMENT, "null argument");
-  if (ctx->graph) {
-    cudaGraphExecDestroy(ctx->graph);
-    ctx->graph = nullptr;
-  }
+  ctx->graph_current = false;
   fgkl::BatchInput in;
   in.num_regions = b->num_regions;
   in.region_reads = b->region_reads;
@@ -271,12 +272,15 @@ int fgkl_batch_run(fgkl_context* ctx) {
   fgkl::Engine& e = *ctx->engine;
   if (e.output_len() == 0) return FGKL_OK;
   cudaStream_t s = e.stream();
+  int rc0 = e.begin_run();
+  if (rc0) return set_error(rc0, e.error());
   if (e.profiling()) {
     // Timed launches: direct, so their events can be read back.
     const int rc = e.run();
-    return rc ? set_error(rc, e.error()) : FGKL_OK;
+    if (rc) return set_error(rc, e.error());
+    return (rc0 = e.end_run()) ? set_error(rc0, e.error()) : FGKL_OK;
   }
-  if (!ctx->graph) {
+  if (!ctx->graph_current) {
     cudaGraph_t g = nullptr;
     if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
       return set_error(FGKL_E_CUDA, "cannot capture the launch sequence");
@@ -287,16 +291,28 @@ int fgkl_batch_run(fgkl_context* ctx) {
       return set_error(rc, e.error());
     }
     if (end != cudaSuccess) return set_error(FGKL_E_CUDA, std::string("capture: ") + cudaGetErrorString(end));
-    const cudaError_t inst = cudaGraphInstantiate(&ctx->graph, g, 0);
+    bool updated = false;
+    if (ctx->graph) {
+      cudaGraphExecUpdateResultInfo info;
+      updated = cudaGraphExecUpdate(ctx->graph, g, &info) == cudaSuccess;
+      if (!updated) {
+        cudaGetLastError();  // a refused update leaves no sticky error; clear the last-error slot
+        cudaGraphExecDestroy(ctx->graph);
+        ctx->graph = nullptr;
+      }
+    }
+    cudaError_t inst = cudaSuccess;
+    if (!updated) inst = cudaGraphInstantiate(&ctx->graph, g, 0);
     cudaGraphDestroy(g);
     if (inst != cudaSuccess) {
       ctx->graph = nullptr;
       return set_error(FGKL_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(inst));
     }
+    ctx->graph_current = true;
   }
   const cudaError_t err = cudaGraphLaunch(ctx->graph, s);
   if (err != cudaSuccess) return set_error(FGKL_E_CUDA, std::string("graph launch: ") + cudaGetErrorString(err));
-  return FGKL_OK;
+  return (rc0 = e.end_run()) ? set_error(rc0, e.error()) : FGKL_OK;
 }
 
 int fgkl_batch_fetch(fgkl_context* ctx, double* out, int64_t out_len, fgkl_stats* stats) {

@@ -5,6 +5,7 @@
 #include <cuda_pipeline.h>
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <type_traits>
 
@@ -197,5 +198,27 @@ __device__ __forceinline__ typename P::V cell_match(const typename P::V& dM, con
 }
 
 }  // namespace
+
+// Resident blocks per SM of a kernel taking `smem` bytes of dynamic shared memory, resolved once per
+// device and kept in `cache` (one per kernel, kMaxDevices entries, blocks + 1, 0 = unresolved).
+// Raising a kernel's dynamic shared memory limit while that kernel runs (another context's batch in
+// flight) waits for it to finish, so the attribute is set on the first query only and later queries
+// (each batch's planning) touch no CUDA state.
+constexpr int kMaxDevices = 64;
+template <class K>
+int resident_blocks(K* kernel, size_t smem, int threads, std::atomic<int>* cache) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const bool keep = dev >= 0 && dev < kMaxDevices;
+  if (keep) {
+    const int c = cache[dev].load(std::memory_order_acquire);
+    if (c) return c - 1;
+  }
+  int blocks = 0;
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, threads, smem);
+  if (keep) cache[dev].store(blocks + 1, std::memory_order_release);
+  return blocks;
+}
 
 }  // namespace fgkl

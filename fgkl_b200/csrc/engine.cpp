@@ -172,11 +172,16 @@ Engine::Engine(int device, cudaStream_t stream) : device_(device), stream_(strea
     cudaEventCreateWithFlags(&join_[i], cudaEventDisableTiming);
   }
   cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming);
+  cudaStreamCreateWithFlags(&copy_, cudaStreamNonBlocking);
+  cudaEventCreateWithFlags(&uploaded_, cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&computed_, cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&fetched_, cudaEventDisableTiming);
 }
 
 Engine::~Engine() {
   cudaSetDevice(device_);
   if (stream_) cudaStreamSynchronize(stream_);
+  if (copy_) cudaStreamSynchronize(copy_);
   cudaFree(d_reads_);
   cudaFree(d_read_off_);
   cudaFree(d_plan_);
@@ -194,6 +199,10 @@ Engine::~Engine() {
     cudaEventDestroy(join_[i]);
   }
   cudaEventDestroy(fork_);
+  cudaEventDestroy(uploaded_);
+  cudaEventDestroy(computed_);
+  cudaEventDestroy(fetched_);
+  if (copy_) cudaStreamDestroy(copy_);
   for (cudaEvent_t e : ev_) cudaEventDestroy(e);
   if (own_stream_) cudaStreamDestroy(stream_);
 }
@@ -495,7 +504,13 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
   const size_t s_qoff = s_tasks + align_up(tasks.size() * sizeof(Task));
   const size_t s_out = s_qoff + align_up((kRowBins + 1) * sizeof(int));
   const size_t stage_bytes = s_out + align_up(static_cast<size_t>(out_len_) * sizeof(double)) + align_up(sizeof(Counters));
-  cudaStreamSynchronize(stream_);  // the staging buffer may still feed an earlier copy
+  int rc0;
+  // This engine's previous batch: its kernels may still read the device inputs about to be
+  // overwritten, and its copies may still read or fill the staging buffer. Events recorded before
+  // anything was enqueued complete at once.
+  if ((rc0 = check(cudaEventSynchronize(computed_), "previous batch"))) return rc0;
+  if ((rc0 = check(cudaEventSynchronize(uploaded_), "previous upload"))) return rc0;
+  if ((rc0 = check(cudaEventSynchronize(fetched_), "previous download"))) return rc0;
   if (stage_bytes > cap_stage_) {
     if (h_stage_) cudaFreeHost(h_stage_);
     h_stage_ = nullptr;
@@ -548,19 +563,20 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
   planned_.host_pack_ms = ms_since(t_pack);
   const auto t_up = std::chrono::steady_clock::now();
   int rc;
-  if ((rc = check(cudaMemcpyAsync(d_reads_, st + s_reads, static_cast<size_t>(read_bytes) * 5, cudaMemcpyHostToDevice, stream_), "upload reads")))
+  if ((rc = check(cudaMemcpyAsync(d_reads_, st + s_reads, static_cast<size_t>(read_bytes) * 5, cudaMemcpyHostToDevice, copy_), "upload reads")))
     return rc;
-  if ((rc = check(cudaMemcpyAsync(d_read_off_, st + s_read_off, (total_reads + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, stream_),
+  if ((rc = check(cudaMemcpyAsync(d_read_off_, st + s_read_off, (total_reads + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, copy_),
                   "upload offsets")))
     return rc;
-  if ((rc = check(cudaMemcpyAsync(d_plan_, st + s_blob, blob_bytes, cudaMemcpyHostToDevice, stream_), "upload plan"))) return rc;
+  if ((rc = check(cudaMemcpyAsync(d_plan_, st + s_blob, blob_bytes, cudaMemcpyHostToDevice, copy_), "upload plan"))) return rc;
   if (!tasks.empty() &&
-      (rc = check(cudaMemcpyAsync(d_tasks_, st + s_tasks, tasks.size() * sizeof(Task), cudaMemcpyHostToDevice, stream_), "upload tasks")))
+      (rc = check(cudaMemcpyAsync(d_tasks_, st + s_tasks, tasks.size() * sizeof(Task), cudaMemcpyHostToDevice, copy_), "upload tasks")))
     return rc;
   if ((rc = check(cudaMemcpyAsync(d_small_ + (n_small_ - 2 * kRowBins - 1), st + s_qoff, (kRowBins + 1) * sizeof(int),
-                                  cudaMemcpyHostToDevice, stream_),
+                                  cudaMemcpyHostToDevice, copy_),
                   "upload queue offsets")))
     return rc;
+  if ((rc = check(cudaEventRecord(uploaded_, copy_), "upload event"))) return rc;
 
   planned_.host_upload_ms = ms_since(t_up);
   view_.bases = d_reads_;
@@ -584,6 +600,16 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
   view_.counters = d_counters_;
   (void)total_haps;
   return FGKL_OK;
+}
+
+int Engine::begin_run() {
+  cudaSetDevice(device_);
+  return check(cudaStreamWaitEvent(stream_, uploaded_, 0), "wait for the uploads");
+}
+
+int Engine::end_run() {
+  cudaSetDevice(device_);
+  return check(cudaEventRecord(computed_, stream_), "kernels event");
 }
 
 int Engine::run() {
@@ -672,13 +698,15 @@ int Engine::fetch(double* out, int64_t out_len, BatchStats* stats) {
   int rc;
   double* h_out = reinterpret_cast<double*>(h_stage_ + out_stage_);
   Counters* h_cnt = reinterpret_cast<Counters*>(h_stage_ + out_stage_ + align_up(static_cast<size_t>(out_len_) * sizeof(double)));
+  if ((rc = check(cudaStreamWaitEvent(copy_, computed_, 0), "wait for the kernels"))) return rc;
   if (out_len_ > 0 &&
-      (rc = check(cudaMemcpyAsync(h_out, d_out_, static_cast<size_t>(out_len_) * sizeof(double), cudaMemcpyDeviceToHost, stream_),
+      (rc = check(cudaMemcpyAsync(h_out, d_out_, static_cast<size_t>(out_len_) * sizeof(double), cudaMemcpyDeviceToHost, copy_),
                   "download results")))
     return rc;
-  if ((rc = check(cudaMemcpyAsync(h_cnt, d_counters_, sizeof(Counters), cudaMemcpyDeviceToHost, stream_), "download counters")))
+  if ((rc = check(cudaMemcpyAsync(h_cnt, d_counters_, sizeof(Counters), cudaMemcpyDeviceToHost, copy_), "download counters")))
     return rc;
-  if ((rc = check(cudaStreamSynchronize(stream_), "kernel execution"))) return rc;
+  if ((rc = check(cudaEventRecord(fetched_, copy_), "download event"))) return rc;
+  if ((rc = check(cudaEventSynchronize(fetched_), "kernel execution"))) return rc;
   if (out_len_ > 0) parallel_copy(reinterpret_cast<uint8_t*>(out), reinterpret_cast<const uint8_t*>(h_out), static_cast<size_t>(out_len_) * sizeof(double));
   planned_.host_fetch_ms = ms_since(t_fetch);
   if (stats) {
@@ -699,7 +727,7 @@ int Engine::compute(const BatchInput& in, const EngineConfig& cfg, double* out, 
     if (stats) *stats = planned_;
     return FGKL_OK;
   }
-  if ((rc = run())) return rc;
+  if ((rc = begin_run()) || (rc = run()) || (rc = end_run())) return rc;
   return fetch(out, out_len, stats);
 }
 

@@ -54,11 +54,19 @@ class Engine {
   Engine(const Engine&) = delete;
   Engine& operator=(const Engine&) = delete;
 
-  // Plans `in` and uploads it; returns 0 or a negative FGKL_E_* code (message in error()).
+  // Plans `in` and uploads it on the engine's copy stream; returns 0 or a negative FGKL_E_* code
+  // (message in error()). Waits only for this engine's own earlier batch, never for other work on
+  // the compute stream, so engines sharing one compute stream can plan one batch while another runs.
   int prepare(const BatchInput& in, const EngineConfig& cfg);
+  // Makes the compute stream wait for the prepared batch's uploads. Called before run() or before
+  // launching a graph captured from run(), outside any capture.
+  int begin_run();
   // Enqueues the first pass and the recomputation on the stream (no host synchronisation).
   int run();
-  // Copies the results (and counters) back and waits for the stream.
+  // Marks the end of the batch's kernels on the compute stream; called after run() or the graph.
+  int end_run();
+  // Copies the results (and counters) back on the copy stream once the batch's kernels are done,
+  // and waits for that copy alone.
   int fetch(double* out, int64_t out_len, BatchStats* stats);
   // prepare + run + fetch.
   int compute(const BatchInput& in, const EngineConfig& cfg, double* out, int64_t out_len, BatchStats* stats);
@@ -102,8 +110,12 @@ class Engine {
 
   int device_ = 0;
   int sms_ = 0;
-  cudaStream_t stream_ = nullptr;
+  cudaStream_t stream_ = nullptr;  // compute: the batch's kernels (may be shared with other engines)
   bool own_stream_ = false;
+  cudaStream_t copy_ = nullptr;    // this engine's uploads and downloads
+  cudaEvent_t uploaded_ = nullptr;  // after the last batch's uploads (copy stream)
+  cudaEvent_t computed_ = nullptr;  // after the last batch's kernels (compute stream)
+  cudaEvent_t fetched_ = nullptr;   // after the last batch's downloads (copy stream)
   cudaStream_t aux_[kAuxStreams] = {};
   cudaEvent_t join_[kAuxStreams] = {};
   cudaEvent_t fork_ = nullptr;

@@ -673,9 +673,8 @@ __global__ void __launch_bounds__(256) collect_kernel(CollectArgs a) {
 template <class P, int R>
 void occ(int* blocks, int* threads) {
   *threads = kWarpsPerBlock * 32;
-  const size_t smem = kWarpsPerBlock * Layout<P, R>::kSmemPerWarp;
-  cudaFuncSetAttribute(pairhmm_kernel<P, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, pairhmm_kernel<P, R>, kWarpsPerBlock * 32, smem);
+  static std::atomic<int> cache[kMaxDevices];
+  *blocks = resident_blocks(pairhmm_kernel<P, R>, kWarpsPerBlock * Layout<P, R>::kSmemPerWarp, kWarpsPerBlock * 32, cache);
 }
 
 template <class P, int R>

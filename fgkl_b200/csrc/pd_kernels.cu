@@ -441,9 +441,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, (PdMinBlocks<P, R>::value
 
 template <class P, int R>
 void pd_occ(int* blocks) {
-  const size_t smem = kWarpsPerBlock * PdLayout<P, R>::kSmemPerWarp;
-  cudaFuncSetAttribute(pd_kernel<P, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, pd_kernel<P, R>, kWarpsPerBlock * 32, smem);
+  static std::atomic<int> cache[kMaxDevices];
+  *blocks = resident_blocks(pd_kernel<P, R>, kWarpsPerBlock * PdLayout<P, R>::kSmemPerWarp, kWarpsPerBlock * 32, cache);
 }
 
 template <class P, int R>

@@ -127,16 +127,22 @@ typedef struct fgkl_batch {
   const int64_t* hap_offsets;
 } fgkl_batch;
 
-/* A context on `device`; `stream` is a cudaStream_t to run on, or NULL for a private stream. */
+/* A context on `device`; `stream` is a cudaStream_t to run its kernels on, or NULL for a private
+ * stream. Each context copies on a private copy stream of its own. To stream batches back to back,
+ * give two contexts the same stream and alternate: prepare and run batch k+1 on one, then fetch
+ * batch k from the other. The host planning of k+1 and its upload overlap the kernels of k, and the
+ * batches' kernels run one after another on the shared stream. */
 fgkl_context* fgkl_context_create(int32_t device, void* stream);
 void fgkl_context_destroy(fgkl_context* ctx);
 
-/* Validates and plans the batch on the host and uploads it. */
+/* Validates and plans the batch on the host and uploads it on the context's copy stream. Waits for
+ * this context's previous batch only (its kernels and copies), never for other work on the stream. */
 int fgkl_batch_prepare(fgkl_context* ctx, const fgkl_batch* batch, const fgkl_config* config);
-/* Enqueues the kernels of the prepared batch on the context's stream, without waiting. The launch
- * sequence is captured into a CUDA graph on the first call and replayed afterwards. */
+/* Enqueues the kernels of the prepared batch on the context's stream, after its upload, without
+ * waiting. The launch sequence is captured into a CUDA graph, updated in place for later batches. */
 int fgkl_batch_run(fgkl_context* ctx);
-/* Waits for the stream and copies the likelihoods (Σ reads x haplotypes) and counters back. */
+/* Copies the likelihoods (Σ reads x haplotypes) and counters back once the batch's kernels are done,
+ * and waits for that copy (not for later work on the stream). */
 int fgkl_batch_fetch(fgkl_context* ctx, double* out, int64_t out_len, fgkl_stats* stats);
 /* prepare + run + fetch. */
 int fgkl_batch_compute(fgkl_context* ctx, const fgkl_batch* batch, const fgkl_config* config, double* out,
