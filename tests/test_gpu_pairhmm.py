@@ -307,3 +307,29 @@ def test_shared_prefix_and_suffix_workload_against_unshared_oracle(gpu):
     assert_close(out, expected, 1e-3, "c2 float")
     assert stats.backward_cells > 0
     assert stats.forward_cells < 0.5 * stats.prefix_only_cells + stats.forward_cells
+
+
+def test_two_contexts_on_one_stream_stream_batches_with_unchanged_bits(gpu):
+    # The streaming pattern of the C ABI: two contexts share a compute stream; batch k+1 is prepared
+    # and run on one before batch k is fetched from the other. Every batch must come back with the
+    # bits a lone, unoverlapped call gives it, including batches of other shapes (graph re-captured
+    # and updated in place) and a PD batch between plain ones.
+    import torch
+
+    from fgkl_b200 import BatchContext
+
+    batches = [synthetic.workload(1, seed=11, regions=16), synthetic.workload(1, seed=12, regions=9),
+               synthetic.workload(3, seed=13, regions=3), synthetic.workload(1, seed=11, regions=16),
+               synthetic.workload(2, seed=14, regions=1)]
+    alone = [BatchContext().compute(w, FLOAT)[0] for w in batches]
+    shared = torch.cuda.Stream()
+    ctxs = [BatchContext(stream=shared.cuda_stream), BatchContext(stream=shared.cuda_stream)]
+    got = [None] * len(batches)
+    for k, w in enumerate(batches):
+        ctxs[k % 2].prepare(w, FLOAT)
+        ctxs[k % 2].run()
+        if k > 0:
+            got[k - 1] = ctxs[(k - 1) % 2].fetch()[0]
+    got[-1] = ctxs[(len(batches) - 1) % 2].fetch()[0]
+    for k in range(len(batches)):
+        assert got[k].tobytes() == alone[k].tobytes(), k
