@@ -200,10 +200,9 @@ __device__ __forceinline__ typename P::V cell_match(const typename P::V& dM, con
 }  // namespace
 
 // Resident blocks per SM of a kernel taking `smem` bytes of dynamic shared memory, resolved once per
-// device and kept in `cache` (one per kernel, kMaxDevices entries, blocks + 1, 0 = unresolved).
-// Raising a kernel's dynamic shared memory limit while that kernel runs (another context's batch in
-// flight) waits for it to finish, so the attribute is set on the first query only and later queries
-// (each batch's planning) touch no CUDA state.
+// device and kept in `cache` (one per kernel, kMaxDevices entries, blocks + 1, 0 = unresolved): the
+// attribute is set and the occupancy queried on the first call only, so each later batch's planning
+// makes no CUDA call for it while other batches run.
 constexpr int kMaxDevices = 64;
 template <class K>
 int resident_blocks(K* kernel, size_t smem, int threads, std::atomic<int>* cache) {
