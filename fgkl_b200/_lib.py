@@ -181,6 +181,10 @@ def lib() -> C.CDLL:
     L.fgkl_adjoint_output_len.restype = C.c_int64
     L.fgkl_adjoint_grad_len.argtypes = [C.c_void_p]
     L.fgkl_adjoint_grad_len.restype = C.c_int64
+    L.fgkl_adjoint_set_stored_columns.argtypes = [C.c_void_p, C.c_int32]
+    L.fgkl_adjoint_set_stored_columns.restype = C.c_int
+    L.fgkl_adjoint_checkpointed_launches.argtypes = [C.c_void_p]
+    L.fgkl_adjoint_checkpointed_launches.restype = C.c_int32
     L.fgkl_pd_row_states.argtypes = [u8p, C.c_int32, C.c_int32, u8p]
     L.fgkl_pd_plan_describe.argtypes = [u8p, u8p, i32p, C.c_int32, i32p, i32p, u8p, u8p, i32p]
     L.fgkl_pd_match_accepts.argtypes = [C.c_uint8, C.c_uint8, C.c_uint8]
@@ -201,5 +205,6 @@ EXPORTED = [
     "fgkl_batch_run", "fgkl_batch_fetch", "fgkl_batch_compute", "fgkl_batch_output_len", "fgkl_synth_config",
     "fgkl_synth_reference_region", "fgkl_synth_view", "fgkl_synth_free", "fgkl_plan_describe", "fgkl_plan_sweeps", "fgkl_probe_fp32_tflops",
     "fgkl_pairhmm_compute_device_noalloc", "fgkl_context_profile", "fgkl_batch_launch_profile", "fgkl_adjoint_prepare", "fgkl_adjoint_run", "fgkl_adjoint_fetch",
-    "fgkl_adjoint_compute", "fgkl_adjoint_output_len", "fgkl_adjoint_grad_len", "fgkl_pd_row_states", "fgkl_pd_plan_describe", "fgkl_pd_match_accepts",
+    "fgkl_adjoint_compute", "fgkl_adjoint_output_len", "fgkl_adjoint_grad_len", "fgkl_adjoint_set_stored_columns",
+    "fgkl_adjoint_checkpointed_launches", "fgkl_pd_row_states", "fgkl_pd_plan_describe", "fgkl_pd_match_accepts",
 ]

@@ -44,7 +44,7 @@ struct AdjLaunch {
   const int* count;      // device-side count (FP64 recomputation queue), or nullptr
   int* task_counter;     // zeroed before the launch
   char* scratch;
-  size_t scratch_stride; // bytes per warp
+  size_t scratch_stride; // bytes per warp: a pair whose backward columns exceed it runs with checkpoints
   int32_t* queue;        // FP32 launches: reads lost in FP32, for FP64 (per-bin slices), or nullptr
   const int* queue_off;  // per rows-per-lane bin: first queue slot (kAdjRowBins + 1 entries)
   int* queue_tail;       // per bin
@@ -58,9 +58,33 @@ __host__ __device__ inline int adj_rows(int len) {
   if (rows > 8) rows = (rows + 1) & ~1;
   return rows;
 }
-// Bytes of per-warp scratch for haplotypes of at most `max_hap_len` bases.
+// Steps per recomputed block for a pair of `steps` forward steps whose per-warp scratch holds `cap`
+// values per lane, with backward records of `rec` values and saved backward states of `state` values:
+// the largest K >= min_k with K * rec + ceil(steps / K) * state <= cap, or 0 when there is none.
+__host__ __device__ inline int adj_block_steps(long long cap, int steps, int rec, int state, int min_k) {
+  long long K = (cap - state) / rec;
+  if (K > steps) K = steps;
+  for (int it = 0; it < 4096 && K >= min_k; ++it) {
+    const long long nb = (steps + K - 1) / K;
+    if (K * rec + nb * state <= cap) return static_cast<int>(K);
+    const long long k2 = (cap - nb * state) / rec;
+    K = k2 < K ? k2 : K - 1;
+  }
+  return 0;
+}
+
+// Bytes of per-warp scratch that store every backward column of haplotypes of at most
+// `max_hap_len` bases.
 size_t adj_scratch_bytes(bool dbl, int rows, int max_hap_len);
-void adj_occupancy(bool dbl, int rows, int* blocks_per_sm, int* threads_per_block);
-cudaError_t adj_launch(bool dbl, int rows, int blocks, const AdjLaunch& a, cudaStream_t stream);
+// The least per-warp scratch with which haplotypes of at most `max_hap_len` bases run with
+// checkpoints: backward states saved every K steps and each block of K columns recomputed before the
+// forward sweep reads it (about sqrt of the stored-column bytes).
+size_t adj_checkpoint_bytes(bool dbl, int rows, int max_hap_len);
+// Bytes of per-warp scratch that store `columns` backward columns.
+size_t adj_column_bytes(bool dbl, int rows, int columns);
+// `checkpointed`: the instantiation that recomputes backward columns from checkpoints for pairs whose
+// columns exceed the launch's per-warp scratch (the other has no such path and must not get them).
+void adj_occupancy(bool dbl, int rows, bool checkpointed, int* blocks_per_sm, int* threads_per_block);
+cudaError_t adj_launch(bool dbl, int rows, bool checkpointed, int blocks, const AdjLaunch& a, cudaStream_t stream);
 
 }  // namespace fgkl

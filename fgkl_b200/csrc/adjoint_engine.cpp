@@ -132,12 +132,29 @@ int AdjointEngine::prepare(const AdjointInput& in, bool double_precision) {
   for (auto* list : {&bins_, &rescue_})
     for (Bin& b : *list) {
       int per_sm = 0, threads = 0;
-      adj_occupancy(b.dbl, b.rows, &per_sm, &threads);
+      adj_occupancy(b.dbl, b.rows, false, &per_sm, &threads);
       if (per_sm <= 0) return fail(FGKL_E_CUDA, "adjoint kernel unavailable on this device");
-      b.stride = align_up(adj_scratch_bytes(b.dbl, b.rows, max_hap));
+      // Per-warp scratch: every backward column of the longest haplotype when that fits the budget
+      // at full occupancy (or the caller's column limit); otherwise what the budget gives each warp,
+      // and pairs whose columns exceed it recompute them from checkpoints. Only when even the
+      // checkpointed form does not fit does the grid shrink.
+      const int64_t want = std::min<int64_t>((b.n_tasks + kWarps - 1) / kWarps, static_cast<int64_t>(per_sm) * sms_);
+      const size_t full = align_up(adj_scratch_bytes(b.dbl, b.rows, max_hap));
+      const size_t least = align_up(adj_checkpoint_bytes(b.dbl, b.rows, max_hap));
+      size_t stride = full;
+      if (stored_columns_ > 0) stride = std::min(stride, align_up(adj_column_bytes(b.dbl, b.rows, stored_columns_)));
+      const size_t fair = kScratchBudget / (static_cast<size_t>(kWarps) * static_cast<size_t>(std::max<int64_t>(want, 1)));
+      if (stride > fair) stride = fair / 256 * 256;
+      b.stride = std::max(std::min(stride, full), least);
+      b.checkpointed = b.stride < full;
+      int64_t fit = want;
+      if (b.checkpointed) {
+        adj_occupancy(b.dbl, b.rows, true, &per_sm, &threads);
+        if (per_sm <= 0) return fail(FGKL_E_CUDA, "adjoint kernel unavailable on this device");
+        fit = std::min<int64_t>((b.n_tasks + kWarps - 1) / kWarps, static_cast<int64_t>(per_sm) * sms_);
+      }
       const int64_t by_budget = static_cast<int64_t>(kScratchBudget / (kWarps * b.stride));
-      b.blocks = static_cast<int>(std::max<int64_t>(
-          1, std::min<int64_t>({(b.n_tasks + kWarps - 1) / kWarps, static_cast<int64_t>(per_sm) * sms_, by_budget})));
+      b.blocks = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(fit, by_budget)));
       scratch = std::max(scratch, static_cast<size_t>(b.blocks) * kWarps * b.stride);
     }
 
@@ -218,6 +235,13 @@ int AdjointEngine::prepare(const AdjointInput& in, bool double_precision) {
   return FGKL_OK;
 }
 
+int AdjointEngine::checkpointed_launches() const {
+  int n = 0;
+  for (const auto* list : {&bins_, &rescue_})
+    for (const Bin& b : *list) n += b.checkpointed ? 1 : 0;
+  return n;
+}
+
 int AdjointEngine::run() {
   cudaSetDevice(device_);
   int rc;
@@ -244,7 +268,7 @@ int AdjointEngine::run() {
       a.queue = (pass == 0 && !dbl_) ? queue_ : nullptr;
       a.queue_off = queue_off;
       a.queue_tail = queue_tail;
-      if ((rc = check(adj_launch(b.dbl, b.rows, b.blocks, a, stream_), "adjoint launch"))) return rc;
+      if ((rc = check(adj_launch(b.dbl, b.rows, b.checkpointed, b.blocks, a, stream_), "adjoint launch"))) return rc;
       ++launches_;
     }
   }

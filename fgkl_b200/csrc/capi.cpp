@@ -522,6 +522,18 @@ int fgkl_adjoint_compute(fgkl_context* ctx, const fgkl_adjoint_batch* b, int32_t
                             grad_len, fp64_reads);
 }
 
+int fgkl_adjoint_set_stored_columns(fgkl_context* ctx, int32_t columns) {
+  t_error.clear();
+  if (!ctx || columns < 0) return set_error(FGKL_E_INVALID_ARGUMENT, "bad stored column count");
+  if (!ctx->adjoint) ctx->adjoint = std::make_unique<fgkl::AdjointEngine>(ctx->device, ctx->stream);
+  ctx->adjoint->set_stored_columns(columns);
+  return FGKL_OK;
+}
+
+int32_t fgkl_adjoint_checkpointed_launches(const fgkl_context* ctx) {
+  return ctx && ctx->adjoint ? ctx->adjoint->checkpointed_launches() : 0;
+}
+
 int64_t fgkl_adjoint_output_len(const fgkl_context* ctx) { return ctx && ctx->adjoint ? ctx->adjoint->output_len() : 0; }
 int64_t fgkl_adjoint_grad_len(const fgkl_context* ctx) { return ctx && ctx->adjoint ? ctx->adjoint->grad_len() : 0; }
 

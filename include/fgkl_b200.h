@@ -210,6 +210,16 @@ int fgkl_adjoint_compute(fgkl_context* ctx, const fgkl_adjoint_batch* batch, int
                          double* grad_base_error, int64_t grad_len, uint64_t* fp64_reads);
 int64_t fgkl_adjoint_output_len(const fgkl_context* ctx);
 int64_t fgkl_adjoint_grad_len(const fgkl_context* ctx);
+/* Row checkpointing for long haplotypes. Each warp keeps a pair's backward columns in its scratch
+ * while they fit (by default, what an 8 GiB scratch budget gives every resident warp: about 1,700
+ * columns at reads of 151). A longer pair saves the backward state every K steps instead and
+ * recomputes each block of K columns just before the forward sweep reads it. K is about
+ * sqrt(columns), memory O(sqrt) instead of O(columns), and the backward sweep runs twice. Results
+ * are bit-identical either way. `columns` > 0 caps the stored columns from the next
+ * fgkl_adjoint_prepare (0 restores the default). */
+int fgkl_adjoint_set_stored_columns(fgkl_context* ctx, int32_t columns);
+/* Launches of the prepared adjoint batch whose longest pairs use checkpoints (0 or more). */
+int32_t fgkl_adjoint_checkpointed_launches(const fgkl_context* ctx);
 
 /* ---- allocation-free form (no counterpart in the reference) ----
  *
