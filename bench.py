@@ -52,6 +52,7 @@ def parse():
                    help="target work of one step of the reference arm")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-extra-configs", action="store_true", help="skip the c2/c3/c4 lines")
+    p.add_argument("--no-autotune", action="store_true", help="keep the default launch configuration")
     p.add_argument("--config", default="c1", choices=["c1", "c2", "c3", "c4"],
                    help="c2/c3/c4: time only that configuration (with --regions to shrink it), for profiling")
     return p.parse_args()
@@ -366,8 +367,25 @@ def ours(args, rank, world, local, pg):
     w = synthetic.workload(1, seed=args.seed + rank, regions=args.regions, threads=threads)
     nominal = w.nominal_cells()
     stream = torch.cuda.Stream(device=device)
-    ctx = BatchContext(device=device, stream=stream.cuda_stream)
     cfg = Config(precision=Precision.FLOAT)
+    # Launch configuration (streams per pass, persistent grid size) from the autotuner, run untimed on
+    # a batch of the same generator with another seed, then fixed for every context below.
+    tuning = None
+    if not args.no_autotune:
+        tw = synthetic.workload(1, seed=args.seed + 7919 + rank, regions=min(args.regions, 1024), threads=threads)
+        tctx = BatchContext(device=device, stream=stream.cuda_stream)
+        chosen, tried = tctx.autotune(tw, cfg, repeats=3)
+        tctx.close()
+        tuning = {"chosen": {"streams": chosen["streams"], "grid_percent": chosen["grid_percent"]},
+                  "candidates_ms": {f"streams={t['streams']},grid={t['grid_percent']}%": round(t["ms"], 3) for t in tried},
+                  "tuned_on": f"{tw.num_regions} regions of the same generator, another seed (untimed)"}
+
+    def tuned(c):
+        if tuning:
+            c.set_tuning(tuning["chosen"]["streams"], tuning["chosen"]["grid_percent"])
+        return c
+
+    ctx = tuned(BatchContext(device=device, stream=stream.cuda_stream))
     n_out = ctx.prepare(w, cfg)
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=f"cuda:{device}")
 
@@ -438,7 +456,8 @@ def ours(args, rank, world, local, pg):
     L = _lib.lib()
     b_in, c_in = w.as_batch(), cfg._c()
     shared = torch.cuda.Stream(device=device)
-    ctxs = [BatchContext(device=device, stream=shared.cuda_stream), BatchContext(device=device, stream=shared.cuda_stream)]
+    ctxs = [tuned(BatchContext(device=device, stream=shared.cuda_stream)),
+            tuned(BatchContext(device=device, stream=shared.cuda_stream))]
     outs = [np.empty(n_out, np.float64) for _ in ctxs]
     st = _lib.Stats()
     for ctx, o in zip(ctxs, outs):  # sizes each context's device and pinned buffers, untimed
@@ -498,7 +517,8 @@ def ours(args, rank, world, local, pg):
                    "forward_cells": int(stats.forward_cells), "backward_cells": int(stats.backward_cells),
                    "prefix_only_cells": int(stats.prefix_only_cells),
                    "l2": f"inputs {w.bases.size * 5 / 2**20:.0f} MiB > L2 126 MiB; L2 also flushed (untimed) between steps",
-                   "parallelism": f"region sharding x{world}, no collective"},
+                   "parallelism": f"region sharding x{world}, no collective",
+                   "launch_tuning": tuning},
         "computed_gcups": stats.computed_cells / step / 1e9,
         "fallback_pairs": int(stats.fallback_pairs), "rescue_reads": int(stats.rescue_reads),
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,

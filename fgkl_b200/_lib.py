@@ -87,6 +87,10 @@ class Batch(C.Structure):
     ]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("streams", C.c_int32), ("grid_percent", C.c_int32), ("ms", C.c_double)]
+
+
 class LaunchProfile(C.Structure):
     _fields_ = [("kind", C.c_int32), ("rows", C.c_int32), ("tasks", C.c_int32), ("blocks", C.c_int32),
                 ("recomputation", C.c_int32), ("forward_cells", C.c_uint64), ("backward_cells", C.c_uint64), ("ms", C.c_float)]
@@ -160,6 +164,13 @@ def lib() -> C.CDLL:
     L.fgkl_batch_compute.argtypes = [C.c_void_p, C.POINTER(Batch), C.POINTER(Config), f64p, C.c_int64, C.POINTER(Stats)]
     L.fgkl_batch_output_len.argtypes = [C.c_void_p]
     L.fgkl_batch_output_len.restype = C.c_int64
+    L.fgkl_context_autotune.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(Tuning),
+                                        C.POINTER(Tuning), C.c_int32, C.POINTER(C.c_int32)]
+    L.fgkl_context_autotune.restype = C.c_int
+    L.fgkl_context_set_tuning.argtypes = [C.c_void_p, C.POINTER(Tuning)]
+    L.fgkl_context_set_tuning.restype = C.c_int
+    L.fgkl_context_get_tuning.argtypes = [C.c_void_p, C.POINTER(Tuning)]
+    L.fgkl_context_get_tuning.restype = C.c_int
     L.fgkl_synth_config.argtypes = [C.c_int32, C.c_uint64, C.c_int32, C.c_int32]
     L.fgkl_synth_config.restype = C.c_void_p
     L.fgkl_synth_reference_region.argtypes = [C.c_uint64, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int32]
@@ -202,7 +213,8 @@ def last_error() -> str:
 EXPORTED = [
     "fgkl_pairhmm_compute", "fgkl_pairhmm_compute_config", "fgkl_pdhmm_compute", "fgkl_pdhmm_compute_config",
     "fgkl_backend", "fgkl_last_error", "fgkl_context_create", "fgkl_context_destroy", "fgkl_batch_prepare",
-    "fgkl_batch_run", "fgkl_batch_fetch", "fgkl_batch_compute", "fgkl_batch_output_len", "fgkl_synth_config",
+    "fgkl_batch_run", "fgkl_batch_fetch", "fgkl_batch_compute", "fgkl_batch_output_len", "fgkl_context_autotune",
+    "fgkl_context_set_tuning", "fgkl_context_get_tuning", "fgkl_synth_config",
     "fgkl_synth_reference_region", "fgkl_synth_view", "fgkl_synth_free", "fgkl_plan_describe", "fgkl_plan_sweeps", "fgkl_probe_fp32_tflops",
     "fgkl_pairhmm_compute_device_noalloc", "fgkl_context_profile", "fgkl_batch_launch_profile", "fgkl_adjoint_prepare", "fgkl_adjoint_run", "fgkl_adjoint_fetch",
     "fgkl_adjoint_compute", "fgkl_adjoint_output_len", "fgkl_adjoint_grad_len", "fgkl_adjoint_set_stored_columns",

@@ -338,6 +338,66 @@ int fgkl_batch_compute(fgkl_context* ctx, const fgkl_batch* batch, const fgkl_co
 
 int64_t fgkl_batch_output_len(const fgkl_context* ctx) { return ctx && ctx->prepared ? ctx->engine->output_len() : 0; }
 
+int fgkl_context_set_tuning(fgkl_context* ctx, const fgkl_tuning* t) {
+  t_error.clear();
+  if (!ctx || !t) return set_error(FGKL_E_INVALID_ARGUMENT, "null argument");
+  if (t->streams < 1 || t->streams > 8 || t->grid_percent < 10 || t->grid_percent > 100)
+    return set_error(FGKL_E_INVALID_ARGUMENT, "streams must be 1-8 and grid_percent 10-100");
+  ctx->engine->set_tuning(fgkl::Engine::Tuning{t->streams, t->grid_percent});
+  ctx->graph_current = false;
+  return FGKL_OK;
+}
+
+int fgkl_context_get_tuning(const fgkl_context* ctx, fgkl_tuning* t) {
+  t_error.clear();
+  if (!ctx || !t) return set_error(FGKL_E_INVALID_ARGUMENT, "null argument");
+  const auto& k = ctx->engine->tuning();
+  t->streams = k.streams;
+  t->grid_percent = k.grid_percent;
+  t->ms = 0.0;
+  return FGKL_OK;
+}
+
+int fgkl_context_autotune(fgkl_context* ctx, const fgkl_batch* batch, const fgkl_config* config, int32_t repeats,
+                          fgkl_tuning* chosen, fgkl_tuning* tried, int32_t tried_cap, int32_t* n_tried) {
+  t_error.clear();
+  if (!ctx || !batch || !config) return set_error(FGKL_E_INVALID_ARGUMENT, "null argument");
+  if (repeats < 1 || tried_cap < 0) return set_error(FGKL_E_INVALID_ARGUMENT, "repeats must be >= 1");
+  fgkl::Engine& e = *ctx->engine;
+  const bool was_profiling = e.profiling();
+  e.set_profiling(false);
+  static const int kStreams[] = {1, 2, 4, 8};
+  static const int kGrid[] = {100, 90, 75, 60};
+  fgkl::Engine::Tuning best{};
+  double best_ms = -1.0;
+  int n = 0, rc = FGKL_OK;
+  for (int gp : kGrid) {
+    for (int st : kStreams) {
+      e.set_tuning(fgkl::Engine::Tuning{st, gp});
+      if ((rc = fgkl_batch_prepare(ctx, batch, config))) break;
+      double ms = 0.0;
+      if ((rc = e.time_run(repeats, &ms))) {
+        rc = set_error(rc, e.error());
+        break;
+      }
+      if (tried && n < tried_cap) tried[n] = fgkl_tuning{st, gp, ms};
+      ++n;
+      if (best_ms < 0 || ms < best_ms) {
+        best_ms = ms;
+        best = fgkl::Engine::Tuning{st, gp};
+      }
+    }
+    if (rc) break;
+  }
+  e.set_profiling(was_profiling);
+  if (n_tried) *n_tried = n;
+  if (rc) return rc;
+  e.set_tuning(best);
+  if ((rc = fgkl_batch_prepare(ctx, batch, config))) return rc;
+  if (chosen) *chosen = fgkl_tuning{best.streams, best.grid_percent, best_ms};
+  return FGKL_OK;
+}
+
 // ---------------------------------------------------------------------------------------------
 // Synthetic workloads and planner diagnostics (test and benchmark support).
 // ---------------------------------------------------------------------------------------------

@@ -425,7 +425,8 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
     int per_sm = 0, threads = 0;
     occupancy(b.kind, b.rows, &per_sm, &threads);
     if (per_sm <= 0) return fail(FGKL_E_CUDA, "kernel instantiation unavailable on this device");
-    b.blocks = std::max(1, std::min((b.n_tasks + kWarpsPerBlock - 1) / kWarpsPerBlock, per_sm * sms_));
+    const int grid = std::max(sms_, per_sm * sms_ * tuning_.grid_percent / 100);
+    b.blocks = std::max(1, std::min((b.n_tasks + kWarpsPerBlock - 1) / kWarpsPerBlock, grid));
     first.push_back({cost, b});
   }
   // The bin with the most work launches first; the others fill the SMs its tail frees.
@@ -639,7 +640,8 @@ int Engine::run() {
     for (size_t b = 0; b < list.size(); ++b) {
       const Bin& bin = list[b];
       // Profiled runs serialise the launches on the main stream so each one's events time it alone.
-      cudaStream_t s = profile_ ? stream_ : aux_[b % kAuxStreams];
+      const int lanes = std::max(1, std::min(tuning_.streams, kAuxStreams));
+      cudaStream_t s = profile_ ? stream_ : aux_[b % lanes];
       if ((rc = check(cudaStreamWaitEvent(s, fork_, 0), "fork wait"))) return rc;
       LaunchArgs a{};
       a.v = view_;
@@ -656,9 +658,10 @@ int Engine::run() {
         return rc;
       if (profile_ && (rc = check(cudaEventRecord(ev_[2 * li + 1], s), "profiling event"))) return rc;
       planned_.kernel_launches++;
-      if ((rc = check(cudaEventRecord(join_[b % kAuxStreams], s), "join"))) return rc;
+      if ((rc = check(cudaEventRecord(join_[b % lanes], s), "join"))) return rc;
     }
-    for (size_t b = 0; b < std::min<size_t>(list.size(), kAuxStreams); ++b)
+    const size_t used = std::min<size_t>(list.size(), static_cast<size_t>(std::max(1, std::min(tuning_.streams, kAuxStreams))));
+    for (size_t b = 0; b < used; ++b)
       if ((rc = check(cudaStreamWaitEvent(stream_, join_[b], 0), "join wait"))) return rc;
     return FGKL_OK;
   };
@@ -669,6 +672,37 @@ int Engine::run() {
     planned_.kernel_launches++;
   }
   if ((rc = pass(rescue_bins_, true))) return rc;
+  return FGKL_OK;
+}
+
+void Engine::set_tuning(const Tuning& t) {
+  tuning_.streams = std::max(1, std::min(t.streams, kAuxStreams));
+  tuning_.grid_percent = std::max(10, std::min(t.grid_percent, 100));
+}
+
+int Engine::time_run(int repeats, double* ms) {
+  cudaSetDevice(device_);
+  if (repeats < 1) repeats = 1;
+  int rc;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if ((rc = check(cudaEventCreate(&e0), "timing event")) || (rc = check(cudaEventCreate(&e1), "timing event"))) return rc;
+  std::vector<double> t;
+  for (int i = 0; i <= repeats && rc == FGKL_OK; ++i) {
+    if ((rc = begin_run())) break;
+    if ((rc = check(cudaEventRecord(e0, stream_), "timing event"))) break;
+    if ((rc = run())) break;
+    if ((rc = check(cudaEventRecord(e1, stream_), "timing event"))) break;
+    if ((rc = end_run())) break;
+    if ((rc = check(cudaEventSynchronize(e1), "timed run"))) break;
+    float f = 0.f;
+    cudaEventElapsedTime(&f, e0, e1);
+    if (i > 0) t.push_back(f);  // the first run is a warm-up
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  std::sort(t.begin(), t.end());
+  *ms = t[t.size() / 2];
   return FGKL_OK;
 }
 

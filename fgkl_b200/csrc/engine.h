@@ -91,6 +91,19 @@ class Engine {
   bool profiling() const { return profile_; }
   int bin_profile(std::vector<BinProfile>* out);
 
+  // Launch configuration of the batched form: how many streams the launches of one pass spread
+  // over (1: one after another; more: bins overlap, the largest first) and each first-pass
+  // persistent grid as a percentage of the resident-block limit. Applies from the next prepare().
+  struct Tuning {
+    int streams = 8;
+    int grid_percent = 100;
+  };
+  void set_tuning(const Tuning& t);
+  const Tuning& tuning() const { return tuning_; }
+  // Times the prepared batch's kernels (direct launches on the stream, after one untimed run):
+  // the median of `repeats` runs, in milliseconds. Host-synchronous.
+  int time_run(int repeats, double* ms);
+
  private:
   struct Bin {
     Kind kind;
@@ -103,6 +116,7 @@ class Engine {
     uint64_t fwd_cells = 0, bwd_cells = 0;  // DP cells its tasks compute (first pass)
   };
   static constexpr int kAuxStreams = 8;
+  Tuning tuning_;
   template <class T>
   T* grow(T*& ptr, size_t& cap, size_t n);
   int fail(int code, const std::string& msg);

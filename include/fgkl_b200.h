@@ -150,6 +150,25 @@ int fgkl_batch_compute(fgkl_context* ctx, const fgkl_batch* batch, const fgkl_co
 /* Number of likelihoods the prepared batch produces. */
 int64_t fgkl_batch_output_len(const fgkl_context* ctx);
 
+/* Launch configuration of a context's batched form (the autotuner's search space). */
+typedef struct fgkl_tuning {
+  int32_t streams;       /* streams the launches of one pass spread over, 1-8 (1: one after another) */
+  int32_t grid_percent;  /* each first-pass persistent grid, % of the kernel's resident-block limit, 10-100 */
+  double ms;             /* autotuner: median device time of one run of the batch with this configuration */
+} fgkl_tuning;
+
+/* Autotuner. Plans `batch` once per candidate configuration (streams in {1, 2, 4, 8} x grid in
+ * {100, 90, 75, 60} %). It times the candidate's kernels with CUDA events: one untimed run, then the
+ * median of `repeats` runs. It keeps the fastest for the context's later batches and leaves `batch`
+ * prepared with it. `tried` (may be NULL) receives up to `tried_cap` candidates in the order they
+ * ran, and `n_tried` their count. Host-synchronous; a batch that represents the caller's workload
+ * (a sample of it will do) gives the configuration that workload runs fastest with. */
+int fgkl_context_autotune(fgkl_context* ctx, const fgkl_batch* batch, const fgkl_config* config, int32_t repeats,
+                          fgkl_tuning* chosen, fgkl_tuning* tried, int32_t tried_cap, int32_t* n_tried);
+/* Sets or reads a context's launch configuration directly (applies from the next prepare). */
+int fgkl_context_set_tuning(fgkl_context* ctx, const fgkl_tuning* tuning);
+int fgkl_context_get_tuning(const fgkl_context* ctx, fgkl_tuning* tuning);
+
 /* Per-launch timing for measurement. With profiling on, fgkl_batch_run issues its launches directly
  * (no CUDA graph), one after another on the context's stream instead of concurrently, with CUDA
  * events around each, so each is timed alone; fgkl_batch_launch_profile

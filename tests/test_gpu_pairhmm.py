@@ -333,3 +333,24 @@ def test_two_contexts_on_one_stream_stream_batches_with_unchanged_bits(gpu):
     got[-1] = ctxs[(len(batches) - 1) % 2].fetch()[0]
     for k in range(len(batches)):
         assert got[k].tobytes() == alone[k].tobytes(), k
+
+
+def test_autotuner_times_every_launch_configuration_and_keeps_the_bits(gpu):
+    from fgkl_b200 import BatchContext
+
+    w = synthetic.workload(1, seed=21, regions=32)
+    default, _ = BatchContext().compute(w, FLOAT)
+    ctx = BatchContext()
+    chosen, tried = ctx.autotune(w, FLOAT, repeats=2)
+    assert len(tried) == 16
+    assert {(t["streams"], t["grid_percent"]) for t in tried} == {(s, g) for s in (1, 2, 4, 8) for g in (100, 90, 75, 60)}
+    assert all(t["ms"] > 0 for t in tried)
+    assert chosen["ms"] == min(t["ms"] for t in tried)
+    assert ctx.tuning() == {"streams": chosen["streams"], "grid_percent": chosen["grid_percent"]}
+    # The batch stays prepared with the chosen configuration; launch shapes never change a result.
+    ctx.run()
+    tuned, _ = ctx.fetch()
+    assert tuned.tobytes() == default.tobytes()
+    ctx.set_tuning(1, 10)
+    narrow, _ = ctx.compute(w, FLOAT)
+    assert narrow.tobytes() == default.tobytes()
