@@ -54,18 +54,37 @@ struct Layout {
   // FP32 kernels look priors up in a per-lane table indexed by haplotype code (A, C, G, T, N);
   // regions holding other haplotype bytes run on the FP64 kernel, which compares codes instead.
   static constexpr int kPriorCodes = P::kDouble ? 0 : 5;
+  // A lane's priors for one code: its rows padded to whole 16-byte chunks, kPer16 rows a chunk.
+  static constexpr int kPer16 = kRound;
+  static constexpr int kRp = up(R);
+  static constexpr int kChunks = kRp / kPer16;
   static constexpr size_t kStageBytes = 2ull * 32 * kStage * sizeof(V);
-  static constexpr size_t kSmemPerWarp = kStageBytes + static_cast<size_t>(kPriorCodes) * R * 32 * sizeof(V);
+  static constexpr size_t kSmemPerWarp = kStageBytes + static_cast<size_t>(kPriorCodes) * kRp * 32 * sizeof(V);
+  // Element of row r's prior for `code` in the table, [code][chunk][lane][row in chunk]: each chunk of
+  // the warp is 512 contiguous bytes, so a step's chunk loads are conflict-free 16-byte loads.
+  __device__ static int prior_at(int code, int r, int lane) {
+    return ((code * kChunks + r / kPer16) * 32 + lane) * kPer16 + r % kPer16;
+  }
 };
 
-// Priors of the lane's rows for every haplotype code, [code][row][lane] in shared memory.
+// Priors of the lane's rows for every haplotype code, in shared memory (Layout::prior_at).
 template <class P, int R>
 __device__ __forceinline__ void put_priors(typename P::V* table, int lane, int r, int c, const RowModel& m) {
   using S = typename P::S;
   for (int code = 0; code < Layout<P, R>::kPriorCodes; ++code) {
     const bool match = code == m.oc || code == kCodeN;
-    P::put(table[(code * R + r) * 32 + lane], c, static_cast<S>(match ? m.pm : m.px));
+    P::put(table[Layout<P, R>::prior_at(code, r, lane)], c, static_cast<S>(match ? m.pm : m.px));
   }
+}
+
+// The lane's priors of every row for `code`, one 16-byte shared-memory load per chunk.
+template <class P, int R>
+__device__ __forceinline__ void load_priors(const typename P::V* table, int code, int lane,
+                                            typename P::V (&pri)[Layout<P, R>::kRp]) {
+  using L = Layout<P, R>;
+  const uint4* src = reinterpret_cast<const uint4*>(table);
+#pragma unroll
+  for (int k = 0; k < L::kChunks; ++k) reinterpret_cast<uint4*>(pri)[k] = src[(code * L::kChunks + k) * 32 + lane];
 }
 
 // Forward coefficients of the lane's rows.
@@ -78,7 +97,7 @@ struct FwdRows {
   const V* table;  // prior table (FP32 kernels)
 
   __device__ V prior(int code, bool isN, int r, int lane) const {
-    if (Layout<P, R>::kPriorCodes) return table[(code * R + r) * 32 + lane];
+    if (Layout<P, R>::kPriorCodes) return table[Layout<P, R>::prior_at(code, r, lane)];
     const bool m0 = (code == oc[0][r]) | isN;
     const bool m1 = (code == oc[P::NC - 1][r]) | isN;
     return P::sel(m0, m1, pm[r], px[r]);
@@ -143,7 +162,7 @@ struct BwdRows {
   const V* table;  // prior table of the rows below (FP32 kernels)
 
   __device__ V prior(int code, bool isN, int r, int lane) const {
-    if (Layout<P, R>::kPriorCodes) return table[(code * R + r) * 32 + lane];
+    if (Layout<P, R>::kPriorCodes) return table[Layout<P, R>::prior_at(code, r, lane)];
     const bool m0 = (code == oc[0][r]) | isN;
     const bool m1 = (code == oc[P::NC - 1][r]) | isN;
     return P::sel(m0, m1, pm[r], px[r]);
@@ -279,10 +298,12 @@ __device__ void backward_pass(const LaunchArgs& a, const Program& prog, const Re
     }
     const int code = ev & kCodeMask;
     const bool isN = code == kCodeN;
+    V pri[L::kRp];
+    if (L::kPriorCodes) load_priors<P, R>(bp.table, code, lane, pri);
     V belowX = rBX, diagM = dBM;
 #pragma unroll
     for (int r = R - 1; r >= 0; --r) {
-      const V into = P::mul(bp.prior(code, isN, r, lane), diagM);
+      const V into = P::mul(L::kPriorCodes ? pri[r] : bp.prior(code, isN, r, lane), diagM);
       const V itm = P::mul(into, bp.im[r]);
       V bx = P::fma(belowX, bp.ii[r], itm);
       const V by = P::fma(BY[r], bp.dd[r], itm);
@@ -434,12 +455,14 @@ __device__ __forceinline__ void forward_step(const LaunchArgs& a, const Program&
   }
   const int code = ev & kCodeMask;
   const bool isN = code == kCodeN;
+  V pri[L::kRp];
+  if (L::kPriorCodes) load_priors<P, R>(fr.table, code, lane, pri);
   // Match and deletion values from the bottom row up: each row reads the old values of the row above
   // (its diagonal) and its own old values (left), so everything updates in place.
 #pragma unroll
   for (int r = R - 1; r >= 0; --r) {
     const V pM = r ? st.M[r - 1] : dM, pX = r ? st.X[r - 1] : dX, pY = r ? st.Y[r - 1] : dY;
-    const V prior = fr.prior(code, isN, r, lane);
+    const V prior = L::kPriorCodes ? pri[r] : fr.prior(code, isN, r, lane);
     st.Y[r] = P::kTransformed ? P::fma(st.Y[r], fr.c4[r], st.M[r]) : P::fma(st.Y[r], fr.c3[r], P::mul(st.M[r], fr.c4[r]));
     st.M[r] = P::mul(prior, cell_match<P>(pM, pX, pY, fr.c0[r], fr.c1[r], fr.c2[r]));
   }
@@ -495,13 +518,20 @@ __device__ void forward_pass(const LaunchArgs& a, const Program& prog, const Rea
   } else {
     const int n = prog.fwd_len;
     const uint32_t* stream = a.v.stream + prog.fwd_off - lane;
-    uint32_t n0 = __ldg(stream), n1 = __ldg(stream + 1);
-    for (int t = 0; t < n + 32; t += 2) {
-      const uint32_t e0 = n0, e1 = n1;
-      n0 = __ldg(stream + t + 2);
-      n1 = __ldg(stream + t + 3);
+    // Four steps an iteration, their stream entries loaded one iteration ahead (the stream carries
+    // kStreamPad zero entries past its end, so the last iteration's look-ahead and the up to three
+    // steps past n + 31 read no events).
+    uint32_t n0 = __ldg(stream), n1 = __ldg(stream + 1), n2 = __ldg(stream + 2), n3 = __ldg(stream + 3);
+    for (int t = 0; t < n + 32; t += 4) {
+      const uint32_t e0 = n0, e1 = n1, e2 = n2, e3 = n3;
+      n0 = __ldg(stream + t + 4);
+      n1 = __ldg(stream + t + 5);
+      n2 = __ldg(stream + t + 6);
+      n3 = __ldg(stream + t + 7);
       forward_step<P, R>(a, prog, rd, lane, fr, an, pad_hi, sc, st, 0, e0, aM, aX, aY, bM, bX, bY);
       forward_step<P, R>(a, prog, rd, lane, fr, an, pad_hi, sc, st, 0, e1, bM, bX, bY, aM, aX, aY);
+      forward_step<P, R>(a, prog, rd, lane, fr, an, pad_hi, sc, st, 0, e2, aM, aX, aY, bM, bX, bY);
+      forward_step<P, R>(a, prog, rd, lane, fr, an, pad_hi, sc, st, 0, e3, bM, bX, bY, aM, aX, aY);
     }
   }
   __pipeline_wait_prior(0);
