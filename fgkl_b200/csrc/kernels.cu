@@ -368,7 +368,9 @@ __device__ __forceinline__ void forward_step(const LaunchArgs& a, const Program&
   uM = P::up(st.M[R - 1]);
   uX = P::up(st.X[R - 1]);
   uY = P::up(st.Y[R - 1]);
-  if (ev & kEvMask) {
+  // END and ACC act in lane 31 alone (the read's last row); the other lanes pass them by without
+  // entering the event code, which every lane otherwise reaches at its own step.
+  if (ev & (lane == 31 ? kEvMask : (kEvMask & ~(EV_END | EV_ACC)))) {
     if (ev & EV_SNAP) {
       const uint32_t slot = ev >> kPayloadShift;
       V* dst[2] = {slot != kPayloadNone ? sc.slot(static_cast<int>(slot), lane) : nullptr,

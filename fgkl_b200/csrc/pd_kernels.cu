@@ -156,7 +156,9 @@ __device__ __forceinline__ void pd_step(const LaunchArgs& a, const Program& prog
   u.BM = P::up(st.BM[R - 1]);
   u.BX = P::up(st.BX[R - 1]);
   u.BY = P::up(st.BY[R - 1]);
-  if (ev & kEvMask) {
+  // END and ACC act in lane 31 alone (the read's last row); the other lanes pass them by without
+  // entering the event code, which every lane otherwise reaches at its own step.
+  if (ev & (lane == 31 ? kEvMask : (kEvMask & ~(EV_END | EV_ACC)))) {
     if (ev & EV_SNAP) {
       const uint32_t slot = ev >> kPdPayloadShift;
       V* dst[2] = {slot != kPdPayloadNone ? sc.slot(static_cast<int>(slot), lane) : nullptr,
