@@ -88,7 +88,7 @@ class Batch(C.Structure):
 
 
 class Tuning(C.Structure):
-    _fields_ = [("streams", C.c_int32), ("grid_percent", C.c_int32), ("ms", C.c_double)]
+    _fields_ = [("streams", C.c_int32), ("grid_percent", C.c_int32), ("reads_per_warp", C.c_int32), ("ms", C.c_double)]
 
 
 class LaunchProfile(C.Structure):

@@ -341,9 +341,10 @@ int64_t fgkl_batch_output_len(const fgkl_context* ctx) { return ctx && ctx->prep
 int fgkl_context_set_tuning(fgkl_context* ctx, const fgkl_tuning* t) {
   t_error.clear();
   if (!ctx || !t) return set_error(FGKL_E_INVALID_ARGUMENT, "null argument");
-  if (t->streams < 1 || t->streams > 8 || t->grid_percent < 10 || t->grid_percent > 100)
-    return set_error(FGKL_E_INVALID_ARGUMENT, "streams must be 1-8 and grid_percent 10-100");
-  ctx->engine->set_tuning(fgkl::Engine::Tuning{t->streams, t->grid_percent});
+  if (t->streams < 1 || t->streams > 8 || t->grid_percent < 10 || t->grid_percent > 100 ||
+      (t->reads_per_warp != 1 && t->reads_per_warp != 2))
+    return set_error(FGKL_E_INVALID_ARGUMENT, "streams must be 1-8, grid_percent 10-100 and reads_per_warp 1 or 2");
+  ctx->engine->set_tuning(fgkl::Engine::Tuning{t->streams, t->grid_percent, t->reads_per_warp});
   ctx->graph_current = false;
   return FGKL_OK;
 }
@@ -354,6 +355,7 @@ int fgkl_context_get_tuning(const fgkl_context* ctx, fgkl_tuning* t) {
   const auto& k = ctx->engine->tuning();
   t->streams = k.streams;
   t->grid_percent = k.grid_percent;
+  t->reads_per_warp = k.reads_per_warp;
   t->ms = 0.0;
   return FGKL_OK;
 }
@@ -366,35 +368,37 @@ int fgkl_context_autotune(fgkl_context* ctx, const fgkl_batch* batch, const fgkl
   fgkl::Engine& e = *ctx->engine;
   const bool was_profiling = e.profiling();
   e.set_profiling(false);
-  static const int kStreams[] = {1, 2, 4, 8};
-  static const int kGrid[] = {100, 90, 75, 60};
+  // Candidates: every streams x grid pair with two reads per warp, then, for an FP32 PD-HMM batch,
+  // one read per warp at 4 and 8 streams with full grids.
+  std::vector<fgkl::Engine::Tuning> cands;
+  for (int gp : {100, 90, 75, 60})
+    for (int st : {1, 2, 4, 8}) cands.push_back(fgkl::Engine::Tuning{st, gp, 2});
+  if (batch->hap_flags && !config->double_precision)
+    for (int st : {4, 8}) cands.push_back(fgkl::Engine::Tuning{st, 100, 1});
   fgkl::Engine::Tuning best{};
   double best_ms = -1.0;
   int n = 0, rc = FGKL_OK;
-  for (int gp : kGrid) {
-    for (int st : kStreams) {
-      e.set_tuning(fgkl::Engine::Tuning{st, gp});
-      if ((rc = fgkl_batch_prepare(ctx, batch, config))) break;
-      double ms = 0.0;
-      if ((rc = e.time_run(repeats, &ms))) {
-        rc = set_error(rc, e.error());
-        break;
-      }
-      if (tried && n < tried_cap) tried[n] = fgkl_tuning{st, gp, ms};
-      ++n;
-      if (best_ms < 0 || ms < best_ms) {
-        best_ms = ms;
-        best = fgkl::Engine::Tuning{st, gp};
-      }
+  for (const auto& c : cands) {
+    e.set_tuning(c);
+    if ((rc = fgkl_batch_prepare(ctx, batch, config))) break;
+    double ms = 0.0;
+    if ((rc = e.time_run(repeats, &ms))) {
+      rc = set_error(rc, e.error());
+      break;
     }
-    if (rc) break;
+    if (tried && n < tried_cap) tried[n] = fgkl_tuning{c.streams, c.grid_percent, c.reads_per_warp, ms};
+    ++n;
+    if (best_ms < 0 || ms < best_ms) {
+      best_ms = ms;
+      best = c;
+    }
   }
   e.set_profiling(was_profiling);
   if (n_tried) *n_tried = n;
   if (rc) return rc;
   e.set_tuning(best);
   if ((rc = fgkl_batch_prepare(ctx, batch, config))) return rc;
-  if (chosen) *chosen = fgkl_tuning{best.streams, best.grid_percent, best_ms};
+  if (chosen) *chosen = fgkl_tuning{best.streams, best.grid_percent, best.reads_per_warp, best_ms};
   return FGKL_OK;
 }
 

@@ -371,8 +371,9 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
         count(Kind::kOneF64Pd, rows, len_of(order[i]));
       }
     } else if (pd) {
-      // PD in FP32: reads above 248 bases one per warp, the others in pairs (FP32x2).
-      while (i < order.size() && packed_rows(len_of(order[i])) > 8) {
+      // PD in FP32: reads above 248 bases one per warp, the others in pairs (FP32x2) unless the
+      // launch configuration asks for one read per warp.
+      while (i < order.size() && (packed_rows(len_of(order[i])) > 8 || tuning_.reads_per_warp == 1)) {
         const int rows = single_rows(len_of(order[i]));
         by_bin[{Kind::kOneF32Pd, rows}].push_back(
             {cost_cols * rows, Task{g, {static_cast<int32_t>(first_read[g] + order[i]), -1}, rows, -1}});
@@ -678,6 +679,7 @@ int Engine::run() {
 void Engine::set_tuning(const Tuning& t) {
   tuning_.streams = std::max(1, std::min(t.streams, kAuxStreams));
   tuning_.grid_percent = std::max(10, std::min(t.grid_percent, 100));
+  tuning_.reads_per_warp = t.reads_per_warp == 1 ? 1 : 2;
 }
 
 int Engine::time_run(int repeats, double* ms) {

@@ -92,11 +92,13 @@ class Engine {
   int bin_profile(std::vector<BinProfile>* out);
 
   // Launch configuration of the batched form: how many streams the launches of one pass spread
-  // over (1: one after another; more: bins overlap, the largest first) and each first-pass
-  // persistent grid as a percentage of the resident-block limit. Applies from the next prepare().
+  // over (1: one after another; more: bins overlap, the largest first), each first-pass persistent
+  // grid as a percentage of the resident-block limit, and how many reads an FP32 PD-HMM warp
+  // carries (two in FP32x2 at 8 warps per SM, or one at 12). Applies from the next prepare().
   struct Tuning {
     int streams = 8;
     int grid_percent = 100;
+    int reads_per_warp = 2;  // FP32 PD-HMM reads of at most 248 bases: 2 (FP32x2 pairs) or 1
   };
   void set_tuning(const Tuning& t);
   const Tuning& tuning() const { return tuning_; }

@@ -152,14 +152,16 @@ int64_t fgkl_batch_output_len(const fgkl_context* ctx);
 
 /* Launch configuration of a context's batched form (the autotuner's search space). */
 typedef struct fgkl_tuning {
-  int32_t streams;       /* streams the launches of one pass spread over, 1-8 (1: one after another) */
-  int32_t grid_percent;  /* each first-pass persistent grid, % of the kernel's resident-block limit, 10-100 */
-  double ms;             /* autotuner: median device time of one run of the batch with this configuration */
+  int32_t streams;         /* streams the launches of one pass spread over, 1-8 (1: one after another) */
+  int32_t grid_percent;    /* each first-pass persistent grid, % of the kernel's resident-block limit, 10-100 */
+  int32_t reads_per_warp;  /* FP32 PD-HMM reads of at most 248 bases: 2 (FP32x2 pairs, the default) or 1 */
+  double ms;               /* autotuner: median device time of one run of the batch with this configuration */
 } fgkl_tuning;
 
 /* Autotuner. Plans `batch` once per candidate configuration (streams in {1, 2, 4, 8} x grid in
- * {100, 90, 75, 60} %). It times the candidate's kernels with CUDA events: one untimed run, then the
- * median of `repeats` runs. It keeps the fastest for the context's later batches and leaves `batch`
+ * {100, 90, 75, 60} %; for an FP32 PD-HMM batch also one read per warp at 4 and 8 streams, full
+ * grids). It times the candidate's kernels with CUDA events: one untimed run, then the median of
+ * `repeats` runs. It keeps the fastest for the context's later batches and leaves `batch`
  * prepared with it. `tried` (may be NULL) receives up to `tried_cap` candidates in the order they
  * ran, and `n_tried` their count. Host-synchronous; a batch that represents the caller's workload
  * (a sample of it will do) gives the configuration that workload runs fastest with. */

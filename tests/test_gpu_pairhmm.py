@@ -346,7 +346,7 @@ def test_autotuner_times_every_launch_configuration_and_keeps_the_bits(gpu):
     assert {(t["streams"], t["grid_percent"]) for t in tried} == {(s, g) for s in (1, 2, 4, 8) for g in (100, 90, 75, 60)}
     assert all(t["ms"] > 0 for t in tried)
     assert chosen["ms"] == min(t["ms"] for t in tried)
-    assert ctx.tuning() == {"streams": chosen["streams"], "grid_percent": chosen["grid_percent"]}
+    assert ctx.tuning() == {"streams": chosen["streams"], "grid_percent": chosen["grid_percent"], "reads_per_warp": 2}
     # The batch stays prepared with the chosen configuration; launch shapes never change a result.
     ctx.run()
     tuned, _ = ctx.fetch()

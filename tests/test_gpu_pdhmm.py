@@ -211,3 +211,22 @@ def test_pd_batch_of_regions_matches_the_oracle(gpu):
     out, _ = ctx.fetch()
     expected = np.concatenate([reference_all(r, h) for r, h in parts])
     assert_close(out, expected, 1e-4, "batched PD")
+
+
+def test_one_or_two_reads_per_warp_give_the_same_bits_and_the_autotuner_tries_both(gpu):
+    # Two reads per warp run the FP32 recurrence in FP32x2 lanes, one read per warp in scalar FP32:
+    # the same round-to-nearest operations in the same order, so every pair keeps its bits.
+    parts = [pd_region(200 + i, 21, 100 + 20 * i, 5, 220) for i in range(3)]
+    w = synthetic.from_regions(parts)
+    pairs = BatchContext()
+    two, _ = pairs.compute(w, FLOAT)
+    single = BatchContext()
+    single.set_tuning(8, 100, 1)
+    one, _ = single.compute(w, FLOAT)
+    assert one.tobytes() == two.tobytes()
+    expected = np.concatenate([reference_all(r, h) for r, h in parts])
+    assert_close(one, expected, 1e-4, "one read per warp")
+    chosen, tried = BatchContext().autotune(w, FLOAT, repeats=1)
+    assert len(tried) == 18
+    assert sorted({t["reads_per_warp"] for t in tried}) == [1, 2]
+    assert chosen["ms"] == min(t["ms"] for t in tried)
