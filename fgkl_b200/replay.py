@@ -20,6 +20,10 @@ where hap-flags is Java's `Arrays.toString(byte[])` rendering ("[0, 1, 0, ...]")
 
 `FGKL_REPLAY_DEBUG[=threshold]` prints every pair further than `threshold` (default 0.5 log10) from
 GATK's value, or not finite, with the inputs that reproduce it.
+
+The dump records no region boundaries: a read boundary shows as the haplotype list starting over,
+so a region whose list repeats its first haplotype cannot be told apart and is split or dropped, as
+in fgkl's tools. GATK's haplotypes within a region are distinct, so its dumps do not hit this.
 """
 from __future__ import annotations
 
