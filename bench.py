@@ -506,18 +506,56 @@ def ours(args, rank, world, local, pg):
         barrier(pg, device)
         return
 
-    # Per-call form: one C-ABI call per region, host buffers, as GATK calls the binding.
-    hmm = PairHmm(cfg)
+    # Per-call form: one fgkl_pairhmm_compute_config call per region from host buffers already in the
+    # JNI layout (as the JNI shim holds them), first on one thread, then from several threads at once
+    # (each calling thread gets its own engine and stream, as GATK's native threads would).
+    import threading
+
+    from fgkl_b200.pairhmm import _Flat
+
     pc_regions = [w.region(g) for g in range(min(args.per_call_regions, w.num_regions))]
-    for reads, haps in pc_regions[:4]:
-        hmm.compute_log10_likelihoods(reads, haps)
+    flats = [_Flat(reads, haps, None) for reads, haps in pc_regions]
+    calls = []
+    for (reads, haps), f in zip(pc_regions, flats):
+        rd, hp = f.structs()
+        n = len(reads) * len(haps)
+        calls.append((rd, hp, np.empty(n, np.float64), n))
+    c_cfg = cfg._c()
+    L_pc = _lib.lib()
+
+    def call(c):
+        rd, hp, o, n = c
+        _check(L_pc.fgkl_pairhmm_compute_config(C.byref(rd), C.byref(hp), C.byref(c_cfg), _ptr(o, _lib.f64p), n, None))
+
+    for c in calls[:4]:
+        call(c)
     pc_cells = sum(sum(len(r.bases) for r in reads) * sum(len(h) for h in haps) for reads, haps in pc_regions)
     torch.cuda.synchronize(device)
     t0 = time.perf_counter()
-    for reads, haps in pc_regions:
-        hmm.compute_log10_likelihoods(reads, haps)
+    for c in calls:
+        call(c)
     pc_secs = time.perf_counter() - t0
     per_call = pc_cells / pc_secs / 1e9 if pc_cells else float("nan")
+    pc_threads = 8
+    gate = threading.Barrier(pc_threads + 1)
+
+    def worker(k):
+        call(calls[k % len(calls)])  # this thread's engine and stream, untimed
+        gate.wait()
+        for c in calls[k::pc_threads]:
+            call(c)
+        gate.wait()
+
+    pool = [threading.Thread(target=worker, args=(k,)) for k in range(pc_threads)]
+    for th in pool:
+        th.start()
+    gate.wait()
+    t0 = time.perf_counter()
+    gate.wait()
+    pc_mt_secs = time.perf_counter() - t0
+    for th in pool:
+        th.join()
+    per_call_mt = pc_cells / pc_mt_secs / 1e9 if pc_cells else float("nan")
 
     line = {
         "metric": METRIC, "value": value, "unit": "GCUPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -550,7 +588,10 @@ def ours(args, rank, world, local, pg):
                            "host_phases_last_call": e2e_phases},
                 "bit_identical_to_device_run": identical},
         "per_call": {"value": per_call, "unit": "GCUPS", "regions": len(pc_regions),
-                     "form": "one fgkl_pairhmm_compute_config call per region from host buffers"},
+                     "form": "one fgkl_pairhmm_compute_config call per region from host buffers in the JNI layout, "
+                             "one calling thread",
+                     "threads": {"value": per_call_mt, "threads": pc_threads,
+                                 "form": "the same calls split over 8 calling threads, each with its own engine and stream"}},
         "batched_over_per_call": value / world / per_call,
         "gpu_launches": planned_launches * args.steps,
         "clocks": clocks.summary(),

@@ -51,14 +51,21 @@ template <class T>
 T* AdjointEngine::grow(T*& p, size_t& cap, size_t n) {
   const size_t bytes = std::max<size_t>(n * sizeof(T), 256);
   if (bytes > cap) {
+    // Half as much again as the old size: a caller whose batches vary in size stops reallocating
+    // after a few calls (cudaFree waits for the whole device, other callers' streams included).
+    const size_t want = cap > 0 ? std::max(bytes, cap + cap / 2) : bytes;
     cudaFree(p);
     p = nullptr;
-    if (cudaMalloc(&p, bytes) != cudaSuccess) {
+    if (cudaMalloc(&p, want) == cudaSuccess) {
+      cap = want;
+    } else if (want > bytes && (cudaGetLastError(), cudaMalloc(&p, bytes) == cudaSuccess)) {
+      cap = bytes;
+    } else {
+      cudaGetLastError();
       cap = 0;
       p = nullptr;
       return nullptr;
     }
-    cap = bytes;
   }
   return p;
 }

@@ -221,14 +221,21 @@ template <class T>
 T* Engine::grow(T*& ptr, size_t& cap, size_t n) {
   const size_t bytes = std::max<size_t>(n * sizeof(T), 256);
   if (bytes > cap) {
+    // Half as much again as the old size: a caller whose batches vary in size stops reallocating
+    // after a few calls (cudaFree waits for the whole device, other callers' streams included).
+    const size_t want = cap > 0 ? std::max(bytes, cap + cap / 2) : bytes;
     cudaFree(ptr);
     ptr = nullptr;
-    if (cudaMalloc(&ptr, bytes) != cudaSuccess) {
+    if (cudaMalloc(&ptr, want) == cudaSuccess) {
+      cap = want;
+    } else if (want > bytes && (cudaGetLastError(), cudaMalloc(&ptr, bytes) == cudaSuccess)) {
+      cap = bytes;
+    } else {
+      cudaGetLastError();
       cap = 0;
       ptr = nullptr;
       return nullptr;
     }
-    cap = bytes;
   }
   return ptr;
 }
@@ -514,13 +521,20 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
   if ((rc0 = check(cudaEventSynchronize(uploaded_), "previous upload"))) return rc0;
   if ((rc0 = check(cudaEventSynchronize(fetched_), "previous download"))) return rc0;
   if (stage_bytes > cap_stage_) {
+    // Grown by half again at least, as the device buffers are (cudaFreeHost waits for the device).
+    const size_t want = cap_stage_ > 0 ? std::max(stage_bytes, cap_stage_ + cap_stage_ / 2) : stage_bytes;
     if (h_stage_) cudaFreeHost(h_stage_);
     h_stage_ = nullptr;
-    if (cudaMallocHost(&h_stage_, stage_bytes) != cudaSuccess) {
+    if (cudaMallocHost(&h_stage_, want) == cudaSuccess) {
+      cap_stage_ = want;
+    } else if (want > stage_bytes && (cudaGetLastError(), cudaMallocHost(&h_stage_, stage_bytes) == cudaSuccess)) {
+      cap_stage_ = stage_bytes;
+    } else {
+      cudaGetLastError();
       cap_stage_ = 0;
+      h_stage_ = nullptr;
       return fail(FGKL_E_CUDA, "pinned host allocation failed");
     }
-    cap_stage_ = stage_bytes;
   }
   out_stage_ = s_out;
   uint8_t* const st = h_stage_;
