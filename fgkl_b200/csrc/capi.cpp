@@ -367,6 +367,7 @@ int fgkl_context_autotune(fgkl_context* ctx, const fgkl_batch* batch, const fgkl
   if (repeats < 1 || tried_cap < 0) return set_error(FGKL_E_INVALID_ARGUMENT, "repeats must be >= 1");
   fgkl::Engine& e = *ctx->engine;
   const bool was_profiling = e.profiling();
+  const fgkl::Engine::Tuning before = e.tuning();
   e.set_profiling(false);
   // Candidates: every streams x grid pair with two reads per warp, then, for an FP32 PD-HMM batch,
   // one read per warp at 4 and 8 streams with full grids.
@@ -395,7 +396,13 @@ int fgkl_context_autotune(fgkl_context* ctx, const fgkl_batch* batch, const fgkl
   }
   e.set_profiling(was_profiling);
   if (n_tried) *n_tried = n;
-  if (rc) return rc;
+  if (rc) {
+    // A failed search leaves the context as it found it (its batch is no longer prepared).
+    e.set_tuning(before);
+    ctx->prepared = false;
+    ctx->graph_current = false;
+    return rc;
+  }
   e.set_tuning(best);
   if ((rc = fgkl_batch_prepare(ctx, batch, config))) return rc;
   if (chosen) *chosen = fgkl_tuning{best.streams, best.grid_percent, best.reads_per_warp, best_ms};
