@@ -326,6 +326,23 @@ def extra_configs(args, device, stream, flush, threads, which=("c2", "c3", "c4")
                      "max_abs_dlog10_sample": float(np.max(np.abs(out[offs[0]:offs[1]] - ref))),
                      "accuracy_sample": "region 0 against the FP64 oracle",
                      "launch_tuning": tuning}
+        if not args.no_cpu_baseline:
+            # fgkl's CPU algorithm for this configuration (oracle/fgkl_cpu.c: the plain kernel for
+            # c2, the PD kernel for c3) on a bounded sample of the same workload, all host threads.
+            regs, cells = cpu_sample_regions(w, 5e9)
+            _, _, secs = run_fgkl_cpu(w, regs, threads)
+            target = 4.0 * cells / secs
+            if target > cells * 1.5:
+                regs, cells = cpu_sample_regions(w, target)
+                _, lost, secs = run_fgkl_cpu(w, regs, threads)
+            else:
+                lost = 0
+            cpu = cells / secs / 1e9
+            res[name]["cpu_baseline"] = {"value": cpu, "unit": "GCUPS", "cores": threads, "kind": "port",
+                                         "sample": f"{len(regs)} regions ({cells:.3g} nominal cells) of the workload; "
+                                                   f"fgkl's batched {'PD' if cfg_id == 3 else 'plain'} CPU kernel "
+                                                   "restated in C (oracle/fgkl_cpu.c), FP32 with FP64 recomputation"}
+            res[name]["device_over_cpu"] = (nominal / t / 1e9) / cpu
         ctx.close()
     if "c4" not in which:
         return res

@@ -470,9 +470,10 @@ static inline double FC_NAME(finish_lane)(double raw, int has_min, double min_ac
 
 /* Runner::run_impl (kernel.rs:220-290): at most FC_L reads against every haplotype of the set,
  * out[lane * n + sorted hap]; lost pairs appended to fallback as (lane, sorted hap), NaN in place. */
-FC_TARGET static void FC_NAME(run_batch_impl)(void* wsp, const fc_read* reads, int n, const fc_haps* hs, double* out,
+FC_TARGET static void FC_NAME(run_batch_impl)(void* wsp, const fc_read* reads, int n, const void* hsp, double* out,
                                               fc_pairs* fallback) {
     FC_NAME(ws)* w = wsp;
+    const fc_haps* hs = hsp;
     FC_NAME(prepare)(w, reads, n, hs);
     if (hs->nsweeps > 0) {
         FC_NAME(fill_last_column_node)(w);
@@ -517,7 +518,7 @@ FC_TARGET static void FC_NAME(run_batch_impl)(void* wsp, const fc_read* reads, i
 }
 
 /* The runner entry: flush subnormals to zero around the batch (simd.rs:204-228). */
-static void FC_NAME(run_batch)(void* wsp, const fc_read* reads, int n, const fc_haps* hs, double* out,
+static void FC_NAME(run_batch)(void* wsp, const fc_read* reads, int n, const void* hs, double* out,
                                fc_pairs* fallback) {
     const unsigned saved = _mm_getcsr();
     _mm_setcsr(saved | 0x8040u);

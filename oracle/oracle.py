@@ -32,7 +32,7 @@ def build() -> Path:
 def lib():
     global _lib
     if _lib is None:
-        sources = ("pairhmm_oracle.c", "fgkl_cpu.c", "fgkl_cpu_kernel.h", "Makefile")
+        sources = ("pairhmm_oracle.c", "fgkl_cpu.c", "fgkl_cpu_kernel.h", "fgkl_cpu_pd_kernel.h", "Makefile")
         if not LIB_PATH.exists() or LIB_PATH.stat().st_mtime < max((HERE / f).stat().st_mtime for f in sources):
             build()
         L = C.CDLL(str(LIB_PATH))
@@ -61,6 +61,9 @@ def lib():
         L.fc_compute_regions.restype = C.c_int64
         L.fc_compute_regions.argtypes = [_u8p] * 5 + [_i64p, _u8p, _i64p, _i64p, _i32p, _i64p, _i32p, _i64p, C.c_int,
                                                       C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _f64p]
+        L.fc_compute_regions_flags.restype = C.c_int64
+        L.fc_compute_regions_flags.argtypes = [_u8p] * 5 + [_i64p, _u8p, _u8p, _i64p, _i64p, _i32p, _i64p, _i32p, _i64p,
+                                                            C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _f64p]
         _lib = L
     return _lib
 
@@ -156,7 +159,8 @@ def cpu_isa() -> int:
 
 def fgkl_cpu_workload(workload, regions=None, threads: int | None = None, double: bool = False,
                       share_suffixes: bool = True, double_fallback: bool = True, isa: int = -1):
-    """fgkl's batched CPU algorithm (fgkl_cpu.c) over a synthetic workload's regions.
+    """fgkl's batched CPU algorithm (fgkl_cpu.c) over a synthetic workload's regions: the PD-HMM
+    kernel when the workload carries haplotype flags, else the plain one.
 
     Returns (results concatenated in output order, pairs that lost precision in the first pass)."""
     threads = threads or os.cpu_count() or 1
@@ -178,10 +182,14 @@ def fgkl_cpu_workload(workload, regions=None, threads: int | None = None, double
     ro = np.ascontiguousarray(workload.read_offsets, np.int64)
     hb = np.ascontiguousarray(workload.hap_bases, np.uint8)
     ho = np.ascontiguousarray(workload.hap_offsets, np.int64)
-    lost = lib().fc_compute_regions(*[_p(c, _u8p) for c in cols], _p(ro, i64), _p(hb, _u8p), _p(ho, i64),
-                                    _p(read_first, i64), _p(n_reads, _i32p), _p(hap_first, i64), _p(n_haps, _i32p),
-                                    _p(out_first, i64), int(sel.size), int(double), int(share_suffixes),
-                                    int(double_fallback), int(threads), int(isa), _p(out, _f64p))
+    hf = np.ascontiguousarray(workload.hap_flags, np.uint8) if workload.hap_flags is not None else None
+    lost = lib().fc_compute_regions_flags(*[_p(c, _u8p) for c in cols], _p(ro, i64), _p(hb, _u8p),
+                                          _p(hf, _u8p) if hf is not None else None, _p(ho, i64),
+                                          _p(read_first, i64), _p(n_reads, _i32p), _p(hap_first, i64), _p(n_haps, _i32p),
+                                          _p(out_first, i64), int(sel.size), int(double), int(share_suffixes),
+                                          int(double_fallback), int(threads), int(isa), _p(out, _f64p))
+    if lost == -2:
+        raise ValueError("a PD region holds more than 256 distinct match sets")
     if lost < 0:
         raise ValueError("fc_compute_regions rejected its arguments")
     return out, int(lost)

@@ -105,3 +105,65 @@ def test_a_subset_of_regions_lands_in_output_order():
     picked = [2, 5, 11]
     part, _ = O.fgkl_cpu_workload(w, picked, 4)
     assert part.tobytes() == np.concatenate([full[offs[g]:offs[g + 1]] for g in picked]).tobytes()
+
+
+def pd_workload():
+    from fgkl_b200 import ALT_C, ALT_G, ALT_T, DEL_END, DEL_START, SNP, PdHaplotype
+
+    parts = [synthetic.reference_pd_region(31 + s, 20 + 5 * s, 60 + 20 * s, 6, 150 + 30 * s).region(0) for s in range(4)]
+    # fgkl's PD edge cases (pd.rs:230-330): flags on the last columns, back-to-back and one-base
+    # deletions, a SNP inside a deletion, nested prefixes with flag splits.
+    hap = b"ACGTTGCAAGGCTTAGGCTTACGATCGATTACAGGT"
+    n = len(hap)
+
+    def flags(**at):
+        f = bytearray(n)
+        for k, v in at.items():
+            f[int(k[1:])] = v
+        return bytes(f)
+
+    haps = [PdHaplotype(hap, flags(**{f"p{n - 3}": DEL_START, f"p{n - 1}": DEL_END})),
+            PdHaplotype(hap, flags(**{f"p{n - 1}": DEL_START | DEL_END})),
+            PdHaplotype(hap, flags(p5=DEL_START, p7=DEL_END, p8=DEL_START | DEL_END, p9=DEL_START, p12=DEL_END)),
+            PdHaplotype(hap, flags(p10=DEL_START, p11=SNP | ALT_T, p13=DEL_END | SNP | ALT_G)),
+            PdHaplotype(hap, flags(p30=SNP | ALT_C)), PdHaplotype(hap, bytes(n)), PdHaplotype(hap[:20], bytes(20)),
+            PdHaplotype(hap + b"ACG", flags(p12=DEL_START, p15=DEL_END) + bytes(3))]
+    reads, _ = synthetic.reference_pd_region(13, 30, 30, 1, n).region(0)
+    parts.append((reads, haps))
+    # A read no haplotype explains underflows FP32 (pd.rs:410-430).
+    deep = Read(b"A" * 80, bytes([40] * 80), bytes([45] * 80), bytes([45] * 80), bytes([10] * 80))
+    f = bytearray(80)
+    f[10] = DEL_START
+    f[20] = DEL_END
+    parts.append(([deep], [PdHaplotype(b"C" * 80, bytes(f)), PdHaplotype(b"C" * 40 + b"A" * 40, bytes(80))]))
+    return synthetic.from_regions(parts)
+
+
+@pytest.fixture(scope="module")
+def pd_mixed():
+    w = pd_workload()
+    return w, O.workload_matrix(w, None, 8)
+
+
+@pytest.mark.parametrize("isa", isas())
+@pytest.mark.parametrize("double", [False, True])
+def test_pd_kernel_matches_the_pd_oracle(pd_mixed, isa, double):
+    w, ref = pd_mixed
+    out, lost = O.fgkl_cpu_workload(w, None, 4, double=double, isa=isa)
+    assert np.isfinite(out).all()
+    assert np.abs(out - ref).max() <= (1e-9 if double else 1e-4)
+    if double:
+        assert lost == 0
+    else:
+        assert lost > 0, "the PD regions hold reads that underflow FP32"
+
+
+def test_pd_results_do_not_depend_on_threads_or_on_the_recomputation_split(pd_mixed):
+    w, ref = pd_mixed
+    one, _ = O.fgkl_cpu_workload(w, None, 1)
+    many, _ = O.fgkl_cpu_workload(w, None, 6)
+    assert one.tobytes() == many.tobytes()
+    nofb, lost = O.fgkl_cpu_workload(w, None, 4, double_fallback=False)
+    assert int(np.isnan(nofb).sum()) == lost
+    keep = ~np.isnan(nofb)
+    assert nofb[keep].tobytes() == one[keep].tobytes()
