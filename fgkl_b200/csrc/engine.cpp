@@ -194,6 +194,7 @@ Engine::~Engine() {
   cudaFree(d_err_);
   cudaFree(d_m2m_);
   if (h_stage_) cudaFreeHost(h_stage_);
+  if (h_reads_) cudaFreeHost(h_reads_);
   for (int i = 0; i < kAuxStreams; ++i) {
     cudaStreamDestroy(aux_[i]);
     cudaEventDestroy(join_[i]);
@@ -246,6 +247,48 @@ double ms_since(std::chrono::steady_clock::time_point t0) {
 }
 }  // namespace
 
+namespace {
+// Grows a pinned host buffer to at least `bytes`, by half again at least (cudaFreeHost waits for the
+// whole device); false when the allocation fails.
+bool grow_pinned(uint8_t*& p, size_t& cap, size_t bytes) {
+  if (bytes <= cap) return true;
+  const size_t want = cap > 0 ? std::max(bytes, cap + cap / 2) : bytes;
+  if (p) cudaFreeHost(p);
+  p = nullptr;
+  if (cudaMallocHost(&p, want) == cudaSuccess) {
+    cap = want;
+    return true;
+  }
+  cudaGetLastError();
+  if (want > bytes && cudaMallocHost(&p, bytes) == cudaSuccess) {
+    cap = bytes;
+    return true;
+  }
+  cudaGetLastError();
+  p = nullptr;
+  cap = 0;
+  return false;
+}
+
+// Runs a callable on a helper thread and joins it when it goes out of scope, so an early return
+// from prepare() never leaves the copy running.
+class Helper {
+ public:
+  template <class F>
+  explicit Helper(bool on, F&& f) {
+    if (on) th_ = std::thread(std::forward<F>(f));
+    else f();
+  }
+  ~Helper() { join(); }
+  void join() {
+    if (th_.joinable()) th_.join();
+  }
+
+ private:
+  std::thread th_;
+};
+}  // namespace
+
 int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
   cudaSetDevice(device_);
   const auto t_start = std::chrono::steady_clock::now();
@@ -280,6 +323,25 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
       if (in.hap_off[h + 1] - in.hap_off[h] <= 0)
         return fail(FGKL_E_EMPTY_HAPLOTYPE, "haplotype " + std::to_string(h - first_hap[g]) + " has no bases");
   }
+
+  // This engine's previous batch: its kernels may still read the device inputs about to be
+  // overwritten, and its copies may still read or fill the staging buffers. Events recorded before
+  // anything was enqueued complete at once.
+  int rc0;
+  if ((rc0 = check(cudaEventSynchronize(computed_), "previous batch"))) return rc0;
+  if ((rc0 = check(cudaEventSynchronize(uploaded_), "previous upload"))) return rc0;
+  if ((rc0 = check(cudaEventSynchronize(fetched_), "previous download"))) return rc0;
+
+  // The five read arrays go to pinned staging on a helper thread while the regions are planned
+  // (large batches only; a small call copies them in line).
+  const int64_t read_bytes = total_reads > 0 ? in.read_off[total_reads] : 0;
+  if (!grow_pinned(h_reads_, cap_h_reads_, static_cast<size_t>(read_bytes) * 5 + 16))
+    return fail(FGKL_E_CUDA, "pinned host allocation failed");
+  Helper read_copy(read_bytes >= (int64_t{8} << 20), [this, &in, read_bytes] {
+    const uint8_t* srcs[5] = {in.bases, in.quals, in.ins, in.del, in.gcp};
+    for (int a = 0; a < 5; ++a)
+      if (read_bytes) parallel_copy(h_reads_ + static_cast<size_t>(a) * read_bytes, srcs[a], static_cast<size_t>(read_bytes));
+  });
 
   // Plan the regions in parallel.
   std::vector<RegionPlan> plans(static_cast<size_t>(N));
@@ -497,7 +559,6 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
   section(static_cast<size_t>(n_sigs) * sizeof(uint32_t) + 16, o_sigs);
 
   // Device buffers.
-  const int64_t read_bytes = total_reads > 0 ? in.read_off[total_reads] : 0;
   n_small_ = static_cast<int>(bins_.size() + rescue_bins_.size()) + 2 * kRowBins + 1;
   if (!grow(d_reads_, cap_reads_, static_cast<size_t>(read_bytes) * 5 + 16) ||
       !grow(d_read_off_, cap_read_off_, static_cast<size_t>(total_reads) + 1) || !grow(d_plan_, cap_plan_, blob_bytes) ||
@@ -506,20 +567,14 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
       !grow(d_scratch_, cap_scratch_, scratch_total))
     return fail(FGKL_E_CUDA, "device allocation failed");
 
-  // Pinned staging: reads (five arrays) | read offsets | plan | tasks | queue offsets | results | counters.
-  const size_t s_reads = 0, s_read_off = s_reads + align_up(static_cast<size_t>(read_bytes) * 5);
+  // Pinned staging (the reads have their own buffer): read offsets | plan | tasks | queue offsets |
+  // results | counters.
+  const size_t s_read_off = 0;
   const size_t s_blob = s_read_off + align_up((total_reads + 1) * sizeof(int64_t));
   const size_t s_tasks = s_blob + align_up(blob_bytes);
   const size_t s_qoff = s_tasks + align_up(tasks.size() * sizeof(Task));
   const size_t s_out = s_qoff + align_up((kRowBins + 1) * sizeof(int));
   const size_t stage_bytes = s_out + align_up(static_cast<size_t>(out_len_) * sizeof(double)) + align_up(sizeof(Counters));
-  int rc0;
-  // This engine's previous batch: its kernels may still read the device inputs about to be
-  // overwritten, and its copies may still read or fill the staging buffer. Events recorded before
-  // anything was enqueued complete at once.
-  if ((rc0 = check(cudaEventSynchronize(computed_), "previous batch"))) return rc0;
-  if ((rc0 = check(cudaEventSynchronize(uploaded_), "previous upload"))) return rc0;
-  if ((rc0 = check(cudaEventSynchronize(fetched_), "previous download"))) return rc0;
   if (stage_bytes > cap_stage_) {
     // Grown by half again at least, as the device buffers are (cudaFreeHost waits for the device).
     const size_t want = cap_stage_ > 0 ? std::max(stage_bytes, cap_stage_ + cap_stage_ / 2) : stage_bytes;
@@ -538,9 +593,6 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
   }
   out_stage_ = s_out;
   uint8_t* const st = h_stage_;
-  const uint8_t* srcs[5] = {in.bases, in.quals, in.ins, in.del, in.gcp};
-  for (int a = 0; a < 5; ++a)
-    if (read_bytes) parallel_copy(st + s_reads + static_cast<size_t>(a) * read_bytes, srcs[a], static_cast<size_t>(read_bytes));
   std::memcpy(st + s_read_off, in.read_off, (total_reads + 1) * sizeof(int64_t));
   {
     uint8_t* blob = st + s_blob;
@@ -576,10 +628,11 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
   if (!tasks.empty()) std::memcpy(st + s_tasks, tasks.data(), tasks.size() * sizeof(Task));
   std::memcpy(st + s_qoff, queue_off.data(), (kRowBins + 1) * sizeof(int));
 
+  read_copy.join();
   planned_.host_pack_ms = ms_since(t_pack);
   const auto t_up = std::chrono::steady_clock::now();
   int rc;
-  if ((rc = check(cudaMemcpyAsync(d_reads_, st + s_reads, static_cast<size_t>(read_bytes) * 5, cudaMemcpyHostToDevice, copy_), "upload reads")))
+  if ((rc = check(cudaMemcpyAsync(d_reads_, h_reads_, static_cast<size_t>(read_bytes) * 5, cudaMemcpyHostToDevice, copy_), "upload reads")))
     return rc;
   if ((rc = check(cudaMemcpyAsync(d_read_off_, st + s_read_off, (total_reads + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, copy_),
                   "upload offsets")))

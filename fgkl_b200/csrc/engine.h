@@ -163,6 +163,8 @@ class Engine {
   // Pinned host staging.
   uint8_t* h_stage_ = nullptr;
   size_t cap_stage_ = 0;
+  uint8_t* h_reads_ = nullptr;  // pinned staging of the five read arrays, filled while planning runs
+  size_t cap_h_reads_ = 0;
   size_t out_stage_ = 0;  // results and counters come back here
 
   // Prepared batch.
