@@ -356,8 +356,9 @@ struct FwdState {
 
 // One forward step: events, then the column. (uM, uX, uY) receive the bottom row of the lane above
 // for this column; (dM, dX, dY) hold it for the previous column, the top row's diagonal. The two sets
-// alternate between consecutive steps, so no copies are needed.
-template <class P, int R>
+// alternate between consecutive steps, so no copies are needed. kEv = false compiles the event code
+// out, for steps where no lane of the warp has an event.
+template <class P, int R, bool kEv = true>
 __device__ __forceinline__ void forward_step(const LaunchArgs& a, const Program& prog, const ReadRef* rd, int lane,
                                              const FwdRows<P, R>& fr, const typename P::V& an, int pad_hi, Scratch<P, R>& sc,
                                              FwdState<P, R>& st, int synth_len, uint32_t ev, typename P::V& uM, typename P::V& uX,
@@ -370,7 +371,7 @@ __device__ __forceinline__ void forward_step(const LaunchArgs& a, const Program&
   uY = P::up(st.Y[R - 1]);
   // END and ACC act in lane 31 alone (the read's last row); the other lanes pass them by without
   // entering the event code, which every lane otherwise reaches at its own step.
-  if (ev & (lane == 31 ? kEvMask : (kEvMask & ~(EV_END | EV_ACC)))) {
+  if (kEv && (ev & (lane == 31 ? kEvMask : (kEvMask & ~(EV_END | EV_ACC))))) {
     if (ev & EV_SNAP) {
       const uint32_t slot = ev >> kPayloadShift;
       V* dst[2] = {slot != kPayloadNone ? sc.slot(static_cast<int>(slot), lane) : nullptr,
@@ -522,7 +523,10 @@ __device__ void forward_pass(const LaunchArgs& a, const Program& prog, const Rea
     const uint32_t* stream = a.v.stream + prog.fwd_off - lane;
     // Four steps an iteration, their stream entries loaded one iteration ahead (the stream carries
     // kStreamPad zero entries past its end, so the last iteration's look-ahead and the up to three
-    // steps past n + 31 read no events).
+    // steps past n + 31 read no events). An iteration where no lane has an event -- about four in
+    // five, as each event column reaches the lanes over 32 steps -- runs a body without event code,
+    // which the compiler schedules across the four steps.
+    const uint32_t keep = lane == 31 ? kEvMask : (kEvMask & ~(EV_END | EV_ACC));
     uint32_t n0 = __ldg(stream), n1 = __ldg(stream + 1), n2 = __ldg(stream + 2), n3 = __ldg(stream + 3);
     for (int t = 0; t < n + 32; t += 4) {
       const uint32_t e0 = n0, e1 = n1, e2 = n2, e3 = n3;
@@ -530,10 +534,17 @@ __device__ void forward_pass(const LaunchArgs& a, const Program& prog, const Rea
       n1 = __ldg(stream + t + 5);
       n2 = __ldg(stream + t + 6);
       n3 = __ldg(stream + t + 7);
-      forward_step<P, R>(a, prog, rd, lane, fr, an, pad_hi, sc, st, 0, e0, aM, aX, aY, bM, bX, bY);
-      forward_step<P, R>(a, prog, rd, lane, fr, an, pad_hi, sc, st, 0, e1, bM, bX, bY, aM, aX, aY);
-      forward_step<P, R>(a, prog, rd, lane, fr, an, pad_hi, sc, st, 0, e2, aM, aX, aY, bM, bX, bY);
-      forward_step<P, R>(a, prog, rd, lane, fr, an, pad_hi, sc, st, 0, e3, bM, bX, bY, aM, aX, aY);
+      if (__any_sync(kFull, (e0 | e1 | e2 | e3) & keep)) {
+        forward_step<P, R>(a, prog, rd, lane, fr, an, pad_hi, sc, st, 0, e0, aM, aX, aY, bM, bX, bY);
+        forward_step<P, R>(a, prog, rd, lane, fr, an, pad_hi, sc, st, 0, e1, bM, bX, bY, aM, aX, aY);
+        forward_step<P, R>(a, prog, rd, lane, fr, an, pad_hi, sc, st, 0, e2, aM, aX, aY, bM, bX, bY);
+        forward_step<P, R>(a, prog, rd, lane, fr, an, pad_hi, sc, st, 0, e3, bM, bX, bY, aM, aX, aY);
+      } else {
+        forward_step<P, R, false>(a, prog, rd, lane, fr, an, pad_hi, sc, st, 0, e0, aM, aX, aY, bM, bX, bY);
+        forward_step<P, R, false>(a, prog, rd, lane, fr, an, pad_hi, sc, st, 0, e1, bM, bX, bY, aM, aX, aY);
+        forward_step<P, R, false>(a, prog, rd, lane, fr, an, pad_hi, sc, st, 0, e2, aM, aX, aY, bM, bX, bY);
+        forward_step<P, R, false>(a, prog, rd, lane, fr, an, pad_hi, sc, st, 0, e3, bM, bX, bY, aM, aX, aY);
+      }
     }
   }
   __pipeline_wait_prior(0);

@@ -141,8 +141,9 @@ struct PdEdge {
 };
 
 // One PD forward step: events, then the column. `u` receives the lane above's bottom row for this
-// column, `d` holds it for the previous column (the top row's diagonal); the two alternate.
-template <class P, int R>
+// column, `d` holds it for the previous column (the top row's diagonal); the two alternate. kEv = false
+// compiles the event code out, for steps where no lane of the warp has an event.
+template <class P, int R, bool kEv = true>
 __device__ __forceinline__ void pd_step(const LaunchArgs& a, const Program& prog, const ReadRef* rd, int lane,
                                         const PdRows<P, R>& pr, const typename P::V& an, int pad_hi, PdScratch<P, R>& sc,
                                         PdState<P, R>& st, int synth_len, uint32_t ev, uint32_t sig, PdEdge<P>& u,
@@ -158,7 +159,7 @@ __device__ __forceinline__ void pd_step(const LaunchArgs& a, const Program& prog
   u.BY = P::up(st.BY[R - 1]);
   // END and ACC act in lane 31 alone (the read's last row); the other lanes pass them by without
   // entering the event code, which every lane otherwise reaches at its own step.
-  if (ev & (lane == 31 ? kEvMask : (kEvMask & ~(EV_END | EV_ACC)))) {
+  if (kEv && (ev & (lane == 31 ? kEvMask : (kEvMask & ~(EV_END | EV_ACC))))) {
     if (ev & EV_SNAP) {
       const uint32_t slot = ev >> kPdPayloadShift;
       V* dst[2] = {slot != kPdPayloadNone ? sc.slot(static_cast<int>(slot), lane) : nullptr,
@@ -339,6 +340,8 @@ __device__ void pd_forward_pass(const LaunchArgs& a, const Program& prog, const 
   } else {
     const int n = prog.fwd_len;
     const uint32_t* stream = a.v.stream + prog.fwd_off - lane;
+    // Two steps an iteration; one where no lane has an event runs a body without event code.
+    const uint32_t keep = lane == 31 ? kEvMask : (kEvMask & ~(EV_END | EV_ACC));
     uint32_t n0 = __ldg(stream), n1 = __ldg(stream + 1);
     uint32_t g0 = __ldg(sigs + (n0 & kCodeMask)), g1 = __ldg(sigs + (n1 & kCodeMask));
     for (int t = 0; t < n + 32; t += 2) {
@@ -347,8 +350,13 @@ __device__ void pd_forward_pass(const LaunchArgs& a, const Program& prog, const 
       n1 = __ldg(stream + t + 3);
       g0 = __ldg(sigs + (n0 & kCodeMask));
       g1 = __ldg(sigs + (n1 & kCodeMask));
-      pd_step<P, R>(a, prog, rd, lane, pr, an, pad_hi, sc, st, 0, e0, s0, ea, eb);
-      pd_step<P, R>(a, prog, rd, lane, pr, an, pad_hi, sc, st, 0, e1, s1, eb, ea);
+      if (__any_sync(kFull, (e0 | e1) & keep)) {
+        pd_step<P, R>(a, prog, rd, lane, pr, an, pad_hi, sc, st, 0, e0, s0, ea, eb);
+        pd_step<P, R>(a, prog, rd, lane, pr, an, pad_hi, sc, st, 0, e1, s1, eb, ea);
+      } else {
+        pd_step<P, R, false>(a, prog, rd, lane, pr, an, pad_hi, sc, st, 0, e0, s0, ea, eb);
+        pd_step<P, R, false>(a, prog, rd, lane, pr, an, pad_hi, sc, st, 0, e1, s1, eb, ea);
+      }
     }
   }
   __pipeline_wait_prior(0);
