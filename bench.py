@@ -554,25 +554,39 @@ def ours(args, rank, world, local, pg):
     pc_secs = time.perf_counter() - t0
     per_call = pc_cells / pc_secs / 1e9 if pc_cells else float("nan")
     pc_threads = 8
-    gate = threading.Barrier(pc_threads + 1)
 
-    def worker(k):
-        call(calls[k % len(calls)])  # this thread's engine and stream, untimed
-        gate.wait()
-        for c in calls[k::pc_threads]:
-            call(c)
-        gate.wait()
+    def per_call_threads(max_batches):
+        # The same calls from pc_threads threads at once: combined into batches when they meet
+        # (max_batches > 0, the library's default), or each run alone on its thread's engine.
+        prev = L_pc.fgkl_set_call_combining(max_batches)
+        gate = threading.Barrier(pc_threads + 1)
 
-    pool = [threading.Thread(target=worker, args=(k,)) for k in range(pc_threads)]
-    for th in pool:
-        th.start()
-    gate.wait()
-    t0 = time.perf_counter()
-    gate.wait()
-    pc_mt_secs = time.perf_counter() - t0
-    for th in pool:
-        th.join()
-    per_call_mt = pc_cells / pc_mt_secs / 1e9 if pc_cells else float("nan")
+        def worker(k):
+            for c in calls:  # untimed: this thread's engine (and the combining engines) at full size
+                call(c)
+            gate.wait()
+            for c in calls[k::pc_threads]:
+                call(c)
+            gate.wait()
+
+        pool = [threading.Thread(target=worker, args=(k,)) for k in range(pc_threads)]
+        for th in pool:
+            th.start()
+        gate.wait()
+        b0, r0 = C.c_uint64(), C.c_uint64()
+        L_pc.fgkl_call_combining_stats(C.byref(b0), C.byref(r0))
+        t0 = time.perf_counter()
+        gate.wait()
+        secs = time.perf_counter() - t0
+        b1, r1 = C.c_uint64(), C.c_uint64()
+        L_pc.fgkl_call_combining_stats(C.byref(b1), C.byref(r1))
+        for th in pool:
+            th.join()
+        L_pc.fgkl_set_call_combining(prev)
+        return pc_cells / secs / 1e9 if pc_cells else float("nan"), b1.value - b0.value, r1.value - r0.value
+
+    per_call_mt, mt_batches, mt_requests = per_call_threads(2)
+    per_call_alone, _, _ = per_call_threads(0)
 
     line = {
         "metric": METRIC, "value": value, "unit": "GCUPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -608,7 +622,11 @@ def ours(args, rank, world, local, pg):
                      "form": "one fgkl_pairhmm_compute_config call per region from host buffers in the JNI layout, "
                              "one calling thread",
                      "threads": {"value": per_call_mt, "threads": pc_threads,
-                                 "form": "the same calls split over 8 calling threads, each with its own engine and stream"}},
+                                 "form": "the same calls split over 8 calling threads; calls that meet run as one batch "
+                                         "(fgkl_set_call_combining, up to 2 batches in flight)",
+                                 "combined_batches": mt_batches, "combined_requests": mt_requests,
+                                 "alone": {"value": per_call_alone,
+                                           "form": "combining off: each call on its own thread's engine and stream"}}},
         "batched_over_per_call": value / world / per_call,
         "gpu_launches": planned_launches * args.steps,
         "clocks": clocks.summary(),

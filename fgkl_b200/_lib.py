@@ -153,6 +153,10 @@ def lib() -> C.CDLL:
     L.fgkl_pdhmm_compute_config.argtypes = L.fgkl_pairhmm_compute_config.argtypes
     for f in (L.fgkl_pairhmm_compute, L.fgkl_pairhmm_compute_config, L.fgkl_pdhmm_compute, L.fgkl_pdhmm_compute_config):
         f.restype = C.c_int
+    L.fgkl_set_call_combining.argtypes = [C.c_int32]
+    L.fgkl_set_call_combining.restype = C.c_int
+    L.fgkl_call_combining_stats.argtypes = [C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+    L.fgkl_call_combining_stats.restype = C.c_int
     L.fgkl_backend.restype = C.c_char_p
     L.fgkl_last_error.restype = C.c_char_p
     L.fgkl_context_create.argtypes = [C.c_int32, C.c_void_p]
@@ -212,7 +216,7 @@ def last_error() -> str:
 # Symbols include/fgkl_b200.h declares; the CPU test suite checks the library exports each one.
 EXPORTED = [
     "fgkl_pairhmm_compute", "fgkl_pairhmm_compute_config", "fgkl_pdhmm_compute", "fgkl_pdhmm_compute_config",
-    "fgkl_backend", "fgkl_last_error", "fgkl_context_create", "fgkl_context_destroy", "fgkl_batch_prepare",
+    "fgkl_set_call_combining", "fgkl_call_combining_stats", "fgkl_backend", "fgkl_last_error", "fgkl_context_create", "fgkl_context_destroy", "fgkl_batch_prepare",
     "fgkl_batch_run", "fgkl_batch_fetch", "fgkl_batch_compute", "fgkl_batch_output_len", "fgkl_context_autotune",
     "fgkl_context_set_tuning", "fgkl_context_get_tuning", "fgkl_synth_config",
     "fgkl_synth_reference_region", "fgkl_synth_view", "fgkl_synth_free", "fgkl_plan_describe", "fgkl_plan_sweeps", "fgkl_probe_fp32_tflops",

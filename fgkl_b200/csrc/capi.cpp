@@ -2,6 +2,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
+#include <condition_variable>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -65,6 +67,240 @@ int check_offsets(const int32_t* offsets, int64_t n, int64_t total, const char* 
 
 void to_stats(const fgkl::BatchStats& bs, fgkl_stats* s);
 
+// One validated per-call request.
+struct CallRequest {
+  const fgkl_reads* reads = nullptr;
+  const fgkl_haplotypes* haps = nullptr;
+  bool pd = false;
+  fgkl::EngineConfig ec;
+  double* out = nullptr;
+  int64_t n_reads = 0, n_haps = 0;
+  enum State { kQueued, kTaken, kDone, kAlone } state = kQueued;  // guarded by the combiner's mutex
+};
+
+// Runs one request on engine `e`; an error is reported on the calling thread.
+int run_on(fgkl::Engine* e, const CallRequest& q, fgkl_stats* stats) {
+  int rc;
+  std::vector<int64_t> roff(static_cast<size_t>(q.n_reads) + 1), hoff(static_cast<size_t>(q.n_haps) + 1);
+  for (int64_t i = 0; i <= q.n_reads; ++i) roff[i] = q.reads->offsets[i];
+  for (int64_t i = 0; i <= q.n_haps; ++i) hoff[i] = q.haps->offsets[i];
+  const int32_t nr = static_cast<int32_t>(q.n_reads), nh = static_cast<int32_t>(q.n_haps);
+  fgkl::BatchInput in;
+  in.num_regions = 1;
+  in.region_reads = &nr;
+  in.region_haps = &nh;
+  in.bases = q.reads->bases;
+  in.quals = q.reads->quals;
+  in.ins = q.reads->ins_gop;
+  in.del = q.reads->del_gop;
+  in.gcp = q.reads->gcp;
+  in.read_off = roff.data();
+  in.hap_bases = q.haps->bases;
+  in.hap_flags = q.pd ? q.haps->flags : nullptr;
+  in.hap_off = hoff.data();
+  fgkl::BatchStats bs;
+  rc = e->compute(in, q.ec, q.out, q.n_reads * q.n_haps, &bs);
+  if (rc) return set_error(rc, e->error());
+  if (stats) to_stats(bs, stats);
+  return FGKL_OK;
+}
+
+// Runs one request on the calling thread's engine.
+int run_alone(const CallRequest& q, fgkl_stats* stats) {
+  int rc;
+  fgkl::Engine* e = thread_engine(&rc);
+  if (!e) return rc;
+  return run_on(e, q, stats);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Combining of concurrent per-call requests.
+//
+// GATK calls the native PairHMM once per region from several threads. One region's tasks occupy a
+// fraction of the SMs, and the launch chains of separate calls queue behind one another on the
+// driver's hardware queues, so separate calls from 8 threads reach about the throughput of one and
+// a half. A call therefore joins the calls waiting when it arrives. The first caller to find fewer
+// than g_max_in_flight batches running takes a free slot, its own request and every waiting one of
+// its kind, concatenates them into one batch on the slot's engine and writes each caller's results;
+// the others sleep until theirs are written. Each slot keeps one engine, so its buffers grow to the
+// largest combined batch once instead of once per calling thread. A region's program and a read's arithmetic do not depend
+// on the batch around them, so the results are bit-identical to separate calls. A combined batch
+// that fails is retried as separate calls, each on its caller's thread, so that every caller gets
+// its own status and message.
+// ---------------------------------------------------------------------------------------------
+
+constexpr int kMaxSlots = 8;                         // batches in flight at most
+std::atomic<int> g_max_in_flight{2};
+constexpr size_t kMaxCombined = 64;                  // requests in one combined batch
+constexpr int64_t kMaxCombinedReadBytes = 64 << 20;  // read bytes of one combined batch
+
+struct Combiner {
+  std::mutex mu;
+  std::condition_variable cv;
+  std::vector<CallRequest*> queue;  // waiting requests, in arrival order
+  int in_flight = 0;                // batches running
+  bool slot_busy[kMaxSlots] = {};
+  // Created on a slot's first batch and kept for the life of the process (never destroyed: their
+  // destructors would run after the CUDA runtime at exit).
+  fgkl::Engine* engines[kMaxSlots] = {};
+};
+Combiner g_combiner;
+std::atomic<uint64_t> g_combined_batches{0}, g_combined_requests{0};
+
+bool same_kind(const CallRequest& a, const CallRequest& b) {
+  return a.pd == b.pd && a.ec.double_precision == b.ec.double_precision && a.ec.double_fallback == b.ec.double_fallback &&
+         a.ec.share_suffixes == b.ec.share_suffixes;
+}
+
+int64_t read_bytes(const CallRequest& q) { return q.reads->bases_len; }
+
+// Concatenation buffers of a leading thread, kept between its batches.
+struct CombinedBuffers {
+  std::vector<uint8_t> bases, quals, ins, del, gcp, hap_bases, hap_flags;
+  std::vector<int64_t> read_off, hap_off;
+  std::vector<int32_t> region_reads, region_haps;
+  std::vector<double> out;
+};
+
+// Runs the requests of `batch` as one batch on engine `e` and scatters the results to their
+// callers; false when the batch failed (nothing is written then that a retry would not overwrite).
+bool run_combined(fgkl::Engine* e, const std::vector<CallRequest*>& batch) {
+  try {
+    thread_local CombinedBuffers b;
+    int64_t rbytes = 0, hbytes = 0, nreads = 0, nhaps = 0, nout = 0;
+    for (const CallRequest* q : batch) {
+      rbytes += q->reads->bases_len;
+      hbytes += q->haps->bases_len;
+      nreads += q->n_reads;
+      nhaps += q->n_haps;
+      nout += q->n_reads * q->n_haps;
+    }
+    const bool pd = batch[0]->pd;
+    for (auto* v : {&b.bases, &b.quals, &b.ins, &b.del, &b.gcp}) v->resize(static_cast<size_t>(rbytes));
+    b.hap_bases.resize(static_cast<size_t>(hbytes));
+    b.hap_flags.resize(pd ? static_cast<size_t>(hbytes) : 0);
+    b.read_off.resize(static_cast<size_t>(nreads) + 1);
+    b.hap_off.resize(static_cast<size_t>(nhaps) + 1);
+    b.region_reads.resize(batch.size());
+    b.region_haps.resize(batch.size());
+    b.out.resize(static_cast<size_t>(nout));
+    int64_t ro = 0, ho = 0, ri = 0, hi = 0;
+    b.read_off[0] = 0;
+    b.hap_off[0] = 0;
+    for (size_t g = 0; g < batch.size(); ++g) {
+      const CallRequest& q = *batch[g];
+      const size_t n = static_cast<size_t>(q.reads->bases_len), m = static_cast<size_t>(q.haps->bases_len);
+      if (n) {
+        std::memcpy(b.bases.data() + ro, q.reads->bases, n);
+        std::memcpy(b.quals.data() + ro, q.reads->quals, n);
+        std::memcpy(b.ins.data() + ro, q.reads->ins_gop, n);
+        std::memcpy(b.del.data() + ro, q.reads->del_gop, n);
+        std::memcpy(b.gcp.data() + ro, q.reads->gcp, n);
+      }
+      if (m) {
+        std::memcpy(b.hap_bases.data() + ho, q.haps->bases, m);
+        if (pd) std::memcpy(b.hap_flags.data() + ho, q.haps->flags, m);
+      }
+      for (int64_t r = 1; r <= q.n_reads; ++r) b.read_off[ri + r] = ro + q.reads->offsets[r];
+      for (int64_t h = 1; h <= q.n_haps; ++h) b.hap_off[hi + h] = ho + q.haps->offsets[h];
+      b.region_reads[g] = static_cast<int32_t>(q.n_reads);
+      b.region_haps[g] = static_cast<int32_t>(q.n_haps);
+      ro += static_cast<int64_t>(n);
+      ho += static_cast<int64_t>(m);
+      ri += q.n_reads;
+      hi += q.n_haps;
+    }
+    fgkl::BatchInput in;
+    in.num_regions = static_cast<int32_t>(batch.size());
+    in.region_reads = b.region_reads.data();
+    in.region_haps = b.region_haps.data();
+    in.bases = b.bases.data();
+    in.quals = b.quals.data();
+    in.ins = b.ins.data();
+    in.del = b.del.data();
+    in.gcp = b.gcp.data();
+    in.read_off = b.read_off.data();
+    in.hap_bases = b.hap_bases.data();
+    in.hap_flags = pd ? b.hap_flags.data() : nullptr;
+    in.hap_off = b.hap_off.data();
+    if (e->compute(in, batch[0]->ec, b.out.data(), nout, nullptr) != FGKL_OK) return false;
+    g_combined_batches.fetch_add(1, std::memory_order_relaxed);
+    g_combined_requests.fetch_add(batch.size(), std::memory_order_relaxed);
+    int64_t o = 0;
+    for (const CallRequest* q : batch) {
+      const int64_t k = q->n_reads * q->n_haps;
+      std::memcpy(q->out, b.out.data() + o, static_cast<size_t>(k) * sizeof(double));
+      o += k;
+    }
+    return true;
+  } catch (...) {
+    return false;
+  }
+}
+
+int combined_call(CallRequest& q) {
+  Combiner& c = g_combiner;
+  std::unique_lock<std::mutex> lk(c.mu);
+  c.queue.push_back(&q);
+  for (;;) {
+    if (q.state == CallRequest::kDone) return FGKL_OK;
+    if (q.state == CallRequest::kAlone) {
+      lk.unlock();
+      return run_alone(q, nullptr);
+    }
+    if (q.state == CallRequest::kQueued &&
+        c.in_flight < std::min(kMaxSlots, std::max(1, g_max_in_flight.load(std::memory_order_relaxed)))) {
+      int slot = 0;
+      while (c.slot_busy[slot]) ++slot;
+      if (!c.engines[slot]) {
+        int d = 0;
+        const int rc = pick_device(&d);
+        if (rc != FGKL_OK) {
+          // No device: this request leaves the queue with the error; the others find the same.
+          c.queue.erase(std::find(c.queue.begin(), c.queue.end(), &q));
+          return rc;
+        }
+        c.engines[slot] = new fgkl::Engine(d);
+      }
+      // Lead: this request first, then the waiting ones of its kind in arrival order.
+      std::vector<CallRequest*> batch{&q};
+      int64_t bytes = read_bytes(q);
+      size_t keep = 0;
+      for (CallRequest* r : c.queue) {
+        if (r != &q && same_kind(*r, q) && batch.size() < kMaxCombined && bytes + read_bytes(*r) <= kMaxCombinedReadBytes) {
+          batch.push_back(r);
+          bytes += read_bytes(*r);
+        } else if (r != &q) {
+          c.queue[keep++] = r;
+        }
+      }
+      c.queue.resize(keep);
+      for (CallRequest* r : batch) r->state = CallRequest::kTaken;
+      ++c.in_flight;
+      c.slot_busy[slot] = true;
+      fgkl::Engine* const e = c.engines[slot];
+      lk.unlock();
+      if (batch.size() == 1) {
+        // Alone after all: the error, if any, is set on this thread directly.
+        const int rc = run_on(e, q, nullptr);
+        lk.lock();
+        --c.in_flight;
+        c.slot_busy[slot] = false;
+        c.cv.notify_all();
+        return rc;
+      }
+      const bool ok = run_combined(e, batch);
+      lk.lock();
+      --c.in_flight;
+      c.slot_busy[slot] = false;
+      for (CallRequest* r : batch) r->state = ok ? CallRequest::kDone : CallRequest::kAlone;
+      c.cv.notify_all();
+      continue;
+    }
+    c.cv.wait(lk);
+  }
+}
+
 int per_call(const fgkl_reads* reads, const fgkl_haplotypes* haps, const fgkl_config* cfg, bool pd, double* out, int64_t out_len,
              fgkl_stats* stats) {
   t_error.clear();
@@ -92,34 +328,18 @@ int per_call(const fgkl_reads* reads, const fgkl_haplotypes* haps, const fgkl_co
       return set_error(FGKL_E_EMPTY_HAPLOTYPE, "haplotype " + std::to_string(h) + " has no bases");
   if (stats) std::memset(stats, 0, sizeof *stats);
   if (expected == 0) return FGKL_OK;
-  fgkl::Engine* e = thread_engine(&rc);
-  if (!e) return rc;
-  std::vector<int64_t> roff(static_cast<size_t>(n_reads) + 1), hoff(static_cast<size_t>(n_haps) + 1);
-  for (int64_t i = 0; i <= n_reads; ++i) roff[i] = reads->offsets[i];
-  for (int64_t i = 0; i <= n_haps; ++i) hoff[i] = haps->offsets[i];
-  const int32_t nr = static_cast<int32_t>(n_reads), nh = static_cast<int32_t>(n_haps);
-  fgkl::BatchInput in;
-  in.num_regions = 1;
-  in.region_reads = &nr;
-  in.region_haps = &nh;
-  in.bases = reads->bases;
-  in.quals = reads->quals;
-  in.ins = reads->ins_gop;
-  in.del = reads->del_gop;
-  in.gcp = reads->gcp;
-  in.read_off = roff.data();
-  in.hap_bases = haps->bases;
-  in.hap_flags = pd ? haps->flags : nullptr;
-  in.hap_off = hoff.data();
-  fgkl::EngineConfig ec;
-  ec.double_precision = cfg->double_precision != 0;
-  ec.double_fallback = cfg->double_fallback != 0;
-  ec.share_suffixes = cfg->share_suffixes != 0;
-  fgkl::BatchStats bs;
-  rc = e->compute(in, ec, out, out_len, &bs);
-  if (rc) return set_error(rc, e->error());
-  if (stats) to_stats(bs, stats);
-  return FGKL_OK;
+  CallRequest q;
+  q.reads = reads;
+  q.haps = haps;
+  q.pd = pd;
+  q.ec.double_precision = cfg->double_precision != 0;
+  q.ec.double_fallback = cfg->double_fallback != 0;
+  q.ec.share_suffixes = cfg->share_suffixes != 0;
+  q.out = out;
+  q.n_reads = n_reads;
+  q.n_haps = n_haps;
+  if (stats || g_max_in_flight.load(std::memory_order_relaxed) == 0) return run_alone(q, stats);
+  return combined_call(q);
 }
 
 fgkl_config default_config(int32_t double_precision) {
@@ -214,6 +434,20 @@ int fgkl_pdhmm_compute(const fgkl_reads* reads, const fgkl_haplotypes* haps, int
 int fgkl_pdhmm_compute_config(const fgkl_reads* reads, const fgkl_haplotypes* haps, const fgkl_config* config, double* out,
                               int64_t out_len, fgkl_stats* stats) {
   return per_call(reads, haps, config, true, out, out_len, stats);
+}
+
+int fgkl_set_call_combining(int32_t max_batches) {
+  t_error.clear();
+  if (max_batches < 0 || max_batches > kMaxSlots) return set_error(FGKL_E_INVALID_ARGUMENT, "max_batches must be 0 to 8");
+  return g_max_in_flight.exchange(max_batches);
+}
+
+int fgkl_call_combining_stats(uint64_t* batches, uint64_t* requests) {
+  t_error.clear();
+  if (!batches || !requests) return set_error(FGKL_E_INVALID_ARGUMENT, "null argument");
+  *batches = g_combined_batches.load(std::memory_order_relaxed);
+  *requests = g_combined_requests.load(std::memory_order_relaxed);
+  return FGKL_OK;
 }
 
 const char* fgkl_backend(void) { return "cuda-sm100a"; }

@@ -10,8 +10,9 @@
  *
  * Threading: any number of threads may call concurrently. The per-call entry points use a
  * context private to the calling thread (created on first use), mirroring fgkl's thread-local
- * workspaces (crates/pairhmm/src/kernel.rs:144-163). Explicit contexts must not be shared between
- * threads without external locking.
+ * workspaces (crates/pairhmm/src/kernel.rs:144-163). Calls from several threads that meet are run
+ * as one batch on an engine kept for combining (fgkl_set_call_combining). Explicit contexts must not
+ * be shared between threads without external locking.
  */
 #ifndef FGKL_B200_H
 #define FGKL_B200_H
@@ -98,6 +99,32 @@ int fgkl_pdhmm_compute(const fgkl_reads* reads, const fgkl_haplotypes* haps, int
                        double* out, int64_t out_len);
 int fgkl_pdhmm_compute_config(const fgkl_reads* reads, const fgkl_haplotypes* haps, const fgkl_config* config,
                               double* out, int64_t out_len, fgkl_stats* stats);
+
+/*
+ * Combining of concurrent per-call requests (no counterpart in the reference, whose calls each run
+ * on the calling thread, crates/jni/src/lib.rs:5-9). The four per-call functions above accept any
+ * number of concurrent callers, as fgkl's do.
+ *
+ * A call made while other threads' calls wait joins them. The first caller to find fewer than
+ * `max_batches` batches in flight takes every waiting request of its kind (same entry point and
+ * the same three config flags). It runs them as one batch and writes each caller's results; the
+ * others wait for theirs.
+ *
+ * Guarantees:
+ * - Results are bit-identical to separate calls.
+ * - A failed batch is retried as separate calls, each on its own thread, so every caller gets its
+ *   own status and fgkl_last_error.
+ * - Calls that ask for stats always run alone.
+ *
+ * Each of the max_batches batches in flight runs on an engine of its own, kept for the process.
+ * max_batches = 0 runs every call alone. The default is 2 and the largest value is 8. Returns the
+ * previous value, or FGKL_E_INVALID_ARGUMENT for a value outside 0..8.
+ */
+int fgkl_set_call_combining(int32_t max_batches);
+
+/* Combined batches of two or more requests run since the library loaded, and the requests they
+ * held. */
+int fgkl_call_combining_stats(uint64_t* batches, uint64_t* requests);
 
 /* Name of the backend, the analogue of backendNative (crates/jni/src/lib.rs:149-156). */
 const char* fgkl_backend(void);

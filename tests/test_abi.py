@@ -120,3 +120,16 @@ def test_without_a_device_the_call_fails_loudly_instead_of_falling_back():
     assert rc == _lib.FGKL_E_NO_DEVICE, msg
     with pytest.raises(Exception):
         PairHmm().compute_log10_likelihoods([good()], [b"ACGT"])
+
+
+def test_call_combining_switch():
+    L = _lib.lib()
+    prev = L.fgkl_set_call_combining(3)
+    assert prev >= 0
+    assert L.fgkl_set_call_combining(-1) == _lib.FGKL_E_INVALID_ARGUMENT
+    assert L.fgkl_set_call_combining(9) == _lib.FGKL_E_INVALID_ARGUMENT
+    assert L.fgkl_set_call_combining(prev) == 3
+    b, r = C.c_uint64(), C.c_uint64()
+    assert L.fgkl_call_combining_stats(C.byref(b), C.byref(r)) == 0
+    assert r.value >= 2 * b.value
+    assert L.fgkl_call_combining_stats(None, C.byref(r)) == _lib.FGKL_E_INVALID_ARGUMENT
