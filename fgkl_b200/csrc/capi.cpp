@@ -79,7 +79,7 @@ struct CallRequest {
 };
 
 // Runs one request on engine `e`; an error is reported on the calling thread.
-int run_on(fgkl::Engine* e, const CallRequest& q, fgkl_stats* stats) {
+int run_on(fgkl::Engine* e, const CallRequest& q, fgkl_stats* stats) try {
   int rc;
   std::vector<int64_t> roff(static_cast<size_t>(q.n_reads) + 1), hoff(static_cast<size_t>(q.n_haps) + 1);
   for (int64_t i = 0; i <= q.n_reads; ++i) roff[i] = q.reads->offsets[i];
@@ -103,14 +103,18 @@ int run_on(fgkl::Engine* e, const CallRequest& q, fgkl_stats* stats) {
   if (rc) return set_error(rc, e->error());
   if (stats) to_stats(bs, stats);
   return FGKL_OK;
+} catch (...) {
+  return set_error(FGKL_E_CUDA, "host memory allocation failed");
 }
 
 // Runs one request on the calling thread's engine.
-int run_alone(const CallRequest& q, fgkl_stats* stats) {
+int run_alone(const CallRequest& q, fgkl_stats* stats) try {
   int rc;
   fgkl::Engine* e = thread_engine(&rc);
   if (!e) return rc;
   return run_on(e, q, stats);
+} catch (...) {
+  return set_error(FGKL_E_CUDA, "host memory allocation failed");
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -162,13 +166,14 @@ struct CombinedBuffers {
   std::vector<double> out;
 };
 
-// Runs the requests of `batch` as one batch on engine `e` and scatters the results to their
+// Runs the n requests of `batch` as one batch on engine `e` and scatters the results to their
 // callers; false when the batch failed (nothing is written then that a retry would not overwrite).
-bool run_combined(fgkl::Engine* e, const std::vector<CallRequest*>& batch) {
+bool run_combined(fgkl::Engine* e, CallRequest* const* batch, size_t n_batch) {
   try {
     thread_local CombinedBuffers b;
     int64_t rbytes = 0, hbytes = 0, nreads = 0, nhaps = 0, nout = 0;
-    for (const CallRequest* q : batch) {
+    for (size_t g = 0; g < n_batch; ++g) {
+      const CallRequest* q = batch[g];
       rbytes += q->reads->bases_len;
       hbytes += q->haps->bases_len;
       nreads += q->n_reads;
@@ -181,13 +186,13 @@ bool run_combined(fgkl::Engine* e, const std::vector<CallRequest*>& batch) {
     b.hap_flags.resize(pd ? static_cast<size_t>(hbytes) : 0);
     b.read_off.resize(static_cast<size_t>(nreads) + 1);
     b.hap_off.resize(static_cast<size_t>(nhaps) + 1);
-    b.region_reads.resize(batch.size());
-    b.region_haps.resize(batch.size());
+    b.region_reads.resize(n_batch);
+    b.region_haps.resize(n_batch);
     b.out.resize(static_cast<size_t>(nout));
     int64_t ro = 0, ho = 0, ri = 0, hi = 0;
     b.read_off[0] = 0;
     b.hap_off[0] = 0;
-    for (size_t g = 0; g < batch.size(); ++g) {
+    for (size_t g = 0; g < n_batch; ++g) {
       const CallRequest& q = *batch[g];
       const size_t n = static_cast<size_t>(q.reads->bases_len), m = static_cast<size_t>(q.haps->bases_len);
       if (n) {
@@ -211,7 +216,7 @@ bool run_combined(fgkl::Engine* e, const std::vector<CallRequest*>& batch) {
       hi += q.n_haps;
     }
     fgkl::BatchInput in;
-    in.num_regions = static_cast<int32_t>(batch.size());
+    in.num_regions = static_cast<int32_t>(n_batch);
     in.region_reads = b.region_reads.data();
     in.region_haps = b.region_haps.data();
     in.bases = b.bases.data();
@@ -225,9 +230,10 @@ bool run_combined(fgkl::Engine* e, const std::vector<CallRequest*>& batch) {
     in.hap_off = b.hap_off.data();
     if (e->compute(in, batch[0]->ec, b.out.data(), nout, nullptr) != FGKL_OK) return false;
     g_combined_batches.fetch_add(1, std::memory_order_relaxed);
-    g_combined_requests.fetch_add(batch.size(), std::memory_order_relaxed);
+    g_combined_requests.fetch_add(n_batch, std::memory_order_relaxed);
     int64_t o = 0;
-    for (const CallRequest* q : batch) {
+    for (size_t g = 0; g < n_batch; ++g) {
+      const CallRequest* q = batch[g];
       const int64_t k = q->n_reads * q->n_haps;
       std::memcpy(q->out, b.out.data() + o, static_cast<size_t>(k) * sizeof(double));
       o += k;
@@ -241,7 +247,12 @@ bool run_combined(fgkl::Engine* e, const std::vector<CallRequest*>& batch) {
 int combined_call(CallRequest& q) {
   Combiner& c = g_combiner;
   std::unique_lock<std::mutex> lk(c.mu);
-  c.queue.push_back(&q);
+  try {
+    c.queue.push_back(&q);
+  } catch (...) {
+    lk.unlock();
+    return run_alone(q, nullptr);
+  }
   for (;;) {
     if (q.state == CallRequest::kDone) return FGKL_OK;
     if (q.state == CallRequest::kAlone) {
@@ -254,33 +265,42 @@ int combined_call(CallRequest& q) {
       while (c.slot_busy[slot]) ++slot;
       if (!c.engines[slot]) {
         int d = 0;
-        const int rc = pick_device(&d);
+        int rc = pick_device(&d);
+        if (rc == FGKL_OK) {
+          try {
+            c.engines[slot] = new fgkl::Engine(d);
+          } catch (...) {
+            rc = set_error(FGKL_E_CUDA, "host memory allocation failed");
+          }
+        }
         if (rc != FGKL_OK) {
-          // No device: this request leaves the queue with the error; the others find the same.
+          // This request leaves the queue with the error; the others meet the same.
           c.queue.erase(std::find(c.queue.begin(), c.queue.end(), &q));
           return rc;
         }
-        c.engines[slot] = new fgkl::Engine(d);
       }
-      // Lead: this request first, then the waiting ones of its kind in arrival order.
-      std::vector<CallRequest*> batch{&q};
+      // Lead: this request first, then the waiting ones of its kind in arrival order (no
+      // allocation here, so nothing can throw while requests are moved out of the queue).
+      CallRequest* batch[kMaxCombined];
+      size_t n_batch = 0;
+      batch[n_batch++] = &q;
       int64_t bytes = read_bytes(q);
       size_t keep = 0;
       for (CallRequest* r : c.queue) {
-        if (r != &q && same_kind(*r, q) && batch.size() < kMaxCombined && bytes + read_bytes(*r) <= kMaxCombinedReadBytes) {
-          batch.push_back(r);
+        if (r != &q && same_kind(*r, q) && n_batch < kMaxCombined && bytes + read_bytes(*r) <= kMaxCombinedReadBytes) {
+          batch[n_batch++] = r;
           bytes += read_bytes(*r);
         } else if (r != &q) {
           c.queue[keep++] = r;
         }
       }
       c.queue.resize(keep);
-      for (CallRequest* r : batch) r->state = CallRequest::kTaken;
+      for (size_t k = 0; k < n_batch; ++k) batch[k]->state = CallRequest::kTaken;
       ++c.in_flight;
       c.slot_busy[slot] = true;
       fgkl::Engine* const e = c.engines[slot];
       lk.unlock();
-      if (batch.size() == 1) {
+      if (n_batch == 1) {
         // Alone after all: the error, if any, is set on this thread directly.
         const int rc = run_on(e, q, nullptr);
         lk.lock();
@@ -289,11 +309,11 @@ int combined_call(CallRequest& q) {
         c.cv.notify_all();
         return rc;
       }
-      const bool ok = run_combined(e, batch);
+      const bool ok = run_combined(e, batch, n_batch);
       lk.lock();
       --c.in_flight;
       c.slot_busy[slot] = false;
-      for (CallRequest* r : batch) r->state = ok ? CallRequest::kDone : CallRequest::kAlone;
+      for (size_t k = 0; k < n_batch; ++k) batch[k]->state = ok ? CallRequest::kDone : CallRequest::kAlone;
       c.cv.notify_all();
       continue;
     }
