@@ -544,7 +544,7 @@ def ours(args, rank, world, local, pg):
         rd, hp, o, n = c
         _check(L_pc.fgkl_pairhmm_compute_config(C.byref(rd), C.byref(hp), C.byref(c_cfg), _ptr(o, _lib.f64p), n, None))
 
-    for c in calls[:4]:
+    for c in calls:  # untimed: the engine that serves these calls at full size
         call(c)
     pc_cells = sum(sum(len(r.bases) for r in reads) * sum(len(h) for h in haps) for reads, haps in pc_regions)
     torch.cuda.synchronize(device)
