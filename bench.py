@@ -236,6 +236,21 @@ def reference_arm(args, rank, world, pg):
 # ncu-measured DRAM traffic of the dominant kernel (profiles/, committed summaries)
 # ---------------------------------------------------------------------------------------------
 
+def hbm_peak_gbs():
+    """HBM bandwidth for a roofline: MEASURED_PEAKS.json's copy bandwidth when the file exists,
+    else 6,650 GB/s, an earlier copy measurement on these B200s."""
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.exists():
+        try:
+            d = json.loads(path.read_text())
+            for k in ("hbm_gbs", "hbm_GBps", "hbm"):
+                if isinstance(d.get(k), (int, float)):
+                    return float(d[k]), f"MEASURED_PEAKS.json {k} (measured)"
+        except (ValueError, OSError):
+            pass
+    return 6650.0, "fallback 6,650 GB/s copy bandwidth (MEASURED_PEAKS.json absent)"
+
+
 def dominant_traffic(kernel, cells):
     """DRAM bytes (read + write) of one launch of `kernel` computing `cells` DP cells: the bytes per
     computed cell ncu measured for that kernel (committed summary
@@ -278,7 +293,7 @@ def time_device(stream, flush, fn, steps):
 def extra_configs(args, device, stream, flush, threads, which=("c2", "c3", "c4"), regions=0):
     """c2 (shared SNP haplotypes), c3 (PD-HMM) and c4 (adjoint), one device-timed line each
     (`regions` > 0 shrinks them, for profiling)."""
-    from fgkl_b200 import BatchContext, Config, Precision, synthetic
+    from fgkl_b200 import BatchContext, Config, Precision, _lib, synthetic
     from fgkl_b200.adjoint import AdjointContext, params_from_quals
     from oracle import oracle
 
@@ -316,6 +331,23 @@ def extra_configs(args, device, stream, flush, threads, which=("c2", "c3", "c4")
         sample = [0]
         ref = oracle.workload_matrix(w, sample, threads)
         offs = w.output_offsets()
+        # FP32 roofline of the dominant first-pass launch and of the whole step (12 FLOP a forward or
+        # PD cell, 11 a backward cell), against the FP32 FMA peak measured live on this GPU.
+        s_tf, p_tf, clk = C.c_double(), C.c_double(), C.c_double()
+        _lib.lib().fgkl_probe_fp32_tflops(device, C.byref(s_tf), C.byref(p_tf), C.byref(clk))
+        peak = max(s_tf.value, p_tf.value)
+        first = [x for x in prof if not x["recomputation"]]
+        dom = max(first, key=lambda x: x["ms"])
+        dom_tf = (FLOP_FORWARD * dom["forward_cells"] + FLOP_BACKWARD * dom["backward_cells"]) / (dom["ms"] / 1e3) / 1e12
+        step_tf = (FLOP_FORWARD * st.forward_cells + FLOP_BACKWARD * st.backward_cells) / t / 1e12
+        kinds = {0: "PackedF32", 1: "OneF32", 2: "OneF64", 3: "OneF32Pd", 4: "OneF64Pd", 5: "PackedF32Pd"}
+        kname = "pd_kernel" if dom["kind"] in (3, 4, 5) else "pairhmm_kernel"
+        roof = {"bound": "fp32", "unit": "TFLOP/s", "peak": peak, "achieved": dom_tf, "frac": dom_tf / peak,
+                "dominant_launch": {"kernel": f"{kname}<{kinds.get(dom['kind'], dom['kind'])}, {dom['rows']}>",
+                                    "ms": dom["ms"], "forward_cells": dom["forward_cells"],
+                                    "backward_cells": dom["backward_cells"],
+                                    "share_of_serialised_time": dom["ms"] / max(1e-9, sum(x["ms"] for x in prof))},
+                "whole_step": {"achieved": step_tf, "frac": step_tf / peak}}
         res[name] = {"workload": note, "regions": w.num_regions, "nominal_gcups": nominal / t / 1e9,
                      "computed_gcups": st.computed_cells / t / 1e9, "ms_per_step": 1e3 * t, "steps": steps,
                      "nominal_cells": nominal, "computed_cells": int(st.computed_cells),
@@ -325,6 +357,7 @@ def extra_configs(args, device, stream, flush, threads, which=("c2", "c3", "c4")
                                        "fp64_recomputation": sum(x["ms"] for x in prof if x["recomputation"])},
                      "max_abs_dlog10_sample": float(np.max(np.abs(out[offs[0]:offs[1]] - ref))),
                      "accuracy_sample": "region 0 against the FP64 oracle",
+                     "roofline": roof,
                      "launch_tuning": tuning}
         if not args.no_cpu_baseline:
             # fgkl's CPU algorithm for this configuration (oracle/fgkl_cpu.c: the plain kernel for
@@ -368,6 +401,17 @@ def extra_configs(args, device, stream, flush, threads, which=("c2", "c3", "c4")
             for k in range(4):
                 g_ref[k, a - lo:b - lo] += gr[k]
     ours_g = [r.gap_open_ins, r.gap_open_del, r.gap_continuation, r.base_error]
+    # HBM roofline: the adjoint stores every column's backward record (BM, BX, BY rows of a lane,
+    # padded to 16 bytes) and reads it back in the forward sweep, 2 x (hap length + 1) x 32 x record
+    # bytes per (read, haplotype) pair; its FP32 and FP64 arithmetic take a few ms of the step.
+    rl = np.diff(w.read_offsets)
+    rec = ((3 * -(-rl // 31) + 3) // 4) * 4 * 4
+    hl = np.diff(w.hap_offsets) + 1
+    rb = np.add.reduceat(rec, np.concatenate([[0], np.cumsum(w.region_reads)[:-1]]))
+    hb = np.add.reduceat(hl, np.concatenate([[0], np.cumsum(w.region_haps)[:-1]]))
+    adj_bytes = float(2 * 32 * np.sum(rb.astype(np.float64) * hb))
+    hbm_peak, hbm_src = hbm_peak_gbs()
+    adj_gbs = adj_bytes / t / 1e9
     rel = [abs(ours_g[k][lo:hi].sum() - g_ref[k].sum()) / abs(g_ref[k].sum()) for k in range(4)]
     res["c4"] = {"workload": "adjoint: 256 regions x 64 reads (151) x 8 haplotypes (350); gradients of the summed log10 "
                              "likelihood w.r.t. gap-open (ins, del), gap continuation, base error per read position",
@@ -375,6 +419,9 @@ def extra_configs(args, device, stream, flush, threads, which=("c2", "c3", "c4")
                  "nominal_cells": nominal, "cells_per_pair_visited": "forward + backward sweep each",
                  "fp64_reads": r.fp64_reads,
                  "max_rel_err_global_gradients_sample": max(rel),
+                 "roofline": {"bound": "hbm", "unit": "GB/s", "achieved": adj_gbs, "peak": hbm_peak,
+                              "frac": adj_gbs / hbm_peak, "algorithmic_bytes_per_step": adj_bytes,
+                              "peak_source": hbm_src},
                  "accuracy_sample": "region 0 against the FP64 scalar adjoint (summed gradients)"}
     actx.close()
     return res
@@ -604,7 +651,8 @@ def ours(args, rank, world, local, pg):
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                      "traffic": traffic,
                      "peak_source": f"measured FP32 FMA probe on this GPU (scalar {s_tf.value:.1f}, packed {p_tf.value:.1f} "
-                                    "TFLOP/s); MEASURED_PEAKS.json holds no FP32 figure",
+                                    "TFLOP/s); MEASURED_PEAKS.json has no FP32 figure (it holds HBM and bf16 ones when "
+                                    "present)",
                      "flop_per_cell": {"forward": FLOP_FORWARD, "backward": FLOP_BACKWARD},
                      "dominant_launch": dominant,
                      "whole_step": {"achieved": step_achieved, "frac": step_achieved / peak,
