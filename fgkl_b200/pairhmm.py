@@ -121,6 +121,23 @@ def _check(rc: int) -> None:
     raise DeviceError(rc, msg)
 
 
+def set_call_combining(max_batches: int) -> int:
+    """Sets how many combined batches of concurrent per-call requests may run at once (0: every
+    call runs alone; at most 8; default 2) and returns the previous value. Calls made through
+    PairHmm / PdPairHmm carry counters and always run alone; the JNI entry points do not."""
+    rc = lib().fgkl_set_call_combining(int(max_batches))
+    if rc < 0:
+        raise ValueError(_lib.last_error())
+    return rc
+
+
+def call_combining_stats() -> tuple[int, int]:
+    """(combined batches of two or more requests, requests they held) since the library loaded."""
+    b, r = C.c_uint64(), C.c_uint64()
+    _check(lib().fgkl_call_combining_stats(C.byref(b), C.byref(r)))
+    return b.value, r.value
+
+
 class _Flat:
     """Reads and haplotypes flattened into the JNI layout, kept alive for the call."""
 

@@ -133,3 +133,13 @@ def test_call_combining_switch():
     assert L.fgkl_call_combining_stats(C.byref(b), C.byref(r)) == 0
     assert r.value >= 2 * b.value
     assert L.fgkl_call_combining_stats(None, C.byref(r)) == _lib.FGKL_E_INVALID_ARGUMENT
+
+
+def test_call_combining_python_mirror():
+    import fgkl_b200
+    prev = fgkl_b200.set_call_combining(1)
+    assert fgkl_b200.set_call_combining(prev) == 1
+    with pytest.raises(ValueError):
+        fgkl_b200.set_call_combining(9)
+    batches, requests = fgkl_b200.call_combining_stats()
+    assert requests >= 2 * batches
