@@ -122,6 +122,30 @@ def test_without_a_device_the_call_fails_loudly_instead_of_falling_back():
         PairHmm().compute_log10_likelihoods([good()], [b"ACGT"])
 
 
+@pytest.mark.skipif(has_gpu(), reason="checks the no-device path")
+def test_concurrent_calls_without_a_device_all_fail_and_none_waits():
+    # Every caller leads in turn (no batch ever starts), finds no device, leaves the queue and
+    # returns its own error; a request left queued would make a later caller wait for ever.
+    import threading
+    results = []
+    lock = threading.Lock()
+
+    def worker():
+        for _ in range(20):
+            rc, msg = raw_call([0, 4], [0, 4])
+            with lock:
+                results.append((rc, msg))
+
+    ts = [threading.Thread(target=worker) for _ in range(8)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join(timeout=60)
+    assert not any(t.is_alive() for t in ts)
+    assert len(results) == 160
+    assert all(rc == _lib.FGKL_E_NO_DEVICE and msg for rc, msg in results)
+
+
 def test_call_combining_switch():
     L = _lib.lib()
     prev = L.fgkl_set_call_combining(3)
