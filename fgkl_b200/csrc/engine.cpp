@@ -4,7 +4,6 @@
 #include <atomic>
 #include <chrono>
 #include <cstring>
-#include <map>
 #include <string>
 #include <thread>
 
@@ -413,35 +412,42 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
   if (n_stream > INT32_MAX || n_seq > INT32_MAX || n_pd_seq > INT32_MAX || n_haps > INT32_MAX)
     return fail(FGKL_E_INVALID_ARGUMENT, "batch too large for 32-bit plan offsets; split it");
 
-  // Tasks: reads sorted longest first; FP32 packs consecutive pairs below 256 bases.
-  struct Key {
-    Kind kind;
-    int rows;
-    bool operator<(const Key& o) const { return kind != o.kind ? kind < o.kind : rows < o.rows; }
+  // Tasks: reads sorted longest first; FP32 packs consecutive pairs below 256 bases. A task costs
+  // its region's stream length times its rows, so within a bin (one rows value) the costliest
+  // regions' tasks come first: regions are visited in that order (ties by index), which lists each
+  // bin's tasks longest first without sorting them.
+  constexpr int kKinds = 6;
+  struct BinList {
+    std::vector<std::pair<uint64_t, Task>> list;
+    uint64_t fwd_cells = 0, bwd_cells = 0;  // forward, backward DP cells
   };
-  std::map<Key, std::vector<std::pair<uint64_t, Task>>> by_bin;
-  std::map<Key, std::pair<uint64_t, uint64_t>> bin_cells;  // forward, backward DP cells per bin
+  std::vector<BinList> by_bin(static_cast<size_t>(kKinds) * kRowBins);
+  auto bin_at = [&](Kind kind, int rows) -> BinList& { return by_bin[static_cast<size_t>(kind) * kRowBins + rows]; };
+  std::vector<int> region_order(static_cast<size_t>(N));
+  for (int g = 0; g < N; ++g) region_order[g] = g;
+  auto cost_of = [&](int g) { return plans[g].prog.fwd.size() + plans[g].prog.bwd.size() + 31; };
+  std::stable_sort(region_order.begin(), region_order.end(), [&](int a, int b) { return cost_of(a) > cost_of(b); });
   std::vector<int> order;
-  for (int g = 0; g < N; ++g) {
+  for (const int g : region_order) {
     const int n_reads = in.region_reads[g];
     if (n_reads == 0 || in.region_haps[g] == 0) continue;
     order.resize(static_cast<size_t>(n_reads));
     for (int r = 0; r < n_reads; ++r) order[r] = r;
     auto len_of = [&](int r) { return static_cast<int>(in.read_off[first_read[g] + r + 1] - in.read_off[first_read[g] + r]); };
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return len_of(a) > len_of(b); });
-    const uint64_t cost_cols = plans[g].prog.fwd.size() + plans[g].prog.bwd.size() + 31;
+    const uint64_t cost_cols = cost_of(g);
     const uint64_t fcols = plans[g].prog.fwd_columns, bcols = plans[g].prog.bwd_columns;
     auto count = [&](Kind kind, int rows, int len) {
-      auto& c = bin_cells[{kind, rows}];
-      c.first += fcols * static_cast<uint64_t>(len);
-      c.second += bcols * static_cast<uint64_t>(len);
+      BinList& c = bin_at(kind, rows);
+      c.fwd_cells += fcols * static_cast<uint64_t>(len);
+      c.bwd_cells += bcols * static_cast<uint64_t>(len);
     };
     size_t i = 0;
     if (pd && cfg.double_precision) {
       // PD in FP64: one read per warp.
       for (; i < order.size(); ++i) {
         const int rows = single_rows(len_of(order[i]));
-        by_bin[{Kind::kOneF64Pd, rows}].push_back(
+        bin_at(Kind::kOneF64Pd, rows).list.push_back(
             {cost_cols * rows, Task{g, {static_cast<int32_t>(first_read[g] + order[i]), -1}, rows, -1}});
         count(Kind::kOneF64Pd, rows, len_of(order[i]));
       }
@@ -450,7 +456,7 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
       // launch configuration asks for one read per warp.
       while (i < order.size() && (packed_rows(len_of(order[i])) > 8 || tuning_.reads_per_warp == 1)) {
         const int rows = single_rows(len_of(order[i]));
-        by_bin[{Kind::kOneF32Pd, rows}].push_back(
+        bin_at(Kind::kOneF32Pd, rows).list.push_back(
             {cost_cols * rows, Task{g, {static_cast<int32_t>(first_read[g] + order[i]), -1}, rows, -1}});
         count(Kind::kOneF32Pd, rows, len_of(order[i]));
         ++i;
@@ -459,20 +465,20 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
         const int rows = packed_rows(len_of(order[i]));
         const int32_t a = static_cast<int32_t>(first_read[g] + order[i]);
         const int32_t b = i + 1 < order.size() ? static_cast<int32_t>(first_read[g] + order[i + 1]) : -1;
-        by_bin[{Kind::kPackedF32Pd, rows}].push_back({cost_cols * rows, Task{g, {a, b}, rows, -1}});
+        bin_at(Kind::kPackedF32Pd, rows).list.push_back({cost_cols * rows, Task{g, {a, b}, rows, -1}});
         count(Kind::kPackedF32Pd, rows, len_of(order[i]) + (i + 1 < order.size() ? len_of(order[i + 1]) : 0));
       }
     } else if (cfg.double_precision || plans[g].extra_codes) {
       for (; i < order.size(); ++i) {
         const int rows = single_rows(len_of(order[i]));
-        by_bin[{Kind::kOneF64, rows}].push_back(
+        bin_at(Kind::kOneF64, rows).list.push_back(
             {cost_cols * rows, Task{g, {static_cast<int32_t>(first_read[g] + order[i]), -1}, rows, -1}});
         count(Kind::kOneF64, rows, len_of(order[i]));
       }
     } else {
       while (i < order.size() && packed_rows(len_of(order[i])) > 8) {
         const int rows = single_rows(len_of(order[i]));
-        by_bin[{Kind::kOneF32, rows}].push_back(
+        bin_at(Kind::kOneF32, rows).list.push_back(
             {cost_cols * rows, Task{g, {static_cast<int32_t>(first_read[g] + order[i]), -1}, rows, -1}});
         count(Kind::kOneF32, rows, len_of(order[i]));
         ++i;
@@ -481,30 +487,36 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
         const int rows = packed_rows(len_of(order[i]));
         const int32_t a = static_cast<int32_t>(first_read[g] + order[i]);
         const int32_t b = i + 1 < order.size() ? static_cast<int32_t>(first_read[g] + order[i + 1]) : -1;
-        by_bin[{Kind::kPackedF32, rows}].push_back({cost_cols * rows, Task{g, {a, b}, rows, -1}});
+        bin_at(Kind::kPackedF32, rows).list.push_back({cost_cols * rows, Task{g, {a, b}, rows, -1}});
         count(Kind::kPackedF32, rows, len_of(order[i]) + (i + 1 < order.size() ? len_of(order[i + 1]) : 0));
       }
     }
   }
   std::vector<Task> tasks;
   std::vector<std::pair<uint64_t, Bin>> first;
-  for (auto& [key, list] : by_bin) {
-    std::stable_sort(list.begin(), list.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
-    Bin b{key.kind, key.rows, static_cast<int>(tasks.size()), static_cast<int>(list.size()), 0, 0, 0};
-    b.fwd_cells = bin_cells[key].first;
-    b.bwd_cells = bin_cells[key].second;
-    uint64_t cost = 0;
-    for (auto& e : list) {
-      tasks.push_back(e.second);
-      cost += e.first;
+  size_t n_tasks_all = 0;
+  for (const BinList& bl : by_bin) n_tasks_all += bl.list.size();
+  tasks.reserve(n_tasks_all);
+  for (int kind = 0; kind < kKinds; ++kind)
+    for (int rows = 0; rows < kRowBins; ++rows) {
+      const BinList& bl = by_bin[static_cast<size_t>(kind) * kRowBins + rows];
+      const auto& list = bl.list;
+      if (list.empty()) continue;
+      Bin b{static_cast<Kind>(kind), rows, static_cast<int>(tasks.size()), static_cast<int>(list.size()), 0, 0, 0};
+      b.fwd_cells = bl.fwd_cells;
+      b.bwd_cells = bl.bwd_cells;
+      uint64_t cost = 0;
+      for (auto& e : list) {
+        tasks.push_back(e.second);
+        cost += e.first;
+      }
+      int per_sm = 0, threads = 0;
+      occupancy(b.kind, b.rows, &per_sm, &threads);
+      if (per_sm <= 0) return fail(FGKL_E_CUDA, "kernel instantiation unavailable on this device");
+      const int grid = std::max(sms_, per_sm * sms_ * tuning_.grid_percent / 100);
+      b.blocks = std::max(1, std::min((b.n_tasks + kWarpsPerBlock - 1) / kWarpsPerBlock, grid));
+      first.push_back({cost, b});
     }
-    int per_sm = 0, threads = 0;
-    occupancy(b.kind, b.rows, &per_sm, &threads);
-    if (per_sm <= 0) return fail(FGKL_E_CUDA, "kernel instantiation unavailable on this device");
-    const int grid = std::max(sms_, per_sm * sms_ * tuning_.grid_percent / 100);
-    b.blocks = std::max(1, std::min((b.n_tasks + kWarpsPerBlock - 1) / kWarpsPerBlock, grid));
-    first.push_back({cost, b});
-  }
   // The bin with the most work launches first; the others fill the SMs its tail frees.
   std::stable_sort(first.begin(), first.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
   for (auto& f : first) bins_.push_back(f.second);
