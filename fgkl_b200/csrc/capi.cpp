@@ -7,6 +7,7 @@
 #include <cstring>
 #include <memory>
 #include <mutex>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -103,8 +104,10 @@ int run_on(fgkl::Engine* e, const CallRequest& q, fgkl_stats* stats) try {
   if (rc) return set_error(rc, e->error());
   if (stats) to_stats(bs, stats);
   return FGKL_OK;
-} catch (...) {
+} catch (const std::bad_alloc&) {
   return set_error(FGKL_E_CUDA, "host memory allocation failed");
+} catch (...) {
+  return set_error(FGKL_E_CUDA, "internal error in the per-call path");
 }
 
 // Runs one request on the calling thread's engine.
@@ -113,8 +116,10 @@ int run_alone(const CallRequest& q, fgkl_stats* stats) try {
   fgkl::Engine* e = thread_engine(&rc);
   if (!e) return rc;
   return run_on(e, q, stats);
-} catch (...) {
+} catch (const std::bad_alloc&) {
   return set_error(FGKL_E_CUDA, "host memory allocation failed");
+} catch (...) {
+  return set_error(FGKL_E_CUDA, "internal error in the per-call path");
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -127,10 +132,10 @@ int run_alone(const CallRequest& q, fgkl_stats* stats) try {
 // than g_max_in_flight batches running takes a free slot, its own request and every waiting one of
 // its kind, concatenates them into one batch on the slot's engine and writes each caller's results;
 // the others sleep until theirs are written. Each slot keeps one engine, so its buffers grow to the
-// largest combined batch once instead of once per calling thread. A region's program and a read's arithmetic do not depend
-// on the batch around them, so the results are bit-identical to separate calls. A combined batch
-// that fails is retried as separate calls, each on its caller's thread, so that every caller gets
-// its own status and message.
+// largest combined batch once instead of once per calling thread. A region's program and a read's
+// arithmetic do not depend on the batch around them, so the results are bit-identical to separate
+// calls. A combined batch that fails is retried as separate calls, each on its caller's thread, so
+// that every caller gets its own status and message.
 // ---------------------------------------------------------------------------------------------
 
 constexpr int kMaxSlots = 8;                         // batches in flight at most
