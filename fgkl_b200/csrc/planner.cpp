@@ -15,11 +15,17 @@ constexpr uint8_t kStandard[5] = {'A', 'C', 'G', 'T', 'N'};
 // A backward sweep must skip at least this many forward columns to pay for its join (plan.rs:9).
 constexpr int32_t kMinSaving = 4;
 
-int standard_code(uint8_t b) {
-  for (int i = 0; i < 5; ++i)
-    if (kStandard[i] == b) return i;
-  return -1;
-}
+// Byte -> ACGTN code (0..4), -1 for any other byte: one table load per haplotype base.
+struct StandardCodes {
+  int8_t code[256];
+  StandardCodes() {
+    for (int b = 0; b < 256; ++b) code[b] = -1;
+    for (int i = 0; i < 5; ++i) code[kStandard[i]] = static_cast<int8_t>(i);
+  }
+};
+const StandardCodes kStandardCodes;
+
+int standard_code(uint8_t b) { return kStandardCodes.code[b]; }
 
 bool lex_less(const HapView& a, const HapView& b) {
   return std::lexicographical_compare(a.bases, a.bases + a.len, b.bases, b.bases + b.len);
@@ -381,6 +387,10 @@ void emit_program(const SortedHaps& s, bool with_suffix, ProgramBuild& out) {
     else if (w.second < 0)
       w.second = n_slots++;
   }
+  // The writes of each segment in column order (the map iterates by writer, then column), so the
+  // column loop below meets them with one comparison a column instead of a lookup.
+  std::vector<std::vector<std::pair<int32_t, std::pair<bool, int32_t>>>> writes_of(static_cast<size_t>(m));
+  for (const auto& [key, w] : writes) writes_of[static_cast<size_t>(key.first)].push_back({key.second, w});
   uint32_t pending = 0;  // post events of the previous column, carried by the next entry
   auto push = [&](std::vector<uint32_t>& v, uint32_t e) {
     v.push_back(e | pending);
@@ -402,18 +412,22 @@ void emit_program(const SortedHaps& s, bool with_suffix, ProgramBuild& out) {
     out.segs.push_back(rec);
     // A cut segment also computes its cut column (stop + 1) as an ordinary column.
     const int32_t last = g.cut.column >= 0 ? g.cut.column : g.stop;
+    const auto& mine = writes_of[static_cast<size_t>(i)];
+    size_t next_write = 0;
+    out.fwd.reserve(out.fwd.size() + static_cast<size_t>(last - g.start) + 1);
     for (int32_t j = g.start + 1; j <= last; ++j) {
       const bool is_cut = g.cut.column >= 0 && j == g.cut.column;
       const uint32_t pd_bits = s.pd ? s.pd_bits[g.hap][j - 1] : 0u;
       push(out.fwd, s.codes[g.hap][j - 1] | pd_bits | (j == g.start + 1 ? EV_BEGIN : 0u) | (is_cut ? EV_ACC : 0u));
-      auto it = is_cut ? writes.end() : writes.find({i, j});
-      if (it != writes.end()) {
+      if (!is_cut && next_write < mine.size() && mine[next_write].first == j) {
+        const auto& w = mine[next_write++].second;
         const uint32_t none = s.pd ? kPdPayloadNone : kPayloadNone;
-        const uint32_t slot = it->second.second >= 0 ? static_cast<uint32_t>(it->second.second) : none;
-        if (it->second.second >= 0 && slot >= none) throw std::invalid_argument("too many snapshot slots for the stream payload");
-        pending |= EV_SNAP | (it->second.first ? EV_STAGE : 0u) | (slot << (s.pd ? kPdPayloadShift : kPayloadShift));
+        const uint32_t slot = w.second >= 0 ? static_cast<uint32_t>(w.second) : none;
+        if (w.second >= 0 && slot >= none) throw std::invalid_argument("too many snapshot slots for the stream payload");
+        pending |= EV_SNAP | (w.first ? EV_STAGE : 0u) | (slot << (s.pd ? kPdPayloadShift : kPayloadShift));
       }
     }
+    if (next_write != mine.size()) throw std::logic_error("snapshot column outside its writer");
     pending |= g.cut.column >= 0 ? EV_JOIN : EV_END;
     out.fwd_columns += static_cast<uint64_t>(last - g.start);
   }
