@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <cstddef>
 #include <cstring>
 #include <string>
 #include <thread>
@@ -252,6 +253,22 @@ double ms_since(std::chrono::steady_clock::time_point t0) {
 }  // namespace
 
 namespace {
+// Whether [p, p + bytes) lies in one page-locked host allocation (cudaMallocHost, cudaHostAlloc or
+// cudaHostRegister): both ends are host memory the device maps, at device addresses `bytes - 1`
+// apart. Pageable memory answers false.
+bool host_pinned(const void* p, size_t bytes) {
+  if (!p || bytes == 0) return false;
+  cudaPointerAttributes lo{}, hi{};
+  if (cudaPointerGetAttributes(&lo, p) != cudaSuccess ||
+      cudaPointerGetAttributes(&hi, static_cast<const uint8_t*>(p) + bytes - 1) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  if (lo.type != cudaMemoryTypeHost || hi.type != cudaMemoryTypeHost || !lo.devicePointer || !hi.devicePointer) return false;
+  return static_cast<const uint8_t*>(hi.devicePointer) - static_cast<const uint8_t*>(lo.devicePointer) ==
+         static_cast<std::ptrdiff_t>(bytes - 1);
+}
+
 // Grows a pinned host buffer to at least `bytes`, by half again at least (cudaFreeHost waits for the
 // whole device); false when the allocation fails.
 bool grow_pinned(uint8_t*& p, size_t& cap, size_t bytes) {
@@ -336,15 +353,19 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
   if ((rc0 = check(cudaEventSynchronize(uploaded_), "previous upload"))) return rc0;
   if ((rc0 = check(cudaEventSynchronize(fetched_), "previous download"))) return rc0;
 
-  // The five read arrays go to pinned staging on a helper thread while the regions are planned
-  // (large batches only; a small call copies them in line).
+  // The five read arrays: uploaded from where they lie when the caller holds them in page-locked
+  // memory; otherwise copied to pinned staging first, on a helper thread while the regions are
+  // planned (large batches only; a small call copies them in line).
   const int64_t read_bytes = total_reads > 0 ? in.read_off[total_reads] : 0;
-  if (!grow_pinned(h_reads_, cap_h_reads_, static_cast<size_t>(read_bytes) * 5 + 16))
+  const uint8_t* const read_arrays[5] = {in.bases, in.quals, in.ins, in.del, in.gcp};
+  bool direct_reads = read_bytes > 0;
+  for (int a = 0; a < 5 && direct_reads; ++a) direct_reads = host_pinned(read_arrays[a], static_cast<size_t>(read_bytes));
+  if (!direct_reads && !grow_pinned(h_reads_, cap_h_reads_, static_cast<size_t>(read_bytes) * 5 + 16))
     return fail(FGKL_E_CUDA, "pinned host allocation failed");
-  Helper read_copy(read_bytes >= (int64_t{8} << 20), [this, &in, read_bytes] {
-    const uint8_t* srcs[5] = {in.bases, in.quals, in.ins, in.del, in.gcp};
+  Helper read_copy(!direct_reads && read_bytes >= (int64_t{8} << 20), [this, &read_arrays, read_bytes, direct_reads] {
+    if (direct_reads) return;
     for (int a = 0; a < 5; ++a)
-      if (read_bytes) parallel_copy(h_reads_ + static_cast<size_t>(a) * read_bytes, srcs[a], static_cast<size_t>(read_bytes));
+      if (read_bytes) parallel_copy(h_reads_ + static_cast<size_t>(a) * read_bytes, read_arrays[a], static_cast<size_t>(read_bytes));
   });
 
   // Plan the regions in parallel, one region a thread for small batches (a region takes about
@@ -650,8 +671,16 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
   planned_.host_pack_ms = ms_since(t_pack);
   const auto t_up = std::chrono::steady_clock::now();
   int rc;
-  if ((rc = check(cudaMemcpyAsync(d_reads_, h_reads_, static_cast<size_t>(read_bytes) * 5, cudaMemcpyHostToDevice, copy_), "upload reads")))
+  if (direct_reads) {
+    for (int a = 0; a < 5; ++a)
+      if ((rc = check(cudaMemcpyAsync(d_reads_ + static_cast<size_t>(a) * read_bytes, read_arrays[a], static_cast<size_t>(read_bytes),
+                                      cudaMemcpyHostToDevice, copy_),
+                      "upload reads")))
+        return rc;
+  } else if ((rc = check(cudaMemcpyAsync(d_reads_, h_reads_, static_cast<size_t>(read_bytes) * 5, cudaMemcpyHostToDevice, copy_),
+                         "upload reads"))) {
     return rc;
+  }
   if ((rc = check(cudaMemcpyAsync(d_read_off_, st + s_read_off, (total_reads + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, copy_),
                   "upload offsets")))
     return rc;
@@ -664,6 +693,8 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
                   "upload queue offsets")))
     return rc;
   if ((rc = check(cudaEventRecord(uploaded_, copy_), "upload event"))) return rc;
+  // Uploaded from the caller's own memory: done before returning, so the caller may reuse it.
+  if (direct_reads && (rc = check(cudaEventSynchronize(uploaded_), "upload reads"))) return rc;
 
   planned_.host_upload_ms = ms_since(t_up);
   view_.bases = d_reads_;
@@ -820,15 +851,17 @@ int Engine::fetch(double* out, int64_t out_len, BatchStats* stats) {
   double* h_out = reinterpret_cast<double*>(h_stage_ + out_stage_);
   Counters* h_cnt = reinterpret_cast<Counters*>(h_stage_ + out_stage_ + align_up(static_cast<size_t>(out_len_) * sizeof(double)));
   if ((rc = check(cudaStreamWaitEvent(copy_, computed_, 0), "wait for the kernels"))) return rc;
+  // Results go straight into a page-locked output array, else through pinned staging.
+  const size_t out_bytes = static_cast<size_t>(out_len_) * sizeof(double);
+  const bool direct_out = out_len_ > 0 && host_pinned(out, out_bytes);
   if (out_len_ > 0 &&
-      (rc = check(cudaMemcpyAsync(h_out, d_out_, static_cast<size_t>(out_len_) * sizeof(double), cudaMemcpyDeviceToHost, copy_),
-                  "download results")))
+      (rc = check(cudaMemcpyAsync(direct_out ? out : h_out, d_out_, out_bytes, cudaMemcpyDeviceToHost, copy_), "download results")))
     return rc;
   if ((rc = check(cudaMemcpyAsync(h_cnt, d_counters_, sizeof(Counters), cudaMemcpyDeviceToHost, copy_), "download counters")))
     return rc;
   if ((rc = check(cudaEventRecord(fetched_, copy_), "download event"))) return rc;
   if ((rc = check(cudaEventSynchronize(fetched_), "kernel execution"))) return rc;
-  if (out_len_ > 0) parallel_copy(reinterpret_cast<uint8_t*>(out), reinterpret_cast<const uint8_t*>(h_out), static_cast<size_t>(out_len_) * sizeof(double));
+  if (out_len_ > 0 && !direct_out) parallel_copy(reinterpret_cast<uint8_t*>(out), reinterpret_cast<const uint8_t*>(h_out), out_bytes);
   planned_.host_fetch_ms = ms_since(t_fetch);
   if (stats) {
     *stats = planned_;

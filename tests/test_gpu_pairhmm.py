@@ -354,3 +354,42 @@ def test_autotuner_times_every_launch_configuration_and_keeps_the_bits(gpu):
     ctx.set_tuning(1, 10)
     narrow, _ = ctx.compute(w, FLOAT)
     assert narrow.tobytes() == default.tobytes()
+
+
+def test_page_locked_inputs_and_outputs_give_the_same_bits(gpu):
+    # Read arrays and an output array in page-locked memory take the direct upload and download
+    # (no staging copy); the bits must not change, nor may prepare return before the upload is done.
+    import ctypes as C
+    import dataclasses
+
+    import torch
+
+    from fgkl_b200 import BatchContext, _lib
+    from fgkl_b200.pairhmm import _check, _ptr
+
+    w = synthetic.workload(1, seed=9, regions=16)
+    ctx = BatchContext()
+    expected, _ = ctx.compute(w, FLOAT)
+
+    def pinned(a):
+        t = torch.empty(a.size, dtype=torch.uint8 if a.dtype == np.uint8 else torch.float64, pin_memory=True)
+        p = t.numpy()
+        p[...] = a
+        return t, p
+
+    keep = []
+    fields = {}
+    for f in ("bases", "quals", "ins_gop", "del_gop", "gcp"):
+        t, p = pinned(getattr(w, f))
+        keep.append(t)
+        fields[f] = p
+    wp = dataclasses.replace(w, **fields)
+    t_out, out = pinned(np.zeros(w.output_len()))
+    b, c = wp.as_batch(), FLOAT._c()
+    st = _lib.Stats()
+    _check(_lib.lib().fgkl_batch_prepare(ctx._ctx, C.byref(b), C.byref(c)))
+    for f in fields.values():
+        f[...] = 0  # the caller reuses its buffers once prepare has returned
+    _check(_lib.lib().fgkl_batch_run(ctx._ctx))
+    _check(_lib.lib().fgkl_batch_fetch(ctx._ctx, _ptr(out, _lib.f64p), out.size, C.byref(st)))
+    assert out.tobytes() == expected.tobytes()
