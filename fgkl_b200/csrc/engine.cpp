@@ -448,69 +448,64 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
   for (int g = 0; g < N; ++g) region_order[g] = g;
   auto cost_of = [&](int g) { return plans[g].prog.fwd.size() + plans[g].prog.bwd.size() + 31; };
   std::stable_sort(region_order.begin(), region_order.end(), [&](int a, int b) { return cost_of(a) > cost_of(b); });
-  std::vector<int> order;
-  for (const int g : region_order) {
+  // Each region's tasks, built in parallel (its reads sorted longest first, then packed), then
+  // appended to the bins serially in region order.
+  struct RegionTask {
+    Kind kind;
+    int rows;
+    int len;  // read bases of the task, for the bin's cell counts
+    Task task;
+  };
+  std::vector<std::vector<RegionTask>> region_tasks(static_cast<size_t>(N));
+  parallel_for(N, std::min(host_threads(), (N + 63) / 64), [&](int64_t gi) {
+    const int g = static_cast<int>(gi);
     const int n_reads = in.region_reads[g];
-    if (n_reads == 0 || in.region_haps[g] == 0) continue;
-    order.resize(static_cast<size_t>(n_reads));
+    if (n_reads == 0 || in.region_haps[g] == 0) return;
+    std::vector<int> order(static_cast<size_t>(n_reads));
     for (int r = 0; r < n_reads; ++r) order[r] = r;
     auto len_of = [&](int r) { return static_cast<int>(in.read_off[first_read[g] + r + 1] - in.read_off[first_read[g] + r]); };
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return len_of(a) > len_of(b); });
-    const uint64_t cost_cols = cost_of(g);
-    const uint64_t fcols = plans[g].prog.fwd_columns, bcols = plans[g].prog.bwd_columns;
-    auto count = [&](Kind kind, int rows, int len) {
-      BinList& c = bin_at(kind, rows);
-      c.fwd_cells += fcols * static_cast<uint64_t>(len);
-      c.bwd_cells += bcols * static_cast<uint64_t>(len);
+    std::vector<RegionTask>& out = region_tasks[g];
+    out.reserve(static_cast<size_t>(n_reads));
+    auto one = [&](Kind kind, int rows, size_t i) {
+      out.push_back({kind, rows, len_of(order[i]), Task{g, {static_cast<int32_t>(first_read[g] + order[i]), -1}, rows, -1}});
+    };
+    auto two = [&](Kind kind, int rows, size_t i) {
+      const int32_t a = static_cast<int32_t>(first_read[g] + order[i]);
+      const int32_t b = i + 1 < order.size() ? static_cast<int32_t>(first_read[g] + order[i + 1]) : -1;
+      out.push_back({kind, rows, len_of(order[i]) + (i + 1 < order.size() ? len_of(order[i + 1]) : 0), Task{g, {a, b}, rows, -1}});
     };
     size_t i = 0;
     if (pd && cfg.double_precision) {
       // PD in FP64: one read per warp.
-      for (; i < order.size(); ++i) {
-        const int rows = single_rows(len_of(order[i]));
-        bin_at(Kind::kOneF64Pd, rows).list.push_back(
-            {cost_cols * rows, Task{g, {static_cast<int32_t>(first_read[g] + order[i]), -1}, rows, -1}});
-        count(Kind::kOneF64Pd, rows, len_of(order[i]));
-      }
+      for (; i < order.size(); ++i) one(Kind::kOneF64Pd, single_rows(len_of(order[i])), i);
     } else if (pd) {
       // PD in FP32: reads above 248 bases one per warp, the others in pairs (FP32x2) unless the
       // launch configuration asks for one read per warp.
-      while (i < order.size() && (packed_rows(len_of(order[i])) > 8 || tuning_.reads_per_warp == 1)) {
-        const int rows = single_rows(len_of(order[i]));
-        bin_at(Kind::kOneF32Pd, rows).list.push_back(
-            {cost_cols * rows, Task{g, {static_cast<int32_t>(first_read[g] + order[i]), -1}, rows, -1}});
-        count(Kind::kOneF32Pd, rows, len_of(order[i]));
-        ++i;
-      }
-      for (; i < order.size(); i += 2) {
-        const int rows = packed_rows(len_of(order[i]));
-        const int32_t a = static_cast<int32_t>(first_read[g] + order[i]);
-        const int32_t b = i + 1 < order.size() ? static_cast<int32_t>(first_read[g] + order[i + 1]) : -1;
-        bin_at(Kind::kPackedF32Pd, rows).list.push_back({cost_cols * rows, Task{g, {a, b}, rows, -1}});
-        count(Kind::kPackedF32Pd, rows, len_of(order[i]) + (i + 1 < order.size() ? len_of(order[i + 1]) : 0));
-      }
+      for (; i < order.size() && (packed_rows(len_of(order[i])) > 8 || tuning_.reads_per_warp == 1); ++i)
+        one(Kind::kOneF32Pd, single_rows(len_of(order[i])), i);
+      for (; i < order.size(); i += 2) two(Kind::kPackedF32Pd, packed_rows(len_of(order[i])), i);
     } else if (cfg.double_precision || plans[g].extra_codes) {
-      for (; i < order.size(); ++i) {
-        const int rows = single_rows(len_of(order[i]));
-        bin_at(Kind::kOneF64, rows).list.push_back(
-            {cost_cols * rows, Task{g, {static_cast<int32_t>(first_read[g] + order[i]), -1}, rows, -1}});
-        count(Kind::kOneF64, rows, len_of(order[i]));
-      }
+      for (; i < order.size(); ++i) one(Kind::kOneF64, single_rows(len_of(order[i])), i);
     } else {
-      while (i < order.size() && packed_rows(len_of(order[i])) > 8) {
-        const int rows = single_rows(len_of(order[i]));
-        bin_at(Kind::kOneF32, rows).list.push_back(
-            {cost_cols * rows, Task{g, {static_cast<int32_t>(first_read[g] + order[i]), -1}, rows, -1}});
-        count(Kind::kOneF32, rows, len_of(order[i]));
-        ++i;
-      }
-      for (; i < order.size(); i += 2) {
-        const int rows = packed_rows(len_of(order[i]));
-        const int32_t a = static_cast<int32_t>(first_read[g] + order[i]);
-        const int32_t b = i + 1 < order.size() ? static_cast<int32_t>(first_read[g] + order[i + 1]) : -1;
-        bin_at(Kind::kPackedF32, rows).list.push_back({cost_cols * rows, Task{g, {a, b}, rows, -1}});
-        count(Kind::kPackedF32, rows, len_of(order[i]) + (i + 1 < order.size() ? len_of(order[i + 1]) : 0));
-      }
+      for (; i < order.size() && packed_rows(len_of(order[i])) > 8; ++i) one(Kind::kOneF32, single_rows(len_of(order[i])), i);
+      for (; i < order.size(); i += 2) two(Kind::kPackedF32, packed_rows(len_of(order[i])), i);
+    }
+  });
+  {
+    std::vector<size_t> bin_size(by_bin.size(), 0);
+    for (const auto& v : region_tasks)
+      for (const RegionTask& t : v) ++bin_size[static_cast<size_t>(t.kind) * kRowBins + t.rows];
+    for (size_t k = 0; k < by_bin.size(); ++k) by_bin[k].list.reserve(bin_size[k]);
+  }
+  for (const int g : region_order) {
+    const uint64_t cost_cols = cost_of(g);
+    const uint64_t fcols = plans[g].prog.fwd_columns, bcols = plans[g].prog.bwd_columns;
+    for (const RegionTask& t : region_tasks[g]) {
+      BinList& bl = bin_at(t.kind, t.rows);
+      bl.list.push_back({cost_cols * static_cast<uint64_t>(t.rows), t.task});
+      bl.fwd_cells += fcols * static_cast<uint64_t>(t.len);
+      bl.bwd_cells += bcols * static_cast<uint64_t>(t.len);
     }
   }
   std::vector<Task> tasks;
