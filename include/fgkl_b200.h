@@ -163,13 +163,17 @@ fgkl_context* fgkl_context_create(int32_t device, void* stream);
 void fgkl_context_destroy(fgkl_context* ctx);
 
 /* Validates and plans the batch on the host and uploads it on the context's copy stream. Waits for
- * this context's previous batch only (its kernels and copies), never for other work on the stream. */
+ * this context's previous batch only (its kernels and copies), never for other work on the stream.
+ * The batch's host arrays may be reused once it returns. Read arrays in page-locked memory
+ * (cudaMallocHost, cudaHostAlloc, cudaHostRegister) are uploaded from where they lie, and the call
+ * waits for that upload. Others are first copied to the context's pinned staging. */
 int fgkl_batch_prepare(fgkl_context* ctx, const fgkl_batch* batch, const fgkl_config* config);
 /* Enqueues the kernels of the prepared batch on the context's stream, after its upload, without
  * waiting. The launch sequence is captured into a CUDA graph, updated in place for later batches. */
 int fgkl_batch_run(fgkl_context* ctx);
 /* Copies the likelihoods (Σ reads x haplotypes) and counters back once the batch's kernels are done,
- * and waits for that copy (not for later work on the stream). */
+ * and waits for that copy (not for later work on the stream). A page-locked `out` receives the
+ * results directly; any other goes through the context's pinned staging. */
 int fgkl_batch_fetch(fgkl_context* ctx, double* out, int64_t out_len, fgkl_stats* stats);
 /* prepare + run + fetch. */
 int fgkl_batch_compute(fgkl_context* ctx, const fgkl_batch* batch, const fgkl_config* config, double* out,
