@@ -367,6 +367,23 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
     for (int a = 0; a < 5; ++a)
       if (read_bytes) parallel_copy(h_reads_ + static_cast<size_t>(a) * read_bytes, read_arrays[a], static_cast<size_t>(read_bytes));
   });
+  // Page-locked reads start uploading now, under the planning. Any return from here on waits for
+  // these copies first: they read the caller's memory.
+  struct UploadGuard {
+    cudaStream_t s = nullptr;
+    ~UploadGuard() {
+      if (s) cudaStreamSynchronize(s);
+    }
+  } upload_guard;
+  if (direct_reads) {
+    if (!grow(d_reads_, cap_reads_, static_cast<size_t>(read_bytes) * 5 + 16)) return fail(FGKL_E_CUDA, "device allocation failed");
+    upload_guard.s = copy_;
+    for (int a = 0; a < 5; ++a)
+      if ((rc0 = check(cudaMemcpyAsync(d_reads_ + static_cast<size_t>(a) * read_bytes, read_arrays[a], static_cast<size_t>(read_bytes),
+                                       cudaMemcpyHostToDevice, copy_),
+                       "upload reads")))
+        return rc0;
+  }
 
   // Plan the regions in parallel, one region a thread for small batches (a region takes about
   // 75 us to plan; a combined batch of per-call requests holds a few).
@@ -666,16 +683,9 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
   planned_.host_pack_ms = ms_since(t_pack);
   const auto t_up = std::chrono::steady_clock::now();
   int rc;
-  if (direct_reads) {
-    for (int a = 0; a < 5; ++a)
-      if ((rc = check(cudaMemcpyAsync(d_reads_ + static_cast<size_t>(a) * read_bytes, read_arrays[a], static_cast<size_t>(read_bytes),
-                                      cudaMemcpyHostToDevice, copy_),
-                      "upload reads")))
-        return rc;
-  } else if ((rc = check(cudaMemcpyAsync(d_reads_, h_reads_, static_cast<size_t>(read_bytes) * 5, cudaMemcpyHostToDevice, copy_),
-                         "upload reads"))) {
+  if (!direct_reads && (rc = check(cudaMemcpyAsync(d_reads_, h_reads_, static_cast<size_t>(read_bytes) * 5, cudaMemcpyHostToDevice, copy_),
+                                   "upload reads")))
     return rc;
-  }
   if ((rc = check(cudaMemcpyAsync(d_read_off_, st + s_read_off, (total_reads + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, copy_),
                   "upload offsets")))
     return rc;
@@ -689,7 +699,10 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
     return rc;
   if ((rc = check(cudaEventRecord(uploaded_, copy_), "upload event"))) return rc;
   // Uploaded from the caller's own memory: done before returning, so the caller may reuse it.
-  if (direct_reads && (rc = check(cudaEventSynchronize(uploaded_), "upload reads"))) return rc;
+  if (direct_reads) {
+    upload_guard.s = nullptr;
+    if ((rc = check(cudaEventSynchronize(uploaded_), "upload reads"))) return rc;
+  }
 
   planned_.host_upload_ms = ms_since(t_up);
   view_.bases = d_reads_;
