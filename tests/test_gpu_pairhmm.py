@@ -393,3 +393,12 @@ def test_page_locked_inputs_and_outputs_give_the_same_bits(gpu):
     _check(_lib.lib().fgkl_batch_run(ctx._ctx))
     _check(_lib.lib().fgkl_batch_fetch(ctx._ctx, _ptr(out, _lib.f64p), out.size, C.byref(st)))
     assert out.tobytes() == expected.tobytes()
+
+    # One read array page-locked and the others not: the staging path; a pageable output.
+    t_bases, p_bases = pinned(w.bases)
+    mixed = dataclasses.replace(w, bases=p_bases)
+    b2 = mixed.as_batch()
+    out2 = np.zeros(w.output_len())
+    _check(_lib.lib().fgkl_batch_compute(ctx._ctx, C.byref(b2), C.byref(c), _ptr(out2, _lib.f64p), out2.size, C.byref(st)))
+    assert out2.tobytes() == expected.tobytes()
+    del t_bases, t_out, keep
