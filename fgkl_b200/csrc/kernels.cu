@@ -24,9 +24,9 @@
 //
 // Events. A lane handles all events of a step in one divergent branch: the stores for the previous
 // column (SNAP, END, NODE) and then the loads for its own (BEGIN, SWEEP). Start states come from a
-// per-warp ping-pong staging buffer in shared memory: the previous segment writes it directly when
-// it is the snapshot's last writer, otherwise the state is prefetched from global scratch with
-// cp.async at the previous segment's BEGIN. Joins only store their forward column; the products
+// per-warp staging buffer in shared memory, one record per lane: the previous segment writes it
+// directly when it is the snapshot's last writer, otherwise the state is prefetched from global
+// scratch with cp.async at the previous segment's BEGIN, after that BEGIN has read the record. Joins only store their forward column; the products
 // with the backward node are summed after the sweep, warp-wide, in an order fixed by the read row.
 #include <cuda_pipeline.h>
 #include <cuda_runtime.h>
@@ -58,7 +58,7 @@ struct Layout {
   static constexpr int kPer16 = kRound;
   static constexpr int kRp = up(R);
   static constexpr int kChunks = kRp / kPer16;
-  static constexpr size_t kStageBytes = 2ull * 32 * kStage * sizeof(V);
+  static constexpr size_t kStageBytes = 32ull * kStage * sizeof(V);
   static constexpr size_t kSmemPerWarp = kStageBytes + static_cast<size_t>(kPriorCodes) * kRp * 32 * sizeof(V);
   // Element of row r's prior for `code` in the table, [code][chunk][lane][row in chunk]: each chunk of
   // the warp is 512 contiguous bytes, so a step's chunk loads are conflict-free 16-byte loads.
@@ -218,7 +218,10 @@ struct Scratch {
   __device__ V* slot(int s, int lane) { return slots + (static_cast<size_t>(s) * 32 + lane) * L::kSnap; }
   __device__ V* node(int n, int lane) { return nodes + (static_cast<size_t>(n) * 32 + lane) * L::kNode; }
   __device__ V* join(int seg, int lane) { return joins + (static_cast<size_t>(seg) * 32 + lane) * L::kJoin; }
-  __device__ V* staged(int buf, int lane) { return stage + (static_cast<size_t>(buf & 1) * 32 + lane) * L::kStage; }
+  // One staging record per lane serves every segment (sweep): a lane writes or prefetches the next
+  // segment's start into it only after loading the current segment's start at its BEGIN (SWEEP), and
+  // each lane touches its own record alone.
+  __device__ V* staged(int, int lane) { return stage + static_cast<size_t>(lane) * L::kStage; }
 };
 
 template <class P, int R>
@@ -231,10 +234,11 @@ __host__ __device__ constexpr size_t scratch_size(int n_slots, int n_nodes, int 
 
 // Resident blocks per SM each instantiation is compiled for, chosen by timing each bin of the uneven
 // workload: four up to 4 rows per lane (R = 4 then spills 8 bytes at 128 registers, and still runs
-// 5% faster than at three blocks), three up to 6, two above, where shared memory allows no more.
+// 5% faster than at three blocks), three up to 7 (R = 7 spills 8 bytes at 168 and runs 8% faster
+// than at two), two at 8 (three spill 76 bytes and run 6% slower).
 template <class P, int R>
 struct MinBlocks {
-  static constexpr int value = P::NC == 2 ? (R <= 4 ? 4 : (R <= 6 ? 3 : 2)) : (P::kDouble ? 1 : 2);
+  static constexpr int value = P::NC == 2 ? (R <= 4 ? 4 : (R <= 7 ? 3 : 2)) : (P::kDouble ? 1 : 2);
 };
 
 // ---------------------------------------------------------------------------------------------

@@ -42,7 +42,7 @@ struct PdLayout {
   static constexpr int up(int x) { return (x + kRound - 1) / kRound * kRound; }
   // M, X, Y rows; branch M, X, Y rows; above-row M, X, Y and branch M, X, Y; accumulated result.
   static constexpr int kSnap = up(6 * R + 7);
-  static constexpr size_t kStageBytes = 2ull * 32 * kSnap * sizeof(V);
+  static constexpr size_t kStageBytes = 32ull * kSnap * sizeof(V);
   static constexpr size_t kSmemPerWarp = kStageBytes;
 };
 
@@ -60,7 +60,9 @@ struct PdScratch {
     stage = smem;
   }
   __device__ V* slot(int s, int lane) { return slots + (static_cast<size_t>(s) * 32 + lane) * L::kSnap; }
-  __device__ V* staged(int buf, int lane) { return stage + (static_cast<size_t>(buf & 1) * 32 + lane) * L::kSnap; }
+  // One staging record per lane serves every segment: a lane writes or prefetches the next
+  // segment's start into it only after loading the current one at its BEGIN.
+  __device__ V* staged(int, int lane) { return stage + static_cast<size_t>(lane) * L::kSnap; }
 };
 
 template <class P, int R>
