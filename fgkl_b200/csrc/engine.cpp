@@ -15,10 +15,33 @@
 namespace fgkl {
 
 namespace {
+std::atomic<int64_t> g_allocation_limit{0};
+}  // namespace
+
+int64_t allocation_limit() { return g_allocation_limit.load(std::memory_order_relaxed); }
+int64_t set_allocation_limit(int64_t bytes) { return g_allocation_limit.exchange(bytes); }
+
+cudaError_t device_alloc(void** p, size_t bytes) {
+  const int64_t lim = allocation_limit();
+  if (lim > 0 && bytes > static_cast<size_t>(lim)) {
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  return cudaMalloc(p, bytes);
+}
+
+cudaError_t pinned_alloc(void** p, size_t bytes) {
+  const int64_t lim = allocation_limit();
+  if (lim > 0 && bytes > static_cast<size_t>(lim)) {
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  return cudaMallocHost(p, bytes);
+}
+
+namespace {
 
 constexpr int kWarpsPerBlock = 4;
-constexpr int kRowBins = 21;  // rows-per-lane values 1..20 index the recomputation queues
-constexpr int64_t kMaxReadLen = 620;  // 31 rows per lane x 20 rows
 
 // Rows per lane: lane 0 holds only padding rows, so 31 * rows >= len.
 int packed_rows(int len) { return (len + 30) / 31; }
@@ -44,6 +67,7 @@ struct RegionPlan {
   uint64_t read_bases = 0, hap_bases = 0;
   int n_distinct = 0;
   bool extra_codes = false;  // a haplotype byte outside ACGTN: the region runs on the FP64 kernel
+  bool generic = false;      // PD: more read bytes than class bits, or more than 256 match sets
 };
 
 // PD regions: the reads' distinct bytes become classes 0..30 (first-seen order) and each match-set
@@ -89,10 +113,10 @@ void plan_region(const BatchInput& in, int g, int64_t first_read, int64_t first_
     return;
   }
   if (pd) {
-    if (!pd_read_classes(in, first_read, n_reads, s, out)) {
-      out.error = "a PD region's reads hold more than 31 distinct bytes";
-      return;
-    }
+    // Regions the class bits cannot describe compare bytes in the kernel instead (every pair then
+    // runs unshared, as fgkl's answer for them does not depend on sharing).
+    out.generic = s.too_many_sets || !pd_read_classes(in, first_read, n_reads, s, out);
+    if (out.generic) out.pd_sigs.clear();
   } else {
     code_table(s, out.codes);
     out.extra_codes = s.num_codes() > 5;
@@ -106,7 +130,15 @@ void plan_region(const BatchInput& in, int g, int64_t first_read, int64_t first_
       src = k;
       if (pd) {
         out.haps[k].seq = static_cast<int32_t>(out.pd_seq.size());
-        for (int32_t j = 0; j < s.bases[k].len; ++j) out.pd_seq.push_back(s.codes[k][j] | s.pd_bits[k][j]);
+        for (int32_t j = 0; j < s.bases[k].len; ++j) {
+          if (out.generic) {
+            // The column's own byte and ALT bits (shifted to bit 0) in place of a match-set code.
+            const MatchSet set = MatchSet::of(s.bases[k].bases[j], s.flags[k][j]);
+            out.pd_seq.push_back(set.base | (static_cast<uint32_t>(set.alts >> 3) << kPdPayloadShift) | s.pd_bits[k][j]);
+          } else {
+            out.pd_seq.push_back(s.codes[k][j] | s.pd_bits[k][j]);
+          }
+        }
       } else {
         out.haps[k].seq = static_cast<int32_t>(out.seq.size());
         out.seq.insert(out.seq.end(), s.codes[k].begin(), s.codes[k].end());
@@ -160,7 +192,7 @@ void parallel_copy(uint8_t* dst, const uint8_t* src, size_t bytes) {
 }  // namespace
 
 Engine::Engine(int device, cudaStream_t stream) : device_(device), stream_(stream) {
-  cudaSetDevice(device_);
+  DeviceGuard device_guard(device_);
   cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device_);
   if (!stream_) {
     cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking);
@@ -184,7 +216,7 @@ Engine::Engine(int device, cudaStream_t stream) : device_(device), stream_(strea
 }
 
 Engine::~Engine() {
-  cudaSetDevice(device_);
+  DeviceGuard device_guard(device_);
   if (stream_) cudaStreamSynchronize(stream_);
   if (copy_) cudaStreamSynchronize(copy_);
   cudaFree(d_reads_);
@@ -232,9 +264,9 @@ T* Engine::grow(T*& ptr, size_t& cap, size_t n) {
     const size_t want = cap > 0 ? std::max(bytes, cap + cap / 2) : bytes;
     cudaFree(ptr);
     ptr = nullptr;
-    if (cudaMalloc(&ptr, want) == cudaSuccess) {
+    if (device_alloc(reinterpret_cast<void**>(&ptr), want) == cudaSuccess) {
       cap = want;
-    } else if (want > bytes && (cudaGetLastError(), cudaMalloc(&ptr, bytes) == cudaSuccess)) {
+    } else if (want > bytes && (cudaGetLastError(), device_alloc(reinterpret_cast<void**>(&ptr), bytes) == cudaSuccess)) {
       cap = bytes;
     } else {
       cudaGetLastError();
@@ -276,12 +308,12 @@ bool grow_pinned(uint8_t*& p, size_t& cap, size_t bytes) {
   const size_t want = cap > 0 ? std::max(bytes, cap + cap / 2) : bytes;
   if (p) cudaFreeHost(p);
   p = nullptr;
-  if (cudaMallocHost(&p, want) == cudaSuccess) {
+  if (pinned_alloc(reinterpret_cast<void**>(&p), want) == cudaSuccess) {
     cap = want;
     return true;
   }
   cudaGetLastError();
-  if (want > bytes && cudaMallocHost(&p, bytes) == cudaSuccess) {
+  if (want > bytes && pinned_alloc(reinterpret_cast<void**>(&p), bytes) == cudaSuccess) {
     cap = bytes;
     return true;
   }
@@ -311,7 +343,7 @@ class Helper {
 }  // namespace
 
 int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
-  cudaSetDevice(device_);
+  DeviceGuard device_guard(device_);
   const auto t_start = std::chrono::steady_clock::now();
   cfg_ = cfg;
   error_.clear();
@@ -336,9 +368,7 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
     for (int64_t r = first_read[g]; r < first_read[g + 1]; ++r) {
       const int64_t len = in.read_off[r + 1] - in.read_off[r];
       if (len <= 0) return fail(FGKL_E_EMPTY_READ, "read " + std::to_string(r - first_read[g]) + " has no bases");
-      if (len > kMaxReadLen)
-        return fail(FGKL_E_UNSUPPORTED, "read " + std::to_string(r - first_read[g]) + " has " + std::to_string(len) +
-                                            " bases; reads of at most 620 bases are supported");
+      if (len > INT32_MAX) return fail(FGKL_E_INVALID_ARGUMENT, "read " + std::to_string(r - first_read[g]) + " is longer than 2^31 - 1 bases");
     }
     for (int64_t h = first_hap[g]; h < first_hap[g + 1]; ++h)
       if (in.hap_off[h + 1] - in.hap_off[h] <= 0)
@@ -361,7 +391,7 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
   bool direct_reads = read_bytes > 0;
   for (int a = 0; a < 5 && direct_reads; ++a) direct_reads = host_pinned(read_arrays[a], static_cast<size_t>(read_bytes));
   if (!direct_reads && !grow_pinned(h_reads_, cap_h_reads_, static_cast<size_t>(read_bytes) * 5 + 16))
-    return fail(FGKL_E_CUDA, "pinned host allocation failed");
+    return fail(FGKL_E_OUT_OF_MEMORY, "pinned host allocation failed");
   Helper read_copy(!direct_reads && read_bytes >= (int64_t{8} << 20), [this, &read_arrays, read_bytes, direct_reads] {
     if (direct_reads) return;
     for (int a = 0; a < 5; ++a)
@@ -376,7 +406,7 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
     }
   } upload_guard;
   if (direct_reads) {
-    if (!grow(d_reads_, cap_reads_, static_cast<size_t>(read_bytes) * 5 + 16)) return fail(FGKL_E_CUDA, "device allocation failed");
+    if (!grow(d_reads_, cap_reads_, static_cast<size_t>(read_bytes) * 5 + 16)) return fail(FGKL_E_OUT_OF_MEMORY, "device allocation failed");
     upload_guard.s = copy_;
     for (int a = 0; a < 5; ++a)
       if ((rc0 = check(cudaMemcpyAsync(d_reads_ + static_cast<size_t>(a) * read_bytes, read_arrays[a], static_cast<size_t>(read_bytes),
@@ -402,7 +432,8 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
   std::vector<Region> regions(static_cast<size_t>(N));
   int64_t n_haps = 0, n_stream = kStreamPad, n_segs = 0, n_sweeps = 0, n_seq = 0, n_pd_seq = 0, n_sigs = 0;
   int max_slots = 1, max_nodes = 1, max_segs = 1;
-  std::vector<int64_t> queue_cap(kRowBins, 0);
+  std::vector<int64_t> queue_cap(kQueueBins, 0);
+  int max_hap_len = 1;  // scratch of the strip-mined kinds: one carry column per haplotype base
   for (int g = 0; g < N; ++g) {
     const RegionPlan& rp = plans[g];
     Region& R = regions[g];
@@ -437,16 +468,15 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
     n_seq += static_cast<int64_t>(rp.seq.size());
     n_pd_seq += static_cast<int64_t>(rp.pd_seq.size());
     R.sig_off = static_cast<int32_t>(n_sigs);
+    R.flags = rp.generic ? kRegionGeneric : 0;
     n_sigs += static_cast<int64_t>(rp.pd_sigs.size());
     planned_.nominal_cells += rp.read_bases * rp.hap_bases;
-    planned_.forward_cells += rp.read_bases * rp.prog.fwd_columns;
-    planned_.backward_cells += rp.read_bases * rp.prog.bwd_columns;
     planned_.prefix_only_cells += rp.read_bases * rp.cols.prefix_only;
+    for (const HapInfo& h : rp.haps) max_hap_len = std::max(max_hap_len, static_cast<int>(h.len));
     if (rp.n_distinct > 0)
       for (int64_t r = first_read[g]; r < first_read[g + 1]; ++r)
-        queue_cap[single_rows(static_cast<int>(in.read_off[r + 1] - in.read_off[r]))] += rp.n_distinct;
+        queue_cap[queue_bin(static_cast<int>(in.read_off[r + 1] - in.read_off[r]), rp.generic)] += rp.n_distinct;
   }
-  planned_.computed_cells = planned_.forward_cells + planned_.backward_cells;
   if (n_stream > INT32_MAX || n_seq > INT32_MAX || n_pd_seq > INT32_MAX || n_haps > INT32_MAX)
     return fail(FGKL_E_INVALID_ARGUMENT, "batch too large for 32-bit plan offsets; split it");
 
@@ -454,7 +484,7 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
   // its region's stream length times its rows, so within a bin (one rows value) the costliest
   // regions' tasks come first: regions are visited in that order (ties by index), which lists each
   // bin's tasks longest first without sorting them.
-  constexpr int kKinds = 6;
+  constexpr int kKinds = kNumKinds;
   struct BinList {
     std::vector<std::pair<uint64_t, Task>> list;
     uint64_t fwd_cells = 0, bwd_cells = 0;  // forward, backward DP cells
@@ -472,6 +502,7 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
     int rows;
     int len;  // read bases of the task, for the bin's cell counts
     Task task;
+    uint64_t cost;  // strip-mined pairs: steps x rows; 0 for the region's program tasks
   };
   std::vector<std::vector<RegionTask>> region_tasks(static_cast<size_t>(N));
   parallel_for(N, std::min(host_threads(), (N + 63) / 64), [&](int64_t gi) {
@@ -485,14 +516,32 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
     std::vector<RegionTask>& out = region_tasks[g];
     out.reserve(static_cast<size_t>(n_reads));
     auto one = [&](Kind kind, int rows, size_t i) {
-      out.push_back({kind, rows, len_of(order[i]), Task{g, {static_cast<int32_t>(first_read[g] + order[i]), -1}, rows, -1}});
+      out.push_back({kind, rows, len_of(order[i]), Task{g, {static_cast<int32_t>(first_read[g] + order[i]), -1}, rows, -1}, 0});
     };
     auto two = [&](Kind kind, int rows, size_t i) {
       const int32_t a = static_cast<int32_t>(first_read[g] + order[i]);
       const int32_t b = i + 1 < order.size() ? static_cast<int32_t>(first_read[g] + order[i + 1]) : -1;
-      out.push_back({kind, rows, len_of(order[i]) + (i + 1 < order.size() ? len_of(order[i + 1]) : 0), Task{g, {a, b}, rows, -1}});
+      out.push_back({kind, rows, len_of(order[i]) + (i + 1 < order.size() ? len_of(order[i + 1]) : 0), Task{g, {a, b}, rows, -1}, 0});
+    };
+    // One task per distinct sorted haplotype of read order[i], strip-mined over row blocks.
+    const RegionPlan& rp = plans[g];
+    auto pairs = [&](Kind kind, size_t i) {
+      const int len = len_of(order[i]);
+      const int rows = long_rows(len, kind == Kind::kLongF32);
+      const uint64_t blocks = static_cast<uint64_t>(long_blocks(len, rows));
+      for (int k = 0; k < static_cast<int>(rp.haps.size()); ++k)
+        if (rp.haps[k].src == k)
+          out.push_back({kind, rows, len, Task{g, {static_cast<int32_t>(first_read[g] + order[i]), -1}, rows, k},
+                         (static_cast<uint64_t>(rp.haps[k].len) + 32) * blocks * static_cast<uint64_t>(rows)});
     };
     size_t i = 0;
+    const bool dbl = cfg.double_precision;
+    if (rp.generic) {
+      for (; i < order.size(); ++i) pairs(dbl ? Kind::kGenericF64Pd : Kind::kGenericF32Pd, i);
+      return;
+    }
+    const Kind long_kind = pd ? (dbl ? Kind::kLongF64Pd : Kind::kLongF32Pd) : ((dbl || rp.extra_codes) ? Kind::kLongF64 : Kind::kLongF32);
+    for (; i < order.size() && len_of(order[i]) > kMaxBlockRead; ++i) pairs(long_kind, i);
     if (pd && cfg.double_precision) {
       // PD in FP64: one read per warp.
       for (; i < order.size(); ++i) one(Kind::kOneF64Pd, single_rows(len_of(order[i])), i);
@@ -520,11 +569,22 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
     const uint64_t fcols = plans[g].prog.fwd_columns, bcols = plans[g].prog.bwd_columns;
     for (const RegionTask& t : region_tasks[g]) {
       BinList& bl = bin_at(t.kind, t.rows);
+      if (t.task.hap >= 0) {
+        // An unshared strip-mined pair: read length x haplotype length forward cells.
+        bl.list.push_back({t.cost, t.task});
+        bl.fwd_cells += static_cast<uint64_t>(plans[g].haps[t.task.hap].len) * static_cast<uint64_t>(t.len);
+        continue;
+      }
       bl.list.push_back({cost_cols * static_cast<uint64_t>(t.rows), t.task});
       bl.fwd_cells += fcols * static_cast<uint64_t>(t.len);
       bl.bwd_cells += bcols * static_cast<uint64_t>(t.len);
     }
   }
+  for (const BinList& bl : by_bin) {
+    planned_.forward_cells += bl.fwd_cells;
+    planned_.backward_cells += bl.bwd_cells;
+  }
+  planned_.computed_cells = planned_.forward_cells + planned_.backward_cells;
   std::vector<Task> tasks;
   std::vector<std::pair<uint64_t, Bin>> first;
   size_t n_tasks_all = 0;
@@ -557,25 +617,29 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
   // Pairs either pass loses (an FP32 underflow, or a joined FP64 result below the backward range)
   // are recomputed in FP64 without sharing, which cannot lose a pair (lib.rs:461-487).
   const bool queue_on = cfg.double_fallback;
-  std::vector<int> queue_off(kRowBins + 1, 0);
+  std::vector<int> queue_off(kQueueBins + 1, 0);
   {
     int64_t acc = 0;
-    for (int r = 0; r < kRowBins; ++r) {
+    for (int r = 0; r < kQueueBins; ++r) {
       queue_off[r] = static_cast<int>(acc);
       if (queue_on) acc += queue_cap[r];
     }
     if (acc > INT32_MAX) return fail(FGKL_E_INVALID_ARGUMENT, "batch too large for the recomputation queue; split it");
-    queue_off[kRowBins] = static_cast<int>(acc);
+    queue_off[kQueueBins] = static_cast<int>(acc);
   }
   if (queue_on) {
-    for (int r = 1; r < kRowBins; ++r) {
-      const int cap = queue_off[r + 1] - queue_off[r];
+    for (int q = 1; q < kQueueBins; ++q) {
+      const int cap = queue_off[q + 1] - queue_off[q];
       if (cap == 0) continue;
-      const Kind kind = pd ? Kind::kOneF64Pd : Kind::kOneF64;
+      // Queue bin -> the FP64 form of the pairs it holds (queue_bin).
+      const int r = queue_bin_rows(q);
+      const Kind kind = q >= 2 * kRowBins ? Kind::kGenericF64Pd
+                                          : (q >= kRowBins ? (pd ? Kind::kLongF64Pd : Kind::kLongF64) : (pd ? Kind::kOneF64Pd : Kind::kOneF64));
       int per_sm = 0, threads = 0;
       occupancy(kind, r, &per_sm, &threads);
       if (per_sm <= 0) return fail(FGKL_E_CUDA, "recomputation kernel unavailable on this device");
-      Bin b{kind, r, queue_off[r], cap, 0, 0, 0};
+      Bin b{kind, r, queue_off[q], cap, 0, 0, 0};
+      b.queue_bin = q;
       b.blocks = std::max(1, std::min((cap + kWarpsPerBlock - 1) / kWarpsPerBlock, per_sm * sms_));
       rescue_bins_.push_back(b);
     }
@@ -586,7 +650,9 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
     const bool rescue = list == &rescue_bins_;
     size_t off = 0;
     for (Bin& b : *list) {
-      b.stride = align_up(rescue ? scratch_bytes(b.kind, b.rows, 0, 0, 1) : scratch_bytes(b.kind, b.rows, max_slots, max_nodes, max_segs));
+      b.stride = align_up(is_long(b.kind) ? long_scratch_bytes(b.kind, b.rows, max_hap_len)
+                          : rescue        ? scratch_bytes(b.kind, b.rows, 0, 0, 1)
+                                          : scratch_bytes(b.kind, b.rows, max_slots, max_nodes, max_segs));
       b.scratch_off = off;
       off += static_cast<size_t>(b.blocks) * kWarpsPerBlock * b.stride;
     }
@@ -610,13 +676,13 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
   section(static_cast<size_t>(n_sigs) * sizeof(uint32_t) + 16, o_sigs);
 
   // Device buffers.
-  n_small_ = static_cast<int>(bins_.size() + rescue_bins_.size()) + 2 * kRowBins + 1;
+  n_small_ = static_cast<int>(bins_.size() + rescue_bins_.size()) + 2 * kQueueBins + 1;
   if (!grow(d_reads_, cap_reads_, static_cast<size_t>(read_bytes) * 5 + 16) ||
       !grow(d_read_off_, cap_read_off_, static_cast<size_t>(total_reads) + 1) || !grow(d_plan_, cap_plan_, blob_bytes) ||
-      !grow(d_tasks_, cap_tasks_, tasks.size() + 1) || !grow(d_queue_, cap_queue_, static_cast<size_t>(queue_off[kRowBins]) + 1) ||
+      !grow(d_tasks_, cap_tasks_, tasks.size() + 1) || !grow(d_queue_, cap_queue_, static_cast<size_t>(queue_off[kQueueBins]) + 1) ||
       !grow(d_small_, cap_small_, static_cast<size_t>(n_small_)) || !grow(d_out_, cap_out_, static_cast<size_t>(out_len_) + 1) ||
       !grow(d_scratch_, cap_scratch_, scratch_total))
-    return fail(FGKL_E_CUDA, "device allocation failed");
+    return fail(FGKL_E_OUT_OF_MEMORY, "device allocation failed");
 
   // Pinned staging (the reads have their own buffer): read offsets | plan | tasks | queue offsets |
   // results | counters.
@@ -624,22 +690,22 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
   const size_t s_blob = s_read_off + align_up((total_reads + 1) * sizeof(int64_t));
   const size_t s_tasks = s_blob + align_up(blob_bytes);
   const size_t s_qoff = s_tasks + align_up(tasks.size() * sizeof(Task));
-  const size_t s_out = s_qoff + align_up((kRowBins + 1) * sizeof(int));
+  const size_t s_out = s_qoff + align_up((kQueueBins + 1) * sizeof(int));
   const size_t stage_bytes = s_out + align_up(static_cast<size_t>(out_len_) * sizeof(double)) + align_up(sizeof(Counters));
   if (stage_bytes > cap_stage_) {
     // Grown by half again at least, as the device buffers are (cudaFreeHost waits for the device).
     const size_t want = cap_stage_ > 0 ? std::max(stage_bytes, cap_stage_ + cap_stage_ / 2) : stage_bytes;
     if (h_stage_) cudaFreeHost(h_stage_);
     h_stage_ = nullptr;
-    if (cudaMallocHost(&h_stage_, want) == cudaSuccess) {
+    if (pinned_alloc(reinterpret_cast<void**>(&h_stage_), want) == cudaSuccess) {
       cap_stage_ = want;
-    } else if (want > stage_bytes && (cudaGetLastError(), cudaMallocHost(&h_stage_, stage_bytes) == cudaSuccess)) {
+    } else if (want > stage_bytes && (cudaGetLastError(), pinned_alloc(reinterpret_cast<void**>(&h_stage_), stage_bytes) == cudaSuccess)) {
       cap_stage_ = stage_bytes;
     } else {
       cudaGetLastError();
       cap_stage_ = 0;
       h_stage_ = nullptr;
-      return fail(FGKL_E_CUDA, "pinned host allocation failed");
+      return fail(FGKL_E_OUT_OF_MEMORY, "pinned host allocation failed");
     }
   }
   out_stage_ = s_out;
@@ -677,7 +743,7 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
     });
   }
   if (!tasks.empty()) std::memcpy(st + s_tasks, tasks.data(), tasks.size() * sizeof(Task));
-  std::memcpy(st + s_qoff, queue_off.data(), (kRowBins + 1) * sizeof(int));
+  std::memcpy(st + s_qoff, queue_off.data(), (kQueueBins + 1) * sizeof(int));
 
   read_copy.join();
   planned_.host_pack_ms = ms_since(t_pack);
@@ -693,7 +759,7 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
   if (!tasks.empty() &&
       (rc = check(cudaMemcpyAsync(d_tasks_, st + s_tasks, tasks.size() * sizeof(Task), cudaMemcpyHostToDevice, copy_), "upload tasks")))
     return rc;
-  if ((rc = check(cudaMemcpyAsync(d_small_ + (n_small_ - 2 * kRowBins - 1), st + s_qoff, (kRowBins + 1) * sizeof(int),
+  if ((rc = check(cudaMemcpyAsync(d_small_ + (n_small_ - 2 * kQueueBins - 1), st + s_qoff, (kQueueBins + 1) * sizeof(int),
                                   cudaMemcpyHostToDevice, copy_),
                   "upload queue offsets")))
     return rc;
@@ -729,24 +795,24 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
 }
 
 int Engine::begin_run() {
-  cudaSetDevice(device_);
+  DeviceGuard device_guard(device_);
   return check(cudaStreamWaitEvent(stream_, uploaded_, 0), "wait for the uploads");
 }
 
 int Engine::end_run() {
-  cudaSetDevice(device_);
+  DeviceGuard device_guard(device_);
   return check(cudaEventRecord(computed_, stream_), "kernels event");
 }
 
 int Engine::run() {
-  cudaSetDevice(device_);
+  DeviceGuard device_guard(device_);
   int rc;
   int* counters = d_small_;                                // one per launch
-  int* queue_off = d_small_ + (n_small_ - 2 * kRowBins - 1);  // kRowBins + 1 entries, uploaded by prepare
-  int* queue_tail = d_small_ + (n_small_ - kRowBins);
+  int* queue_off = d_small_ + (n_small_ - 2 * kQueueBins - 1);  // kQueueBins + 1 entries, uploaded by prepare
+  int* queue_tail = d_small_ + (n_small_ - kQueueBins);
   const size_t n_launch = bins_.size() + rescue_bins_.size();
   if ((rc = check(cudaMemsetAsync(counters, 0, n_launch * sizeof(int), stream_), "reset task counters"))) return rc;
-  if ((rc = check(cudaMemsetAsync(queue_tail, 0, kRowBins * sizeof(int), stream_), "reset queues"))) return rc;
+  if ((rc = check(cudaMemsetAsync(queue_tail, 0, kQueueBins * sizeof(int), stream_), "reset queues"))) return rc;
   if ((rc = check(cudaMemsetAsync(d_counters_, 0, sizeof(Counters), stream_), "reset counters"))) return rc;
   planned_.kernel_launches = 0;
   int i = 0;
@@ -772,7 +838,7 @@ int Engine::run() {
       a.v = view_;
       a.tasks = (rescue ? d_queue_ : d_tasks_) + bin.task_off;
       a.n_tasks = bin.n_tasks;
-      a.count = rescue ? queue_tail + bin.rows : nullptr;
+      a.count = rescue ? queue_tail + bin.queue_bin : nullptr;
       a.task_counter = counters + i++;
       a.scratch = d_scratch_ + bin.scratch_off;
       a.scratch_stride = bin.stride;
@@ -807,7 +873,7 @@ void Engine::set_tuning(const Tuning& t) {
 }
 
 int Engine::time_run(int repeats, double* ms) {
-  cudaSetDevice(device_);
+  DeviceGuard device_guard(device_);
   if (repeats < 1) repeats = 1;
   int rc;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -833,7 +899,7 @@ int Engine::time_run(int repeats, double* ms) {
 }
 
 int Engine::bin_profile(std::vector<BinProfile>* out) {
-  cudaSetDevice(device_);
+  DeviceGuard device_guard(device_);
   out->clear();
   if (!profile_) return fail(FGKL_E_INVALID_ARGUMENT, "profiling is off");
   int rc;
@@ -850,7 +916,7 @@ int Engine::bin_profile(std::vector<BinProfile>* out) {
 }
 
 int Engine::fetch(double* out, int64_t out_len, BatchStats* stats) {
-  cudaSetDevice(device_);
+  DeviceGuard device_guard(device_);
   const auto t_fetch = std::chrono::steady_clock::now();
   if (out_len != out_len_)
     return fail(FGKL_E_OUTPUT_LENGTH, "output has " + std::to_string(out_len) + " elements but reads x haplotypes is " +

@@ -14,6 +14,36 @@
 
 namespace fgkl {
 
+// Failure injection (fgkl_set_allocation_limit): device and page-locked host allocations larger
+// than this many bytes fail as if out of memory; 0 = no limit.
+int64_t allocation_limit();
+int64_t set_allocation_limit(int64_t bytes);
+// cudaMalloc / cudaMallocHost under that limit.
+cudaError_t device_alloc(void** p, size_t bytes);
+cudaError_t pinned_alloc(void** p, size_t bytes);
+
+// Makes `device` current for its scope and gives the calling thread its own current device back at
+// the end, so an engine's calls leave the caller's device as they found it.
+class DeviceGuard {
+ public:
+  explicit DeviceGuard(int device) {
+    if (cudaGetDevice(&prev_) != cudaSuccess) {
+      cudaGetLastError();
+      prev_ = -1;
+    }
+    if (prev_ != device) cudaSetDevice(device);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    if (prev_ >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev_) cudaSetDevice(prev_);
+  }
+  DeviceGuard(const DeviceGuard&) = delete;
+  DeviceGuard& operator=(const DeviceGuard&) = delete;
+
+ private:
+  int prev_ = -1;
+};
+
 struct EngineConfig {
   bool double_precision = false;  // Precision::Double (lib.rs:72-77)
   bool double_fallback = true;    // recompute lost pairs (lib.rs:218-222)
@@ -116,6 +146,7 @@ class Engine {
     size_t stride;       // scratch bytes per warp
     size_t scratch_off;  // this bin's slice of the scratch
     uint64_t fwd_cells = 0, bwd_cells = 0;  // DP cells its tasks compute (first pass)
+    int queue_bin = 0;   // recomputation bins: the queue bin (queue_bin) the tasks come from
   };
   static constexpr int kAuxStreams = 8;
   Tuning tuning_;

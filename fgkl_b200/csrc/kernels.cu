@@ -344,6 +344,9 @@ struct FwdState {
   // The next segment's record, loaded a segment ahead so a BEGIN never waits on memory.
   int nx_staged, nx_slot;
   S nx_init;
+  // Strip-mined reads: the row above lane 0's top row for this step's column (the previous block's
+  // bottom row, or GATK's row 0 in the first block). Read only by forward_step<..., kCarry = true>.
+  V cM, cX, cY;
 
   __device__ void load_next(const BatchView& v, const Program& prog, int seg) {
     if (seg < prog.n_segs) {
@@ -362,8 +365,9 @@ struct FwdState {
 // One forward step: events, then the column. (uM, uX, uY) receive the bottom row of the lane above
 // for this column; (dM, dX, dY) hold it for the previous column, the top row's diagonal. The two sets
 // alternate between consecutive steps, so no copies are needed. kEv = false compiles the event code
-// out, for steps where no lane of the warp has an event.
-template <class P, int R, bool kEv = true>
+// out, for steps where no lane of the warp has an event. kCarry = true gives lane 0 the row above
+// from the state's carry values instead of its own bottom row (strip-mined reads).
+template <class P, int R, bool kEv = true, bool kCarry = false>
 __device__ __forceinline__ void forward_step(const LaunchArgs& a, const Program& prog, const ReadRef* rd, int lane,
                                              const FwdRows<P, R>& fr, const typename P::V& an, int pad_hi, Scratch<P, R>& sc,
                                              FwdState<P, R>& st, int synth_len, uint32_t ev, typename P::V& uM, typename P::V& uX,
@@ -374,6 +378,11 @@ __device__ __forceinline__ void forward_step(const LaunchArgs& a, const Program&
   uM = P::up(st.M[R - 1]);
   uX = P::up(st.X[R - 1]);
   uY = P::up(st.Y[R - 1]);
+  if (kCarry && lane == 0) {
+    uM = st.cM;
+    uX = st.cX;
+    uY = st.cY;
+  }
   // END and ACC act in lane 31 alone (the read's last row); the other lanes pass them by without
   // entering the event code, which every lane otherwise reaches at its own step.
   if (kEv && (ev & (lane == 31 ? kEvMask : (kEvMask & ~(EV_END | EV_ACC))))) {
@@ -696,25 +705,185 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, (MinBlocks<P, R>::value))
 }
 
 // Queues every pair the first pass lost -- its output is NaN -- as an FP64 recomputation task, one
-// per (read, distinct sorted haplotype), in the bin of the read's rows-per-lane. One block per
-// region; nothing to do (one load per block) when no pair was lost.
+// per (read, distinct sorted haplotype), in the queue bin of its form and rows-per-lane (queue_bin).
+// One block per region; nothing to do (one load per block) when no pair was lost.
 __global__ void __launch_bounds__(256) collect_kernel(CollectArgs a) {
   if (a.v.counters->lost_pairs == 0) return;
   const Region region = a.v.regions[blockIdx.x];
   const int64_t pairs = static_cast<int64_t>(region.n_reads) * region.n_haps;
+  const bool generic = (region.flags & kRegionGeneric) != 0;
   for (int64_t e = threadIdx.x; e < pairs; e += blockDim.x) {
     const int r = static_cast<int>(e / region.n_haps), k = static_cast<int>(e % region.n_haps);
     const HapInfo info = a.v.haps[region.hap_off + k];
     if (info.src != k) continue;
     if (!isnan(a.v.out[region.out_off + static_cast<int64_t>(r) * region.n_haps + info.order])) continue;
     const int read = region.read_off + r;
-    int rows = static_cast<int>((a.v.read_off[read + 1] - a.v.read_off[read] + 30) / 31);
-    if (rows > 8) rows = (rows + 1) & ~1;
-    const int slot = atomicAdd(a.queue_tail + rows, 1);
-    if (slot < a.queue_off[rows + 1] - a.queue_off[rows]) {
-      a.queue[a.queue_off[rows] + slot] = Task{static_cast<int32_t>(blockIdx.x), {read, -1}, rows, k};
+    const int len = static_cast<int>(a.v.read_off[read + 1] - a.v.read_off[read]);
+    const int bin = queue_bin(len, generic);
+    const int rows = queue_bin_rows(bin);
+    const int slot = atomicAdd(a.queue_tail + bin, 1);
+    if (slot < a.queue_off[bin + 1] - a.queue_off[bin]) {
+      a.queue[a.queue_off[bin] + slot] = Task{static_cast<int32_t>(blockIdx.x), {read, -1}, rows, k};
       atomicAdd(&a.v.counters->rescue_reads, 1ull);
     }
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Strip-mined reads (longer than 620 bases; fgkl sizes its row tables by the batch's longest read,
+// kernel.rs:485-577, so any length is accepted): one read against one distinct haplotype, unshared,
+// from a stream synthesised from the haplotype's codes (the recomputation form above), with the read's
+// rows cut into B = ceil(len / 32R) blocks of 32R rows that the warp runs one after another. The
+// padding rows sit at the top of the first block. Lane 0's row above comes from a carry row instead of
+// its own bottom row: GATK's row 0 (M = X = 0, Y = INITIAL / hap_len) in the first block, the previous
+// block's bottom row after that, which lane 31 writes to the warp's scratch column by column. Lane 0
+// reads column j at step j, and lane 31 of the same block overwrites it at step j + 31 with a value
+// computed from it through the wavefront, so one carry row serves every block in place.
+// ---------------------------------------------------------------------------------------------
+
+// A column of a block's bottom row: M, X, Y (the FP32 kernels' X/mi and Y/md), padded to 16 bytes.
+constexpr int kCarryVals = 4;
+
+template <class P>
+__host__ __device__ constexpr size_t long_scratch_size(int max_hap_len) {
+  return 16 + static_cast<size_t>(max_hap_len) * kCarryVals * sizeof(typename P::V);
+}
+
+template <class P, int R>
+__device__ __forceinline__ void long_store(typename P::V* carry, const FwdState<P, R>& st, int lane, int t, int n, bool last) {
+  const int p = t - 31;  // lane 31's position at step t
+  if (!last && lane == 31 && p >= 0 && p < n) {
+    typename P::V rec[kCarryVals] = {st.M[R - 1], st.X[R - 1], st.Y[R - 1], P::zero()};
+    store_record(carry + static_cast<size_t>(p) * kCarryVals, rec);
+  }
+}
+
+template <class P, int R>
+__device__ __forceinline__ void long_fetch(const typename P::V* carry, typename P::V (&rec)[kCarryVals], int lane, int p, int n,
+                                           bool first) {
+  if (!first && lane == 0 && p < n) load_record(rec, carry + static_cast<size_t>(p) * kCarryVals);
+}
+
+// One block of a strip-mined pair: rd's pad is relative to the block (negative below the first).
+template <class P, int R>
+__device__ void long_block(const LaunchArgs& a, const ReadRef* rd, int lane, const FwdRows<P, R>& fr, typename P::V an,
+                           Scratch<P, R>& sc, const uint8_t* seq, int n, typename P::V* carry, bool first, bool last) {
+  using V = typename P::V;
+  using S = typename P::S;
+  const int pad_hi = rd[0].pad;
+  FwdState<P, R> st;
+#pragma unroll
+  for (int r = 0; r < R; ++r) st.M[r] = st.X[r] = st.Y[r] = P::zero();
+  st.acc = P::zero();
+  st.seg_i = -1;
+  st.nx_staged = 0;
+  st.nx_slot = -1;
+  st.nx_init = S(0);
+  st.cM = st.cX = P::zero();
+  st.cY = first ? static_cast<S>(Consts<P::kDouble>::kInitial / n) : P::zero();
+  const Program prog{};  // unused: the stream is synthesised
+  V aM = P::zero(), aX = P::zero(), aY = P::zero(), bM = P::zero(), bX = P::zero(), bY = P::zero();
+  // Lane 0's carry values for the next iteration's two steps, loaded an iteration ahead.
+  V n0[kCarryVals], n1[kCarryVals];
+#pragma unroll
+  for (int i = 0; i < kCarryVals; ++i) n0[i] = n1[i] = P::zero();
+  long_fetch<P, R>(carry, n0, lane, 0, n, first);
+  long_fetch<P, R>(carry, n1, lane, 1, n, first);
+  for (int t = 0; t < n + 32; t += 2) {
+    const uint32_t e0 = synth_entry(seq, n, t - lane), e1 = synth_entry(seq, n, t + 1 - lane);
+    V c0[kCarryVals], c1[kCarryVals];
+#pragma unroll
+    for (int i = 0; i < kCarryVals; ++i) {
+      c0[i] = n0[i];
+      c1[i] = n1[i];
+    }
+    long_fetch<P, R>(carry, n0, lane, t + 2, n, first);
+    long_fetch<P, R>(carry, n1, lane, t + 3, n, first);
+    if (!first) {
+      st.cM = c0[0];
+      st.cX = c0[1];
+      st.cY = c0[2];
+    }
+    forward_step<P, R, true, true>(a, prog, rd, lane, fr, an, pad_hi, sc, st, n, e0, aM, aX, aY, bM, bX, bY);
+    long_store<P, R>(carry, st, lane, t, n, last);
+    if (!first) {
+      st.cM = c1[0];
+      st.cX = c1[1];
+      st.cY = c1[2];
+    }
+    forward_step<P, R, true, true>(a, prog, rd, lane, fr, an, pad_hi, sc, st, n, e1, bM, bX, bY, aM, aX, aY);
+    long_store<P, R>(carry, st, lane, t + 1, n, last);
+  }
+}
+
+template <class P, int R>
+struct LongMinBlocks {
+  static constexpr int value = P::kDouble ? 1 : 2;
+};
+
+template <class P, int R>
+constexpr size_t long_smem_per_warp() {
+  using L = Layout<P, R>;
+  return static_cast<size_t>(L::kPriorCodes) * L::kRp * 32 * sizeof(typename P::V);
+}
+
+template <class P, int R>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, (LongMinBlocks<P, R>::value)) long_kernel(LaunchArgs a) {
+  using V = typename P::V;
+  using S = typename P::S;
+  using C = Consts<P::kDouble>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31;
+  const int warp_in_block = threadIdx.x >> 5;
+  const int warp = blockIdx.x * kWarpsPerBlock + warp_in_block;
+  V* priors = reinterpret_cast<V*>(smem_raw + warp_in_block * long_smem_per_warp<P, R>());
+  const int count = a.count ? min(*a.count, a.n_tasks) : a.n_tasks;
+  char* scratch = a.scratch + static_cast<size_t>(warp) * a.scratch_stride;
+  V* carry = reinterpret_cast<V*>(scratch + 16);
+  for (;;) {
+    int t = 0;
+    if (lane == 0) t = atomicAdd(a.task_counter, 1);
+    t = __shfl_sync(kFull, t, 0);
+    if (t >= count) break;
+    const Task task = a.tasks[t];
+    const Region region = a.v.regions[task.region];
+    const HapInfo info = a.v.haps[region.hap_off + task.hap];
+    const uint8_t* seq = a.v.hap_codes + region.seq_off + info.seq;
+    const int n = info.len;
+    ReadRef rd[1];
+    rd[0].off = a.v.read_off[task.read[0]];
+    rd[0].len = static_cast<int>(a.v.read_off[task.read[0] + 1] - rd[0].off);
+    const int blocks = long_blocks(rd[0].len, R);
+    const int pad0 = 32 * R * blocks - rd[0].len;
+    const uint8_t* codes = a.v.code_of_byte + region.code_off;
+    Scratch<P, R> sc(scratch, priors, 0, 0, 0);
+    sc.priors = priors;
+    // X factor of the read's last row: the accumulated result is the sum of M + mi_n * X^.
+    const V an = static_cast<S>(P::kTransformed ? err_prob(a.v, a.v.ins[rd[0].off + rd[0].len - 1]) : 1.0);
+    for (int b = 0; b < blocks; ++b) {
+      rd[0].pad = pad0 - 32 * R * b;
+      FwdRows<P, R> fr;
+      fr.load(a.v, rd, lane, codes, priors);
+      __syncwarp();
+      long_block<P, R>(a, rd, lane, fr, an, sc, seq, n, carry, b == 0, b == blocks - 1);
+      __syncwarp();
+    }
+    // Thresholds of an unshared pair (fgkl kernel.rs:897-914): FP32 results below 1e-28 or not finite
+    // go to the FP64 recomputation.
+    const double raw = sc.seg_raw[0];
+    bool lost = a.min_accept_plain ? !(raw >= C::kMinAccepted) : (raw != raw);
+    if (!P::kDouble) lost |= isinf(raw);
+    const double result = lost ? __longlong_as_double(0x7ff8000000000000ll) : log10(raw) - C::kLog10Initial;
+    const int read_local = task.read[0] - region.read_off;
+    unsigned long long lost_count = 0;
+    for (int k = lane; k < region.n_haps; k += 32) {
+      const HapInfo h = a.v.haps[region.hap_off + k];
+      if (h.src != task.hap) continue;
+      a.v.out[region.out_off + static_cast<int64_t>(read_local) * region.n_haps + h.order] = result;
+      lost_count += lost;
+    }
+    if (lost_count) atomicAdd(&a.v.counters->lost_pairs, lost_count);
+    __syncwarp();
   }
 }
 
@@ -808,7 +977,15 @@ auto dispatch(Kind k, int rows, Args&&... args) -> decltype(F<PackedF32, 1>::run
   return Ret{};
 }
 
+bool valid_long_rows(Kind k, int rows) {
+  const bool wide = k == Kind::kLongF32;
+  for (int i = 0; i < long_rows_count(wide); ++i)
+    if (long_rows_value(i, wide) == rows) return true;
+  return false;
+}
+
 bool valid_rows(Kind k, int rows) {
+  if (is_long(k)) return valid_long_rows(k, rows);
   switch (k) {
     case Kind::kPackedF32:
       return rows >= 1 && rows <= 8;
@@ -820,16 +997,80 @@ bool valid_rows(Kind k, int rows) {
       return (rows >= 1 && rows <= 8) || (rows >= 10 && rows <= 20 && rows % 2 == 0);
     case Kind::kPackedF32Pd:
       return rows >= 1 && rows <= 8;
+    default:
+      break;
   }
   return false;
+}
+
+// Strip-mined plain kinds over the rows-per-lane values of long_rows: 8..16 in FP32, 4..8 in FP64.
+template <class F>
+auto long_rows_narrow(int rows, F&& f) {
+  switch (rows) {
+    case 4: return f(std::integral_constant<int, 4>{});
+    case 6: return f(std::integral_constant<int, 6>{});
+    default: return f(std::integral_constant<int, 8>{});
+  }
+}
+template <class F>
+auto long_rows_wide(int rows, F&& f) {
+  switch (rows) {
+    case 8: return f(std::integral_constant<int, 8>{});
+    case 10: return f(std::integral_constant<int, 10>{});
+    case 12: return f(std::integral_constant<int, 12>{});
+    default: return f(std::integral_constant<int, 16>{});
+  }
+}
+
+template <class P, int R>
+void long_occ(int* blocks) {
+  static std::atomic<int> cache[kMaxDevices];
+  *blocks = resident_blocks(long_kernel<P, R>, kWarpsPerBlock * long_smem_per_warp<P, R>(), kWarpsPerBlock * 32, cache);
+}
+
+template <class P, int R>
+cudaError_t long_go(int blocks, const LaunchArgs& a, cudaStream_t s) {
+  long_kernel<P, R><<<blocks, kWarpsPerBlock * 32, kWarpsPerBlock * long_smem_per_warp<P, R>(), s>>>(a);
+  return cudaGetLastError();
 }
 
 }  // namespace
 
 int max_rows(Kind) { return 20; }
 
+size_t long_scratch_bytes(Kind k, int rows, int max_hap_len) {
+  if (!is_long(k) || !valid_long_rows(k, rows)) return 0;
+  if (is_pd(k)) return pd_long_scratch_bytes(k, rows, max_hap_len);
+  return k == Kind::kLongF64 ? long_scratch_size<OneF64>(max_hap_len) : long_scratch_size<OneF32>(max_hap_len);
+}
+
+void long_occupancy(Kind k, int rows, int* blocks, int* threads) {
+  *blocks = 0;
+  *threads = kWarpsPerBlock * 32;
+  if (!is_long(k) || !valid_long_rows(k, rows)) return;
+  if (is_pd(k)) return pd_long_occupancy(k, rows, blocks, threads);
+  if (k == Kind::kLongF64)
+    long_rows_narrow(rows, [&](auto r) {
+      long_occ<OneF64, decltype(r)::value>(blocks);
+      return 0;
+    });
+  else
+    long_rows_wide(rows, [&](auto r) {
+      long_occ<OneF32, decltype(r)::value>(blocks);
+      return 0;
+    });
+}
+
+cudaError_t long_launch(Kind k, int rows, int blocks, const LaunchArgs& args, cudaStream_t stream) {
+  if (!is_long(k) || !valid_long_rows(k, rows)) return cudaErrorInvalidValue;
+  if (is_pd(k)) return pd_long_launch(k, rows, blocks, args, stream);
+  if (k == Kind::kLongF64)
+    return long_rows_narrow(rows, [&](auto r) { return long_go<OneF64, decltype(r)::value>(blocks, args, stream); });
+  return long_rows_wide(rows, [&](auto r) { return long_go<OneF32, decltype(r)::value>(blocks, args, stream); });
+}
+
 size_t scratch_bytes(Kind k, int rows, int max_slots, int max_nodes, int max_segs) {
-  if (!valid_rows(k, rows)) return 0;
+  if (is_long(k) || !valid_rows(k, rows)) return 0;
   if (is_pd(k)) return pd_scratch_bytes(pd_form(k), rows, max_slots, max_segs);
   return dispatch<SizeF>(k, rows, max_slots, max_nodes, max_segs);
 }
@@ -838,6 +1079,7 @@ void occupancy(Kind k, int rows, int* blocks, int* threads) {
   *blocks = 0;
   *threads = kWarpsPerBlock * 32;
   if (!valid_rows(k, rows)) return;
+  if (is_long(k)) return long_occupancy(k, rows, blocks, threads);
   if (is_pd(k)) return pd_occupancy(pd_form(k), rows, blocks, threads);
   dispatch<OccF>(k, rows, blocks, threads);
 }
@@ -850,6 +1092,7 @@ cudaError_t launch_collect(const CollectArgs& args, int n_regions, cudaStream_t 
 
 cudaError_t launch(Kind k, int rows, int blocks, const LaunchArgs& args, cudaStream_t stream) {
   if (!valid_rows(k, rows)) return cudaErrorInvalidValue;
+  if (is_long(k)) return long_launch(k, rows, blocks, args, stream);
   if (is_pd(k)) return pd_launch(pd_form(k), rows, blocks, args, stream);
   return dispatch<GoF>(k, rows, blocks, args, stream);
 }
@@ -864,7 +1107,7 @@ cudaError_t launch(Kind k, int rows, int blocks, const LaunchArgs& args, cudaStr
 namespace {
 
 constexpr size_t kNoAllocScratchBytes = size_t{2} << 20;  // 2 MiB (FGKL_NOALLOC_SCRATCH_BYTES): header + 8191 warps
-constexpr size_t kNoAllocHeader = 256;                    // the pair counter (must be 0 at launch)
+constexpr size_t kNoAllocHeader = 256;                    // the 64-bit pair counter (must be 0 at launch)
 constexpr size_t kNoAllocPerWarp = 256;                   // one warp's segment result, 256-aligned
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
@@ -877,7 +1120,7 @@ struct NoAllocArgs {
   const uint8_t* hap_bases;
   const int64_t* hap_off;
   int n_reads, n_haps;
-  int* counter;   // pairs claimed so far
+  unsigned long long* counter;  // pairs claimed so far (64-bit: every warp claims one past the last pair)
   char* scratch;  // kNoAllocPerWarp bytes per warp
   double* out;    // n_reads x n_haps, row-major
 };
@@ -929,13 +1172,13 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 1) noalloc_kernel(NoAlloc
   const int warp = blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
   LaunchArgs a{};
   a.v = na.v;
-  const int pairs = na.n_reads * na.n_haps;
+  const long long pairs = static_cast<long long>(na.n_reads) * na.n_haps;
   for (;;) {
-    int t = 0;
-    if (lane == 0) t = atomicAdd(na.counter, 1);
-    t = __shfl_sync(kFull, t, 0);
+    unsigned long long claimed = 0;
+    if (lane == 0) claimed = atomicAdd(na.counter, 1ull);
+    const long long t = static_cast<long long>(__shfl_sync(kFull, claimed, 0));
     if (t >= pairs) break;
-    const int r = t / na.n_haps, h = t % na.n_haps;
+    const int r = static_cast<int>(t / na.n_haps), h = static_cast<int>(t % na.n_haps);
     ReadRef rd[1];
     rd[0].off = na.v.read_off[r];
     const int64_t read_len = na.v.read_off[r + 1] - rd[0].off;
@@ -996,6 +1239,10 @@ int noalloc_rows(int max_read_len) {
   return rows;
 }
 
+cudaError_t noalloc_scratch_address(char** scratch) {
+  return cudaGetSymbolAddress(reinterpret_cast<void**>(scratch), g_noalloc_scratch);
+}
+
 cudaError_t noalloc_setup(NoAllocDevice* d, const double* err, size_t n_err, const double* m2m, size_t n_m2m,
                           const uint8_t codes[256]) {
   cudaError_t e;
@@ -1033,10 +1280,10 @@ cudaError_t noalloc_launch(const NoAllocDevice& d, const NoAllocCall& c, int row
   na.hap_off = c.hap_off;
   na.n_reads = c.n_reads;
   na.n_haps = c.n_haps;
-  na.counter = reinterpret_cast<int*>(d.scratch);
+  na.counter = reinterpret_cast<unsigned long long*>(d.scratch);
   na.scratch = d.scratch + d.header_bytes;
   na.out = c.out;
-  cudaError_t e = cudaMemsetAsync(d.scratch, 0, sizeof(int), stream);  // the pair counter starts at zero
+  cudaError_t e = cudaMemsetAsync(d.scratch, 0, sizeof(unsigned long long), stream);  // the pair counter starts at zero
   if (e != cudaSuccess) return e;
   return noalloc_dispatch(rows, [&](auto r) { return noalloc_go<decltype(r)::value>(blocks, na, stream); });
 }

@@ -14,9 +14,63 @@ enum class Kind : int {
   kOneF32Pd = 3,   // PD-HMM, one read, FP32, rows-per-lane 1..8 and 10..20 (even)
   kOneF64Pd = 4,   // PD-HMM, one read, FP64, same rows
   kPackedF32Pd = 5,  // PD-HMM, two reads per lane set in FP32x2, rows-per-lane 1..8
+  // Reads longer than kMaxBlockRead bases: one read against one distinct haplotype, unshared, the
+  // rows strip-mined over blocks of 32 * R rows (rows-per-lane R from long_rows).
+  kLongF32 = 6,
+  kLongF64 = 7,
+  kLongF32Pd = 8,
+  kLongF64Pd = 9,
+  // PD-HMM regions whose reads hold more read bytes than the class bit sets cover: every pair as in
+  // the long kinds, with the prior decided by comparing bytes (any read length).
+  kGenericF32Pd = 10,
+  kGenericF64Pd = 11,
 };
+constexpr int kNumKinds = 12;
 
-inline bool is_pd(Kind k) { return k == Kind::kOneF32Pd || k == Kind::kOneF64Pd || k == Kind::kPackedF32Pd; }
+// Longest read a single 32 * R-row block holds (lane 0 is padding: 31 rows per lane x 20).
+constexpr int kMaxBlockRead = 620;
+// Rows-per-lane values of the strip-mined kinds: 8, 10, 12 and 16 for plain FP32 (kLongF32); 4, 6
+// and 8 for the others, whose per-row state (FP64 values, PD branch values) takes more registers.
+constexpr int kNumLongRows = 4;
+__host__ __device__ constexpr int long_rows_value(int i, bool wide) {
+  return wide ? (i == 0 ? 8 : (i == 1 ? 10 : (i == 2 ? 12 : 16))) : (i == 0 ? 4 : (i == 1 ? 6 : 8));
+}
+__host__ __device__ constexpr int long_rows_count(bool wide) { return wide ? 4 : 3; }
+// Rows per lane of a strip-mined read of `len` bases: the value whose blocks waste the fewest
+// padding rows (ties: the smaller). Blocks = ceil(len / (32 * R)). `wide`: the plain FP32 kind.
+__host__ __device__ inline int long_rows(int len, bool wide) {
+  int best = 8;
+  long long best_rows = -1;
+  for (int i = 0; i < long_rows_count(wide); ++i) {
+    const int r = long_rows_value(i, wide);
+    const long long rows = (static_cast<long long>(len) + 32 * r - 1) / (32 * r) * (32 * r);
+    if (best_rows < 0 || rows < best_rows) {
+      best_rows = rows;
+      best = r;
+    }
+  }
+  return best;
+}
+__host__ __device__ inline int long_blocks(int len, int rows) { return (len + 32 * rows - 1) / (32 * rows); }
+
+// Recomputation queue bins: rows-per-lane 1..20 of single-block reads, then kRowBins + R for
+// strip-mined reads and 2 * kRowBins + R for the pairs of byte-compared PD regions.
+constexpr int kRowBins = 21;
+constexpr int kQueueBins = 3 * kRowBins;
+__host__ __device__ inline int queue_bin(int len, bool generic) {
+  if (generic) return 2 * kRowBins + long_rows(len, false);
+  if (len > kMaxBlockRead) return kRowBins + long_rows(len, false);
+  int rows = (len + 30) / 31;
+  if (rows > 8) rows = (rows + 1) & ~1;
+  return rows;
+}
+__host__ __device__ inline int queue_bin_rows(int bin) { return bin % kRowBins; }
+
+inline bool is_long(Kind k) { return static_cast<int>(k) >= static_cast<int>(Kind::kLongF32); }
+inline bool is_pd(Kind k) {
+  return k == Kind::kOneF32Pd || k == Kind::kOneF64Pd || k == Kind::kPackedF32Pd || k == Kind::kLongF32Pd ||
+         k == Kind::kLongF64Pd || k == Kind::kGenericF32Pd || k == Kind::kGenericF64Pd;
+}
 
 // The PD instantiation a PD kind selects.
 enum class PdForm : int { kOneF32 = 0, kOneF64 = 1, kPackedF32 = 2 };
@@ -55,6 +109,15 @@ cudaError_t launch(Kind k, int rows, int blocks, const LaunchArgs& args, cudaStr
 size_t pd_scratch_bytes(PdForm form, int rows, int max_slots, int max_segs);
 void pd_occupancy(PdForm form, int rows, int* blocks_per_sm, int* threads_per_block);
 cudaError_t pd_launch(PdForm form, int rows, int blocks, const LaunchArgs& args, cudaStream_t stream);
+// Strip-mined kinds (is_long): per-warp scratch for haplotypes of at most `max_hap_len` bases (the
+// bottom row a block hands to the next, plus the pair's result), occupancy and launch. The plain
+// ones live in kernels.cu, the PD ones in pd_kernels.cu.
+size_t long_scratch_bytes(Kind k, int rows, int max_hap_len);
+void long_occupancy(Kind k, int rows, int* blocks_per_sm, int* threads_per_block);
+cudaError_t long_launch(Kind k, int rows, int blocks, const LaunchArgs& args, cudaStream_t stream);
+size_t pd_long_scratch_bytes(Kind k, int rows, int max_hap_len);
+void pd_long_occupancy(Kind k, int rows, int* blocks_per_sm, int* threads_per_block);
+cudaError_t pd_long_launch(Kind k, int rows, int blocks, const LaunchArgs& args, cudaStream_t stream);
 
 // Launches the lost-pair collection over `n_regions` regions.
 cudaError_t launch_collect(const CollectArgs& args, int n_regions, cudaStream_t stream);
@@ -87,6 +150,9 @@ struct NoAllocCall {
 
 // Rows per lane for reads of at most `max_read_len` bases.
 int noalloc_rows(int max_read_len);
+// The current device's address of the file-scope scratch array (changes when the device's primary
+// context is reset and recreated).
+cudaError_t noalloc_scratch_address(char** scratch);
 // Resolves the file-scope arrays of the current device and uploads the tables (synchronous).
 cudaError_t noalloc_setup(NoAllocDevice* d, const double* err, size_t n_err, const double* m2m, size_t n_m2m,
                           const uint8_t codes[256]);

@@ -83,6 +83,17 @@ struct PdRows {
     return P::sel((sig & cls[0][r]) != 0u, (sig & cls[P::NC - 1][r]) != 0u, pm[r], px[r]);
   }
 
+  // Regions whose reads hold more distinct bytes than the class bits cover compare bytes instead:
+  // after load_generic, cls holds the row's read byte (bits 0-7), whether it is N (bit 8) and the ALT
+  // bit it answers to (bits 9-12), and a stream entry carries the column's haplotype byte (bits 0-7)
+  // and its ALT bits (kPdPayloadShift up), so the column accepts the row's base exactly when
+  // MatchSet::accepts would (fgkl pd_kernel.rs:196-214).
+  __device__ V prior_generic(uint32_t ev, int r) const {
+    const uint32_t base = ev & kCodeMask, alts = (ev >> kPdPayloadShift) & 0xFu, c = cls[0][r];
+    const bool match = c != 0u && (((c & 0xFFu) == base) || base == 'N' || ((c >> 8) & 1u) || (((c >> 9) & alts) != 0u));
+    return match ? pm[r] : px[r];
+  }
+
   __device__ void load(const BatchView& v, const ReadRef* rd, int lane, const uint8_t* classes) {
 #pragma unroll
     for (int r = 0; r < R; ++r) {
@@ -124,6 +135,22 @@ struct PdRows {
       }
     }
   }
+
+  // As load, with the byte-comparison row descriptors of prior_generic in cls (one read).
+  __device__ void load_generic(const BatchView& v, const ReadRef* rd, int lane, const uint8_t* classes) {
+    load(v, rd, lane, classes);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int q = lane * R + r - rd[0].pad;
+      uint32_t d = 0;
+      if (rd[0].len > 0 && q >= 0 && q < rd[0].len) {
+        const uint32_t b = v.bases[rd[0].off + q];
+        const uint32_t alt = (b == 'A' || b == 'a') ? 1u : (b == 'C' || b == 'c') ? 2u : (b == 'G' || b == 'g') ? 4u : (b == 'T' || b == 't') ? 8u : 0u;
+        d = b | (b == 'N' ? 1u << 8 : 0u) | (alt << 9) | (1u << 13);  // bit 13: a read row (never 0)
+      }
+      cls[0][r] = d;
+    }
+  }
 };
 
 template <class P, int R>
@@ -133,6 +160,9 @@ struct PdState {
   V BM[R], BX[R], BY[R];
   V acc;
   int seg_i;
+  // Strip-mined reads: the row above lane 0's top row for this step's column, values and branch
+  // values (read only by pd_step<..., kCarry = true>).
+  V cM, cX, cY, cBM, cBX, cBY;
 };
 
 // The lane above's bottom row: values and branch values.
@@ -144,8 +174,10 @@ struct PdEdge {
 
 // One PD forward step: events, then the column. `u` receives the lane above's bottom row for this
 // column, `d` holds it for the previous column (the top row's diagonal); the two alternate. kEv = false
-// compiles the event code out, for steps where no lane of the warp has an event.
-template <class P, int R, bool kEv = true>
+// compiles the event code out, for steps where no lane of the warp has an event. kCarry = true gives
+// lane 0 the row above from the state's carry values (strip-mined reads); kGeneric = true decides
+// priors by comparing bytes (PdRows::prior_generic) instead of by class bits.
+template <class P, int R, bool kEv = true, bool kCarry = false, bool kGeneric = false>
 __device__ __forceinline__ void pd_step(const LaunchArgs& a, const Program& prog, const ReadRef* rd, int lane,
                                         const PdRows<P, R>& pr, const typename P::V& an, int pad_hi, PdScratch<P, R>& sc,
                                         PdState<P, R>& st, int synth_len, uint32_t ev, uint32_t sig, PdEdge<P>& u,
@@ -159,6 +191,14 @@ __device__ __forceinline__ void pd_step(const LaunchArgs& a, const Program& prog
   u.BM = P::up(st.BM[R - 1]);
   u.BX = P::up(st.BX[R - 1]);
   u.BY = P::up(st.BY[R - 1]);
+  if (kCarry && lane == 0) {
+    u.M = st.cM;
+    u.X = st.cX;
+    u.Y = st.cY;
+    u.BM = st.cBM;
+    u.BX = st.cBX;
+    u.BY = st.cBY;
+  }
   // END and ACC act in lane 31 alone (the read's last row); the other lanes pass them by without
   // entering the event code, which every lane otherwise reaches at its own step.
   if (kEv && (ev & (lane == 31 ? kEvMask : (kEvMask & ~(EV_END | EV_ACC))))) {
@@ -269,7 +309,7 @@ __device__ __forceinline__ void pd_step(const LaunchArgs& a, const Program& prog
         st.BX[r] = P::sel(inside[0], inside[P::NC - 1], st.BX[r], lX);
         st.BY[r] = P::sel(inside[0], inside[P::NC - 1], st.BY[r], lY);
       }
-      const V prior = pr.prior(sig, r);
+      const V prior = kGeneric ? pr.prior_generic(ev, r) : pr.prior(sig, r);
       st.Y[r] = P::kTransformed ? P::fma(lY, pr.c4[r], lM) : P::fma(lY, pr.c3[r], P::mul(lM, pr.c4[r]));
       st.M[r] = P::mul(prior, cell_match<P>(pM, pX, pY, pr.c0[r], pr.c1[r], pr.c2[r]));
     }
@@ -286,7 +326,7 @@ __device__ __forceinline__ void pd_step(const LaunchArgs& a, const Program& prog
 #pragma unroll
     for (int r = R - 1; r >= 0; --r) {
       const V pM = r ? st.M[r - 1] : d.M, pX = r ? st.X[r - 1] : d.X, pY = r ? st.Y[r - 1] : d.Y;
-      const V prior = pr.prior(sig, r);
+      const V prior = kGeneric ? pr.prior_generic(ev, r) : pr.prior(sig, r);
       st.Y[r] = P::kTransformed ? P::fma(st.Y[r], pr.c4[r], st.M[r]) : P::fma(st.Y[r], pr.c3[r], P::mul(st.M[r], pr.c4[r]));
       st.M[r] = P::mul(prior, cell_match<P>(pM, pX, pY, pr.c0[r], pr.c1[r], pr.c2[r]));
     }
@@ -451,6 +491,150 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, (PdMinBlocks<P, R>::value
   }
 }
 
+// ---------------------------------------------------------------------------------------------
+// Strip-mined PD pairs (reads longer than 620 bases), and every pair of a region whose reads hold
+// more distinct bytes than the class bits cover (kGeneric): one read against one distinct
+// haplotype, unshared, over the haplotype's forward entries, the rows cut into blocks of 32 R rows
+// run one after another. Lane 0's row above -- values and branch values -- comes from a carry row:
+// GATK's row 0 in the first block (M = X = 0, Y = INITIAL / hap_len, no branch values), after that
+// the previous block's bottom row, written by lane 31 column by column and read by lane 0 31 steps
+// before lane 31 of the next block overwrites it (the plain strip-mined kernel's scheme). The
+// state a block's top row starts in is the previous row's, which the entries' later-row state
+// carries; only the read's first row (in the first block) takes the first-row state.
+// ---------------------------------------------------------------------------------------------
+
+constexpr int kPdCarryVals = 8;  // M, X, Y, BM, BX, BY, padded to 16 bytes
+
+template <class P>
+constexpr size_t pd_long_scratch_size(int max_hap_len) {
+  return 16 + static_cast<size_t>(max_hap_len) * kPdCarryVals * sizeof(typename P::V);
+}
+
+template <class P, int R>
+__device__ __forceinline__ void pd_long_store(typename P::V* carry, const PdState<P, R>& st, int lane, int t, int n, bool last) {
+  const int p = t - 31;
+  if (!last && lane == 31 && p >= 0 && p < n) {
+    typename P::V rec[kPdCarryVals] = {st.M[R - 1],  st.X[R - 1],  st.Y[R - 1], st.BM[R - 1],
+                                       st.BX[R - 1], st.BY[R - 1], P::zero(),   P::zero()};
+    store_record(carry + static_cast<size_t>(p) * kPdCarryVals, rec);
+  }
+}
+
+template <class P>
+__device__ __forceinline__ void pd_long_fetch(const typename P::V* carry, typename P::V (&rec)[kPdCarryVals], int lane, int p, int n,
+                                              bool first) {
+  if (!first && lane == 0 && p < n) load_record(rec, carry + static_cast<size_t>(p) * kPdCarryVals);
+}
+
+template <class P, int R>
+__device__ __forceinline__ void pd_set_carry(PdState<P, R>& st, const typename P::V (&c)[kPdCarryVals]) {
+  st.cM = c[0];
+  st.cX = c[1];
+  st.cY = c[2];
+  st.cBM = c[3];
+  st.cBX = c[4];
+  st.cBY = c[5];
+}
+
+template <class P, int R, bool kGeneric>
+__device__ void pd_long_block(const LaunchArgs& a, const ReadRef* rd, int lane, const PdRows<P, R>& pr, typename P::V an,
+                              PdScratch<P, R>& sc, const uint32_t* seq, const uint32_t* sigs, int n, typename P::V* carry,
+                              bool first, bool last) {
+  using V = typename P::V;
+  using S = typename P::S;
+  const int pad_hi = rd[0].pad;
+  PdState<P, R> st;
+#pragma unroll
+  for (int r = 0; r < R; ++r) st.M[r] = st.X[r] = st.Y[r] = st.BM[r] = st.BX[r] = st.BY[r] = P::zero();
+  st.acc = P::zero();
+  st.seg_i = -1;
+  st.cM = st.cX = st.cBM = st.cBX = st.cBY = P::zero();
+  st.cY = first ? static_cast<S>(Consts<P::kDouble>::kInitial / n) : P::zero();
+  const Program prog{};
+  PdEdge<P> ea, eb;
+  ea.M = ea.X = ea.Y = ea.BM = ea.BX = ea.BY = P::zero();
+  eb = ea;
+  V n0[kPdCarryVals], n1[kPdCarryVals];
+#pragma unroll
+  for (int i = 0; i < kPdCarryVals; ++i) n0[i] = n1[i] = P::zero();
+  pd_long_fetch<P>(carry, n0, lane, 0, n, first);
+  pd_long_fetch<P>(carry, n1, lane, 1, n, first);
+  for (int t = 0; t < n + 32; t += 2) {
+    const uint32_t e0 = pd_synth_entry(seq, n, t - lane), e1 = pd_synth_entry(seq, n, t + 1 - lane);
+    const uint32_t s0 = kGeneric ? 0u : __ldg(sigs + (e0 & kCodeMask)), s1 = kGeneric ? 0u : __ldg(sigs + (e1 & kCodeMask));
+    V c0[kPdCarryVals], c1[kPdCarryVals];
+#pragma unroll
+    for (int i = 0; i < kPdCarryVals; ++i) {
+      c0[i] = n0[i];
+      c1[i] = n1[i];
+    }
+    pd_long_fetch<P>(carry, n0, lane, t + 2, n, first);
+    pd_long_fetch<P>(carry, n1, lane, t + 3, n, first);
+    if (!first) pd_set_carry<P, R>(st, c0);
+    pd_step<P, R, true, true, kGeneric>(a, prog, rd, lane, pr, an, pad_hi, sc, st, n, e0, s0, ea, eb);
+    pd_long_store<P, R>(carry, st, lane, t, n, last);
+    if (!first) pd_set_carry<P, R>(st, c1);
+    pd_step<P, R, true, true, kGeneric>(a, prog, rd, lane, pr, an, pad_hi, sc, st, n, e1, s1, eb, ea);
+    pd_long_store<P, R>(carry, st, lane, t + 1, n, last);
+  }
+}
+
+template <class P, int R, bool kGeneric>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, (P::kDouble ? 1 : 2)) pd_long_kernel(LaunchArgs a) {
+  using V = typename P::V;
+  using S = typename P::S;
+  using C = Consts<P::kDouble>;
+  const int lane = threadIdx.x & 31;
+  const int warp = blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+  const int count = a.count ? min(*a.count, a.n_tasks) : a.n_tasks;
+  char* scratch = a.scratch + static_cast<size_t>(warp) * a.scratch_stride;
+  V* carry = reinterpret_cast<V*>(scratch + 16);
+  for (;;) {
+    int t = 0;
+    if (lane == 0) t = atomicAdd(a.task_counter, 1);
+    t = __shfl_sync(kFull, t, 0);
+    if (t >= count) break;
+    const Task task = a.tasks[t];
+    const Region region = a.v.regions[task.region];
+    const HapInfo info = a.v.haps[region.hap_off + task.hap];
+    const uint32_t* seq = a.v.pd_entries + region.seq_off + info.seq;
+    const uint32_t* sigs = a.v.pd_sigs + region.sig_off;
+    const uint8_t* classes = a.v.code_of_byte + region.code_off;
+    const int n = info.len;
+    ReadRef rd[1];
+    rd[0].off = a.v.read_off[task.read[0]];
+    rd[0].len = static_cast<int>(a.v.read_off[task.read[0] + 1] - rd[0].off);
+    const int blocks = long_blocks(rd[0].len, R);
+    const int pad0 = 32 * R * blocks - rd[0].len;
+    PdScratch<P, R> sc(scratch, nullptr, 0);
+    const V an = static_cast<S>(P::kTransformed ? err_prob(a.v, a.v.ins[rd[0].off + rd[0].len - 1]) : 1.0);
+    for (int b = 0; b < blocks; ++b) {
+      rd[0].pad = pad0 - 32 * R * b;
+      PdRows<P, R> pr;
+      if (kGeneric)
+        pr.load_generic(a.v, rd, lane, classes);
+      else
+        pr.load(a.v, rd, lane, classes);
+      pd_long_block<P, R, kGeneric>(a, rd, lane, pr, an, sc, seq, sigs, n, carry, b == 0, b == blocks - 1);
+      __syncwarp();
+    }
+    const double raw = sc.seg_raw[0];
+    bool lost = a.min_accept_plain ? !(raw >= C::kMinAccepted) : (raw != raw);
+    if (!P::kDouble) lost |= isinf(raw);
+    const double result = lost ? __longlong_as_double(0x7ff8000000000000ll) : log10(raw) - C::kLog10Initial;
+    const int read_local = task.read[0] - region.read_off;
+    unsigned long long lost_count = 0;
+    for (int k = lane; k < region.n_haps; k += 32) {
+      const HapInfo h = a.v.haps[region.hap_off + k];
+      if (h.src != task.hap) continue;
+      a.v.out[region.out_off + static_cast<int64_t>(read_local) * region.n_haps + h.order] = result;
+      lost_count += lost;
+    }
+    if (lost_count) atomicAdd(&a.v.counters->lost_pairs, lost_count);
+    __syncwarp();
+  }
+}
+
 template <class P, int R>
 void pd_occ(int* blocks) {
   static std::atomic<int> cache[kMaxDevices];
@@ -501,7 +685,57 @@ auto pd_rows8(int rows, F&& f) {
   }
 }
 
+template <class F>
+auto pd_long_rows(int rows, F&& f) {
+  switch (rows) {
+    case 4: return f(std::integral_constant<int, 4>{});
+    case 6: return f(std::integral_constant<int, 6>{});
+    default: return f(std::integral_constant<int, 8>{});
+  }
+}
+
+template <class P, int R, bool kGeneric>
+void pd_long_occ(int* blocks) {
+  static std::atomic<int> cache[kMaxDevices];
+  *blocks = resident_blocks(pd_long_kernel<P, R, kGeneric>, 0, kWarpsPerBlock * 32, cache);
+}
+
 }  // namespace
+
+size_t pd_long_scratch_bytes(Kind k, int, int max_hap_len) {
+  const bool dbl = k == Kind::kLongF64Pd || k == Kind::kGenericF64Pd;
+  return dbl ? pd_long_scratch_size<OneF64>(max_hap_len) : pd_long_scratch_size<OneF32>(max_hap_len);
+}
+
+void pd_long_occupancy(Kind k, int rows, int* blocks, int* threads) {
+  *threads = kWarpsPerBlock * 32;
+  *blocks = 0;
+  pd_long_rows(rows, [&](auto r) {
+    constexpr int R = decltype(r)::value;
+    switch (k) {
+      case Kind::kLongF32Pd: pd_long_occ<OneF32, R, false>(blocks); break;
+      case Kind::kLongF64Pd: pd_long_occ<OneF64, R, false>(blocks); break;
+      case Kind::kGenericF32Pd: pd_long_occ<OneF32, R, true>(blocks); break;
+      case Kind::kGenericF64Pd: pd_long_occ<OneF64, R, true>(blocks); break;
+      default: break;
+    }
+    return 0;
+  });
+}
+
+cudaError_t pd_long_launch(Kind k, int rows, int blocks, const LaunchArgs& a, cudaStream_t s) {
+  return pd_long_rows(rows, [&](auto r) -> cudaError_t {
+    constexpr int R = decltype(r)::value;
+    switch (k) {
+      case Kind::kLongF32Pd: pd_long_kernel<OneF32, R, false><<<blocks, kWarpsPerBlock * 32, 0, s>>>(a); break;
+      case Kind::kLongF64Pd: pd_long_kernel<OneF64, R, false><<<blocks, kWarpsPerBlock * 32, 0, s>>>(a); break;
+      case Kind::kGenericF32Pd: pd_long_kernel<OneF32, R, true><<<blocks, kWarpsPerBlock * 32, 0, s>>>(a); break;
+      case Kind::kGenericF64Pd: pd_long_kernel<OneF64, R, true><<<blocks, kWarpsPerBlock * 32, 0, s>>>(a); break;
+      default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+  });
+}
 
 size_t pd_scratch_bytes(PdForm form, int rows, int max_slots, int max_segs) {
   switch (form) {

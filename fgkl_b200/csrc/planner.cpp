@@ -281,11 +281,14 @@ SortedHaps SortedHaps::make_pd(const std::vector<HapView>& haps, const std::vect
     s.flags.push_back(f);
     s.end_state.push_back(ends[i]);
     s.codes[k].resize(h.len);
-    for (int32_t j = 0; j < h.len; ++j) {
+    for (int32_t j = 0; j < h.len && !s.too_many_sets; ++j) {
       const MatchSet set = MatchSet::of(h.bases[j], f[j]);
       auto it = std::find(s.match_sets.begin(), s.match_sets.end(), set);
       if (it == s.match_sets.end()) {
-        if (s.match_sets.size() >= 256) throw std::invalid_argument("more than 256 distinct PD match sets");
+        if (s.match_sets.size() >= 256) {
+          s.too_many_sets = true;
+          break;
+        }
         s.match_sets.push_back(set);
         it = s.match_sets.end() - 1;
       }

@@ -86,6 +86,9 @@ struct SortedHaps {
   std::vector<MatchSet> match_sets;
   std::vector<std::vector<uint32_t>> pd_bits;
   std::vector<uint8_t> end_state;
+  // More than 256 distinct match sets: codes do not fit the stream's code byte and are left zero;
+  // such a region compares bytes instead (the entries then carry base and ALT bits).
+  bool too_many_sets = false;
 
   static SortedHaps make(const std::vector<HapView>& haps, bool share_suffixes);
   // Prefix sharing only, as fgkl's PD kernel.

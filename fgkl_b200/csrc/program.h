@@ -100,8 +100,11 @@ struct Region {
   int32_t code_off; // 256-entry byte -> prior code table (PD: read byte -> read class)
   int32_t seq_off;  // sorted haplotypes' prior codes (PD: forward entries), concatenated (recomputation streams)
   int32_t sig_off;  // PD: per match-set code, the bit set of read classes it accepts
-  int32_t pad_;
+  int32_t flags;    // kRegion* bits
 };
+
+// Region flags.
+constexpr int32_t kRegionGeneric = 1;  // PD: prior by byte comparison (more read bytes than class bits)
 
 // Per sorted haplotype: where its result goes and where it comes from.
 struct HapInfo {
