@@ -23,6 +23,7 @@ FGKL_E_INVALID_ARGUMENT = -7
 FGKL_E_UNSUPPORTED = -8
 FGKL_E_NO_DEVICE = -9
 FGKL_E_CUDA = -10
+FGKL_E_OUT_OF_MEMORY = -11
 
 u8p = C.POINTER(C.c_uint8)
 i32p = C.POINTER(C.c_int32)
@@ -157,6 +158,8 @@ def lib() -> C.CDLL:
     L.fgkl_set_call_combining.restype = C.c_int
     L.fgkl_call_combining_stats.argtypes = [C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
     L.fgkl_call_combining_stats.restype = C.c_int
+    L.fgkl_set_allocation_limit.argtypes = [C.c_int64]
+    L.fgkl_set_allocation_limit.restype = C.c_int64
     L.fgkl_backend.restype = C.c_char_p
     L.fgkl_last_error.restype = C.c_char_p
     L.fgkl_context_create.argtypes = [C.c_int32, C.c_void_p]
@@ -196,10 +199,6 @@ def lib() -> C.CDLL:
     L.fgkl_adjoint_output_len.restype = C.c_int64
     L.fgkl_adjoint_grad_len.argtypes = [C.c_void_p]
     L.fgkl_adjoint_grad_len.restype = C.c_int64
-    L.fgkl_adjoint_set_stored_columns.argtypes = [C.c_void_p, C.c_int32]
-    L.fgkl_adjoint_set_stored_columns.restype = C.c_int
-    L.fgkl_adjoint_checkpointed_launches.argtypes = [C.c_void_p]
-    L.fgkl_adjoint_checkpointed_launches.restype = C.c_int32
     L.fgkl_pd_row_states.argtypes = [u8p, C.c_int32, C.c_int32, u8p]
     L.fgkl_pd_plan_describe.argtypes = [u8p, u8p, i32p, C.c_int32, i32p, i32p, u8p, u8p, i32p]
     L.fgkl_pd_match_accepts.argtypes = [C.c_uint8, C.c_uint8, C.c_uint8]
@@ -216,11 +215,10 @@ def last_error() -> str:
 # Symbols include/fgkl_b200.h declares; the CPU test suite checks the library exports each one.
 EXPORTED = [
     "fgkl_pairhmm_compute", "fgkl_pairhmm_compute_config", "fgkl_pdhmm_compute", "fgkl_pdhmm_compute_config",
-    "fgkl_set_call_combining", "fgkl_call_combining_stats", "fgkl_backend", "fgkl_last_error", "fgkl_context_create", "fgkl_context_destroy", "fgkl_batch_prepare",
+    "fgkl_set_call_combining", "fgkl_call_combining_stats", "fgkl_set_allocation_limit", "fgkl_backend", "fgkl_last_error", "fgkl_context_create", "fgkl_context_destroy", "fgkl_batch_prepare",
     "fgkl_batch_run", "fgkl_batch_fetch", "fgkl_batch_compute", "fgkl_batch_output_len", "fgkl_context_autotune",
     "fgkl_context_set_tuning", "fgkl_context_get_tuning", "fgkl_synth_config",
     "fgkl_synth_reference_region", "fgkl_synth_view", "fgkl_synth_free", "fgkl_plan_describe", "fgkl_plan_sweeps", "fgkl_probe_fp32_tflops",
     "fgkl_pairhmm_compute_device_noalloc", "fgkl_context_profile", "fgkl_batch_launch_profile", "fgkl_adjoint_prepare", "fgkl_adjoint_run", "fgkl_adjoint_fetch",
-    "fgkl_adjoint_compute", "fgkl_adjoint_output_len", "fgkl_adjoint_grad_len", "fgkl_adjoint_set_stored_columns",
-    "fgkl_adjoint_checkpointed_launches", "fgkl_pd_row_states", "fgkl_pd_plan_describe", "fgkl_pd_match_accepts",
+    "fgkl_adjoint_compute", "fgkl_adjoint_output_len", "fgkl_adjoint_grad_len", "fgkl_pd_row_states", "fgkl_pd_plan_describe", "fgkl_pd_match_accepts",
 ]

@@ -43,16 +43,56 @@ int pick_device(int* device) {
   return FGKL_OK;
 }
 
-// One engine per calling thread for the per-call entry points.
+// One engine per calling thread for the per-call entry points. Engines are never destroyed: a
+// thread that exits hands its engine to a pool, from which the next new thread on that device takes
+// it. So no CUDA call runs from a destructor -- at a thread's exit, or at the process's exit, when
+// the main thread's thread-local objects are destroyed while the CUDA runtime's own teardown may
+// already be under way -- and a caller whose threads come and go (a JVM thread pool) reuses the
+// engines' device buffers instead of allocating new ones.
+struct EnginePool {
+  std::mutex mu;
+  std::vector<std::pair<int, fgkl::Engine*>> idle;  // (device, engine)
+};
+EnginePool& engine_pool() {
+  static EnginePool* pool = new EnginePool;  // never destroyed, like its engines
+  return *pool;
+}
+
+struct ThreadEngine {
+  fgkl::Engine* engine = nullptr;
+  int device = -1;
+  ~ThreadEngine() {
+    if (!engine) return;
+    EnginePool& p = engine_pool();
+    std::lock_guard<std::mutex> lock(p.mu);
+    try {
+      p.idle.emplace_back(device, engine);
+    } catch (...) {
+      // Out of host memory at thread exit: the engine is left unreferenced rather than destroyed.
+    }
+  }
+};
+
 fgkl::Engine* thread_engine(int* rc) {
-  thread_local std::unique_ptr<fgkl::Engine> engine;
-  if (!engine) {
+  thread_local ThreadEngine te;
+  if (!te.engine) {
     int d = 0;
     if ((*rc = pick_device(&d)) != FGKL_OK) return nullptr;
-    engine = std::make_unique<fgkl::Engine>(d);
+    {
+      EnginePool& p = engine_pool();
+      std::lock_guard<std::mutex> lock(p.mu);
+      for (size_t i = 0; i < p.idle.size(); ++i)
+        if (p.idle[i].first == d) {
+          te.engine = p.idle[i].second;
+          p.idle.erase(p.idle.begin() + static_cast<std::ptrdiff_t>(i));
+          break;
+        }
+    }
+    if (!te.engine) te.engine = new fgkl::Engine(d);
+    te.device = d;
   }
   *rc = FGKL_OK;
-  return engine.get();
+  return te.engine;
 }
 
 // Offset table -> (start, end) checks of crates/jni/src/lib.rs:343-363.
@@ -105,7 +145,7 @@ int run_on(fgkl::Engine* e, const CallRequest& q, fgkl_stats* stats) try {
   if (stats) to_stats(bs, stats);
   return FGKL_OK;
 } catch (const std::bad_alloc&) {
-  return set_error(FGKL_E_CUDA, "host memory allocation failed");
+  return set_error(FGKL_E_OUT_OF_MEMORY, "host memory allocation failed");
 } catch (...) {
   return set_error(FGKL_E_CUDA, "internal error in the per-call path");
 }
@@ -117,7 +157,7 @@ int run_alone(const CallRequest& q, fgkl_stats* stats) try {
   if (!e) return rc;
   return run_on(e, q, stats);
 } catch (const std::bad_alloc&) {
-  return set_error(FGKL_E_CUDA, "host memory allocation failed");
+  return set_error(FGKL_E_OUT_OF_MEMORY, "host memory allocation failed");
 } catch (...) {
   return set_error(FGKL_E_CUDA, "internal error in the per-call path");
 }
@@ -275,7 +315,7 @@ int combined_call(CallRequest& q) {
           try {
             c.engines[slot] = new fgkl::Engine(d);
           } catch (...) {
-            rc = set_error(FGKL_E_CUDA, "host memory allocation failed");
+            rc = set_error(FGKL_E_OUT_OF_MEMORY, "host memory allocation failed");
           }
         }
         if (rc != FGKL_OK) {
@@ -402,7 +442,13 @@ int noalloc_device(fgkl::NoAllocDevice** out) {
   if (d >= kNoAllocMaxDevices) return set_error(FGKL_E_NO_DEVICE, "device ordinal beyond the 64 the entry tracks");
   fgkl::NoAllocDevice& dev = g_noalloc[d];
   std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-  if (!dev.ready) {
+  // The array's address is looked up on every call (a host-side query): after a device reset the
+  // primary context, and with it the array and the uploaded tables, are new, so the set-up is redone.
+  char* scratch = nullptr;
+  if (cudaError_t e = fgkl::noalloc_scratch_address(&scratch); e != cudaSuccess)
+    return set_error(FGKL_E_CUDA, std::string("allocation-free entry: ") + cudaGetErrorString(e));
+  if (!dev.ready || scratch != dev.scratch) {
+    dev.ready = false;
     int major = 0, minor = 0, sms = 0;
     if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, d) != cudaSuccess ||
         cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, d) != cudaSuccess ||
@@ -475,6 +521,12 @@ int fgkl_call_combining_stats(uint64_t* batches, uint64_t* requests) {
   return FGKL_OK;
 }
 
+int64_t fgkl_set_allocation_limit(int64_t bytes) {
+  t_error.clear();
+  if (bytes < 0) return set_error(FGKL_E_INVALID_ARGUMENT, "the allocation limit must not be negative");
+  return fgkl::set_allocation_limit(bytes);
+}
+
 const char* fgkl_backend(void) { return "cuda-sm100a"; }
 
 const char* fgkl_last_error(void) { return t_error.c_str(); }
@@ -495,6 +547,7 @@ fgkl_context* fgkl_context_create(int32_t device, void* stream) {
 
 void fgkl_context_destroy(fgkl_context* ctx) {
   if (!ctx) return;
+  fgkl::DeviceGuard device_guard(ctx->device);
   if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
   delete ctx;
 }
@@ -528,6 +581,7 @@ int fgkl_batch_prepare(fgkl_context* ctx, const fgkl_batch* b, const fgkl_config
 int fgkl_batch_run(fgkl_context* ctx) {
   t_error.clear();
   if (!ctx || !ctx->prepared) return set_error(FGKL_E_INVALID_ARGUMENT, "no prepared batch");
+  fgkl::DeviceGuard device_guard(ctx->device);  // capture and graph launch on the context's device
   fgkl::Engine& e = *ctx->engine;
   if (e.output_len() == 0) return FGKL_OK;
   cudaStream_t s = e.stream();
@@ -850,18 +904,6 @@ int fgkl_adjoint_compute(fgkl_context* ctx, const fgkl_adjoint_batch* b, int32_t
   if ((rc = fgkl_adjoint_run(ctx, nullptr))) return rc;
   return fgkl_adjoint_fetch(ctx, log10_out, out_len, grad_gap_open_ins, grad_gap_open_del, grad_gap_continuation, grad_base_error,
                             grad_len, fp64_reads);
-}
-
-int fgkl_adjoint_set_stored_columns(fgkl_context* ctx, int32_t columns) {
-  t_error.clear();
-  if (!ctx || columns < 0) return set_error(FGKL_E_INVALID_ARGUMENT, "bad stored column count");
-  if (!ctx->adjoint) ctx->adjoint = std::make_unique<fgkl::AdjointEngine>(ctx->device, ctx->stream);
-  ctx->adjoint->set_stored_columns(columns);
-  return FGKL_OK;
-}
-
-int32_t fgkl_adjoint_checkpointed_launches(const fgkl_context* ctx) {
-  return ctx && ctx->adjoint ? ctx->adjoint->checkpointed_launches() : 0;
 }
 
 int64_t fgkl_adjoint_output_len(const fgkl_context* ctx) { return ctx && ctx->adjoint ? ctx->adjoint->output_len() : 0; }

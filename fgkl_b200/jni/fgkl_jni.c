@@ -11,7 +11,13 @@ static void throw_for(JNIEnv* env, int rc) {
   (*env)->ThrowNew(env, (*env)->FindClass(env, cls), fgkl_last_error());
 }
 
-/* Copies a Java byte[] (NULL when the JVM is out of memory: an exception is then pending). */
+/* A native allocation failed: fgkl's panic path (crates/jni/src/lib.rs:39-74) throws RuntimeException. */
+static void throw_out_of_memory(JNIEnv* env) {
+  if ((*env)->ExceptionCheck(env)) return;
+  (*env)->ThrowNew(env, (*env)->FindClass(env, "java/lang/RuntimeException"), "native memory allocation failed");
+}
+
+/* Copies a Java byte[] into native memory; NULL when malloc fails. */
 static jbyte* bytes(JNIEnv* env, jbyteArray a, jsize* n) {
   *n = (*env)->GetArrayLength(env, a);
   jbyte* p = malloc(*n ? (size_t)*n : 1);
@@ -34,9 +40,13 @@ static void compute(JNIEnv* env, int pd, jbyteArray bases, jbyteArray quals, jby
         *hf = pd ? bytes(env, hap_flags, &nhf) : NULL;
   jint *ro = ints(env, read_offsets, &nro), *ho = ints(env, hap_offsets, &nho);
   double* out = NULL;
+  jsize n_out = 0;
   if (!(*env)->ExceptionCheck(env)) {
-    const jsize n_out = (*env)->GetArrayLength(env, likelihoods);
+    n_out = (*env)->GetArrayLength(env, likelihoods);
     out = malloc(n_out ? (size_t)n_out * sizeof(double) : 1);
+    if (!b || !q || !i || !d || !g || !hb || (pd && !hf) || !ro || !ho || !out) throw_out_of_memory(env);
+  }
+  if (!(*env)->ExceptionCheck(env)) {
     fgkl_reads r = {(const uint8_t*)b, nb, (const uint8_t*)q, nq, (const uint8_t*)i, ni,
                     (const uint8_t*)d, nd, (const uint8_t*)g, ng, ro, nro};
     fgkl_haplotypes h = {(const uint8_t*)hb, nhb, (const uint8_t*)hf, nhf, ho, nho};

@@ -8,6 +8,7 @@ C ABI. ``BatchContext`` is the batched, persistent form over many regions.
 from __future__ import annotations
 
 import ctypes as C
+import sys
 import enum
 from dataclasses import dataclass
 from typing import Sequence
@@ -126,6 +127,16 @@ def set_call_combining(max_batches: int) -> int:
     call runs alone; at most 8; default 2) and returns the previous value. Calls made through
     PairHmm / PdPairHmm carry counters and always run alone; the JNI entry points do not."""
     rc = lib().fgkl_set_call_combining(int(max_batches))
+    if rc < 0:
+        raise ValueError(_lib.last_error())
+    return rc
+
+
+def set_allocation_limit(limit_bytes: int) -> int:
+    """Failure injection: device and page-locked host allocations of more than ``limit_bytes`` fail
+    as out of memory (``DeviceError`` with code ``FGKL_E_OUT_OF_MEMORY``) until the limit is removed
+    with 0. Returns the previous limit."""
+    rc = int(lib().fgkl_set_allocation_limit(int(limit_bytes)))
     if rc < 0:
         raise ValueError(_lib.last_error())
     return rc
@@ -416,6 +427,10 @@ class BatchContext:
             self._ctx = None
 
     def __del__(self):
+        # At interpreter shutdown the context is left to the process's exit: destroying it then
+        # would run CUDA calls while the runtimes in the process are being torn down.
+        if sys.is_finalizing():
+            return
         try:
             self.close()
         except Exception:

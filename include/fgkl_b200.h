@@ -32,9 +32,10 @@ extern "C" {
 #define FGKL_E_OUTPUT_LENGTH (-5)               /* Error::OutputLength */
 #define FGKL_E_BAD_OFFSETS (-6)                 /* offset table checks of crates/jni/src/lib.rs:343-363 */
 #define FGKL_E_INVALID_ARGUMENT (-7)            /* NULL pointer or negative size */
-#define FGKL_E_UNSUPPORTED (-8)                 /* a read of more than 620 bases; a PD region whose reads hold more than 31 distinct bytes */
+#define FGKL_E_UNSUPPORTED (-8)                 /* an input outside what an entry point takes (adjoint: a haplotype over 2^24 bases; allocation-free entry: its limits) */
 #define FGKL_E_NO_DEVICE (-9)                   /* no CUDA device, or not an sm_100 part */
 #define FGKL_E_CUDA (-10)                       /* CUDA runtime error (message in fgkl_last_error) */
+#define FGKL_E_OUT_OF_MEMORY (-11)              /* a device or page-locked host allocation failed; the caller may retry smaller */
 
 /* How to compute (crates/pairhmm/src/lib.rs:211-238). */
 typedef struct fgkl_config {
@@ -125,6 +126,14 @@ int fgkl_set_call_combining(int32_t max_batches);
 /* Combined batches of two or more requests run since the library loaded, and the requests they
  * held. */
 int fgkl_call_combining_stats(uint64_t* batches, uint64_t* requests);
+
+/* Failure injection (no counterpart in the reference; its Rust allocator aborts instead). From now on
+ * every device or page-locked host allocation the library asks for that is larger than `bytes`
+ * fails as if the device were out of memory, so a caller's handling of FGKL_E_OUT_OF_MEMORY can be
+ * exercised without exhausting a real device. Buffers the library already holds are not touched,
+ * and a call that fails leaves its engine or context usable for later calls. `bytes` = 0 removes
+ * the limit. Process-wide; returns the previous limit, or FGKL_E_INVALID_ARGUMENT when negative. */
+int64_t fgkl_set_allocation_limit(int64_t bytes);
 
 /* Name of the backend, the analogue of backendNative (crates/jni/src/lib.rs:149-156). */
 const char* fgkl_backend(void);
@@ -230,11 +239,15 @@ int fgkl_batch_launch_profile(fgkl_context* ctx, fgkl_launch_profile* out, int32
  * agrees with 1 - dI - dD to about 1e-6 but is not differentiable, hence this parameterisation.
  * Haplotype bytes compare as bytes, N matching everything (reference.rs:20-64).
  *
- * Computed with FP32 forward and backward values and FP64 accumulation of the gradients; a read
- * whose FP32 likelihood falls below 1e-28 against any haplotype is recomputed in FP64
- * (`fp64_reads` counts them). double_precision = 1 runs everything in FP64. The likelihoods
- * (log10 L per pair, row-major per region as fgkl_batch_fetch) come out too. Reads of at most 620
- * bases. The context's stream is used. */
+ * Computed with FP32 forward and backward values and FP32 products, summed per read position over
+ * 32 columns at a time and accumulated in FP64; a read whose FP32 likelihood falls below 1e-28
+ * against any haplotype is recomputed in FP64 (`fp64_reads` counts them). double_precision = 1 runs
+ * everything in FP64. The likelihoods (log10 L per pair, row-major per region as fgkl_batch_fetch)
+ * come out too. Row checkpointing: the backward values are never stored per cell; the backward
+ * sweep saves its state every few columns and each block of columns is recomputed just before the
+ * forward sweep uses it, so memory grows with the pair's columns / 8, not its cells. Reads of any
+ * length (longer than 620 bases: strip-mined over blocks of 256 rows). The context's stream is
+ * used. */
 typedef struct fgkl_adjoint_batch {
   int32_t num_regions;
   const int32_t* region_reads;
@@ -262,16 +275,6 @@ int fgkl_adjoint_compute(fgkl_context* ctx, const fgkl_adjoint_batch* batch, int
                          double* grad_base_error, int64_t grad_len, uint64_t* fp64_reads);
 int64_t fgkl_adjoint_output_len(const fgkl_context* ctx);
 int64_t fgkl_adjoint_grad_len(const fgkl_context* ctx);
-/* Row checkpointing for long haplotypes. Each warp keeps a pair's backward columns in its scratch
- * while they fit (by default, what an 8 GiB scratch budget gives every resident warp: about 1,700
- * columns at reads of 151). A longer pair saves the backward state every K steps instead and
- * recomputes each block of K columns just before the forward sweep reads it. K is about
- * sqrt(columns), memory O(sqrt) instead of O(columns), and the backward sweep runs twice. Results
- * are bit-identical either way. `columns` > 0 caps the stored columns from the next
- * fgkl_adjoint_prepare (0 restores the default). */
-int fgkl_adjoint_set_stored_columns(fgkl_context* ctx, int32_t columns);
-/* Launches of the prepared adjoint batch whose longest pairs use checkpoints (0 or more). */
-int32_t fgkl_adjoint_checkpointed_launches(const fgkl_context* ctx);
 
 /* ---- allocation-free form (no counterpart in the reference) ----
  *

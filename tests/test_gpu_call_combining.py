@@ -11,7 +11,7 @@ import threading
 import numpy as np
 import pytest
 
-from fgkl_b200 import Config, Precision, Read, _lib, synthetic
+from fgkl_b200 import Config, Precision, Read, _lib, set_allocation_limit, synthetic
 from fgkl_b200.pairhmm import DeviceError, _check, _Flat, _ptr
 
 pytestmark = pytest.mark.gpu
@@ -105,21 +105,30 @@ def test_combined_calls_are_bit_identical_to_calls_alone(gpu, combining):
 
 
 def test_each_caller_gets_its_own_error(gpu, combining):
+    """One request needs more device memory than the injected allocation limit allows (found only
+    once its batch is planned, so it fails the combined batch); the batch is retried as separate
+    calls and that caller alone sees the error."""
     jobs = plain_jobs(31, 6, FLOAT)
-    n = 700  # above the 620-base limit; checked once the batch is planned, so it fails the batch
+    n = 700
     long_read = Read(b"A" * n, bytes([30] * n), bytes([45] * n), bytes([45] * n), bytes([10] * n))
-    bad = lambda: call(FLOAT, [long_read], [b"ACGT" * 50])  # noqa: E731
+    huge_hap = b"ACGT" * 5_000_000  # the strip-mined read's carry row: 320 MB a warp
+    bad = lambda: call(FLOAT, [long_read], [huge_hap])  # noqa: E731
     jobs = jobs[:15] + [bad] + jobs[15:]
-    expected = alone(jobs)
-    for _ in range(3):
-        got, errors = run_threads(8, jobs)
-        for i, (g, e, x) in enumerate(zip(got, errors, expected)):
-            if i == 15:
-                assert isinstance(e, DeviceError) and e.code == _lib.FGKL_E_UNSUPPORTED
-                assert "620" in str(e)
-            else:
-                assert e is None, e
-                assert g.tobytes() == x.tobytes()
+    prev = set_allocation_limit(768 << 20)
+    try:
+        expected = alone(jobs)
+        assert isinstance(expected[15], DeviceError) and expected[15].code == _lib.FGKL_E_OUT_OF_MEMORY
+        for _ in range(3):
+            got, errors = run_threads(8, jobs)
+            for i, (g, e, x) in enumerate(zip(got, errors, expected)):
+                if i == 15:
+                    assert isinstance(e, DeviceError) and e.code == _lib.FGKL_E_OUT_OF_MEMORY
+                    assert "allocation failed" in str(e)
+                else:
+                    assert e is None, e
+                    assert g.tobytes() == x.tobytes()
+    finally:
+        set_allocation_limit(prev)
 
 
 def test_requests_of_different_kinds_are_not_mixed(gpu, combining):

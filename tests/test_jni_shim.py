@@ -5,14 +5,13 @@ On the CPU: the shim turns every input error into an IllegalArgumentException ca
 message, and a missing device into a RuntimeException. On a B200: its likelihoods are the per-call
 C ABI's, written back with one SetDoubleArrayRegion."""
 import ctypes as C
-import re
 import subprocess
 from pathlib import Path
 
 import numpy as np
 import pytest
 
-from fgkl_b200 import Config, PairHmm, PdHaplotype, PdPairHmm, Precision, _lib, synthetic
+from fgkl_b200 import Config, PairHmm, PdHaplotype, PdPairHmm, Precision, _lib, set_allocation_limit, synthetic
 
 ROOT = Path(__file__).resolve().parent.parent
 IAE = "java/lang/IllegalArgumentException"
@@ -67,12 +66,6 @@ def call(L, cols, roff, hb, hf, hoff, double=False, n_out=None):
 
 def region(seed=3):
     return synthetic.reference_region(seed, 6, 50, 3, 90).region(0)
-
-
-def test_the_integration_guide_shows_the_shim_that_is_tested():
-    doc = (ROOT / "INTEGRATION.md").read_text()
-    block = re.search(r"```c\n(/\* fgkl_jni\.c:.*?)```", doc, re.S).group(1)
-    assert block == (ROOT / "fgkl_b200" / "jni" / "fgkl_jni.c").read_text()
 
 
 def test_backend_native_names_the_backend(shim):
@@ -143,13 +136,27 @@ def test_gpu_pd_shim_likelihoods_are_the_per_call_abi_bits(gpu, shim):
 
 
 @pytest.mark.gpu
-def test_gpu_a_read_longer_than_supported_raises_illegal_argument(gpu, shim):
-    # The length limit is checked once a device is found, so this case needs one.
-    _, haps = region()
-    n = 700
-    cols = [np.full(n, v, np.int8) for v in (65, 30, 45, 45, 10)]
-    _, _, hb, _, hoff = flat(region()[0], haps)
-    exc, _, region_calls = call(shim, cols, np.array([0, n], np.int32), hb, None, hoff)
-    assert exc is not None and exc[0] == IAE and exc[1] == _lib.last_error()
-    assert "620" in exc[1]
+def test_gpu_a_long_read_gets_the_per_call_abi_bits(gpu, shim):
+    reads, haps = synthetic.reference_region(8, 2, 700, 3, 820).region(0)
+    exc, out, region_calls = call(shim, *flat(reads, haps))
+    assert exc is None, exc
+    assert region_calls == 1
+    assert out.tobytes() == PairHmm(Config(precision=Precision.FLOAT)).compute_log10_likelihoods(reads, haps).tobytes()
+
+
+@pytest.mark.gpu
+def test_gpu_a_failed_allocation_raises_runtime_exception(gpu, shim):
+    """fgkl's panic path throws RuntimeException (crates/jni/src/lib.rs:39-74); an allocation the
+    injected limit refuses takes the same path."""
+    reads, haps = region()
+    prev = set_allocation_limit(1024)
+    try:
+        exc, _, region_calls = call(shim, *flat(reads, haps))
+    finally:
+        set_allocation_limit(prev)
+    assert exc is not None and exc[0] == RTE and exc[1] == _lib.last_error()
+    assert "allocation failed" in exc[1]
     assert region_calls == 0
+    exc, out, _ = call(shim, *flat(reads, haps))
+    assert exc is None, exc
+    assert out.tobytes() == PairHmm(Config(precision=Precision.FLOAT)).compute_log10_likelihoods(reads, haps).tobytes()

@@ -13,6 +13,7 @@ import numpy as np
 import pytest
 
 from fgkl_b200 import Config, PairHmm, Precision, Read, _lib, synthetic
+from oracle import oracle as O
 from refgen import Rng
 
 pytestmark = pytest.mark.gpu
@@ -106,6 +107,22 @@ def test_matches_the_regular_entry_on_two_calls_in_a_row(gpu, shape):
     second = call(reg, out)
     assert_close(first, expected)
     assert_close(second, expected)
+    assert_close(first, O.compute_matrix(reads, haps))
+
+
+def test_calls_take_no_device_memory(gpu):
+    """After the first call on the device, a larger region leaves the device's free memory as it was."""
+    import torch
+
+    small = uneven_region(11, 8, 3, 300, 40, 150)
+    large = uneven_region(12, 60, 8, 600, 100, 500)
+    reg_s, keep_s, out_s = device_region(*small)
+    reg_l, keep_l, out_l = device_region(*large)
+    call(reg_s, out_s)
+    free_before = torch.cuda.mem_get_info()[0]
+    got = call(reg_l, out_l)
+    assert torch.cuda.mem_get_info()[0] == free_before
+    assert_close(got, regular(*large))
 
 
 def test_a_bound_above_the_reads_gives_the_same_results(gpu):
