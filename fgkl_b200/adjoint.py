@@ -8,6 +8,7 @@ with MM = 1 - dI - dD.
 from __future__ import annotations
 
 import ctypes as C
+import sys
 from dataclasses import dataclass
 
 import numpy as np
@@ -70,15 +71,6 @@ class AdjointContext:
         self._keep = (workload, arrays, b)
         _check(lib().fgkl_adjoint_prepare(self._ctx, C.byref(b), int(double_precision)))
 
-    def set_stored_columns(self, columns: int) -> None:
-        """Caps the backward columns a warp stores per pair; longer pairs recompute them from
-        checkpoints (row checkpointing). 0 restores the default (the scratch budget's share)."""
-        _check(lib().fgkl_adjoint_set_stored_columns(self._ctx, int(columns)))
-
-    def checkpointed_launches(self) -> int:
-        """Launches of the prepared batch whose longest pairs use checkpoints."""
-        return int(lib().fgkl_adjoint_checkpointed_launches(self._ctx))
-
     def run(self) -> int:
         n = C.c_uint64()
         _check(lib().fgkl_adjoint_run(self._ctx, C.byref(n)))
@@ -105,6 +97,10 @@ class AdjointContext:
             self._ctx = None
 
     def __del__(self):
+        # At interpreter shutdown the context is left to the process's exit: destroying it then
+        # would run CUDA calls while the runtimes in the process are being torn down.
+        if sys.is_finalizing():
+            return
         try:
             self.close()
         except Exception:

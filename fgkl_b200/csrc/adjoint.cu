@@ -4,20 +4,36 @@
 // One warp per read: for each haplotype of the read's region, in caller order,
 //   1. a backward sweep (the reverse wavefront of the suffix-sharing backward pass, right to left
 //      over the haplotype) computes B = d(raw)/d(cell state) for M, X and Y, scaled by 2^120 in FP32
-//      at the read's last row, and stores each column's values in the warp's scratch; the padding row
-//      above the read collects the start mass, so raw = (INITIAL / hap_len) * s / scale is known
-//      before any forward value;
-//   2. a forward sweep recomputes F (the plain recurrence) and, at every cell, combines the forward
-//      values already in registers -- the diagonal, the cell above and the cell to the left -- with
-//      the stored B of the cell into the expected-count terms of the gradient:
+//      at the read's last row. It keeps nothing per cell: it saves its state every K steps, and the
+//      padding row above the read collects the start mass, so raw = (INITIAL / hap_len) * s / scale
+//      is known before any forward value;
+//   2. a forward sweep recomputes F (the plain recurrence) in blocks of K steps. Because the two
+//      wavefronts are skewed oppositely, forward step t of every lane reads the backward values of
+//      backward step n - 1 - t, so before forward block [bK, bK + K) the K backward steps it needs
+//      are recomputed from the saved state into shared memory. Each cell then combines the forward
+//      values in registers -- the diagonal, the cell above and the cell to the left -- with its
+//      backward values into the expected-count terms of the gradient:
 //        d raw/d dI  += -F_M(diag) p B_M + F_M(up) B_X
 //        d raw/d dD  += -F_M(diag) p B_M + F_M(left) B_Y
 //        d raw/d eps += -(F_X + F_Y)(diag) p B_M + F_X(up) B_X + F_Y(left) B_Y
 //        d raw/d e   += dp/de (F_M(diag) MM + (F_X + F_Y)(diag) IM) B_M,  dp/de = -1 or 1/3
-//      each scaled by 1 / (raw ln 10) and accumulated in FP64 per read row.
-// The F x B products are formed in FP64 (their FP32 factors can each be near the FP32 range limits).
-// A read whose FP32 raw falls below 1e-28 or is not finite for any haplotype is recomputed whole by
-// the FP64 instantiation (INITIAL 2^1020, no backward scale), which cannot lose it.
+//      each divided by raw ln 10.
+// The products are FP32. The recurrences are linear in their starting values, so F is computed from
+// INITIAL * 2^-a / hap_len and the recomputed B from a sink times c = 2^a / (raw * scale * ln 10):
+// each product F * B is then the normalised term itself, and a = the mean of log2 raw and log2 of
+// the row-0 constant centres the range of F near 1, which keeps both factors of every term that
+// matters inside the FP32 range (F runs from the row-0 constant down to about raw, B * c the other
+// way). Each lane sums its rows' terms over the forward steps in FP32 and adds the sums into the
+// FP64 per-position gradients every 32 steps (atomic adds; a lane alone owns its rows, so the order
+// is fixed). A read whose FP32 raw falls below 1e-28 or is not finite for any haplotype is
+// recomputed whole by the FP64 instantiation (INITIAL 2^1020, no backward scale, a = 0), which
+// cannot lose it.
+//
+// Reads longer than 620 bases are strip-mined over row blocks of 32 R rows (R = 8), padding at the
+// top of the first. The backward sweeps run the blocks bottom to top; lane 31's row below comes
+// from the top row the block below stored column by column (its BM and BX). The forward sweeps run
+// them top to bottom; lane 0's row above comes from the bottom row the block above stored, or GATK's
+// row 0 in the first block.
 //
 // Haplotype bases are compared as bytes: prior code = the byte with 'N' and byte 4 swapped, so N is
 // code kCodeN (matches every read base); a read N matches everything through its mismatch prior.
@@ -32,22 +48,44 @@ namespace {
 
 __device__ __forceinline__ uint32_t adj_code(uint32_t b) { return b == 'N' ? kCodeN : (b == kCodeN ? 'N' : b); }
 
+// Sizes of one instantiation: a lane's record of one backward step (BM, BX, BY rows) and its saved
+// backward state (BM, BY rows, the diagonal BM and the two values shuffled from the lane below), in
+// 16-byte chunks; the backward steps recomputed per block, as many as about 28 KB of shared memory
+// per warp holds (at most 8).
 template <class P, int R>
-struct AdjRows {
+struct AdjSizes {
+  using V = typename P::V;
+  static constexpr int kPer16 = 16 / static_cast<int>(sizeof(V));
+  static constexpr int kRecChunks = (3 * R + kPer16 - 1) / kPer16;
+  static constexpr int kRecVals = kRecChunks * kPer16;
+  static constexpr int kStateVals = 2 * R + 3;
+  static constexpr int kStateChunks = (kStateVals + kPer16 - 1) / kPer16;
+  static constexpr int kStepBytes = kRecChunks * 32 * 16;
+  static constexpr int kRawK = 28672 / kStepBytes;
+  static constexpr int K = kRawK < 1 ? 1 : (kRawK > 8 ? 8 : kRawK);
+  static constexpr size_t kSmemPerWarp = static_cast<size_t>(K) * kStepBytes;
+};
+
+constexpr int kFlushSteps = 32;  // forward steps between FP64 additions of the FP32 sums
+
+// The lane's rows: their own forward transitions and priors, and the row below each (backward).
+// Read row q = lane * R + r - pad, pad relative to the row block (negative below the first).
+template <class P, int R>
+struct AdjCoef {
   using V = typename P::V;
   using S = typename P::S;
-  // Own row: forward transitions and priors.
   V mm[R], im[R], mi[R], ii[R], md[R], dd[R], pm[R], px[R];
-  int oc[R];
-  bool readN[R];
-  bool real[R];
+  V bmm[R], bim[R], bmi[R], bii[R], bpm[R], bpx[R];
+  int oc[R], boc[R];
+  uint32_t nmask;  // bit r: the row's read base is N
+  uint32_t real;   // bit r: a read row
 
   __device__ void load(const AdjView& v, int64_t off, int len, int pad, int lane) {
+    nmask = real = 0u;
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       const int q = lane * R + r - pad;
-      real[r] = q >= 0 && q < len;
-      if (real[r]) {
+      if (q >= 0 && q < len) {
         const int64_t o = off + q;
         const double di = v.d_ins[o], dl = v.d_del[o], ep = v.eps[o], e = v.err[o];
         const uint8_t b = v.bases[o];
@@ -60,84 +98,54 @@ struct AdjRows {
         pm[r] = static_cast<S>(1.0 - e);
         px[r] = b == 'N' ? pm[r] : static_cast<S>(e / 3.0);
         oc[r] = static_cast<int>(adj_code(b));
-        readN[r] = b == 'N';
+        real |= 1u << r;
+        if (b == 'N') nmask |= 1u << r;
       } else {
         // Padding rows keep M = X = 0 and Y = INITIAL / hap_len: GATK's row 0.
         mm[r] = im[r] = mi[r] = ii[r] = md[r] = pm[r] = px[r] = P::zero();
         dd[r] = static_cast<S>(1.0);
         oc[r] = -1;
-        readN[r] = false;
       }
-    }
-  }
-  __device__ V prior(uint32_t code, int r) const { return (static_cast<int>(code) == oc[r] || code == kCodeN) ? pm[r] : px[r]; }
-  __device__ bool match(uint32_t code, int r) const { return static_cast<int>(code) == oc[r] || code == kCodeN || readN[r]; }
-};
-
-// The row below each lane row, for the backward recurrence.
-template <class P, int R>
-struct AdjBelow {
-  using V = typename P::V;
-  using S = typename P::S;
-  V mm[R], im[R], mi[R], ii[R], pm[R], px[R];
-  int oc[R];
-
-  __device__ void load(const AdjView& v, int64_t off, int len, int pad, int lane) {
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const int q = lane * R + r + 1 - pad;
-      if (q >= 0 && q < len) {
-        const int64_t o = off + q;
+      const int qb = q + 1;
+      if (qb >= 0 && qb < len) {
+        const int64_t o = off + qb;
         const double di = v.d_ins[o], dl = v.d_del[o], ep = v.eps[o], e = v.err[o];
         const uint8_t b = v.bases[o];
-        mm[r] = static_cast<S>(1.0 - di - dl);
-        im[r] = static_cast<S>(1.0 - ep);
-        mi[r] = static_cast<S>(di);
-        ii[r] = static_cast<S>(ep);
-        pm[r] = static_cast<S>(1.0 - e);
-        px[r] = b == 'N' ? pm[r] : static_cast<S>(e / 3.0);
-        oc[r] = static_cast<int>(adj_code(b));
+        bmm[r] = static_cast<S>(1.0 - di - dl);
+        bim[r] = static_cast<S>(1.0 - ep);
+        bmi[r] = static_cast<S>(di);
+        bii[r] = static_cast<S>(ep);
+        bpm[r] = static_cast<S>(1.0 - e);
+        bpx[r] = b == 'N' ? bpm[r] : static_cast<S>(e / 3.0);
+        boc[r] = static_cast<int>(adj_code(b));
       } else {
-        mm[r] = im[r] = mi[r] = ii[r] = pm[r] = px[r] = P::zero();
-        oc[r] = -1;
+        bmm[r] = bim[r] = bmi[r] = bii[r] = bpm[r] = bpx[r] = P::zero();
+        boc[r] = -1;
       }
     }
   }
-  __device__ V prior(uint32_t code, int r) const { return (static_cast<int>(code) == oc[r] || code == kCodeN) ? pm[r] : px[r]; }
-};
-
-// Column j's backward values of one lane: a record of BM, BX, BY rows padded to 16 bytes,
-// [column][lane][record], so a lane stores and fetches its record with 16-byte moves.
-template <class P, int R>
-struct AdjCol {
-  using V = typename P::V;
-  static constexpr int kPer16 = 16 / static_cast<int>(sizeof(V));
-  static constexpr int kRec = (3 * R + kPer16 - 1) / kPer16 * kPer16;
-  // Columns fetched ahead of the forward sweep into a per-warp shared-memory ring (about 16 KB).
-  static constexpr int kDepthRaw = 16384 / (32 * kRec * static_cast<int>(sizeof(V)));
-  static constexpr int kDepth = kDepthRaw < 2 ? 2 : (kDepthRaw > 8 ? 8 : kDepthRaw);
-  static constexpr size_t kRingBytes = static_cast<size_t>(kDepth) * 32 * kRec * sizeof(V);
-  __device__ static V* at(char* scratch, int j, int lane) {
-    return reinterpret_cast<V*>(scratch) + (static_cast<size_t>(j) * 32 + lane) * kRec;
+  __device__ bool matches(uint32_t code, int r) const { return static_cast<int>(code) == oc[r] || code == kCodeN; }
+  __device__ V bprior(uint32_t code, int r) const {
+    return (static_cast<int>(code) == boc[r] || code == kCodeN) ? bpm[r] : bpx[r];
   }
 };
 
-// The backward sweep's state between two steps: BM and BY rows and the values the next step
-// shuffles from the lane below, padded to 16 bytes so a lane saves and restores it with 16-byte moves.
+// The backward sweep's state between two steps.
 template <class P, int R>
-struct AdjBwdState {
+struct AdjBwd {
   using V = typename P::V;
-  static constexpr int kPer16 = 16 / static_cast<int>(sizeof(V));
-  static constexpr int kRec = (2 * R + 3 + kPer16 - 1) / kPer16 * kPer16;
+  using Z = AdjSizes<P, R>;
   V BM[R], BY[R];
   V dBM, topBM, topBX;
+
   __device__ __forceinline__ void zero() {
 #pragma unroll
     for (int r = 0; r < R; ++r) BM[r] = BY[r] = P::zero();
     dBM = topBM = topBX = P::zero();
   }
-  __device__ __forceinline__ void save(V* dst) const {
-    V rec[kRec];
+  // Saved as [chunk][lane] 16-byte chunks, so each chunk of the warp is 512 contiguous bytes.
+  __device__ __forceinline__ void save(V* dst, int lane) const {
+    V rec[Z::kStateChunks * Z::kPer16];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       rec[r] = BM[r];
@@ -147,45 +155,42 @@ struct AdjBwdState {
     rec[2 * R + 1] = topBM;
     rec[2 * R + 2] = topBX;
 #pragma unroll
-    for (int i = 2 * R + 3; i < kRec; ++i) rec[i] = P::zero();
-    store_record(dst, rec);
+    for (int i = 2 * R + 3; i < Z::kStateChunks * Z::kPer16; ++i) rec[i] = P::zero();
+#pragma unroll
+    for (int c = 0; c < Z::kStateChunks; ++c)
+      reinterpret_cast<uint4*>(dst)[c * 32 + lane] = reinterpret_cast<const uint4*>(rec)[c];
   }
-  __device__ __forceinline__ void restore(const V* src) {
-    V rec[kRec];
-    load_record(rec, src);
+  // Restores a saved state multiplied by `scale`.
+  __device__ __forceinline__ void restore(const V* src, int lane, V scale) {
+    V rec[Z::kStateChunks * Z::kPer16];
+#pragma unroll
+    for (int c = 0; c < Z::kStateChunks; ++c)
+      reinterpret_cast<uint4*>(rec)[c] = reinterpret_cast<const uint4*>(src)[c * 32 + lane];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      BM[r] = rec[r];
-      BY[r] = rec[R + r];
+      BM[r] = P::mul(rec[r], scale);
+      BY[r] = P::mul(rec[R + r], scale);
     }
-    dBM = rec[2 * R];
-    topBM = rec[2 * R + 1];
-    topBX = rec[2 * R + 2];
+    dBM = P::mul(rec[2 * R], scale);
+    topBM = P::mul(rec[2 * R + 1], scale);
+    topBX = P::mul(rec[2 * R + 2], scale);
   }
 };
 
-// Scratch of a pair whose backward columns do not all fit: a block buffer of K backward steps'
-// records, then one saved state per block, [block][lane][AdjBwdState::kRec].
-template <class P, int R>
-struct AdjCkpt {
+// One backward step at lane position p (column m - p). `sink` is the scale added at the read's last
+// row (lane 31 of the last row block). With `below` (lane 31 of a row block above another), the row
+// below comes from that block's stored top row: cBX its BX at this column, cBM its BM, the next
+// step's diagonal. kRec: keep the column's BM, BX, BY rows in `rec`.
+template <class P, int R, bool kRec>
+__device__ __forceinline__ void adj_bwd_step(AdjBwd<P, R>& s, const AdjCoef<P, R>& c, typename P::V sink, uint32_t code, int p,
+                                             bool below, typename P::V cBM, typename P::V cBX,
+                                             typename P::V (&rec)[AdjSizes<P, R>::kRecVals]) {
   using V = typename P::V;
-  __device__ static V* block(char* scratch, int i, int lane) {
-    return reinterpret_cast<V*>(scratch) + (static_cast<size_t>(i) * 32 + lane) * AdjCol<P, R>::kRec;
+  V rBM = P::down(s.topBM), rBX = P::down(s.topBX);
+  if (below) {
+    rBM = cBM;
+    rBX = cBX;
   }
-  __device__ static V* state(char* scratch, int K, int b, int lane) {
-    return reinterpret_cast<V*>(scratch) + static_cast<size_t>(K) * 32 * AdjCol<P, R>::kRec +
-           (static_cast<size_t>(b) * 32 + lane) * AdjBwdState<P, R>::kRec;
-  }
-};
-
-// One step of the backward sweep at lane position p (column m - p): the lane's record of the column
-// (BM, BX, BY rows) in `rec`. `md` and `dd` are the lane rows' own deletion transitions.
-template <class P, int R>
-__device__ __forceinline__ void adj_bwd_step(AdjBwdState<P, R>& s, const AdjBelow<P, R>& bl, const typename P::V (&md)[R],
-                                             const typename P::V (&dd)[R], typename P::V sink, uint32_t code, int p,
-                                             typename P::V (&rec)[AdjCol<P, R>::kRec]) {
-  using V = typename P::V;
-  const V rBM = P::down(s.topBM), rBX = P::down(s.topBX);
   if (p == 0) {
     // The all-zero column beyond the haplotype.
 #pragma unroll
@@ -195,11 +200,11 @@ __device__ __forceinline__ void adj_bwd_step(AdjBwdState<P, R>& s, const AdjBelo
   V belowX = rBX, diagM = s.dBM;
 #pragma unroll
   for (int r = R - 1; r >= 0; --r) {
-    const V into = P::mul(bl.prior(code, r), diagM);
-    const V itm = P::mul(into, bl.im[r]);
-    V bx = P::fma(belowX, bl.ii[r], itm);
-    const V by = P::fma(s.BY[r], dd[r], itm);
-    V bm = P::fma(s.BY[r], md[r], P::fma(belowX, bl.mi[r], P::mul(into, bl.mm[r])));
+    const V into = P::mul(c.bprior(code, r), diagM);
+    const V itm = P::mul(into, c.bim[r]);
+    V bx = P::fma(belowX, c.bii[r], itm);
+    const V by = P::fma(s.BY[r], c.dd[r], itm);
+    V bm = P::fma(s.BY[r], c.md[r], P::fma(belowX, c.bmi[r], P::mul(into, c.bmm[r])));
     if (r == R - 1) {
       bm = P::add(bm, sink);
       bx = P::add(bx, sink);
@@ -208,12 +213,12 @@ __device__ __forceinline__ void adj_bwd_step(AdjBwdState<P, R>& s, const AdjBelo
     s.BM[r] = bm;
     s.BY[r] = by;
     belowX = bx;
-    rec[r] = bm;
-    rec[R + r] = bx;
-    rec[2 * R + r] = by;
+    if (kRec) {
+      rec[r] = bm;
+      rec[R + r] = bx;
+      rec[2 * R + r] = by;
+    }
   }
-#pragma unroll
-  for (int i = 3 * R; i < AdjCol<P, R>::kRec; ++i) rec[i] = P::zero();
   s.topBM = s.BM[0];
   s.topBX = belowX;
   s.dBM = rBM;
@@ -226,36 +231,87 @@ __device__ __forceinline__ uint32_t adj_bwd_code(const uint8_t* hap, int m, int 
   return (p >= 0 && jj >= 0 && jj < m) ? adj_code(__ldg(hap + jj)) : 0u;
 }
 
-// Backward sweep of one pair over steps 0 .. m + 31; returns, in every lane, the padding row's start
-// mass s. Without checkpoints (K == 0) it stores every column's record for the forward sweep. With
-// checkpoints it stores none and saves, instead, the state entering each block of K steps that the
-// forward sweep recomputes (adj_backward_block), block b of forward steps [bK, bK + K) reading
-// backward steps [n - (b + 1)K, n - 1 - bK], n = m + 31.
-template <class P, int R, bool kCk>
-__device__ typename P::V adj_backward(const AdjView& v, const AdjRows<P, R>& own, int64_t off, int len, int pad,
-                                      const uint8_t* hap, int m, int lane, char* scratch, int K) {
+// A pair's per-warp scratch: checkpoints [row block][state][chunk][lane], then the top rows of row
+// blocks 1.. [block - 1][column 0..m] (BM, BX), then one bottom row [column] (M, X, Y, 0).
+template <class P, int R>
+struct AdjScratch {
+  using V = typename P::V;
+  using Z = AdjSizes<P, R>;
+  static constexpr size_t kStateBytes = static_cast<size_t>(Z::kStateChunks) * 32 * 16;
+  char* base;
+  int n_states;  // per row block
+  int m;
+  int blocks;
+
+  __host__ __device__ static size_t align(size_t x) { return (x + 255) / 256 * 256; }
+  __host__ __device__ static size_t states_bytes(int blocks, int n_states) {
+    return align(static_cast<size_t>(blocks) * n_states * kStateBytes);
+  }
+  __host__ __device__ static size_t up_bytes(int blocks, int m) {
+    return align(static_cast<size_t>(blocks > 1 ? blocks - 1 : 0) * (m + 1) * 2 * sizeof(V));
+  }
+  __host__ __device__ static size_t down_bytes(int blocks, int m) { return blocks > 1 ? align(static_cast<size_t>(m) * 4 * sizeof(V)) : 0; }
+  __host__ __device__ static size_t bytes(int read_len, int hap_len) {
+    const int blocks = adj_row_blocks(read_len, R);
+    const int n = hap_len + 31;
+    const int n_states = (n + Z::K - 1) / Z::K;
+    return states_bytes(blocks, n_states) + up_bytes(blocks, hap_len) + down_bytes(blocks, hap_len);
+  }
+  __device__ V* state(int block, int i) const {
+    return reinterpret_cast<V*>(base + (static_cast<size_t>(block) * n_states + i) * kStateBytes);
+  }
+  __device__ V* up(int block, int column) const {  // block >= 1
+    return reinterpret_cast<V*>(base + states_bytes(blocks, n_states)) + (static_cast<size_t>(block - 1) * (m + 1) + column) * 2;
+  }
+  __device__ V* down(int p) const {
+    return reinterpret_cast<V*>(base + states_bytes(blocks, n_states) + up_bytes(blocks, m)) + static_cast<size_t>(p) * 4;
+  }
+};
+
+// Backward sweep of row block `blk` over steps 0 .. m + 31, saving the state entering every K-th
+// step before the end (the state entering backward step n - (i + 1) K as checkpoint i, n = m + 31)
+// and, for a block below another, its top row (lane 0) at every column. Returns, in every lane, the
+// start mass s of the padding row above the read (first row block only).
+template <class P, int R>
+__device__ typename P::V adj_backward(const AdjCoef<P, R>& c, const uint8_t* hap, int m, int lane, const AdjScratch<P, R>& sc,
+                                      int blk, int pad) {
   using V = typename P::V;
   using S = typename P::S;
-  AdjBelow<P, R> bl;
-  bl.load(v, off, len, pad, lane);
-  const V sink = lane == 31 ? static_cast<S>(Consts<P::kDouble>::kBackwardScale) : P::zero();
-  AdjBwdState<P, R> st;
+  using Z = AdjSizes<P, R>;
+  const bool last = blk == sc.blocks - 1;
+  const V sink = (lane == 31 && last) ? static_cast<S>(Consts<P::kDouble>::kBackwardScale) : P::zero();
+  const bool below = lane == 31 && !last;
+  AdjBwd<P, R> st;
   st.zero();
-  const int pad_row = pad - 1;  // the padding row right above the read
-  const int pad_lane = pad_row / R, pad_r = pad_row % R;
+  const int pad_row = pad - 1;  // the padding row right above the read (first block)
+  const int pad_lane = pad_row >= 0 ? pad_row / R : 0, pad_r = pad_row >= 0 ? pad_row % R : 0;
   const int n = m + 31;
   V start_mass = P::zero();
   uint32_t next_code = adj_bwd_code(hap, m, -(31 - lane));
-  for (int t = 0; t < m + 1 + 31; ++t) {
-    if (kCk && K > 0 && t > 0 && t < n && (n - t) % K == 0) st.save(AdjCkpt<P, R>::state(scratch, K, (n - t) / K - 1, lane));
-    const int p = t - (31 - lane);  // position: column m - p
-    const int j = m - p;
+  V cBM = P::zero(), cBX = P::zero();
+  V rec[Z::kRecVals];
+  for (int t = 0; t < m + 32; ++t) {
+    if (t > 0 && t < n && (n - t) % Z::K == 0) st.save(sc.state(blk, (n - t) / Z::K - 1), lane);
+    const int p = t - (31 - lane);
     const uint32_t code = next_code;
     next_code = adj_bwd_code(hap, m, p + 1);
-    V rec[AdjCol<P, R>::kRec];
-    adj_bwd_step<P, R>(st, bl, own.md, own.dd, sink, code, p, rec);
-    if ((!kCk || K == 0) && p >= 0 && j >= 1) store_record(AdjCol<P, R>::at(scratch, j, lane), rec);
-    if (p == m && lane == pad_lane) {
+    if (below) {
+      // Lane 31 is at position t: column m - t of the block below's top row.
+      if (t <= m) {
+        const V* u = sc.up(blk + 1, m - t);
+        cBM = u[0];
+        cBX = u[1];
+      } else {
+        cBM = cBX = P::zero();
+      }
+    }
+    adj_bwd_step<P, R, false>(st, c, sink, code, p, below, cBM, cBX, rec);
+    if (blk > 0 && lane == 0 && p >= 0 && p <= m) {
+      V* u = sc.up(blk, m - p);
+      u[0] = st.topBM;
+      u[1] = st.topBX;
+    }
+    if (blk == 0 && p == m && lane == pad_lane) {
 #pragma unroll
       for (int r = 0; r < R; ++r)
         if (r == pad_r) start_mass = st.BY[r];
@@ -264,253 +320,202 @@ __device__ typename P::V adj_backward(const AdjView& v, const AdjRows<P, R>& own
   return __shfl_sync(kFull, start_mass, pad_lane);
 }
 
-// Recomputes backward steps [t_lo, t_hi] of one pair from the state saved at t_lo (or the initial
-// state when t_lo == 0) into the block buffer, record of step t at index t - t_lo. The arithmetic is
-// the full sweep's, step for step, so the records are bit-identical to the stored ones. Not inlined:
-// the forward sweep's registers are saved around the call, once per block.
-template <class P, int R>
-__device__ __noinline__ void adj_backward_block(const uint8_t* bases, const double* d_ins, const double* d_del,
-                                                const double* eps, const double* err, int64_t off, int len, int pad,
-                                                const uint8_t* hap, int m, int lane, char* scratch, int K, int b, int t_lo,
-                                                int t_hi) {
-  using V = typename P::V;
-  using S = typename P::S;
-  AdjView pv{};
-  pv.bases = bases;
-  pv.d_ins = d_ins;
-  pv.d_del = d_del;
-  pv.eps = eps;
-  pv.err = err;
-  const AdjView* v = &pv;
-  AdjBelow<P, R> bl;
-  bl.load(*v, off, len, pad, lane);
-  // The lane rows' own deletion transitions, as AdjRows holds them.
-  V md[R], dd[R];
-#pragma unroll
-  for (int r = 0; r < R; ++r) {
-    const int q = lane * R + r - pad;
-    if (q >= 0 && q < len) {
-      md[r] = static_cast<S>(v->d_del[off + q]);
-      dd[r] = static_cast<S>(v->eps[off + q]);
-    } else {
-      md[r] = P::zero();
-      dd[r] = static_cast<S>(1.0);
-    }
-  }
-  const V sink = lane == 31 ? static_cast<S>(Consts<P::kDouble>::kBackwardScale) : P::zero();
-  AdjBwdState<P, R> st;
-  if (t_lo > 0)
-    st.restore(AdjCkpt<P, R>::state(scratch, K, b, lane));
-  else
-    st.zero();
-  uint32_t next_code = adj_bwd_code(hap, m, t_lo - (31 - lane));
-  for (int t = t_lo; t <= t_hi; ++t) {
-    const int p = t - (31 - lane);
-    const uint32_t code = next_code;
-    next_code = adj_bwd_code(hap, m, p + 1);
-    V rec[AdjCol<P, R>::kRec];
-    adj_bwd_step<P, R>(st, bl, md, dd, sink, code, p, rec);
-    store_record(AdjCkpt<P, R>::block(scratch, t - t_lo, lane), rec);
-  }
-}
-
 // The forward sweep's registers: M, X, Y rows, the row above the lane's top row on the diagonal,
 // and the accumulated result.
 template <class P, int R>
-struct AdjFwdState {
+struct AdjFwd {
   using V = typename P::V;
   V M[R], X[R], Y[R];
   V dM, dX, dY, acc;
 };
 
-// One forward step's arithmetic: the column's forward values from the diagonal (d*), the row above
-// (u*) and the lane's own registers, and, for a live step, the gradient terms against the column's
-// backward record (bM, bX, bY).
-template <class P, int R>
-__device__ __forceinline__ void adj_fwd_math(AdjFwdState<P, R>& f, const AdjRows<P, R>& own, uint32_t code, bool live,
-                                             const typename P::V (&bM)[R], const typename P::V (&bX)[R],
-                                             const typename P::V (&bY)[R], typename P::V uM, typename P::V uX, double norm,
-                                             double (&gi)[R], double (&gd)[R], double (&ge)[R], double (&gq)[R]) {
+// One forward step: the column's forward values from the diagonal (d*), the row above (uM, uX) and
+// the lane's registers, and the gradient terms against the column's backward values (rec: BM, BX,
+// BY rows, already multiplied by c). kMask: steps where some lane lies outside the haplotype, whose
+// terms are dropped.
+template <class P, int R, bool kMask>
+__device__ __forceinline__ void adj_fwd_step(AdjFwd<P, R>& f, const AdjCoef<P, R>& c, uint32_t code, bool live,
+                                             const typename P::V (&rec)[AdjSizes<P, R>::kRecVals], typename P::V uM,
+                                             typename P::V uX, typename P::V (&gi)[R], typename P::V (&gd)[R],
+                                             typename P::V (&ge)[R], typename P::V (&gq)[R]) {
   using V = typename P::V;
+  using S = typename P::S;
+  const V third = static_cast<S>(1.0 / 3.0), minus_one = static_cast<S>(-1.0);
   // Match and deletion values from the bottom row up (each row reads the old row above).
 #pragma unroll
   for (int r = R - 1; r >= 0; --r) {
     const V pM = r ? f.M[r - 1] : f.dM, pX = r ? f.X[r - 1] : f.dX, pY = r ? f.Y[r - 1] : f.dY;
     const V mOld = f.M[r], yOld = f.Y[r];
-    const V prior = own.prior(code, r);
+    const bool match = c.matches(code, r);
+    const V prior = match ? c.pm[r] : c.px[r];
     const V sxy = P::add(pX, pY);
-    const V s = P::fma(pM, own.mm[r], P::mul(sxy, own.im[r]));
-    f.Y[r] = P::fma(yOld, own.dd[r], P::mul(mOld, own.md[r]));
+    const V s = P::fma(pM, c.mm[r], P::mul(sxy, c.im[r]));
+    f.Y[r] = P::fma(yOld, c.dd[r], P::mul(mOld, c.md[r]));
     f.M[r] = P::mul(prior, s);
-    if (live && own.real[r]) {
-      const double bm_n = static_cast<double>(bM[r]) * norm, by_n = static_cast<double>(bY[r]) * norm;
-      const double bm_p = bm_n * static_cast<double>(prior);
-      const double t1 = static_cast<double>(pM) * bm_p;
-      gi[r] -= t1;
-      gd[r] += static_cast<double>(mOld) * by_n - t1;
-      ge[r] += static_cast<double>(yOld) * by_n - static_cast<double>(sxy) * bm_p;
-      gq[r] += (own.match(code, r) ? -1.0 : 1.0 / 3.0) * static_cast<double>(s) * bm_n;
-    }
+    V bm = rec[r], by = rec[2 * R + r];
+    if (kMask && !live) bm = by = P::zero();
+    const V bmp = P::mul(bm, prior);
+    gi[r] = P::fma(-pM, bmp, gi[r]);
+    gd[r] = P::fma(-pM, bmp, P::fma(mOld, by, gd[r]));
+    ge[r] = P::fma(-sxy, bmp, P::fma(yOld, by, ge[r]));
+    const V kq = (match || ((c.nmask >> r) & 1u)) ? minus_one : third;
+    gq[r] = P::fma(s, P::mul(bm, kq), gq[r]);
   }
   // Insertion values from the top row down (each row reads the new row above).
 #pragma unroll
   for (int r = 0; r < R; ++r) {
     const V qM = r ? f.M[r - 1] : uM, qX = r ? f.X[r - 1] : uX;
-    f.X[r] = P::fma(qX, own.ii[r], P::mul(qM, own.mi[r]));
-    if (live && own.real[r]) {
-      const double bx_n = static_cast<double>(bX[r]) * norm;
-      gi[r] += static_cast<double>(qM) * bx_n;
-      ge[r] += static_cast<double>(qX) * bx_n;
-    }
+    f.X[r] = P::fma(qX, c.ii[r], P::mul(qM, c.mi[r]));
+    V bx = rec[R + r];
+    if (kMask && !live) bx = P::zero();
+    gi[r] = P::fma(qM, bx, gi[r]);
+    ge[r] = P::fma(qX, bx, ge[r]);
   }
   if (live) f.acc = P::add(f.acc, P::add(f.M[R - 1], f.X[R - 1]));
 }
 
-// Column 0 of the forward sweep: the row-0 constant in the padding rows (and in the row above the
-// lane's top row when that is padding).
+// Adds the lane's FP32 (FP64) sums into the per-position gradients and clears them.
 template <class P, int R>
-__device__ __forceinline__ void adj_fwd_column0(AdjFwdState<P, R>& f, int pad, int lane, typename P::S init) {
+__device__ __forceinline__ void adj_flush(const AdjView& v, const AdjCoef<P, R>& c, int64_t off, int pad, int lane,
+                                          typename P::V (&gi)[R], typename P::V (&gd)[R], typename P::V (&ge)[R],
+                                          typename P::V (&gq)[R]) {
 #pragma unroll
   for (int r = 0; r < R; ++r) {
-    f.M[r] = f.X[r] = P::zero();
-    f.Y[r] = lane * R + r < pad ? init : P::zero();
+    if ((c.real >> r) & 1u) {
+      const int64_t o = off + lane * R + r - pad;
+      atomicAdd(v.g_ins + o, static_cast<double>(gi[r]));
+      atomicAdd(v.g_del + o, static_cast<double>(gd[r]));
+      atomicAdd(v.g_eps + o, static_cast<double>(ge[r]));
+      atomicAdd(v.g_err + o, static_cast<double>(gq[r]));
+    }
+    gi[r] = gd[r] = ge[r] = gq[r] = P::zero();
   }
-  f.dM = f.dX = P::zero();
-  f.dY = lane * R - 1 < pad ? init : P::zero();
-  f.acc = P::zero();
 }
 
-// Forward sweep of one pair, accumulating the pair's gradient terms scaled by `norm`; returns the
-// raw result (lane 31). Without checkpoints (K == 0) it reads the backward records the backward sweep
-// stored; with checkpoints it recomputes them block by block (adj_backward_block) first. Either way
-// the records reach the lanes through a shared-memory ring filled D steps ahead by cp.async, one
-// commit group per record.
-template <class P, int R, bool kCk>
-__device__ typename P::V adj_forward(const AdjView& v, const AdjRows<P, R>& own, int64_t off, int len, int pad,
-                                     const uint8_t* hap, int m, int lane, char* scratch, typename P::V* ring, int K,
-                                     double norm, double (&gi)[R], double (&gd)[R], double (&ge)[R], double (&gq)[R]) {
+// Forward sweep of row block `blk`, block by block of K steps with the backward values recomputed
+// into shared memory first, accumulating the gradient terms; returns lane 31's accumulated result
+// (meaningful in the last row block). `c_fac` scales the recomputed backward values, `init` is the
+// row-0 constant of the scaled forward values.
+template <class P, int R>
+__device__ typename P::V adj_forward(const AdjView& v, const AdjCoef<P, R>& c, int64_t off, int pad, const uint8_t* hap, int m, int lane,
+                                     const AdjScratch<P, R>& sc, int blk, typename P::V* smem, typename P::V c_fac,
+                                     typename P::V init) {
   using V = typename P::V;
   using S = typename P::S;
-  using Col = AdjCol<P, R>;
-  constexpr int D = Col::kDepth;
-  const S init = static_cast<S>(Consts<P::kDouble>::kInitial / m);
-  AdjFwdState<P, R> f;
+  using Z = AdjSizes<P, R>;
+  constexpr int K = Z::K;
+  const bool first = blk == 0, last = blk == sc.blocks - 1;
+  const int n = m + 31;
+  const V sink = (lane == 31 && last) ? P::mul(static_cast<S>(Consts<P::kDouble>::kBackwardScale), c_fac) : P::zero();
+  const bool below = lane == 31 && !last;
+  AdjFwd<P, R> f;
 #pragma unroll
   for (int r = 0; r < R; ++r) f.M[r] = f.X[r] = f.Y[r] = P::zero();
-  f.acc = f.dM = f.dX = f.dY = P::zero();
-  const int n = m + 31;
-  // The lane's record for column k + 1 (k = 0..m-1) sits in ring slot k % D.
-  auto slot = [&](int k) { return ring + (static_cast<size_t>(k % D) * 32 + lane) * Col::kRec; };
-  auto copy = [&](int k, const V* src) {
-    V* dst = slot(k);
+  f.dM = f.dX = f.dY = f.acc = P::zero();
+  V gi[R], gd[R], ge[R], gq[R];
 #pragma unroll
-    for (int i = 0; i < Col::kRec / Col::kPer16; ++i)
-      __pipeline_memcpy_async(reinterpret_cast<char*>(dst) + 16 * i, reinterpret_cast<const char*>(src) + 16 * i, 16);
-  };
-  uint32_t next_code = (m > 0 && lane == 0) ? adj_code(__ldg(hap)) : 0u;
-  // One step: the row above's values shuffled down from the lane above (before column 0's reset, as
-  // in the unrolled recurrence), column 0's row-0 constant, the arithmetic, and the diagonal kept.
-  auto step = [&](int p, const V (&bM)[R], const V (&bX)[R], const V (&bY)[R], bool live, uint32_t code) {
-    const V uM = P::up(f.M[R - 1]), uX = P::up(f.X[R - 1]), uY = P::up(f.Y[R - 1]);
-    if (p == 0) adj_fwd_column0<P, R>(f, pad, lane, init);
-    adj_fwd_math<P, R>(f, own, code, live, bM, bX, bY, uM, uX, norm, gi, gd, ge, gq);
-    f.dM = uM;
-    f.dX = uX;
-    f.dY = uY;
-  };
-  if (!kCk || K == 0) {
-    // Columns fetched D ahead, keyed by the lane position k.
-    auto fetch = [&](int k) {
-      if (k < m) copy(k, Col::at(scratch, k + 1, lane));
-      __pipeline_commit();
-    };
+  for (int r = 0; r < R; ++r) gi[r] = gd[r] = ge[r] = gq[r] = P::zero();
+  uint4* buf = reinterpret_cast<uint4*>(smem);
+  for (int t0 = 0; t0 < n; t0 += K) {
+    const int t1 = min(t0 + K, n);
+    const int lo = max(0, n - t1), hi = n - 1 - t0;
+    // Backward steps [lo, hi] from the checkpoint entering lo (or the start), scaled by c_fac, into
+    // the block buffer [step - lo][chunk][lane].
+    {
+      AdjBwd<P, R> st;
+      if (lo > 0)
+        st.restore(sc.state(blk, (n - lo) / K - 1), lane, c_fac);
+      else
+        st.zero();
+      uint32_t next_code = adj_bwd_code(hap, m, lo - (31 - lane));
+      for (int tb = lo; tb <= hi; ++tb) {
+        const int p = tb - (31 - lane);
+        const uint32_t code = next_code;
+        next_code = adj_bwd_code(hap, m, p + 1);
+        V cBM = P::zero(), cBX = P::zero();
+        if (below && tb <= m) {
+          const V* u = sc.up(blk + 1, m - tb);
+          cBM = P::mul(u[0], c_fac);
+          cBX = P::mul(u[1], c_fac);
+        }
+        V rec[Z::kRecVals];
+        adj_bwd_step<P, R, true>(st, c, sink, code, p, below, cBM, cBX, rec);
 #pragma unroll
-    for (int k = 0; k < D; ++k) fetch(k);
-    for (int t = 0; t < n; ++t) {
+        for (int i = 3 * R; i < Z::kRecVals; ++i) rec[i] = P::zero();
+#pragma unroll
+        for (int ch = 0; ch < Z::kRecChunks; ++ch)
+          buf[((tb - lo) * Z::kRecChunks + ch) * 32 + lane] = reinterpret_cast<const uint4*>(rec)[ch];
+      }
+    }
+    __syncwarp();
+    const bool uniform = t0 >= 31 && t1 <= m;  // every lane inside the haplotype at every step
+    for (int t = t0; t < t1; ++t) {
       const int p = t - lane;  // column p + 1
       const bool live = p >= 0 && p < m;
-      const uint32_t code = next_code;
-      next_code = (p + 1 >= 0 && p + 1 < m) ? adj_code(__ldg(hap + p + 1)) : 0u;
-      V bM[R], bX[R], bY[R];
-      if (live) {
-        __pipeline_wait_prior(D - 1);
-        V rec[Col::kRec];
-        load_record(rec, slot(p));
+      const uint32_t code = live ? adj_code(__ldg(hap + p)) : 0u;
+      V rec[Z::kRecVals];
+      const int slot = n - 1 - t - lo;
+#pragma unroll
+      for (int ch = 0; ch < Z::kRecChunks; ++ch) reinterpret_cast<uint4*>(rec)[ch] = buf[(slot * Z::kRecChunks + ch) * 32 + lane];
+      V uM = P::up(f.M[R - 1]), uX = P::up(f.X[R - 1]), uY = P::up(f.Y[R - 1]);
+      if (lane == 0) {
+        if (first) {
+          uM = uX = P::zero();
+          uY = init;
+        } else if (p >= 0 && p < m) {
+          const V* d = sc.down(p);
+          uM = d[0];
+          uX = d[1];
+          uY = d[2];
+        }
+      }
+      if (p == 0) {
+        // Column 0: the row-0 constant in the padding rows (and above the lane's top row when that
+        // is padding).
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-          bM[r] = rec[r];
-          bX[r] = rec[R + r];
-          bY[r] = rec[2 * R + r];
+          f.M[r] = f.X[r] = P::zero();
+          f.Y[r] = lane * R + r < pad ? init : P::zero();
         }
-      } else {
-#pragma unroll
-        for (int r = 0; r < R; ++r) bM[r] = bX[r] = bY[r] = P::zero();
+        f.dM = f.dX = P::zero();
+        f.dY = lane * R - 1 < pad ? init : P::zero();
+        f.acc = P::zero();
       }
-      step(p, bM, bX, bY, live, code);
-      if (live) fetch(p + D);  // into the slot just read (its values are consumed above)
-    }
-  } else if (kCk) {
-    // Block b: forward steps [t0, t1) read backward steps n - 1 - t, recomputed into the block
-    // buffer at index n - 1 - t - lo. Every step commits one group, the one for step t + D (empty
-    // beyond the block), so the group of a live step is always complete after wait_prior(D - 1).
-    for (int t0 = 0; t0 < n; t0 += K) {
-      const int t1 = min(t0 + K, n);
-      const int lo = max(0, n - t1), hi = n - 1 - t0;
-      adj_backward_block<P, R>(v.bases, v.d_ins, v.d_del, v.eps, v.err, off, len, pad, hap, m, lane, scratch, K, t0 / K, lo, hi);
-      // The lane's records are fetched back by its own asynchronous copies.
-      __threadfence_block();
-      __syncwarp();
-      auto fetch = [&](int tt) {
-        const int k = tt - lane;
-        if (tt < t1 && k >= 0 && k < m) copy(k, AdjCkpt<P, R>::block(scratch, n - 1 - tt - lo, lane));
-        __pipeline_commit();
-      };
-      for (int i = 0; i < D; ++i) fetch(t0 + i);
-      for (int t = t0; t < t1; ++t) {
-        const int p = t - lane;
-        const bool live = p >= 0 && p < m;
-        const uint32_t code = next_code;
-        next_code = (p + 1 >= 0 && p + 1 < m) ? adj_code(__ldg(hap + p + 1)) : 0u;
-        V bM[R], bX[R], bY[R];
-        if (live) {
-          __pipeline_wait_prior(D - 1);
-          V rec[Col::kRec];
-          load_record(rec, slot(p));
-#pragma unroll
-          for (int r = 0; r < R; ++r) {
-            bM[r] = rec[r];
-            bX[r] = rec[R + r];
-            bY[r] = rec[2 * R + r];
-          }
-        } else {
-#pragma unroll
-          for (int r = 0; r < R; ++r) bM[r] = bX[r] = bY[r] = P::zero();
-        }
-        step(p, bM, bX, bY, live, code);
-        fetch(t + D);
+      if (uniform)
+        adj_fwd_step<P, R, false>(f, c, code, true, rec, uM, uX, gi, gd, ge, gq);
+      else
+        adj_fwd_step<P, R, true>(f, c, code, live, rec, uM, uX, gi, gd, ge, gq);
+      f.dM = uM;
+      f.dX = uX;
+      f.dY = uY;
+      if (!last && lane == 31 && live) {
+        V* d = sc.down(p);
+        d[0] = f.M[R - 1];
+        d[1] = f.X[R - 1];
+        d[2] = f.Y[R - 1];
       }
-      __pipeline_wait_prior(0);
+      if ((t + 1) % kFlushSteps == 0 || t + 1 == n) adj_flush<P, R>(v, c, off, pad, lane, gi, gd, ge, gq);
     }
+    __syncwarp();
   }
-  __pipeline_wait_prior(0);
   return __shfl_sync(kFull, f.acc, 31);
 }
 
 template <class P, int R>
 struct AdjMinBlocks {
-  static constexpr int value = 1;
+  static constexpr int value = P::kDouble ? 1 : (R <= 6 ? 3 : 2);
 };
 
-// kCk: the instantiation for launches whose longest pairs exceed the per-warp scratch, which
-// recomputes those pairs' backward columns from checkpoints; the other keeps no checkpoint code.
-template <class P, int R, bool kCk>
+template <class P, int R>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, (AdjMinBlocks<P, R>::value)) adjoint_kernel(AdjLaunch a) {
+  using V = typename P::V;
+  using S = typename P::S;
   using C = Consts<P::kDouble>;
+  using Z = AdjSizes<P, R>;
   extern __shared__ __align__(16) unsigned char adj_smem[];
   const int lane = threadIdx.x & 31;
   const int warp = blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
-  char* scratch = a.scratch + static_cast<size_t>(warp) * a.scratch_stride;
-  typename P::V* ring = reinterpret_cast<typename P::V*>(adj_smem + (threadIdx.x >> 5) * AdjCol<P, R>::kRingBytes);
+  V* smem = reinterpret_cast<V*>(adj_smem + (threadIdx.x >> 5) * Z::kSmemPerWarp);
   const int count = a.count ? min(*a.count, a.n_tasks) : a.n_tasks;
   const double ln10 = 2.302585092994045684017991454684364208;
   for (;;) {
@@ -522,55 +527,74 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, (AdjMinBlocks<P, R>::valu
     const int g = a.v.read_region[read];
     const int64_t off = a.v.read_off[read];
     const int len = static_cast<int>(a.v.read_off[read + 1] - off);
-    const int pad = 32 * R - len;
+    const int blocks = adj_row_blocks(len, R);
+    const int pad0 = 32 * R * blocks - len;
     const int h0 = a.v.region_hap[g], nh = a.v.region_nhap[g];
     const int read_local = read - a.v.region_read[g];
-    AdjRows<P, R> own;
-    own.load(a.v, off, len, pad, lane);
-    double gi[R], gd[R], ge[R], gq[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) gi[r] = gd[r] = ge[r] = gq[r] = 0.0;
     bool lost = false;
     for (int h = 0; h < nh && !lost; ++h) {
       const int64_t hlo = a.v.hap_off[h0 + h];
       const int m = static_cast<int>(a.v.hap_off[h0 + h + 1] - hlo);
       const uint8_t* hap = a.v.hap_bases + hlo;
-      // Backward columns stored whole when they fit the warp's scratch, else recomputed from
-      // checkpoints block by block (the host sized the scratch so one of the two fits).
-      int K = 0;
-      const long long cap = static_cast<long long>(a.scratch_stride / (32 * sizeof(typename P::V)));
-      if (static_cast<long long>(m + 1) * AdjCol<P, R>::kRec > cap) {
-        if (!kCk) {
-          lost = true;
-          break;
-        }
-        K = adj_block_steps(cap, m + 31, AdjCol<P, R>::kRec, AdjBwdState<P, R>::kRec, AdjCol<P, R>::kDepth);
-        if (K == 0) {
-          lost = true;
-          break;
-        }
+      AdjScratch<P, R> sc;
+      sc.base = a.scratch + static_cast<size_t>(warp) * a.scratch_stride;
+      sc.m = m;
+      sc.blocks = blocks;
+      sc.n_states = (m + 31 + Z::K - 1) / Z::K;
+      // 1. Backward sweeps, bottom row block first; the first block yields the start mass.
+      V s = P::zero();
+      for (int blk = blocks - 1; blk >= 0; --blk) {
+        AdjCoef<P, R> c;
+        c.load(a.v, off, len, pad0 - 32 * R * blk, lane);
+        s = adj_backward<P, R>(c, hap, m, lane, sc, blk, pad0 - 32 * R * blk);
+        __syncwarp();
       }
-      const double s = static_cast<double>(adj_backward<P, R, kCk>(a.v, own, off, len, pad, hap, m, lane, scratch, K));
-      // raw = (INITIAL / m) * s / scale: the pair's scaled likelihood, from the backward values.
-      const double raw = (C::kInitial / m) * s / C::kBackwardScale;
+      const double init = C::kInitial / m;
+      const double raw = init * static_cast<double>(s) / C::kBackwardScale;
       if (!P::kDouble && (!(raw >= C::kMinAccepted) || isinf(raw))) {
         lost = true;
         break;
       }
-      const double norm = 1.0 / ((C::kInitial / m) * s * ln10);
-      // The lane's backward records are fetched back by its own asynchronous copies.
-      __threadfence_block();
-      __syncwarp();
-      const double fwd =
-          static_cast<double>(adj_forward<P, R, kCk>(a.v, own, off, len, pad, hap, m, lane, scratch, ring, K, norm, gi, gd, ge, gq));
-      if (!P::kDouble && (!(fwd >= C::kMinAccepted) || isinf(fwd))) {
+      // 2. The scale split: F from init * 2^-a, B times 2^a / (raw * scale * ln 10).
+      int shift = 0;
+      if (!P::kDouble) {
+        shift = static_cast<int>(floor(0.5 * (log2(raw) + log2(init))));
+        shift = max(0, min(shift, 240));
+      }
+      const V c_fac = static_cast<S>(ldexp(1.0, shift) / (raw * C::kBackwardScale * ln10));
+      const V init_a = static_cast<S>(ldexp(init, -shift));
+      // 3. Forward sweeps, top row block first, with the gradient terms.
+      V fwd = P::zero();
+      for (int blk = 0; blk < blocks; ++blk) {
+        AdjCoef<P, R> c;
+        const int pad = pad0 - 32 * R * blk;
+        c.load(a.v, off, len, pad, lane);
+        fwd = adj_forward<P, R>(a.v, c, off, pad, hap, m, lane, sc, blk, smem, c_fac, init_a);
+        __syncwarp();
+      }
+      const double fwd_raw = ldexp(static_cast<double>(fwd), shift);
+      if (!P::kDouble && (!(fwd_raw >= C::kMinAccepted) || isinf(fwd_raw))) {
         lost = true;
         break;
       }
-      if (lane == 0) a.v.out[a.v.region_out[g] + static_cast<int64_t>(read_local) * nh + h] = log10(fwd) - C::kLog10Initial;
+      if (lane == 0) a.v.out[a.v.region_out[g] + static_cast<int64_t>(read_local) * nh + h] = log10(fwd_raw) - C::kLog10Initial;
       __syncwarp();
     }
     if (lost) {
+      // The FP64 recomputation sums this read's gradients afresh: clear what earlier haplotypes added,
+      // each position by the lane that added to it (atomics of one thread to one address keep their
+      // order).
+      for (int blk = 0; blk < blocks; ++blk)
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int q = lane * R + r - (pad0 - 32 * R * blk);
+          if (q < 0 || q >= len) continue;
+          atomicExch(reinterpret_cast<unsigned long long*>(a.v.g_ins + off + q), 0ull);
+          atomicExch(reinterpret_cast<unsigned long long*>(a.v.g_del + off + q), 0ull);
+          atomicExch(reinterpret_cast<unsigned long long*>(a.v.g_eps + off + q), 0ull);
+          atomicExch(reinterpret_cast<unsigned long long*>(a.v.g_err + off + q), 0ull);
+        }
+      __syncwarp();
       if (lane == 0) {
         atomicAdd(a.v.lost, 1ull);
         if (a.queue) {
@@ -579,30 +603,23 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, (AdjMinBlocks<P, R>::valu
           if (slot < a.queue_off[bin + 1] - a.queue_off[bin]) a.queue[a.queue_off[bin] + slot] = read;
         }
       }
-      continue;
-    }
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      if (!own.real[r]) continue;
-      const int64_t o = off + lane * R + r - pad;
-      a.v.g_ins[o] = gi[r];
-      a.v.g_del[o] = gd[r];
-      a.v.g_eps[o] = ge[r];
-      a.v.g_err[o] = gq[r];
     }
   }
 }
 
-template <class P, int R, bool kCk>
+template <class P, int R>
 void adj_occ(int* blocks) {
   static std::atomic<int> cache[kMaxDevices];
-  *blocks = resident_blocks(adjoint_kernel<P, R, kCk>, kWarpsPerBlock * AdjCol<P, R>::kRingBytes, kWarpsPerBlock * 32, cache);
+  *blocks = resident_blocks(adjoint_kernel<P, R>, kWarpsPerBlock * AdjSizes<P, R>::kSmemPerWarp, kWarpsPerBlock * 32, cache);
 }
 
-template <class P, int R, bool kCk>
+template <class P, int R>
 cudaError_t adj_go(int blocks, const AdjLaunch& a, cudaStream_t s) {
-  const size_t smem = kWarpsPerBlock * AdjCol<P, R>::kRingBytes;
-  adjoint_kernel<P, R, kCk><<<blocks, kWarpsPerBlock * 32, smem, s>>>(a);
+  const size_t smem = kWarpsPerBlock * AdjSizes<P, R>::kSmemPerWarp;
+  // resident_blocks set the kernel's dynamic shared-memory limit on this device.
+  int per_sm = 0;
+  adj_occ<P, R>(&per_sm);
+  adjoint_kernel<P, R><<<blocks, kWarpsPerBlock * 32, smem, s>>>(a);
   return cudaGetLastError();
 }
 
@@ -628,63 +645,30 @@ auto adj_dispatch_rows(int rows, F&& f) {
 
 }  // namespace
 
-namespace {
-// Record sizes (values per lane) of an instantiation: backward column, saved state, ring depth.
-struct AdjSizes {
-  int rec, state, depth;
-  size_t value;
-};
-AdjSizes adj_sizes(bool dbl, int rows) {
-  if (dbl)
-    return adj_dispatch_rows(rows, [](auto r) {
-      constexpr int R = decltype(r)::value;
-      return AdjSizes{AdjCol<OneF64, R>::kRec, AdjBwdState<OneF64, R>::kRec, AdjCol<OneF64, R>::kDepth, sizeof(double)};
-    });
-  return adj_dispatch_rows(rows, [](auto r) {
+size_t adj_scratch_bytes(bool dbl, int rows, int read_len, int hap_len) {
+  return adj_dispatch_rows(rows, [&](auto r) {
     constexpr int R = decltype(r)::value;
-    return AdjSizes{AdjCol<OneF32, R>::kRec, AdjBwdState<OneF32, R>::kRec, AdjCol<OneF32, R>::kDepth, sizeof(float)};
+    return dbl ? AdjScratch<OneF64, R>::bytes(read_len, hap_len) : AdjScratch<OneF32, R>::bytes(read_len, hap_len);
   });
 }
-}  // namespace
 
-size_t adj_column_bytes(bool dbl, int rows, int columns) {
-  const AdjSizes z = adj_sizes(dbl, rows);
-  return static_cast<size_t>(columns) * 32 * z.rec * z.value;
-}
-
-size_t adj_scratch_bytes(bool dbl, int rows, int max_hap_len) { return adj_column_bytes(dbl, rows, max_hap_len + 1); }
-
-size_t adj_checkpoint_bytes(bool dbl, int rows, int max_hap_len) {
-  const AdjSizes z = adj_sizes(dbl, rows);
-  const long long steps = max_hap_len + 31;
-  // K * rec + ceil(steps / K) * state is least near K = sqrt(steps * state / rec).
-  long long best = -1;
-  long long k0 = static_cast<long long>(std::sqrt(static_cast<double>(steps) * z.state / z.rec));
-  for (long long K = std::max<long long>(z.depth, k0 - 2); K <= std::max<long long>(z.depth, k0 + 2); ++K) {
-    const long long need = K * z.rec + (steps + K - 1) / K * z.state;
-    if (best < 0 || need < best) best = need;
-  }
-  return static_cast<size_t>(best) * 32 * z.value;
-}
-
-void adj_occupancy(bool dbl, int rows, bool checkpointed, int* blocks, int* threads) {
+void adj_occupancy(bool dbl, int rows, int* blocks, int* threads) {
   *threads = kWarpsPerBlock * 32;
   *blocks = 0;
   adj_dispatch_rows(rows, [&](auto r) {
     constexpr int R = decltype(r)::value;
     if (dbl)
-      checkpointed ? adj_occ<OneF64, R, true>(blocks) : adj_occ<OneF64, R, false>(blocks);
+      adj_occ<OneF64, R>(blocks);
     else
-      checkpointed ? adj_occ<OneF32, R, true>(blocks) : adj_occ<OneF32, R, false>(blocks);
+      adj_occ<OneF32, R>(blocks);
     return 0;
   });
 }
 
-cudaError_t adj_launch(bool dbl, int rows, bool checkpointed, int blocks, const AdjLaunch& a, cudaStream_t s) {
+cudaError_t adj_launch(bool dbl, int rows, int blocks, const AdjLaunch& a, cudaStream_t s) {
   return adj_dispatch_rows(rows, [&](auto r) {
     constexpr int R = decltype(r)::value;
-    if (dbl) return checkpointed ? adj_go<OneF64, R, true>(blocks, a, s) : adj_go<OneF64, R, false>(blocks, a, s);
-    return checkpointed ? adj_go<OneF32, R, true>(blocks, a, s) : adj_go<OneF32, R, false>(blocks, a, s);
+    return dbl ? adj_go<OneF64, R>(blocks, a, s) : adj_go<OneF32, R>(blocks, a, s);
   });
 }
 

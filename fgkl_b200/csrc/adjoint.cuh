@@ -30,7 +30,7 @@ struct AdjView {
   const int32_t* region_read;  // region -> first global read
   const int64_t* region_out;   // region -> first output element
   double* out;              // log10 L, row-major per region (reads x haplotypes)
-  double* g_ins;            // gradients, per read position
+  double* g_ins;            // gradients, per read position; zero before the first launch, then summed into
   double* g_del;
   double* g_eps;
   double* g_err;
@@ -44,47 +44,33 @@ struct AdjLaunch {
   const int* count;      // device-side count (FP64 recomputation queue), or nullptr
   int* task_counter;     // zeroed before the launch
   char* scratch;
-  size_t scratch_stride; // bytes per warp: a pair whose backward columns exceed it runs with checkpoints
+  size_t scratch_stride; // bytes per warp (adj_scratch_bytes of the launch's largest pair)
   int32_t* queue;        // FP32 launches: reads lost in FP32, for FP64 (per-bin slices), or nullptr
   const int* queue_off;  // per rows-per-lane bin: first queue slot (kAdjRowBins + 1 entries)
   int* queue_tail;       // per bin
 };
 
 constexpr int kAdjRowBins = 21;
+constexpr int kAdjMaxBlockRead = 620;  // longest read one 32 x 20-row block holds
+constexpr int kAdjLongRows = 8;        // rows per lane of longer reads, strip-mined over row blocks
 
-// Rows per lane for a read of `len` positions (31 * rows >= len; even above 8).
+// Rows per lane for a read of `len` positions: 31 * rows >= len (even above 8) up to 620 bases,
+// kAdjLongRows beyond.
 __host__ __device__ inline int adj_rows(int len) {
+  if (len > kAdjMaxBlockRead) return kAdjLongRows;
   int rows = (len + 30) / 31;
   if (rows > 8) rows = (rows + 1) & ~1;
   return rows;
 }
-// Steps per recomputed block for a pair of `steps` forward steps whose per-warp scratch holds `cap`
-// values per lane, with backward records of `rec` values and saved backward states of `state` values:
-// the largest K >= min_k with K * rec + ceil(steps / K) * state <= cap, or 0 when there is none.
-__host__ __device__ inline int adj_block_steps(long long cap, int steps, int rec, int state, int min_k) {
-  long long K = (cap - state) / rec;
-  if (K > steps) K = steps;
-  for (int it = 0; it < 4096 && K >= min_k; ++it) {
-    const long long nb = (steps + K - 1) / K;
-    if (K * rec + nb * state <= cap) return static_cast<int>(K);
-    const long long k2 = (cap - nb * state) / rec;
-    K = k2 < K ? k2 : K - 1;
-  }
-  return 0;
-}
+// Row blocks of 32 * rows rows that a read of `len` positions spans, with at least one padding row
+// above the read (the row that collects the backward start mass): 1 up to 620 bases.
+__host__ __device__ inline int adj_row_blocks(int len, int rows) { return (len + 32 * rows) / (32 * rows); }
 
-// Bytes of per-warp scratch that store every backward column of haplotypes of at most
-// `max_hap_len` bases.
-size_t adj_scratch_bytes(bool dbl, int rows, int max_hap_len);
-// The least per-warp scratch with which haplotypes of at most `max_hap_len` bases run with
-// checkpoints: backward states saved every K steps and each block of K columns recomputed before the
-// forward sweep reads it (about sqrt of the stored-column bytes).
-size_t adj_checkpoint_bytes(bool dbl, int rows, int max_hap_len);
-// Bytes of per-warp scratch that store `columns` backward columns.
-size_t adj_column_bytes(bool dbl, int rows, int columns);
-// `checkpointed`: the instantiation that recomputes backward columns from checkpoints for pairs whose
-// columns exceed the launch's per-warp scratch (the other has no such path and must not get them).
-void adj_occupancy(bool dbl, int rows, bool checkpointed, int* blocks_per_sm, int* threads_per_block);
-cudaError_t adj_launch(bool dbl, int rows, bool checkpointed, int blocks, const AdjLaunch& a, cudaStream_t stream);
+// Bytes of per-warp scratch a pair of a `read_len`-position read and a `hap_len`-base haplotype
+// needs: the backward checkpoints of every row block, and, for a strip-mined read, the rows that
+// pass between row blocks.
+size_t adj_scratch_bytes(bool dbl, int rows, int read_len, int hap_len);
+void adj_occupancy(bool dbl, int rows, int* blocks_per_sm, int* threads_per_block);
+cudaError_t adj_launch(bool dbl, int rows, int blocks, const AdjLaunch& a, cudaStream_t stream);
 
 }  // namespace fgkl

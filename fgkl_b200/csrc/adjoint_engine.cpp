@@ -5,27 +5,27 @@
 #include <map>
 
 #include "../../include/fgkl_b200.h"
+#include "engine.h"
 
 namespace fgkl {
 
 namespace {
 
 constexpr int kWarps = 4;                             // warps per block of the adjoint kernels
-constexpr size_t kScratchBudget = size_t{8} << 30;    // per-warp column stores of one launch, at most 8 GiB
-constexpr int64_t kMaxReadLen = 620;
+constexpr size_t kScratchBudget = size_t{8} << 30;    // per-warp checkpoints of one launch, at most 8 GiB
 
 size_t align_up(size_t x, size_t a = 256) { return (x + a - 1) / a * a; }
 
 }  // namespace
 
 AdjointEngine::AdjointEngine(int device, cudaStream_t stream) : device_(device), stream_(stream) {
-  cudaSetDevice(device_);
+  DeviceGuard device_guard(device_);
   cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device_);
   cudaMalloc(&d_lost_, sizeof(unsigned long long));
 }
 
 AdjointEngine::~AdjointEngine() {
-  cudaSetDevice(device_);
+  DeviceGuard device_guard(device_);
   if (stream_) cudaStreamSynchronize(stream_);
   cudaFree(d_bytes_);
   cudaFree(d_params_);
@@ -56,9 +56,9 @@ T* AdjointEngine::grow(T*& p, size_t& cap, size_t n) {
     const size_t want = cap > 0 ? std::max(bytes, cap + cap / 2) : bytes;
     cudaFree(p);
     p = nullptr;
-    if (cudaMalloc(&p, want) == cudaSuccess) {
+    if (device_alloc(reinterpret_cast<void**>(&p), want) == cudaSuccess) {
       cap = want;
-    } else if (want > bytes && (cudaGetLastError(), cudaMalloc(&p, bytes) == cudaSuccess)) {
+    } else if (want > bytes && (cudaGetLastError(), device_alloc(reinterpret_cast<void**>(&p), bytes) == cudaSuccess)) {
       cap = bytes;
     } else {
       cudaGetLastError();
@@ -71,7 +71,7 @@ T* AdjointEngine::grow(T*& p, size_t& cap, size_t n) {
 }
 
 int AdjointEngine::prepare(const AdjointInput& in, bool double_precision) {
-  cudaSetDevice(device_);
+  DeviceGuard device_guard(device_);
   error_.clear();
   dbl_ = double_precision;
   bins_.clear();
@@ -99,7 +99,7 @@ int AdjointEngine::prepare(const AdjointInput& in, bool double_precision) {
   for (int64_t r = 0; r < total_reads; ++r) {
     const int64_t len = in.read_off[r + 1] - in.read_off[r];
     if (len <= 0) return fail(FGKL_E_EMPTY_READ, "read " + std::to_string(r) + " has no bases");
-    if (len > kMaxReadLen) return fail(FGKL_E_UNSUPPORTED, "reads of at most 620 bases are supported");
+    if (len > (int64_t{1} << 24)) return fail(FGKL_E_UNSUPPORTED, "read longer than 2^24 bases");
   }
   for (int64_t h = 0; h < total_haps; ++h) {
     const int64_t len = in.hap_off[h + 1] - in.hap_off[h];
@@ -108,19 +108,26 @@ int AdjointEngine::prepare(const AdjointInput& in, bool double_precision) {
     max_hap = std::max<int>(max_hap, static_cast<int>(len));
   }
 
-  // Tasks: one per read, binned by rows per lane, costliest first.
+  // Tasks: one per read, binned by rows per lane, costliest first. Each bin's per-warp scratch is
+  // what its largest pair needs (adj_scratch_bytes: the read's length and its region's longest
+  // haplotype).
   std::vector<int32_t> read_region(static_cast<size_t>(total_reads));
   std::map<int, std::vector<std::pair<int64_t, int32_t>>> by_rows;
   std::vector<int> per_rows(kAdjRowBins, 0);
+  std::vector<size_t> need(kAdjRowBins, 0);
   for (int g = 0; g < N; ++g) {
     const int64_t hap_sum = total_haps > 0 ? in.hap_off[first_hap[g + 1]] - in.hap_off[first_hap[g]] : 0;
+    int longest = 1;
+    for (int64_t h = first_hap[g]; h < first_hap[g + 1]; ++h)
+      longest = std::max(longest, static_cast<int>(in.hap_off[h + 1] - in.hap_off[h]));
     for (int64_t r = first_read[g]; r < first_read[g + 1]; ++r) {
       read_region[r] = g;
       if (in.region_haps[g] == 0) continue;
       const int len = static_cast<int>(in.read_off[r + 1] - in.read_off[r]);
       const int rows = adj_rows(len);
-      by_rows[rows].push_back({static_cast<int64_t>(rows) * hap_sum, static_cast<int32_t>(r)});
+      by_rows[rows].push_back({static_cast<int64_t>(rows) * adj_row_blocks(len, rows) * hap_sum, static_cast<int32_t>(r)});
       per_rows[rows]++;
+      need[rows] = std::max(need[rows], std::max(adj_scratch_bytes(dbl_, rows, len, longest), adj_scratch_bytes(true, rows, len, longest)));
     }
   }
   std::vector<int32_t> tasks;
@@ -135,33 +142,18 @@ int AdjointEngine::prepare(const AdjointInput& in, bool double_precision) {
   if (!dbl_)
     for (int r = 1; r < kAdjRowBins; ++r)
       if (per_rows[r]) rescue_.push_back(Bin{true, r, queue_off[r], per_rows[r], 0, 0});
+  // Bins run one after another, so they share the scratch; a bin's grid shrinks only when its warps'
+  // scratch would exceed the budget (very long pairs).
   size_t scratch = 256;
   for (auto* list : {&bins_, &rescue_})
     for (Bin& b : *list) {
       int per_sm = 0, threads = 0;
-      adj_occupancy(b.dbl, b.rows, false, &per_sm, &threads);
+      adj_occupancy(b.dbl, b.rows, &per_sm, &threads);
       if (per_sm <= 0) return fail(FGKL_E_CUDA, "adjoint kernel unavailable on this device");
-      // Per-warp scratch: every backward column of the longest haplotype when that fits the budget
-      // at full occupancy (or the caller's column limit); otherwise what the budget gives each warp,
-      // and pairs whose columns exceed it recompute them from checkpoints. Only when even the
-      // checkpointed form does not fit does the grid shrink.
       const int64_t want = std::min<int64_t>((b.n_tasks + kWarps - 1) / kWarps, static_cast<int64_t>(per_sm) * sms_);
-      const size_t full = align_up(adj_scratch_bytes(b.dbl, b.rows, max_hap));
-      const size_t least = align_up(adj_checkpoint_bytes(b.dbl, b.rows, max_hap));
-      size_t stride = full;
-      if (stored_columns_ > 0) stride = std::min(stride, align_up(adj_column_bytes(b.dbl, b.rows, stored_columns_)));
-      const size_t fair = kScratchBudget / (static_cast<size_t>(kWarps) * static_cast<size_t>(std::max<int64_t>(want, 1)));
-      if (stride > fair) stride = fair / 256 * 256;
-      b.stride = std::max(std::min(stride, full), least);
-      b.checkpointed = b.stride < full;
-      int64_t fit = want;
-      if (b.checkpointed) {
-        adj_occupancy(b.dbl, b.rows, true, &per_sm, &threads);
-        if (per_sm <= 0) return fail(FGKL_E_CUDA, "adjoint kernel unavailable on this device");
-        fit = std::min<int64_t>((b.n_tasks + kWarps - 1) / kWarps, static_cast<int64_t>(per_sm) * sms_);
-      }
+      b.stride = align_up(std::max<size_t>(need[b.rows], 256));
       const int64_t by_budget = static_cast<int64_t>(kScratchBudget / (kWarps * b.stride));
-      b.blocks = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(fit, by_budget)));
+      b.blocks = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(want, by_budget)));
       scratch = std::max(scratch, static_cast<size_t>(b.blocks) * kWarps * b.stride);
     }
 
@@ -174,7 +166,7 @@ int AdjointEngine::prepare(const AdjointInput& in, bool double_precision) {
       !grow(d_off_, cap_off_, n_off + 1) || !grow(d_idx_, cap_idx_, n_idx + 1) ||
       !grow(d_out_, cap_out_, static_cast<size_t>(out_len_) + 4 * static_cast<size_t>(grad_len_) + 1) ||
       !grow(d_small_, cap_small_, static_cast<size_t>(n_small_)) || !grow(d_scratch_, cap_scratch_, scratch))
-    return fail(FGKL_E_CUDA, "device allocation failed");
+    return fail(FGKL_E_OUT_OF_MEMORY, "device allocation failed");
 
   std::vector<int32_t> region_hap(N), region_nhap(N), region_read(N);
   for (int g = 0; g < N; ++g) {
@@ -242,15 +234,8 @@ int AdjointEngine::prepare(const AdjointInput& in, bool double_precision) {
   return FGKL_OK;
 }
 
-int AdjointEngine::checkpointed_launches() const {
-  int n = 0;
-  for (const auto* list : {&bins_, &rescue_})
-    for (const Bin& b : *list) n += b.checkpointed ? 1 : 0;
-  return n;
-}
-
 int AdjointEngine::run() {
-  cudaSetDevice(device_);
+  DeviceGuard device_guard(device_);
   int rc;
   const size_t n_launch = bins_.size() + rescue_.size();
   int* counters = d_small_;
@@ -259,6 +244,10 @@ int AdjointEngine::run() {
   if ((rc = check(cudaMemsetAsync(counters, 0, n_launch * sizeof(int), stream_), "reset counters"))) return rc;
   if ((rc = check(cudaMemsetAsync(queue_tail, 0, kAdjRowBins * sizeof(int), stream_), "reset queues"))) return rc;
   if ((rc = check(cudaMemsetAsync(d_lost_, 0, sizeof(unsigned long long), stream_), "reset counters"))) return rc;
+  // The kernels add each pair's gradient terms into the per-position arrays.
+  if (grad_len_ > 0 &&
+      (rc = check(cudaMemsetAsync(view_.g_ins, 0, 4 * static_cast<size_t>(grad_len_) * sizeof(double), stream_), "reset gradients")))
+    return rc;
   launches_ = 0;
   int i = 0;
   for (int pass = 0; pass < 2; ++pass) {
@@ -275,7 +264,7 @@ int AdjointEngine::run() {
       a.queue = (pass == 0 && !dbl_) ? queue_ : nullptr;
       a.queue_off = queue_off;
       a.queue_tail = queue_tail;
-      if ((rc = check(adj_launch(b.dbl, b.rows, b.checkpointed, b.blocks, a, stream_), "adjoint launch"))) return rc;
+      if ((rc = check(adj_launch(b.dbl, b.rows, b.blocks, a, stream_), "adjoint launch"))) return rc;
       ++launches_;
     }
   }
@@ -284,7 +273,7 @@ int AdjointEngine::run() {
 
 int AdjointEngine::fetch(double* out, int64_t out_len, double* g_ins, double* g_del, double* g_eps, double* g_err, int64_t grad_len,
                          uint64_t* fp64_reads) {
-  cudaSetDevice(device_);
+  DeviceGuard device_guard(device_);
   if (out_len != out_len_) return fail(FGKL_E_OUTPUT_LENGTH, "likelihood output has the wrong length");
   if (grad_len != grad_len_) return fail(FGKL_E_OUTPUT_LENGTH, "gradient arrays must hold one value per read position");
   int rc;

@@ -34,11 +34,6 @@ class AdjointEngine {
   AdjointEngine& operator=(const AdjointEngine&) = delete;
 
   int prepare(const AdjointInput& in, bool double_precision);
-  // Backward columns stored per pair before the kernel switches to checkpointed recomputation
-  // (0: as many as the scratch budget gives every resident warp). Applies from the next prepare.
-  void set_stored_columns(int columns) { stored_columns_ = columns > 0 ? columns : 0; }
-  // Launches of the prepared batch whose longest pairs recompute backward columns from checkpoints.
-  int checkpointed_launches() const;
   int run();
   // Likelihoods (Σ reads x haplotypes) and the four gradient arrays (Σ read lengths).
   int fetch(double* out, int64_t out_len, double* g_ins, double* g_del, double* g_eps, double* g_err, int64_t grad_len,
@@ -56,14 +51,12 @@ class AdjointEngine {
     int n_tasks;
     int blocks;
     size_t stride;
-    bool checkpointed = false;
   };
   int fail(int code, const std::string& msg);
   int check(cudaError_t e, const char* what);
   template <class T>
   T* grow(T*& p, size_t& cap, size_t n);
 
-  int stored_columns_ = 0;
   int device_ = 0, sms_ = 0;
   cudaStream_t stream_ = nullptr;
   std::string error_;

@@ -159,58 +159,52 @@ def test_torch_autograd_function_wraps_the_adjoint(gpu):
         np.testing.assert_allclose(inputs[k].grad.numpy(), ref_g[k], rtol=1e-8, atol=1e-12)
 
 
-@pytest.mark.parametrize("double", [False, True])
-def test_row_checkpointing_gives_the_stored_columns_bits(gpu, double):
-    # With at most 48 stored backward columns, every pair here (haplotypes of 120 bases, and a
-    # longer region of 300) recomputes its backward columns block by block from checkpoints; the
-    # arithmetic is the stored sweep's, so every likelihood and gradient keeps its bits.
-    parts = [synthetic.reference_region(7 + g, 6, 60, 3, 120).region(0) for g in range(3)]
-    parts.append(synthetic.reference_region(40, 5, 151, 2, 300).region(0))
-    w = synthetic.from_regions(parts)
-    p = params_from_quals(w)
-    stored = AdjointContext().compute(w, p, double)
-    ctx = AdjointContext()
-    ctx.set_stored_columns(48)
-    ctx.prepare(w, p, double)
-    assert ctx.checkpointed_launches() >= 1
-    ctx.run()
-    ckpt = ctx.fetch()
-    assert ckpt.log10.tobytes() == stored.log10.tobytes()
-    for name in NAMES:
-        assert getattr(ckpt, name).tobytes() == getattr(stored, name).tobytes(), name
-    assert ckpt.fp64_reads == stored.fp64_reads
+def compare_with_scalar_adjoint(w, p, res, tol):
+    ll, g = oracle_all(w, p)
+    np.testing.assert_allclose(res.log10, ll, rtol=0, atol=tol)
+    for k, name in enumerate(NAMES):
+        assert rel(getattr(res, name).sum(), g[k].sum()) <= tol, name
+        scale = np.abs(g[k]).max()
+        np.testing.assert_allclose(getattr(res, name), g[k], rtol=0, atol=tol * scale, err_msg=name)
 
 
-def test_long_haplotypes_with_checkpoints_match_the_fp64_scalar_adjoint(gpu):
-    # Haplotypes of about 2,400 bases against reads of 80, with 200 stored columns: about 12 blocks
-    # of recomputed columns per pair; a short region in the same launch keeps its stored columns.
+def test_long_haplotypes_match_the_fp64_scalar_adjoint(gpu):
+    # Haplotypes of about 2,400 bases against reads of 80: hundreds of recomputed backward blocks per
+    # pair; a short region in the same launch.
     long_parts = [synthetic.reference_region(61, 3, 80, 2, 2400).region(0)]
     short_parts = [synthetic.reference_region(62, 4, 80, 2, 150).region(0)]
     w = synthetic.from_regions(long_parts + short_parts)
     p = params_from_quals(w)
-    ctx = AdjointContext()
-    ctx.set_stored_columns(200)
-    ctx.prepare(w, p, False)
-    assert ctx.checkpointed_launches() >= 1
-    ctx.run()
-    res = ctx.fetch()
-    ll, g = oracle_all(w, p)
-    np.testing.assert_allclose(res.log10, ll, rtol=0, atol=1e-4)
-    for k, name in enumerate(NAMES):
-        assert rel(getattr(res, name).sum(), g[k].sum()) <= 1e-4, name
-        scale = np.abs(g[k]).max()
-        np.testing.assert_allclose(getattr(res, name), g[k], rtol=0, atol=1e-4 * scale, err_msg=name)
+    compare_with_scalar_adjoint(w, p, AdjointContext().compute(w, p, False), 1e-4)
 
 
-def test_stored_columns_below_the_checkpointed_minimum_still_compute(gpu):
-    # A limit of one column is below what checkpointing needs; the scratch is sized to the least that
-    # works instead, and the results keep their bits.
-    w, _ = workload(seed=9, regions=2, reads=4, read_len=40, haps=2, hap_len=200)
+@pytest.mark.parametrize("read_len", [621, 1000, 2500])
+@pytest.mark.parametrize("double", [False, True])
+def test_long_reads_match_the_fp64_scalar_adjoint(gpu, read_len, double):
+    """Reads beyond one 32 x 20-row block are strip-mined over row blocks of 256 rows."""
+    w, _ = workload(seed=70 + read_len, regions=1, reads=2, read_len=read_len, haps=2, hap_len=read_len + 120)
     p = params_from_quals(w)
-    stored = AdjointContext().compute(w, p, False)
-    ctx = AdjointContext()
-    ctx.set_stored_columns(1)
-    ckpt = ctx.compute(w, p, False)
-    assert ckpt.log10.tobytes() == stored.log10.tobytes()
-    for name in NAMES:
-        assert getattr(ckpt, name).tobytes() == getattr(stored, name).tobytes(), name
+    compare_with_scalar_adjoint(w, p, AdjointContext().compute(w, p, double), 1e-9 if double else 1e-4)
+
+
+def test_a_read_lost_on_a_later_haplotype_is_summed_afresh_in_fp64(gpu):
+    """The FP32 pass adds a read's terms haplotype by haplotype; when a later haplotype loses the read,
+    the FP64 recomputation must not count the earlier haplotypes twice."""
+    n = 80
+    bases = b"ACGTACGTAC" * 8
+    reads = [Read(bases, bytes([30] * n), bytes([45] * n), bytes([45] * n), bytes([10] * n))]
+    haps = [b"ACGTACGTAC" * 9, b"T" * 90]
+    w = synthetic.from_regions([(reads, haps)])
+    p = params_from_quals(w)
+    res = AdjointContext().compute(w, p, False)
+    assert res.fp64_reads == 1
+    compare_with_scalar_adjoint(w, p, res, 1e-4)
+
+
+def test_runs_are_deterministic(gpu):
+    w, _ = workload(seed=13, regions=3, reads=6, read_len=100, haps=3, hap_len=250)
+    p = params_from_quals(w)
+    a = AdjointContext().compute(w, p, False)
+    b = AdjointContext().compute(w, p, False)
+    for name in ("log10",) + NAMES:
+        assert getattr(a, name).tobytes() == getattr(b, name).tobytes(), name
