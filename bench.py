@@ -203,10 +203,11 @@ def fgkl_cpu_sample(threads, regions, cells, lost):
 def reference_arm(args, rank, world, pg):
     if rank != 0:
         return
-    from fgkl_b200 import synthetic
+    from oracle import oracle
 
     threads = os.cpu_count() or 1
-    w = synthetic.workload(1, seed=args.seed, regions=args.regions, threads=threads)
+    # The workload generators built into the oracle library: this arm never loads the CUDA library.
+    w = oracle.synth_workload(1, seed=args.seed, regions=args.regions, threads=threads)
     # Calibrate the per-step sample to a few seconds of work on this host.
     regions, cells = cpu_sample_regions(w, 2e10)
     _, _, secs = run_fgkl_cpu(w, regions, threads)
@@ -234,7 +235,7 @@ def reference_arm(args, rank, world, pg):
 
 
 # ---------------------------------------------------------------------------------------------
-# ncu-measured DRAM traffic of the dominant kernel (profiles/, committed summaries)
+# peaks
 # ---------------------------------------------------------------------------------------------
 
 def hbm_peak_gbs():
@@ -250,24 +251,6 @@ def hbm_peak_gbs():
         except (ValueError, OSError):
             pass
     return 6650.0, "fallback 6,650 GB/s copy bandwidth (MEASURED_PEAKS.json absent)"
-
-
-def dominant_traffic(kernel, cells):
-    """DRAM bytes (read + write) of one launch of `kernel` computing `cells` DP cells: the bytes per
-    computed cell ncu measured for that kernel (committed summary
-    profiles/dram_traffic_pairhmm_kernel_uneven.md, a table row `| kernel | bytes per cell | ...`)
-    times the launch's cells."""
-    path = ROOT / "profiles" / "dram_traffic_pairhmm_kernel_uneven.md"
-    if not path.exists():
-        return None
-    for line in path.read_text().splitlines():
-        row = [c.strip() for c in line.strip().strip("|").split("|")]
-        if len(row) >= 2 and row[0].strip("`") == kernel:
-            try:
-                return float(row[1].replace(",", "")) * cells
-            except ValueError:
-                return None
-    return None
 
 
 # ---------------------------------------------------------------------------------------------
@@ -518,7 +501,6 @@ def ours(args, rank, world, local, pg):
                 "forward_cells": dom["forward_cells"], "backward_cells": dom["backward_cells"],
                 "share_of_serialised_time": dom["ms"] / max(1e-9, sum(x["ms"] for x in launches)),
                 "serialised_total_ms": sum(x["ms"] for x in launches)}
-    traffic = dominant_traffic(dominant["kernel"], dom["forward_cells"] + dom["backward_cells"])
 
     # End to end through the C ABI from host buffers: every step plans, stages and uploads its batch,
     # runs it and downloads its results (fgkl_batch_prepare / fgkl_batch_run / fgkl_batch_fetch).
@@ -665,7 +647,9 @@ def ours(args, rank, world, local, pg):
         "computed_gcups": stats.computed_cells / step / 1e9,
         "fallback_pairs": int(stats.fallback_pairs), "rescue_reads": int(stats.rescue_reads),
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                     "traffic": traffic,
+                     # DRAM bytes come from an ncu capture (one pass per launch), which a timed run cannot
+                     # make; they are kept with the profile summaries.
+                     "traffic": None,
                      "peak_source": f"measured FP32 FMA probe on this GPU (scalar {s_tf.value:.1f}, packed {p_tf.value:.1f} "
                                     "TFLOP/s); MEASURED_PEAKS.json has no FP32 figure (it holds HBM and bf16 ones when "
                                     "present)",
@@ -682,16 +666,6 @@ def ours(args, rank, world, local, pg):
                            "form": "one fgkl_batch_compute call at a time, nothing overlapped",
                            "host_phases_last_call": e2e_phases},
                 "bit_identical_to_device_run": identical},
-        "per_call": {"value": per_call, "unit": "GCUPS", "regions": len(pc_regions),
-                     "form": "one fgkl_pairhmm_compute_config call per region from host buffers in the JNI layout, "
-                             "one calling thread",
-                     "threads": {"value": per_call_mt, "threads": pc_threads,
-                                 "form": "the same calls split over 8 calling threads; calls that meet run as one batch "
-                                         "(fgkl_set_call_combining, up to 2 batches in flight)",
-                                 "combined_batches": mt_batches, "combined_requests": mt_requests,
-                                 "alone": {"value": per_call_alone,
-                                           "form": "combining off: each call on its own thread's engine and stream"}}},
-        "batched_over_per_call": value / world / per_call,
         "gpu_launches": planned_launches * args.steps,
         "clocks": clocks.summary(),
     }
@@ -723,6 +697,13 @@ def ours(args, rank, world, local, pg):
         line["cpu_baseline"] = {"value": cells / secs / 1e9, "unit": "GCUPS", "cores": threads, "kind": "port",
                                 "sample": fgkl_cpu_sample(threads, regions, cells, lost),
                                 "max_abs_dlog10_vs_gpu": float(np.max(np.abs(mine - cpu)))}
+    # Last in the line, so that a reader keeping only the end of a long line keeps them.
+    line["per_call"] = {"value": per_call, "unit": "GCUPS", "regions": len(pc_regions),
+                        "form": "one fgkl_pairhmm_compute_config call per region, JNI layout, one thread",
+                        "threads": {"value": per_call_mt, "threads": pc_threads, "combined_batches": mt_batches,
+                                    "combined_requests": mt_requests, "form": "8 threads, concurrent calls combined",
+                                    "alone": {"value": per_call_alone, "form": "8 threads, combining off"}}}
+    line["batched_over_per_call"] = value / world / per_call
     print(json.dumps(line), flush=True)
     barrier(pg, device)
 
@@ -754,12 +735,6 @@ def main():
         ours(args, rank, world, local, pg)
     if pg is not None:
         pg.destroy_process_group()
-    # The result line is out. Leave without the interpreter's teardown: one run in about ten ended
-    # with SIGSEGV during it, after its line was printed, with no GPU fault recorded and no cause
-    # found in this code.
-    sys.stdout.flush()
-    sys.stderr.flush()
-    os._exit(0)
 
 
 if __name__ == "__main__":

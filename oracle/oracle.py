@@ -32,7 +32,8 @@ def build() -> Path:
 def lib():
     global _lib
     if _lib is None:
-        sources = ("pairhmm_oracle.c", "fgkl_cpu.c", "fgkl_cpu_kernel.h", "fgkl_cpu_pd_kernel.h", "Makefile")
+        sources = ("pairhmm_oracle.c", "fgkl_cpu.c", "fgkl_cpu_kernel.h", "fgkl_cpu_pd_kernel.h", "Makefile", "synth_shim.cpp",
+                   "../fgkl_b200/csrc/synthetic.cpp", "../fgkl_b200/csrc/synthetic.h", "../fgkl_b200/csrc/tables.cpp")
         if not LIB_PATH.exists() or LIB_PATH.stat().st_mtime < max((HERE / f).stat().st_mtime for f in sources):
             build()
         L = C.CDLL(str(LIB_PATH))
@@ -64,8 +65,40 @@ def lib():
         L.fc_compute_regions_flags.restype = C.c_int64
         L.fc_compute_regions_flags.argtypes = [_u8p] * 5 + [_i64p, _u8p, _u8p, _i64p, _i64p, _i32p, _i64p, _i32p, _i64p,
                                                             C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _f64p]
+        L.or_synth_config.restype = C.c_void_p
+        L.or_synth_config.argtypes = [C.c_int32, C.c_uint64, C.c_int32, C.c_int32]
+        L.or_synth_arrays.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), _i64p]
+        L.or_synth_free.argtypes = [C.c_void_p]
         _lib = L
     return _lib
+
+
+def synth_workload(which: int, seed: int = 0, regions: int = 0, threads: int = 8):
+    """The benchmark workload `which` (the generators of fgkl_b200/csrc/synthetic.cpp, built into
+    this library), as a ``fgkl_b200.synthetic.Workload``, without loading the CUDA library."""
+    from fgkl_b200.synthetic import Workload
+
+    L = lib()
+    h = L.or_synth_config(which, seed, regions, threads)
+    if not h:
+        raise ValueError(f"no synthetic workload {which}")
+    try:
+        ptrs = (C.c_void_p * 11)()
+        sizes = (C.c_int64 * 5)()
+        L.or_synth_arrays(h, ptrs, sizes)
+        n, nr, nrb, nh, nhb = (int(x) for x in sizes)
+
+        def arr(i, count, dtype):
+            if count == 0 or not ptrs[i]:
+                return np.zeros(0, dtype)
+            return np.ctypeslib.as_array(C.cast(ptrs[i], C.POINTER(np.ctypeslib.as_ctypes_type(dtype))), shape=(count,)).copy()
+
+        return Workload(region_reads=arr(0, n, np.int32), region_haps=arr(1, n, np.int32), bases=arr(2, nrb, np.uint8),
+                        quals=arr(3, nrb, np.uint8), ins_gop=arr(4, nrb, np.uint8), del_gop=arr(5, nrb, np.uint8),
+                        gcp=arr(6, nrb, np.uint8), read_offsets=arr(7, nr + 1, np.int64), hap_bases=arr(8, nhb, np.uint8),
+                        hap_flags=arr(9, nhb, np.uint8) if ptrs[9] else None, hap_offsets=arr(10, nh + 1, np.int64))
+    finally:
+        L.or_synth_free(h)
 
 
 def _u8(b) -> np.ndarray:
