@@ -8,8 +8,10 @@ pairhmm-bench does (crates/pairhmm/src/bin/bench.rs:59, :102).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Under torchrun each rank runs its own batch (seed + rank) on its own GPU: regions are independent,
-so there is no data-path collective (weak scaling); the step time is the max over ranks.
+Under torchrun with N ranks, every rank draws the same batch of N x 4096 regions and partitions it
+by the planner's computed cells (fgkl_b200.shard); each rank runs its part, about 4096 regions, on
+its own GPU. Regions are independent, so there is no data-path collective (weak scaling: the work
+per GPU stays fixed as N grows); the step time is the max over ranks.
 """
 from __future__ import annotations
 
@@ -423,7 +425,16 @@ def ours(args, rank, world, local, pg):
     device = local
     torch.cuda.set_device(device)
     threads = os.cpu_count() or 1
-    w = synthetic.workload(1, seed=args.seed + rank, regions=args.regions, threads=threads)
+    if world == 1:
+        w = synthetic.workload(1, seed=args.seed, regions=args.regions, threads=threads)
+    else:
+        # One batch of world x regions, partitioned by planned cells; this rank runs its part.
+        from fgkl_b200.shard import partition_regions, region_costs
+
+        whole = synthetic.workload(1, seed=args.seed, regions=args.regions * world, threads=threads)
+        part = partition_regions(region_costs(whole), world)[rank]
+        w = whole.subset(part)
+        del whole
     nominal = w.nominal_cells()
     stream = torch.cuda.Stream(device=device)
     cfg = Config(precision=Precision.FLOAT)
@@ -642,7 +653,7 @@ def ours(args, rank, world, local, pg):
                    "forward_cells": int(stats.forward_cells), "backward_cells": int(stats.backward_cells),
                    "prefix_only_cells": int(stats.prefix_only_cells),
                    "l2": f"inputs {w.bases.size * 5 / 2**20:.0f} MiB > L2 126 MiB; L2 also flushed (untimed) between steps",
-                   "parallelism": f"region sharding x{world}, no collective",
+                   "parallelism": f"one batch of {world} x {args.regions} regions partitioned by planned cells over {world} GPU(s), no collective",
                    "launch_tuning": tuning},
         "computed_gcups": stats.computed_cells / step / 1e9,
         "fallback_pairs": int(stats.fallback_pairs), "rescue_reads": int(stats.rescue_reads),

@@ -158,6 +158,8 @@ def lib() -> C.CDLL:
     L.fgkl_set_call_combining.restype = C.c_int
     L.fgkl_call_combining_stats.argtypes = [C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
     L.fgkl_call_combining_stats.restype = C.c_int
+    L.fgkl_plan_region_cells.argtypes = [C.POINTER(Batch), C.POINTER(Config), C.POINTER(C.c_uint64)]
+    L.fgkl_plan_region_cells.restype = C.c_int
     L.fgkl_set_allocation_limit.argtypes = [C.c_int64]
     L.fgkl_set_allocation_limit.restype = C.c_int64
     L.fgkl_backend.restype = C.c_char_p
@@ -218,7 +220,7 @@ EXPORTED = [
     "fgkl_set_call_combining", "fgkl_call_combining_stats", "fgkl_set_allocation_limit", "fgkl_backend", "fgkl_last_error", "fgkl_context_create", "fgkl_context_destroy", "fgkl_batch_prepare",
     "fgkl_batch_run", "fgkl_batch_fetch", "fgkl_batch_compute", "fgkl_batch_output_len", "fgkl_context_autotune",
     "fgkl_context_set_tuning", "fgkl_context_get_tuning", "fgkl_synth_config",
-    "fgkl_synth_reference_region", "fgkl_synth_view", "fgkl_synth_free", "fgkl_plan_describe", "fgkl_plan_sweeps", "fgkl_probe_fp32_tflops",
+    "fgkl_synth_reference_region", "fgkl_synth_view", "fgkl_synth_free", "fgkl_plan_describe", "fgkl_plan_region_cells", "fgkl_plan_sweeps", "fgkl_probe_fp32_tflops",
     "fgkl_pairhmm_compute_device_noalloc", "fgkl_context_profile", "fgkl_batch_launch_profile", "fgkl_adjoint_prepare", "fgkl_adjoint_run", "fgkl_adjoint_fetch",
     "fgkl_adjoint_compute", "fgkl_adjoint_output_len", "fgkl_adjoint_grad_len", "fgkl_pd_row_states", "fgkl_pd_plan_describe", "fgkl_pd_match_accepts",
 ]

@@ -800,6 +800,36 @@ int fgkl_plan_describe(const uint8_t* hap_bases, const int32_t* hap_offsets, int
   }
 }
 
+int fgkl_plan_region_cells(const fgkl_batch* b, const fgkl_config* config, uint64_t* cells) {
+  t_error.clear();
+  if (!b || !config || (b->num_regions > 0 && (!cells || !b->region_reads || !b->region_haps || !b->read_offsets || !b->hap_offsets)))
+    return set_error(FGKL_E_INVALID_ARGUMENT, "null argument");
+  try {
+    fgkl::BatchInput in;
+    in.num_regions = b->num_regions;
+    in.region_reads = b->region_reads;
+    in.region_haps = b->region_haps;
+    in.bases = b->bases;
+    in.quals = b->quals;
+    in.ins = b->ins_gop;
+    in.del = b->del_gop;
+    in.gcp = b->gcp;
+    in.read_off = b->read_offsets;
+    in.hap_bases = b->hap_bases;
+    in.hap_flags = b->hap_flags;
+    in.hap_off = b->hap_offsets;
+    fgkl::EngineConfig ec;
+    ec.double_precision = config->double_precision != 0;
+    ec.double_fallback = config->double_fallback != 0;
+    ec.share_suffixes = config->share_suffixes != 0;
+    std::string err;
+    const int rc = fgkl::plan_region_cells(in, ec, cells, &err);
+    return rc ? set_error(rc, err) : FGKL_OK;
+  } catch (const std::bad_alloc&) {
+    return set_error(FGKL_E_OUT_OF_MEMORY, "host memory allocation failed");
+  }
+}
+
 // The sweeps of a plan: per sweep (hap, resume, need, start, first write, write count) in
 // `sweeps` (6 ints each) and the (depth, node) writes in `writes` (2 ints each).
 int fgkl_plan_sweeps(const uint8_t* hap_bases, const int32_t* hap_offsets, int32_t num_haps, int32_t* sweeps, int32_t max_sweeps,

@@ -342,6 +342,42 @@ class Helper {
 };
 }  // namespace
 
+int plan_region_cells(const BatchInput& in, const EngineConfig& cfg, uint64_t* cells, std::string* error) {
+  const int N = in.num_regions;
+  if (N < 0) return (*error = "negative region count", FGKL_E_INVALID_ARGUMENT);
+  std::vector<int64_t> first_read(N + 1, 0), first_hap(N + 1, 0);
+  for (int g = 0; g < N; ++g) {
+    if (in.region_reads[g] < 0 || in.region_haps[g] < 0) return (*error = "negative region size", FGKL_E_INVALID_ARGUMENT);
+    first_read[g + 1] = first_read[g] + in.region_reads[g];
+    first_hap[g + 1] = first_hap[g] + in.region_haps[g];
+  }
+  for (int64_t h = 0; h < first_hap[N]; ++h)
+    if (in.hap_off[h + 1] - in.hap_off[h] <= 0) return (*error = "haplotype " + std::to_string(h) + " has no bases", FGKL_E_EMPTY_HAPLOTYPE);
+  for (int64_t r = 0; r < first_read[N]; ++r)
+    if (in.read_off[r + 1] - in.read_off[r] <= 0) return (*error = "read " + std::to_string(r) + " has no bases", FGKL_E_EMPTY_READ);
+  // The cells each region's tasks compute (the counts prepare() gives the launches): reads of one
+  // block walk the region's program (forward and backward columns); strip-mined reads and the reads
+  // of byte-compared PD regions run each distinct haplotype unshared.
+  parallel_for(N, host_threads(), [&](int64_t gi) {
+    const int g = static_cast<int>(gi);
+    RegionPlan rp;
+    plan_region(in, g, first_read[g], first_hap[g], cfg.share_suffixes, rp);
+    uint64_t distinct_len = 0;
+    for (int k = 0; k < static_cast<int>(rp.haps.size()); ++k)
+      if (rp.haps[k].src == k) distinct_len += static_cast<uint64_t>(rp.haps[k].len);
+    uint64_t c = 0;
+    for (int64_t r = first_read[g]; r < first_read[g + 1]; ++r) {
+      const uint64_t len = static_cast<uint64_t>(in.read_off[r + 1] - in.read_off[r]);
+      if (rp.generic || len > static_cast<uint64_t>(kMaxBlockRead))
+        c += len * distinct_len;
+      else
+        c += len * (rp.prog.fwd_columns + rp.prog.bwd_columns);
+    }
+    cells[g] = rp.error.empty() ? c : 0;
+  });
+  return FGKL_OK;
+}
+
 int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
   DeviceGuard device_guard(device_);
   const auto t_start = std::chrono::steady_clock::now();

@@ -77,6 +77,10 @@ struct BatchStats {
   double host_fetch_ms = 0;         // waiting for the kernels and copying results out
 };
 
+// Per region, the DP cells a batched run of `in` computes (forward and backward, as the planner
+// emits them): the cost to balance when regions are split across devices. Host only.
+int plan_region_cells(const BatchInput& in, const EngineConfig& cfg, uint64_t* cells, std::string* error);
+
 class Engine {
  public:
   explicit Engine(int device, cudaStream_t stream = nullptr);

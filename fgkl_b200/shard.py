@@ -1,22 +1,37 @@
-"""Region sharding across GPUs (one process per GPU).
+"""Region sharding across GPUs: one batch split over several devices.
 
 Regions are independent and nothing is exchanged between them (fgkl docs/design.md:37-39), so a
-batch splits across ranks with no data-path collective: each rank plans, uploads and runs its own
-regions on its own GPU. `partition_regions` balances ranks greedily by estimated cost (longest
-first onto the least-loaded rank); `assemble` puts each rank's outputs back in the caller's region
-order. Timing is the max over ranks; the only collectives are that max and the optional gather of
-results, neither on the hot path.
+batch splits across devices with no data-path collective: each device plans, uploads and runs its
+own regions. `region_costs` asks the planner for the DP cells each region's batched run computes
+(prefix and suffix sharing included); `partition_regions` balances devices greedily by that cost
+(longest first onto the least-loaded device); `assemble` puts each device's outputs back in the
+caller's region order. Two ways to use it:
+
+- `MultiDeviceContext`: one process drives several devices (one batch context each).
+- one process per GPU (torchrun): every rank partitions the same batch and runs its own part;
+  timing is the max over ranks, and the only collectives are that max and the optional gather of
+  results, neither on the hot path.
 """
 from __future__ import annotations
 
+import ctypes as C
 from typing import Sequence
 
 import numpy as np
 
 
-def region_costs(workload) -> np.ndarray:
-    """Per-region cost estimate: nominal cells (Σ read lengths x Σ haplotype lengths)."""
-    return workload.region_nominal_cells().astype(np.float64)
+def region_costs(workload, config=None) -> np.ndarray:
+    """Per region, the DP cells a batched run computes (fgkl_plan_region_cells; host only)."""
+    from . import _lib
+    from .pairhmm import Config, _check
+
+    cells = np.zeros(workload.num_regions, np.uint64)
+    if workload.num_regions == 0:
+        return cells.astype(np.float64)
+    b = workload.as_batch()
+    cfg = (config or Config())._c()
+    _check(_lib.lib().fgkl_plan_region_cells(C.byref(b), C.byref(cfg), cells.ctypes.data_as(C.POINTER(C.c_uint64))))
+    return cells.astype(np.float64)
 
 
 def partition_regions(costs: Sequence[float], world: int) -> list[list[int]]:
@@ -64,3 +79,33 @@ def max_over_ranks(value: float, dist=None, device: str = "cpu") -> float:
     t = torch.tensor([value], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+class MultiDeviceContext:
+    """One batch over several devices from one process: regions partitioned by planned cells, one
+    batch context (engine, streams, CUDA graph) per device, each part planned and launched before the
+    next is planned, results reassembled in the caller's order. `devices` may repeat a device (two
+    contexts sharing it)."""
+
+    def __init__(self, devices: Sequence[int]):
+        from .pairhmm import BatchContext
+
+        if not devices:
+            raise ValueError("at least one device")
+        self.devices = list(devices)
+        self.contexts = [BatchContext(d) for d in self.devices]
+        self.partition: list[list[int]] = []
+
+    def compute(self, workload, config=None) -> np.ndarray:
+        self.partition = partition_regions(region_costs(workload, config), len(self.contexts))
+        parts = [rank_workload(workload, p) for p in self.partition]
+        for ctx, w in zip(self.contexts, parts):
+            if w.num_regions:
+                ctx.prepare(w, config)
+                ctx.run()
+        outputs = [ctx.fetch()[0] if w.num_regions else np.zeros(0) for ctx, w in zip(self.contexts, parts)]
+        return assemble(workload, self.partition, outputs)
+
+    def close(self) -> None:
+        for ctx in self.contexts:
+            ctx.close()

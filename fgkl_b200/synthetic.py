@@ -88,8 +88,32 @@ class Workload:
         return np.r_[0, np.cumsum(sizes)]
 
     def subset(self, regions: Sequence[int] | range) -> "Workload":
-        parts = [self.region(g) for g in regions]
-        return from_regions(parts)
+        """The regions `regions`, in that order, as a workload of their own (array slices)."""
+        regions = [int(g) for g in regions]
+        rr = self.region_reads.astype(np.int64)
+        rh = self.region_haps.astype(np.int64)
+        first_read = np.r_[0, np.cumsum(rr)]
+        first_hap = np.r_[0, np.cumsum(rh)]
+        read_idx = [np.arange(first_read[g], first_read[g + 1]) for g in regions]
+        hap_idx = [np.arange(first_hap[g], first_hap[g + 1]) for g in regions]
+        reads = np.concatenate(read_idx) if read_idx else np.zeros(0, np.int64)
+        haps = np.concatenate(hap_idx) if hap_idx else np.zeros(0, np.int64)
+
+        def gather(data, offsets, idx):
+            lo, hi = offsets[idx], offsets[idx + 1]
+            new_off = np.r_[0, np.cumsum(hi - lo)].astype(np.int64)
+            if idx.size == 0:
+                return data[:0].copy(), new_off
+            pos = np.repeat(lo - new_off[:-1], hi - lo) + np.arange(int(new_off[-1]))
+            return data[pos], new_off
+
+        cols = []
+        for a in (self.bases, self.quals, self.ins_gop, self.del_gop, self.gcp):
+            col, roff = gather(a, self.read_offsets, reads)
+            cols.append(col)
+        hb, hoff = gather(self.hap_bases, self.hap_offsets, haps)
+        hf = gather(self.hap_flags, self.hap_offsets, haps)[0] if self.hap_flags is not None else None
+        return Workload(self.region_reads[regions].copy(), self.region_haps[regions].copy(), *cols, roff, hb, hf, hoff)
 
 
 from typing import Sequence  # noqa: E402

@@ -351,6 +351,10 @@ void fgkl_synth_free(fgkl_synth* s);
 int fgkl_plan_describe(const uint8_t* hap_bases, const int32_t* hap_offsets, int32_t num_haps, int32_t share_suffixes,
                        int32_t* order, int32_t* lcp, uint8_t* dup, int32_t* cut_column, int32_t* cut_node,
                        int32_t* num_sweeps, int32_t* num_nodes, uint64_t columns[3]);
+/* Per region of `batch`, the DP cells (forward + backward) a batched run computes under `config`, as
+ * the planner emits them (host only, no device): the cost by which regions are balanced across
+ * devices (fgkl runs regions independently, docs/design.md:37-39). `cells` has num_regions entries. */
+int fgkl_plan_region_cells(const fgkl_batch* batch, const fgkl_config* config, uint64_t* cells);
 /* Backward sweeps: 6 ints each (hap, resume, need, start, first write, write count) and the
  * (depth, node) writes, 2 ints each. */
 int fgkl_plan_sweeps(const uint8_t* hap_bases, const int32_t* hap_offsets, int32_t num_haps, int32_t* sweeps,
