@@ -37,6 +37,7 @@ WORKLOAD = ("batched uneven PairHMM: 4096 regions, 8-256 reads (75% of length 15
             "haplotypes (longest read + 50-400 bases), FP32 + FP64 recomputation, prefix+suffix sharing")
 FLOP_FORWARD = 12  # 4 FMUL + 4 FFMA per forward cell (fgkl kernel.rs:1011-1013)
 FLOP_BACKWARD = 11  # 3 FMUL + 4 FFMA per backward cell (kernel.rs:1080-1088)
+FLOP_ADJOINT = 40   # adjoint cell: backward 11 + forward 11 + gradient terms 18
 L2_BYTES = 126 * 1024 * 1024
 
 
@@ -387,27 +388,24 @@ def extra_configs(args, device, stream, flush, threads, which=("c2", "c3", "c4")
             for k in range(4):
                 g_ref[k, a - lo:b - lo] += gr[k]
     ours_g = [r.gap_open_ins, r.gap_open_del, r.gap_continuation, r.base_error]
-    # HBM roofline: the adjoint stores every column's backward record (BM, BX, BY rows of a lane,
-    # padded to 16 bytes) and reads it back in the forward sweep, 2 x (hap length + 1) x 32 x record
-    # bytes per (read, haplotype) pair; its FP32 and FP64 arithmetic take a few ms of the step.
-    rl = np.diff(w.read_offsets)
-    rec = ((3 * -(-rl // 31) + 3) // 4) * 4 * 4
-    hl = np.diff(w.hap_offsets) + 1
-    rb = np.add.reduceat(rec, np.concatenate([[0], np.cumsum(w.region_reads)[:-1]]))
-    hb = np.add.reduceat(hl, np.concatenate([[0], np.cumsum(w.region_haps)[:-1]]))
-    adj_bytes = float(2 * 32 * np.sum(rb.astype(np.float64) * hb))
-    hbm_peak, hbm_src = hbm_peak_gbs()
-    adj_gbs = adj_bytes / t / 1e9
+    # FP32 roofline: per cell the backward recurrence (11 FLOP), the forward recurrence (11) and the
+    # gradient terms (18: four products against the backward values, each an FMA into a per-row sum,
+    # plus the prior and sign products). The backward values are recomputed once from checkpoints
+    # (another 11 FLOP a cell, not counted: it is the price of keeping them on chip).
+    s_tf, p_tf, clk = C.c_double(), C.c_double(), C.c_double()
+    _lib.lib().fgkl_probe_fp32_tflops(device, C.byref(s_tf), C.byref(p_tf), C.byref(clk))
+    fp32_peak = max(s_tf.value, p_tf.value)
+    adj_tf = FLOP_ADJOINT * nominal / t / 1e12
     rel = [abs(ours_g[k][lo:hi].sum() - g_ref[k].sum()) / abs(g_ref[k].sum()) for k in range(4)]
     res["c4"] = {"workload": "adjoint: 256 regions x 64 reads (151) x 8 haplotypes (350); gradients of the summed log10 "
                              "likelihood w.r.t. gap-open (ins, del), gap continuation, base error per read position",
                  "regions": w.num_regions, "nominal_gcups": nominal / t / 1e9, "ms_per_step": 1e3 * t, "steps": steps,
-                 "nominal_cells": nominal, "cells_per_pair_visited": "forward + backward sweep each",
+                 "nominal_cells": nominal, "cells_per_pair_visited": "backward sweep twice (checkpoints, then blocks), forward once",
                  "fp64_reads": r.fp64_reads,
                  "max_rel_err_global_gradients_sample": max(rel),
-                 "roofline": {"bound": "hbm", "unit": "GB/s", "achieved": adj_gbs, "peak": hbm_peak,
-                              "frac": adj_gbs / hbm_peak, "algorithmic_bytes_per_step": adj_bytes,
-                              "peak_source": hbm_src},
+                 "roofline": {"bound": "fp32", "unit": "TFLOP/s", "achieved": adj_tf, "peak": fp32_peak,
+                              "frac": adj_tf / fp32_peak, "flop_per_cell": FLOP_ADJOINT,
+                              "peak_source": "measured FP32 FMA probe on this GPU"},
                  "accuracy_sample": "region 0 against the FP64 scalar adjoint (summed gradients)"}
     actx.close()
     return res
