@@ -32,7 +32,7 @@ def build() -> Path:
 def lib():
     global _lib
     if _lib is None:
-        sources = ("pairhmm_oracle.c", "fgkl_cpu.c", "fgkl_cpu_kernel.h", "fgkl_cpu_pd_kernel.h", "Makefile", "synth_shim.cpp",
+        sources = ("pairhmm_oracle.c", "sw_oracle.c", "fgkl_cpu.c", "fgkl_cpu_kernel.h", "fgkl_cpu_pd_kernel.h", "Makefile", "synth_shim.cpp",
                    "../fgkl_b200/csrc/synthetic.cpp", "../fgkl_b200/csrc/synthetic.h", "../fgkl_b200/csrc/tables.cpp")
         if not LIB_PATH.exists() or LIB_PATH.stat().st_mtime < max((HERE / f).stat().st_mtime for f in sources):
             build()
@@ -65,6 +65,9 @@ def lib():
         L.fc_compute_regions_flags.restype = C.c_int64
         L.fc_compute_regions_flags.argtypes = [_u8p] * 5 + [_i64p, _u8p, _u8p, _i64p, _i64p, _i32p, _i64p, _i32p, _i64p,
                                                             C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _f64p]
+        L.or_sw_align.restype = C.c_int
+        L.or_sw_align.argtypes = [_u8p, C.c_int, _u8p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _u8p,
+                                  C.POINTER(C.c_uint32), C.c_int, C.POINTER(C.c_int32)]
         L.or_synth_config.restype = C.c_void_p
         L.or_synth_config.argtypes = [C.c_int32, C.c_uint64, C.c_int32, C.c_int32]
         L.or_synth_arrays.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), _i64p]
@@ -243,3 +246,21 @@ def adj_gradient(hap: bytes, read_bases: bytes, d_ins, d_del, eps, err):
     ll = lib().or_adj_gradient(_p(h, _u8p), h.size, _p(b, _u8p), b.size, *[_p(a, _f64p) for a in arrs],
                                *[_p(x, _f64p) for x in g])
     return (ll, *g)
+
+
+def sw_align(reference: bytes, alternate: bytes, params, strategy: int) -> tuple[str, int]:
+    """Smith-Waterman as GATK's SmithWatermanJavaAligner (sw_oracle.c): (CIGAR string, offset).
+    `params` = (match, mismatch, gap open, gap extend); strategy 0 SoftClip, 1 Indel, 2 LeadingIndel,
+    3 Ignore."""
+    if not reference or not alternate:
+        raise ValueError("empty sequence")
+    r, a = _u8(reference), _u8(alternate)
+    cap = len(reference) + len(alternate) + 4
+    ops = np.zeros(cap, np.uint8)
+    lens = np.zeros(cap, np.uint32)
+    off = C.c_int32()
+    k = lib().or_sw_align(_p(r, _u8p), r.size, _p(a, _u8p), a.size, *[int(x) for x in params], int(strategy),
+                          _p(ops, _u8p), lens.ctypes.data_as(C.POINTER(C.c_uint32)), cap, C.byref(off))
+    if k < 0 or k > cap:
+        raise ValueError("alignment failed")
+    return "".join(f"{int(lens[e])}{chr(ops[e])}" for e in range(k)), int(off.value)
