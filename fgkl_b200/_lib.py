@@ -24,6 +24,7 @@ FGKL_E_UNSUPPORTED = -8
 FGKL_E_NO_DEVICE = -9
 FGKL_E_CUDA = -10
 FGKL_E_OUT_OF_MEMORY = -11
+FGKL_E_EMPTY_SEQUENCE = -12
 
 u8p = C.POINTER(C.c_uint8)
 i32p = C.POINTER(C.c_int32)
@@ -86,6 +87,16 @@ class Batch(C.Structure):
         ("hap_flags", u8p),
         ("hap_offsets", i64p),
     ]
+
+
+class SwParams(C.Structure):
+    _fields_ = [("match_value", C.c_int32), ("mismatch_penalty", C.c_int32), ("gap_open_penalty", C.c_int32),
+                ("gap_extend_penalty", C.c_int32)]
+
+
+class SwBatch(C.Structure):
+    _fields_ = [("num_pairs", C.c_int64), ("ref_bases", C.POINTER(C.c_uint8)), ("ref_offsets", C.POINTER(C.c_int64)),
+                ("alt_bases", C.POINTER(C.c_uint8)), ("alt_offsets", C.POINTER(C.c_int64))]
 
 
 class Tuning(C.Structure):
@@ -160,6 +171,14 @@ def lib() -> C.CDLL:
     L.fgkl_call_combining_stats.restype = C.c_int
     L.fgkl_plan_region_cells.argtypes = [C.POINTER(Batch), C.POINTER(Config), C.POINTER(C.c_uint64)]
     L.fgkl_plan_region_cells.restype = C.c_int
+    L.fgkl_sw_align.argtypes = [C.POINTER(C.c_uint8), C.c_int64, C.POINTER(C.c_uint8), C.c_int64, C.POINTER(SwParams), C.c_int32,
+                                C.c_char_p, C.c_int64, C.POINTER(C.c_int32)]
+    L.fgkl_sw_align.restype = C.c_int
+    L.fgkl_sw_cigar_capacity.argtypes = [C.POINTER(SwBatch)]
+    L.fgkl_sw_cigar_capacity.restype = C.c_int64
+    L.fgkl_sw_align_batch.argtypes = [C.c_void_p, C.POINTER(SwBatch), C.POINTER(SwParams), C.c_int32, C.POINTER(C.c_uint32),
+                                      C.c_int64, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+    L.fgkl_sw_align_batch.restype = C.c_int
     L.fgkl_set_allocation_limit.argtypes = [C.c_int64]
     L.fgkl_set_allocation_limit.restype = C.c_int64
     L.fgkl_backend.restype = C.c_char_p
@@ -223,4 +242,5 @@ EXPORTED = [
     "fgkl_synth_reference_region", "fgkl_synth_view", "fgkl_synth_free", "fgkl_plan_describe", "fgkl_plan_region_cells", "fgkl_plan_sweeps", "fgkl_probe_fp32_tflops",
     "fgkl_pairhmm_compute_device_noalloc", "fgkl_context_profile", "fgkl_batch_launch_profile", "fgkl_adjoint_prepare", "fgkl_adjoint_run", "fgkl_adjoint_fetch",
     "fgkl_adjoint_compute", "fgkl_adjoint_output_len", "fgkl_adjoint_grad_len", "fgkl_pd_row_states", "fgkl_pd_plan_describe", "fgkl_pd_match_accepts",
+    "fgkl_sw_align", "fgkl_sw_cigar_capacity", "fgkl_sw_align_batch",
 ]

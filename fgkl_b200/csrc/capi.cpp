@@ -15,6 +15,7 @@
 #include "adjoint_engine.h"
 #include "engine.h"
 #include "planner.h"
+#include "sw_engine.h"
 #include "synthetic.h"
 #include "tables.h"
 
@@ -93,6 +94,50 @@ fgkl::Engine* thread_engine(int* rc) {
   }
   *rc = FGKL_OK;
   return te.engine;
+}
+
+// The calling thread's Smith-Waterman engine, pooled and never destroyed like the PairHMM engines.
+struct SwPool {
+  std::mutex mu;
+  std::vector<std::pair<int, fgkl::SwEngine*>> idle;
+};
+SwPool& sw_pool() {
+  static SwPool* pool = new SwPool;
+  return *pool;
+}
+struct ThreadSw {
+  fgkl::SwEngine* engine = nullptr;
+  int device = -1;
+  ~ThreadSw() {
+    if (!engine) return;
+    SwPool& p = sw_pool();
+    std::lock_guard<std::mutex> lock(p.mu);
+    try {
+      p.idle.emplace_back(device, engine);
+    } catch (...) {
+    }
+  }
+};
+fgkl::SwEngine* thread_sw(int* rc) {
+  thread_local ThreadSw ts;
+  if (!ts.engine) {
+    int d = 0;
+    if ((*rc = pick_device(&d)) != FGKL_OK) return nullptr;
+    {
+      SwPool& p = sw_pool();
+      std::lock_guard<std::mutex> lock(p.mu);
+      for (size_t i = 0; i < p.idle.size(); ++i)
+        if (p.idle[i].first == d) {
+          ts.engine = p.idle[i].second;
+          p.idle.erase(p.idle.begin() + static_cast<std::ptrdiff_t>(i));
+          break;
+        }
+    }
+    if (!ts.engine) ts.engine = new fgkl::SwEngine(d);
+    ts.device = d;
+  }
+  *rc = FGKL_OK;
+  return ts.engine;
 }
 
 // Offset table -> (start, end) checks of crates/jni/src/lib.rs:343-363.
@@ -472,6 +517,7 @@ int noalloc_device(fgkl::NoAllocDevice** out) {
 struct fgkl_context {
   std::unique_ptr<fgkl::Engine> engine;
   std::unique_ptr<fgkl::AdjointEngine> adjoint;  // created on the first adjoint call
+  std::unique_ptr<fgkl::SwEngine> sw;            // created on the first Smith-Waterman call
   // The executable graph of the last batch run. A new batch re-captures its launch sequence and
   // updates this graph in place when the topology allows: destroying an executable graph waits for
   // the whole device, which would stall a caller streaming batches through several contexts.
@@ -970,6 +1016,58 @@ int fgkl_pd_plan_describe(const uint8_t* hap_bases, const uint8_t* hap_flags, co
 
 int fgkl_pd_match_accepts(uint8_t base, uint8_t flag, uint8_t read_base) {
   return fgkl::MatchSet::of(base, flag).accepts(read_base) ? 1 : 0;
+}
+
+int fgkl_sw_align(const uint8_t* ref, int64_t ref_len, const uint8_t* alt, int64_t alt_len, const fgkl_sw_params* params,
+                  int32_t strategy, char* cigar, int64_t cigar_cap, int32_t* offset) try {
+  t_error.clear();
+  if (!params || !cigar || !offset || ref_len < 0 || alt_len < 0 || (ref_len > 0 && !ref) || (alt_len > 0 && !alt))
+    return set_error(FGKL_E_INVALID_ARGUMENT, "null argument or negative length");
+  if (strategy < FGKL_SW_SOFTCLIP || strategy > FGKL_SW_IGNORE)
+    return set_error(FGKL_E_INVALID_ARGUMENT, "unknown overhang strategy code " + std::to_string(strategy));
+  if (ref_len == 0 || alt_len == 0) return set_error(FGKL_E_EMPTY_SEQUENCE, "Smith-Waterman needs non-empty sequences");
+  int rc;
+  fgkl::SwEngine* e = thread_sw(&rc);
+  if (!e) return rc;
+  const int64_t roff[2] = {0, ref_len}, aoff[2] = {0, alt_len};
+  fgkl::SwBatch in{1, ref, roff, alt, aoff};
+  std::vector<uint32_t> elems(static_cast<size_t>(fgkl::sw_cigar_slot(ref_len, alt_len)));
+  int32_t count = 0, off = 0;
+  rc = e->align(in, fgkl::SwScores{params->match_value, params->mismatch_penalty, params->gap_open_penalty, params->gap_extend_penalty},
+                strategy, elems.data(), static_cast<int64_t>(elems.size()), &count, &off);
+  if (rc) return set_error(rc, e->error());
+  std::string text;
+  static const char kOps[] = {'M', 'I', 'D', 'N', 'S'};
+  for (int32_t i = 0; i < count; ++i) {
+    text += std::to_string(elems[i] >> 4);
+    text += kOps[elems[i] & 0xF];
+  }
+  if (static_cast<int64_t>(text.size()) + 1 > cigar_cap)
+    return set_error(FGKL_E_OUTPUT_LENGTH, "the CIGAR string needs " + std::to_string(text.size() + 1) + " bytes");
+  std::memcpy(cigar, text.c_str(), text.size() + 1);
+  *offset = off;
+  return FGKL_OK;
+} catch (const std::bad_alloc&) {
+  return set_error(FGKL_E_OUT_OF_MEMORY, "host memory allocation failed");
+}
+
+int64_t fgkl_sw_cigar_capacity(const fgkl_sw_batch* b) {
+  if (!b || b->num_pairs < 0 || (b->num_pairs > 0 && (!b->ref_offsets || !b->alt_offsets))) return 0;
+  return b->ref_offsets[b->num_pairs] + b->alt_offsets[b->num_pairs] + 2 * b->num_pairs;
+}
+
+int fgkl_sw_align_batch(fgkl_context* ctx, const fgkl_sw_batch* b, const fgkl_sw_params* params, int32_t strategy, uint32_t* cigar,
+                        int64_t cigar_len, int32_t* counts, int32_t* offsets) try {
+  t_error.clear();
+  if (!ctx || !b || !params) return set_error(FGKL_E_INVALID_ARGUMENT, "null argument");
+  if (!ctx->sw) ctx->sw = std::make_unique<fgkl::SwEngine>(ctx->device, ctx->stream);
+  fgkl::SwBatch in{b->num_pairs, b->ref_bases, b->ref_offsets, b->alt_bases, b->alt_offsets};
+  const int rc = ctx->sw->align(in, fgkl::SwScores{params->match_value, params->mismatch_penalty, params->gap_open_penalty,
+                                                   params->gap_extend_penalty},
+                                strategy, cigar, cigar_len, counts, offsets);
+  return rc ? set_error(rc, ctx->sw->error()) : FGKL_OK;
+} catch (const std::bad_alloc&) {
+  return set_error(FGKL_E_OUT_OF_MEMORY, "host memory allocation failed");
 }
 
 int fgkl_pairhmm_compute_device_noalloc(const fgkl_device_region* region, double* out, void* stream) {

@@ -1,0 +1,302 @@
+// sm_100a Smith-Waterman: GATK's SmithWatermanJavaAligner (fgkl crates/smithwaterman/src/reference.rs,
+// lib.rs) over a batch of (reference, alternate) pairs, one warp per pair.
+//
+// Rows are reference positions, on lanes: lane l holds rows l*8+1 .. l*8+8 of a 256-row block, and a
+// longer reference runs as consecutive blocks. Columns are alternate positions, walked as an
+// anti-diagonal wavefront: at step t lane l is at column t - l + 1, and the row above arrives from
+// lane l - 1 by shuffle (lane 0 takes GATK's row 0, or, below the first block, the bottom row the
+// block above stored per column). Per cell (reference.rs:69-110), in integers:
+//   diag  = H(i-1, j-1) + (ref[i] == alt[j] ? match : mismatch)
+//   F(i, j) = max over the vertical gap: F(i-1, j) + extend, or H(i-1, j) + open when that is larger
+//   E(i, j) = the same along the row from (i, j-1)
+//   H = diag when diag >= F and diag >= E, else E when E >= F, else F; never below -1e8.
+// Each cell keeps one traceback byte: the direction (diagonal, horizontal, vertical) and whether its
+// vertical and its horizontal gap extend the neighbour's (not opened here), from which the traceback
+// recovers GATK's gap lengths. The bytes are stored anti-diagonal-major ([block][step][lane][8
+// rows]), so each step's stores are one contiguous 256-byte run. After the fill, lane 0 picks the
+// end cell from the last column and last row with GATK's tie rules and walks back (reference.rs:
+// 113-203). For the SoftClip and Ignore strategies an alternate that occurs exactly in the
+// reference short-circuits to one match (lib.rs:602-607, the last occurrence), found first by the
+// warp testing 32 start positions at a time.
+#include <climits>
+#include <cstdint>
+
+#include "dp_common.cuh"
+#include "sw.cuh"
+
+namespace fgkl {
+
+namespace {
+
+constexpr int kBlockRows = 32 * kSwRows;
+constexpr int kCutoff = -100000000;  // GATK's MATRIX_MIN_CUTOFF
+constexpr int kLowInit = INT_MIN / 2;  // GATK's lowInitValue
+constexpr uint32_t kExtV = 4, kExtH = 8;
+
+__host__ __device__ inline size_t sw_align256(size_t x) { return (x + 255) / 256 * 256; }
+
+// A pair's per-warp scratch.
+struct SwScratch {
+  uint8_t* tb;         // [block][step][lane][8 rows]
+  int32_t* last_col;   // H(i, m), i = 1..n
+  int32_t* last_row;   // H(n, j), j = 1..m
+  int2* carry;         // bottom row of a block: (H, F) per column
+  int m;
+
+  __host__ __device__ static size_t tb_bytes(int64_t n, int64_t m) {
+    return sw_align256(static_cast<size_t>((n + kBlockRows - 1) / kBlockRows) * static_cast<size_t>(m + 31) * kBlockRows);
+  }
+  __host__ __device__ static size_t bytes(int64_t n, int64_t m) {
+    return tb_bytes(n, m) + sw_align256(4 * static_cast<size_t>(n)) + sw_align256(4 * static_cast<size_t>(m)) +
+           sw_align256(8 * static_cast<size_t>(m));
+  }
+  __device__ SwScratch(char* base, int n, int m_) : m(m_) {
+    tb = reinterpret_cast<uint8_t*>(base);
+    last_col = reinterpret_cast<int32_t*>(base + tb_bytes(n, m_));
+    last_row = reinterpret_cast<int32_t*>(base + tb_bytes(n, m_) + sw_align256(4 * static_cast<size_t>(n)));
+    carry = reinterpret_cast<int2*>(base + tb_bytes(n, m_) + sw_align256(4 * static_cast<size_t>(n)) +
+                                    sw_align256(4 * static_cast<size_t>(m_)));
+  }
+  // Traceback byte of cell (i, j), 1 <= i <= n, 1 <= j <= m.
+  __device__ uint32_t at(int i, int j) const {
+    const int b = (i - 1) / kBlockRows, rl = (i - 1) - b * kBlockRows, ln = rl / kSwRows, r = rl % kSwRows;
+    const size_t t = static_cast<size_t>(j - 1) + ln;
+    return tb[((static_cast<size_t>(b) * (m + 31) + t) * 32 + ln) * kSwRows + r];
+  }
+};
+
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, 8) sw_kernel(SwArgs a) {
+  const int lane = threadIdx.x & 31;
+  const int warp = blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+  char* const base = a.scratch + static_cast<size_t>(warp) * a.stride;
+  const bool edge = a.strategy == kSwIndel || a.strategy == kSwLeadingIndel;
+  const int open = a.open, extend = a.extend;
+  // H of row 0 at column x, and of column 0 at row x (reference.rs:50-62).
+  auto edge_val = [&](int x) { return (edge && x >= 1) ? open + (x - 1) * extend : 0; };
+  for (;;) {
+    int task = 0;
+    if (lane == 0) task = atomicAdd(a.counter, 1);
+    task = __shfl_sync(kFull, task, 0);
+    if (task >= a.n_pairs) break;
+    const int k = a.order ? a.order[task] : task;
+    const uint8_t* ref = a.ref + a.ref_off[k];
+    const uint8_t* alt = a.alt + a.alt_off[k];
+    const int n = static_cast<int>(a.ref_off[k + 1] - a.ref_off[k]);
+    const int m = static_cast<int>(a.alt_off[k + 1] - a.alt_off[k]);
+    uint32_t* cig = a.cigar + a.cigar_slot[k];
+
+    // The exact-substring shortcut (reference.rs:15-23): the last occurrence of the alternate.
+    if ((a.strategy == kSwSoftClip || a.strategy == kSwIgnore) && m <= n) {
+      int found = -1;
+      for (int start = n - m; start >= 0; start -= 32) {
+        const int s = start - lane;
+        bool ok = s >= 0;
+        for (int q = 0; ok && q < m; ++q) ok = __ldg(ref + s + q) == __ldg(alt + q);
+        const unsigned hits = __ballot_sync(kFull, ok);
+        if (hits) {
+          found = start - (__ffs(hits) - 1);
+          break;
+        }
+      }
+      if (found >= 0) {
+        if (lane == 0) {
+          cig[0] = (static_cast<uint32_t>(m) << 4) | kSwOpM;
+          a.count[k] = 1;
+          a.offset[k] = found;
+        }
+        __syncwarp();
+        continue;
+      }
+    }
+
+    // The fill, one row block after another.
+    SwScratch sc(base, n, m);
+    const int blocks = (n + kBlockRows - 1) / kBlockRows;
+    for (int b = 0; b < blocks; ++b) {
+      const int top = b * kBlockRows + lane * kSwRows + 1;  // the lane's first row (1-based)
+      int rb[kSwRows], H[kSwRows], E[kSwRows];
+#pragma unroll
+      for (int r = 0; r < kSwRows; ++r) {
+        rb[r] = top + r <= n ? static_cast<int>(__ldg(ref + top + r - 1)) : -1;
+        H[r] = 0;
+        E[r] = kLowInit;
+      }
+      int dH = 0;                  // H of the row above at the previous column (the top row's diagonal)
+      int bH = 0, bF = kLowInit;   // this lane's bottom row at its last column, for the lane below
+      uint8_t* tbb = sc.tb + static_cast<size_t>(b) * (m + 31) * kBlockRows;
+      for (int t = 0; t < m + 31; ++t) {
+        const int j = t - lane + 1;
+        int uH = __shfl_up_sync(kFull, bH, 1), uF = __shfl_up_sync(kFull, bF, 1);
+        const bool active = j >= 1 && j <= m;
+        if (lane == 0) {
+          if (b == 0) {
+            uH = edge_val(j);
+            uF = kLowInit;
+          } else if (active) {
+            const int2 c = sc.carry[j - 1];
+            uH = c.x;
+            uF = c.y;
+          }
+        }
+        if (j == 1) {
+          // Column 0: GATK's edge values, no horizontal gap yet.
+#pragma unroll
+          for (int r = 0; r < kSwRows; ++r) {
+            H[r] = edge_val(top + r);
+            E[r] = kLowInit;
+          }
+          dH = edge_val(top - 1);
+        }
+        uint32_t lo = 0, hi = 0;
+        if (active) {
+          const int ab = __ldg(alt + j - 1);
+          int upH = uH, upF = uF, dg = dH;
+#pragma unroll
+          for (int r = 0; r < kSwRows; ++r) {
+            const int sd = dg + (rb[r] == ab ? a.match : a.mismatch);
+            const int fe = upF + extend, fo = upH + open;
+            const bool vreset = fo > fe;
+            const int F = vreset ? fo : fe;
+            const int ee = E[r] + extend, eo = H[r] + open;
+            const bool hreset = eo > ee;
+            E[r] = hreset ? eo : ee;
+            int h;
+            uint32_t dir;
+            if (sd >= F && sd >= E[r]) {
+              h = sd;
+              dir = 0;
+            } else if (E[r] >= F) {
+              h = E[r];
+              dir = 1;
+            } else {
+              h = F;
+              dir = 2;
+            }
+            h = h > kCutoff ? h : kCutoff;
+            const uint32_t byte = dir | (vreset ? 0u : kExtV) | (hreset ? 0u : kExtH);
+            if (r < 4)
+              lo |= byte << (8 * r);
+            else
+              hi |= byte << (8 * (r - 4));
+            dg = H[r];
+            H[r] = h;
+            upH = h;
+            upF = F;
+            if (top + r == n) sc.last_row[j - 1] = h;
+            if (j == m && top + r <= n) sc.last_col[top + r - 1] = h;
+          }
+          bH = upH;
+          bF = upF;
+          if (lane == 31 && b + 1 < blocks) sc.carry[j - 1] = make_int2(bH, bF);
+        }
+        dH = uH;
+        *reinterpret_cast<uint2*>(tbb + (static_cast<size_t>(t) * 32 + lane) * kSwRows) = make_uint2(lo, hi);
+      }
+      __syncwarp();
+    }
+    __threadfence_block();
+    __syncwarp();
+
+    // End cell and traceback (reference.rs:113-203), lane 0.
+    if (lane == 0) {
+      int p1 = 0, p2 = m, seg = 0;
+      int best = INT_MIN;
+      if (a.strategy == kSwIndel) {
+        p1 = n;
+      } else {
+        for (int i = 1; i <= n; ++i) {
+          const int cur = sc.last_col[i - 1];
+          if (cur >= best) {
+            p1 = i;
+            best = cur;
+          }
+        }
+        if (a.strategy != kSwLeadingIndel) {
+          for (int j = 1; j <= m; ++j) {
+            const int cur = sc.last_row[j - 1];
+            if (cur > best || (cur == best && abs(n - j) < abs(p1 - p2))) {
+              p1 = n;
+              p2 = j;
+              best = cur;
+              seg = m - j;
+            }
+          }
+        }
+      }
+      // Elements last to first, reversed at the end.
+      int e = 0;
+      if (seg > 0 && a.strategy == kSwSoftClip) {
+        cig[e++] = (static_cast<uint32_t>(seg) << 4) | kSwOpS;
+        seg = 0;
+      }
+      uint32_t state = kSwOpM;
+      do {
+        const uint32_t byte = sc.at(p1, p2);
+        const uint32_t dir = byte & 3u;
+        uint32_t next;
+        int step = 1;
+        if (dir == 2) {
+          next = kSwOpD;
+          // GATK's gap length: one more than the run of extending cells above (row 1 always opens).
+          for (int q = p1; q > 1 && (sc.at(q, p2) & kExtV); --q) ++step;
+          p1 -= step;
+        } else if (dir == 1) {
+          next = kSwOpI;
+          for (int q = p2; q > 1 && (sc.at(p1, q) & kExtH); --q) ++step;
+          p2 -= step;
+        } else {
+          next = kSwOpM;
+          p1 -= 1;
+          p2 -= 1;
+        }
+        if (next == state) {
+          seg += step;
+        } else {
+          if (seg > 0) cig[e++] = (static_cast<uint32_t>(seg) << 4) | state;
+          seg = step;
+          state = next;
+        }
+      } while (p1 > 0 && p2 > 0);
+      int off = 0;
+      if (a.strategy == kSwSoftClip) {
+        cig[e++] = (static_cast<uint32_t>(seg) << 4) | state;
+        if (p2 > 0) cig[e++] = (static_cast<uint32_t>(p2) << 4) | kSwOpS;
+        off = p1;
+      } else if (a.strategy == kSwIgnore) {
+        cig[e++] = (static_cast<uint32_t>(seg + p2) << 4) | state;
+        off = p1 - p2;
+      } else {
+        cig[e++] = (static_cast<uint32_t>(seg) << 4) | state;
+        if (p1 > 0)
+          cig[e++] = (static_cast<uint32_t>(p1) << 4) | kSwOpD;
+        else if (p2 > 0)
+          cig[e++] = (static_cast<uint32_t>(p2) << 4) | kSwOpI;
+      }
+      for (int x = 0, y = e - 1; x < y; ++x, --y) {
+        const uint32_t tmp = cig[x];
+        cig[x] = cig[y];
+        cig[y] = tmp;
+      }
+      a.count[k] = e;
+      a.offset[k] = off;
+    }
+    __syncwarp();
+  }
+}
+
+}  // namespace
+
+size_t sw_scratch_bytes(int64_t ref_len, int64_t alt_len) { return SwScratch::bytes(ref_len, alt_len); }
+
+void sw_occupancy(int* blocks_per_sm, int* threads_per_block) {
+  *threads_per_block = kWarpsPerBlock * 32;
+  static std::atomic<int> cache[kMaxDevices];
+  *blocks_per_sm = resident_blocks(sw_kernel, 0, kWarpsPerBlock * 32, cache);
+}
+
+cudaError_t sw_launch(int blocks, const SwArgs& a, cudaStream_t stream) {
+  sw_kernel<<<blocks, kWarpsPerBlock * 32, 0, stream>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace fgkl

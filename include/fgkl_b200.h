@@ -36,6 +36,7 @@ extern "C" {
 #define FGKL_E_NO_DEVICE (-9)                   /* no CUDA device, or not an sm_100 part */
 #define FGKL_E_CUDA (-10)                       /* CUDA runtime error (message in fgkl_last_error) */
 #define FGKL_E_OUT_OF_MEMORY (-11)              /* a device or page-locked host allocation failed; the caller may retry smaller */
+#define FGKL_E_EMPTY_SEQUENCE (-12)             /* Smith-Waterman: fgkl_smithwaterman::Error::EmptySequence */
 
 /* How to compute (crates/pairhmm/src/lib.rs:211-238). */
 typedef struct fgkl_config {
@@ -275,6 +276,48 @@ int fgkl_adjoint_compute(fgkl_context* ctx, const fgkl_adjoint_batch* batch, int
                          double* grad_base_error, int64_t grad_len, uint64_t* fp64_reads);
 int64_t fgkl_adjoint_output_len(const fgkl_context* ctx);
 int64_t fgkl_adjoint_grad_len(const fgkl_context* ctx);
+
+/* ---- Smith-Waterman (crates/smithwaterman: GATK's SmithWatermanJavaAligner) ----
+ *
+ * Alignments identical to GATK's (fgkl reference.rs:9-203): integer affine-gap scores, ties resolved
+ * in favour of the diagonal, then the insertion, then the deletion, and GATK's overhang strategies.
+ * CIGAR elements are packed as in BAM: length << 4 | operation, with M = 0, I = 1, D = 2, S = 4, in
+ * alternate order. `offset` is GATK's alignmentOffset. Both sequences must be non-empty
+ * (FGKL_E_EMPTY_SEQUENCE); an unknown strategy is FGKL_E_INVALID_ARGUMENT. */
+#define FGKL_SW_SOFTCLIP 0      /* SWOverhangStrategy codes as FgklSmithWaterman numbers them (jni/src/lib.rs:290-296) */
+#define FGKL_SW_INDEL 1
+#define FGKL_SW_LEADING_INDEL 2
+#define FGKL_SW_IGNORE 3
+
+/* SWParameters (crates/smithwaterman/src/lib.rs:42-66): a positive match value, negative penalties. */
+typedef struct fgkl_sw_params {
+  int32_t match_value;
+  int32_t mismatch_penalty;
+  int32_t gap_open_penalty;
+  int32_t gap_extend_penalty;
+} fgkl_sw_params;
+
+/* A batch of (reference, alternate) pairs, each side concatenated with num_pairs + 1 offsets. */
+typedef struct fgkl_sw_batch {
+  int64_t num_pairs;
+  const uint8_t* ref_bases;
+  const int64_t* ref_offsets;
+  const uint8_t* alt_bases;
+  const int64_t* alt_offsets;
+} fgkl_sw_batch;
+
+/* The analogue of FgklSmithWaterman.alignNative (crates/jni/src/lib.rs:271-313): one pair on the
+ * calling thread's engine. Writes the CIGAR string, NUL-terminated, into `cigar` (`cigar_cap` bytes,
+ * FGKL_E_OUTPUT_LENGTH when short) and the offset into *offset. */
+int fgkl_sw_align(const uint8_t* ref, int64_t ref_len, const uint8_t* alt, int64_t alt_len, const fgkl_sw_params* params,
+                  int32_t strategy, char* cigar, int64_t cigar_cap, int32_t* offset);
+/* Elements a batch's CIGAR array must hold: Σ over pairs of (reference + alternate length + 2). */
+int64_t fgkl_sw_cigar_capacity(const fgkl_sw_batch* batch);
+/* The batched form on a context (its device and stream): every pair in one persistent launch, the
+ * costliest first. Pair k's elements start at Σ_{j<k} (ref_j + alt_j + 2) in `cigar`, counts[k] of
+ * them; offsets[k] its offset. Synchronous. */
+int fgkl_sw_align_batch(fgkl_context* ctx, const fgkl_sw_batch* batch, const fgkl_sw_params* params, int32_t strategy,
+                        uint32_t* cigar, int64_t cigar_len, int32_t* counts, int32_t* offsets);
 
 /* ---- allocation-free form (no counterpart in the reference) ----
  *

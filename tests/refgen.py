@@ -42,3 +42,34 @@ def edited(rng: Rng, alphabet: bytes, base: bytes) -> bytes:
 
 def reference_like(rng: Rng, alphabet: bytes, n: int) -> bytes:
     return bytes(alphabet[rng.below(len(alphabet))] for _ in range(n))
+
+
+def related_pair(rng: Rng, ref_len: int, alt_len: int) -> tuple[bytes, bytes]:
+    """A reference and an edited copy of a window of it, like a haplotype or a read: fgkl's
+    Smith-Waterman test generator (crates/smithwaterman/src/lib.rs:773-807), draw for draw."""
+    reference = bytes(rng.base() for _ in range(ref_len))
+    start = rng.below(max(ref_len - alt_len, 0) + 1)
+    alt = bytearray(reference[start:min(start + alt_len, ref_len)])
+    for _ in range(rng.below(4)):
+        if not alt:
+            break
+        pos = rng.below(len(alt))
+        kind = rng.below(3)
+        if kind == 0:
+            alt[pos] = rng.base()
+        elif kind == 1:
+            ins = bytes(rng.base() for _ in range(1 + rng.below(6)))
+            alt[pos:pos] = ins
+        else:
+            end = min(pos + 1 + rng.below(6), len(alt))
+            if len(alt) > end - pos:
+                del alt[pos:end]
+    if rng.chance(0.3):
+        extra = bytes(rng.base() for _ in range(1 + rng.below(20)))
+        if rng.chance(0.5):
+            alt[0:0] = extra
+        else:
+            alt.extend(extra)
+    if not alt:
+        alt.append(ord("A"))
+    return reference, bytes(alt)

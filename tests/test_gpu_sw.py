@@ -1,0 +1,111 @@
+"""GPU Smith-Waterman against the oracle (oracle/sw_oracle.c, GATK's SmithWatermanJavaAligner as fgkl
+restates it in crates/smithwaterman/src/reference.rs), through the C ABI.
+
+Restates fgkl's own Smith-Waterman tests (crates/smithwaterman/src/lib.rs:854-1065): the known
+answers, random related and unrelated pairs under the three parameter sets and four overhang
+strategies, odd scores, and pairs whose reference spans several 256-row blocks. Alignments are
+integers, so CIGAR and offset must be identical.
+"""
+import pytest
+
+from fgkl_b200 import _lib
+from fgkl_b200.pairhmm import DeviceError
+from fgkl_b200.sw import (ALIGNMENT_TO_BEST_HAPLOTYPE, HAPLOTYPE_TO_REFERENCE, ORIGINAL_DEFAULT, Alignment, OverhangStrategy,
+                          SwParameters, align, align_batch)
+from oracle import oracle as O
+from refgen import Rng, related_pair
+
+pytestmark = pytest.mark.gpu
+
+HAP_TO_REF, READ_TO_HAP, ORIGINAL = HAPLOTYPE_TO_REFERENCE, ALIGNMENT_TO_BEST_HAPLOTYPE, ORIGINAL_DEFAULT
+STRATEGIES = list(OverhangStrategy)
+
+
+def expected(ref, alt, params, strategy):
+    cigar, offset = O.sw_align(ref, alt, (params.match_value, params.mismatch_penalty, params.gap_open_penalty,
+                                          params.gap_extend_penalty), int(strategy))
+    return Alignment(cigar, offset)
+
+
+def check_batch(pairs, params, strategy):
+    got = align_batch(pairs, params, strategy)
+    for k, ((r, a), g) in enumerate(zip(pairs, got)):
+        assert g == expected(r, a, params, strategy), (k, len(r), len(a), strategy, params)
+
+
+def test_exact_substring_short_circuits_for_softclip_and_ignore(gpu):
+    assert align(b"AAACGTACGTAAA", b"ACGTACGT", HAP_TO_REF, OverhangStrategy.SOFTCLIP) == Alignment("8M", 2)
+    assert align(b"ACGTACGTACGT", b"ACGT", HAP_TO_REF, OverhangStrategy.IGNORE).offset == 8
+
+
+def test_simple_indels_are_reported_with_gatk_conventions(gpu):
+    reference = b"NNNNNNNNNNACGTTTGCAAGGCTTAGGCTNNNNNNNNNN"
+    assert align(reference, b"NNNNNNNNNNACGTTTGCGGCTTAGGCTNNNNNNNNNN", HAP_TO_REF, OverhangStrategy.INDEL) == \
+        Alignment("18M2D20M", 0)
+    assert align(reference, b"NNNNNNNNNNACGTTTGCAAGGCTTTTAGGCTNNNNNNNNNN", HAP_TO_REF, OverhangStrategy.INDEL) == \
+        Alignment("23M2I17M", 0)
+
+
+def test_soft_clips_read_bases_beyond_the_reference_ends(gpu):
+    read = b"GGGGACGTACGTAGGCCTTAGCAGGGG"
+    assert align(b"ACGTACGTAGGCCTTAGCA", read, READ_TO_HAP, OverhangStrategy.SOFTCLIP) == Alignment("4S19M4S", 0)
+    padded = b"TTTTTTTTTTACGTACGTAGGCCTTAGCATTTTTTTTTT"
+    assert align(padded, read, READ_TO_HAP, OverhangStrategy.SOFTCLIP).cigar == "4I19M4I"
+
+
+def test_empty_sequences_and_unknown_strategies_are_rejected(gpu):
+    with pytest.raises(DeviceError) as e:
+        align(b"", b"A", HAP_TO_REF, OverhangStrategy.SOFTCLIP)
+    assert e.value.code == _lib.FGKL_E_EMPTY_SEQUENCE
+    with pytest.raises(DeviceError) as e:
+        align(b"A", b"", HAP_TO_REF, OverhangStrategy.INDEL)
+    assert e.value.code == _lib.FGKL_E_EMPTY_SEQUENCE
+    with pytest.raises(DeviceError) as e:
+        align(b"ACGT", b"ACG", HAP_TO_REF, 7)
+    assert e.value.code == _lib.FGKL_E_INVALID_ARGUMENT
+
+
+@pytest.mark.parametrize("strategy", STRATEGIES)
+@pytest.mark.parametrize("params", [HAP_TO_REF, READ_TO_HAP, ORIGINAL], ids=["hap_to_ref", "read_to_hap", "original"])
+def test_matches_the_oracle_on_random_related_sequences(gpu, params, strategy):
+    rng = Rng(7)
+    pairs = []
+    for case in range(200):
+        ref_len, alt_len = (40 + rng.below(300), 20 + rng.below(200)) if case % 2 == 0 else (5 + rng.below(30), 3 + rng.below(30))
+        pairs.append(related_pair(rng, ref_len, alt_len))
+    check_batch(pairs, params, strategy)
+
+
+@pytest.mark.parametrize("strategy", STRATEGIES)
+def test_matches_the_oracle_on_unrelated_sequences(gpu, strategy):
+    rng = Rng(11)
+    pairs = [(bytes(rng.base() for _ in range(5 + rng.below(80))), bytes(rng.base() for _ in range(5 + rng.below(80))))
+             for _ in range(100)]
+    check_batch(pairs, HAP_TO_REF, strategy)
+    check_batch(pairs, READ_TO_HAP, strategy)
+
+
+@pytest.mark.parametrize("strategy", STRATEGIES)
+def test_odd_scores(gpu, strategy):
+    rng = Rng(31)
+    dangling = SwParameters(25, -50, -110, -6)
+    pairs = [related_pair(rng, 40 + rng.below(200), 20 + rng.below(150)) for _ in range(50)]
+    check_batch(pairs, dangling, strategy)
+
+
+@pytest.mark.parametrize("strategy", STRATEGIES)
+def test_references_spanning_several_row_blocks(gpu, strategy):
+    """References of 257 to 1,500 bases run over consecutive 256-row blocks."""
+    rng = Rng(13)
+    pairs = [related_pair(rng, 600, 520), related_pair(rng, 257, 200), related_pair(rng, 1500, 900), related_pair(rng, 513, 40)]
+    r = bytes(rng.base() for _ in range(700))
+    pairs.append((r, bytes(rng.base() for _ in range(700))))  # unrelated: short local alignments deep in the matrix
+    check_batch(pairs, HAP_TO_REF, strategy)
+    check_batch(pairs, READ_TO_HAP, strategy)
+
+
+def test_batch_and_per_call_agree(gpu):
+    rng = Rng(23)
+    pairs = [related_pair(rng, 30 + rng.below(400), 10 + rng.below(300)) for _ in range(40)]
+    batch = align_batch(pairs, READ_TO_HAP, OverhangStrategy.SOFTCLIP)
+    assert batch == [align(r, a, READ_TO_HAP, OverhangStrategy.SOFTCLIP) for r, a in pairs]
