@@ -1,4 +1,4 @@
-/* fgkl_jni.c: fgkl's JNI entry points (crates/jni/src/lib.rs:150-254) over include/fgkl_b200.h. */
+/* fgkl_jni.c: fgkl's JNI entry points (crates/jni/src/lib.rs:150-313) over include/fgkl_b200.h. */
 #include <jni.h>
 #include <stdint.h>
 #include <stdlib.h>
@@ -6,7 +6,8 @@
 
 static void throw_for(JNIEnv* env, int rc) {
   if ((*env)->ExceptionCheck(env)) return;
-  const char* cls = (rc >= FGKL_E_INVALID_ARGUMENT && rc <= FGKL_E_EMPTY_READ) || rc == FGKL_E_UNSUPPORTED
+  const char* cls = (rc >= FGKL_E_INVALID_ARGUMENT && rc <= FGKL_E_EMPTY_READ) || rc == FGKL_E_UNSUPPORTED ||
+                            rc == FGKL_E_EMPTY_SEQUENCE
                         ? "java/lang/IllegalArgumentException" : "java/lang/RuntimeException";
   (*env)->ThrowNew(env, (*env)->FindClass(env, cls), fgkl_last_error());
 }
@@ -81,6 +82,41 @@ JNIEXPORT jobject JNICALL Java_com_fulcrumgenomics_fgkl_pairhmm_FgklPairHmm_back
   return (*env)->NewStringUTF(env, fgkl_backend());
 }
 JNIEXPORT jobject JNICALL Java_com_fulcrumgenomics_fgkl_pdhmm_FgklPdHmm_backendNative(JNIEnv* env, jclass c) {
+  (void)c;
+  return (*env)->NewStringUTF(env, fgkl_backend());
+}
+
+/* FgklSmithWaterman.alignNative (crates/jni/src/lib.rs:271-313): the CIGAR string, with the
+ * alignment offset written to offset[0]. */
+JNIEXPORT jobject JNICALL Java_com_fulcrumgenomics_fgkl_smithwaterman_FgklSmithWaterman_alignNative(
+    JNIEnv* env, jclass cls, jbyteArray reference, jbyteArray alternate, jint match_value, jint mismatch_penalty,
+    jint gap_open, jint gap_extend, jint strategy, jintArray offset) {
+  (void)cls;
+  jsize nr, na;
+  jbyte *r = bytes(env, reference, &nr), *a = bytes(env, alternate, &na);
+  const size_t cap = 16 * ((size_t)nr + (size_t)na + 4);
+  char* cigar = NULL;
+  jobject result = NULL;
+  if (!(*env)->ExceptionCheck(env)) {
+    cigar = malloc(cap);
+    if (!r || !a || !cigar) throw_out_of_memory(env);
+  }
+  if (!(*env)->ExceptionCheck(env)) {
+    const fgkl_sw_params p = {match_value, mismatch_penalty, gap_open, gap_extend};
+    int32_t off = 0;
+    const int rc = fgkl_sw_align((const uint8_t*)r, nr, (const uint8_t*)a, na, &p, strategy, cigar, (int64_t)cap, &off);
+    if (rc != FGKL_OK) {
+      throw_for(env, rc);
+    } else {
+      (*env)->SetIntArrayRegion(env, offset, 0, 1, &off);
+      result = (*env)->NewStringUTF(env, cigar);
+    }
+  }
+  free(r); free(a); free(cigar);
+  return result;
+}
+
+JNIEXPORT jobject JNICALL Java_com_fulcrumgenomics_fgkl_smithwaterman_FgklSmithWaterman_backendNative(JNIEnv* env, jclass c) {
   (void)c;
   return (*env)->NewStringUTF(env, fgkl_backend());
 }

@@ -12,7 +12,7 @@ struct fake_object {
   int kind; /* 1 byte[], 2 int[], 3 double[], 4 class, 5 string */
   jsize len;
   void* data;
-  char name[128];
+  char name[2048];
 };
 
 typedef struct {
@@ -30,7 +30,7 @@ static jboolean exception_check(JNIEnv* env) { return (jboolean)(state(env)->thr
 static jint throw_new(JNIEnv* env, jclass cls, const char* msg) {
   fake_state* s = state(env);
   s->thrown = 1;
-  snprintf(s->cls, sizeof s->cls, "%s", cls ? cls->name : "");
+  snprintf(s->cls, sizeof s->cls, "%.127s", cls ? cls->name : "");
   snprintf(s->msg, sizeof s->msg, "%s", msg ? msg : "");
   return 0;
 }
@@ -54,6 +54,10 @@ static void set_doubles(JNIEnv* env, jdoubleArray a, jsize start, jsize len, con
   state(env)->region_calls++;
   if (len > 0) memcpy((jdouble*)a->data + start, buf, (size_t)len * sizeof(jdouble));
 }
+static void set_ints(JNIEnv* env, jintArray a, jsize start, jsize len, const jint* buf) {
+  (void)env;
+  if (len > 0) memcpy((jint*)a->data + start, buf, (size_t)len * sizeof(jint));
+}
 static jstring new_string(JNIEnv* env, const char* utf) {
   fake_state* s = state(env);
   s->str.kind = 5;
@@ -69,6 +73,8 @@ void Java_com_fulcrumgenomics_fgkl_pdhmm_FgklPdHmm_computeNative(JNIEnv*, jclass
                                                                 jbyteArray, jbyteArray, jintArray, jbyteArray, jbyteArray,
                                                                 jintArray, jboolean, jdoubleArray);
 jobject Java_com_fulcrumgenomics_fgkl_pairhmm_FgklPairHmm_backendNative(JNIEnv*, jclass);
+jobject Java_com_fulcrumgenomics_fgkl_smithwaterman_FgklSmithWaterman_alignNative(JNIEnv*, jclass, jbyteArray, jbyteArray, jint,
+                                                                                  jint, jint, jint, jint, jintArray);
 
 static struct fake_object arr(int kind, const void* data, jsize len) {
   struct fake_object o;
@@ -89,7 +95,7 @@ int harness_compute(const int8_t* bases, int nb, const int8_t* quals, int nq, co
   fake_state s;
   memset(&s, 0, sizeof s);
   struct JNINativeInterface_ fns = {&s, exception_check, throw_new, find_class, array_length,
-                                    get_bytes, get_ints, set_doubles, new_string};
+                                    get_bytes, get_ints, set_doubles, new_string, set_ints};
   JNIEnv env = &fns;
   struct fake_object b = arr(1, bases, nb), q = arr(1, quals, nq), i = arr(1, ins, ni), d = arr(1, del, nd),
                      g = arr(1, gcp, ng), ro = arr(2, roff, nro), hb = arr(1, hap_bases, nhb), hf = arr(1, hap_flags, nhf),
@@ -111,8 +117,28 @@ void harness_backend(char* out, int cap) {
   fake_state s;
   memset(&s, 0, sizeof s);
   struct JNINativeInterface_ fns = {&s, exception_check, throw_new, find_class, array_length,
-                                    get_bytes, get_ints, set_doubles, new_string};
+                                    get_bytes, get_ints, set_doubles, new_string, set_ints};
   JNIEnv env = &fns;
   jobject str = Java_com_fulcrumgenomics_fgkl_pairhmm_FgklPairHmm_backendNative(&env, NULL);
   snprintf(out, (size_t)cap, "%s", str ? str->name : "");
+}
+
+/* Calls FgklSmithWaterman.alignNative; returns 1 if it threw (class and message copied out), else 0
+ * with the CIGAR string in `cigar` and the offset in *offset. */
+int harness_sw_align(const int8_t* ref, int nr, const int8_t* alt, int na, int match, int mismatch, int open, int extend,
+                     int strategy, char* cigar, int cap, int32_t* offset, char* cls, char* msg) {
+  fake_state s;
+  memset(&s, 0, sizeof s);
+  struct JNINativeInterface_ fns = {&s, exception_check, throw_new, find_class, array_length,
+                                    get_bytes, get_ints, set_doubles, new_string, set_ints};
+  JNIEnv env = &fns;
+  int32_t off[1] = {-1};
+  struct fake_object r = arr(1, ref, nr), a = arr(1, alt, na), o = arr(2, off, 1);
+  jobject str = Java_com_fulcrumgenomics_fgkl_smithwaterman_FgklSmithWaterman_alignNative(&env, NULL, &r, &a, match, mismatch,
+                                                                                          open, extend, strategy, &o);
+  snprintf(cigar, (size_t)cap, "%s", str ? str->name : "");
+  *offset = off[0];
+  strcpy(cls, s.cls);
+  strcpy(msg, s.msg);
+  return s.thrown;
 }

@@ -33,6 +33,7 @@ struct JNINativeInterface_ {
   void (*GetIntArrayRegion)(JNIEnv* env, jintArray a, jsize start, jsize len, jint* buf);
   void (*SetDoubleArrayRegion)(JNIEnv* env, jdoubleArray a, jsize start, jsize len, const jdouble* buf);
   jstring (*NewStringUTF)(JNIEnv* env, const char* utf);
+  void (*SetIntArrayRegion)(JNIEnv* env, jintArray a, jsize start, jsize len, const jint* buf);
 };
 
 #define JNIEXPORT __attribute__((visibility("default")))

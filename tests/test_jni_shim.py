@@ -33,7 +33,18 @@ def shim(tmp_path_factory):
                                                       f64, C.c_int, C.c_char_p, C.c_char_p, C.POINTER(C.c_int)]
     L.harness_compute.restype = C.c_int
     L.harness_backend.argtypes = [C.c_char_p, C.c_int]
+    L.harness_sw_align.argtypes = [i8, C.c_int, i8, C.c_int] + [C.c_int] * 5 + [C.c_char_p, C.c_int, i32, C.c_char_p, C.c_char_p]
+    L.harness_sw_align.restype = C.c_int
     return L
+
+
+def sw_call(L, ref: bytes, alt: bytes, params=(10, -15, -30, -5), strategy=0):
+    i8 = C.POINTER(C.c_int8)
+    r, a = np.frombuffer(ref, np.int8).copy(), np.frombuffer(alt, np.int8).copy()
+    cigar, cls, msg, off = C.create_string_buffer(2048), C.create_string_buffer(128), C.create_string_buffer(512), C.c_int32()
+    thrown = L.harness_sw_align(r.ctypes.data_as(i8), r.size, a.ctypes.data_as(i8), a.size, *params, strategy, cigar, 2048,
+                                C.byref(off), cls, msg)
+    return (cls.value.decode(), msg.value.decode()) if thrown else None, cigar.value.decode(), off.value
 
 
 def flat(reads, haps):
@@ -160,3 +171,22 @@ def test_gpu_a_failed_allocation_raises_runtime_exception(gpu, shim):
     exc, out, _ = call(shim, *flat(reads, haps))
     assert exc is None, exc
     assert out.tobytes() == PairHmm(Config(precision=Precision.FLOAT)).compute_log10_likelihoods(reads, haps).tobytes()
+
+
+@pytest.mark.parametrize("ref, alt, strategy", [(b"", b"ACGT", 0), (b"ACGT", b"", 1), (b"ACGT", b"ACG", 9)])
+def test_smith_waterman_input_errors_raise_illegal_argument(shim, ref, alt, strategy):
+    exc, cigar, _ = sw_call(shim, ref, alt, strategy=strategy)
+    assert exc is not None and exc[0] == IAE and exc[1] == _lib.last_error()
+    assert cigar == ""
+
+
+@pytest.mark.gpu
+def test_gpu_smith_waterman_shim_returns_the_abi_alignment(gpu, shim):
+    from fgkl_b200.sw import ALIGNMENT_TO_BEST_HAPLOTYPE, OverhangStrategy, align
+
+    hap = b"ACGTACGTAGGCCTTAGCA"
+    read = b"GGGGACGTACGTAGGCCTTAGCAGGGG"
+    exc, cigar, off = sw_call(shim, hap, read)
+    assert exc is None, exc
+    assert (cigar, off) == ("4S19M4S", 0)
+    assert align(hap, read, ALIGNMENT_TO_BEST_HAPLOTYPE, OverhangStrategy.SOFTCLIP).cigar == cigar
