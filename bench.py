@@ -57,7 +57,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-extra-configs", action="store_true", help="skip the c2/c3/c4 lines")
     p.add_argument("--no-autotune", action="store_true", help="keep the default launch configuration")
-    p.add_argument("--config", default="c1", choices=["c1", "c2", "c3", "c4"],
+    p.add_argument("--sw-pairs", type=int, default=16384, help="pairs of the Smith-Waterman line")
+    p.add_argument("--config", default="c1", choices=["c1", "c2", "c3", "c4", "sw"],
                    help="c2/c3/c4: time only that configuration (with --regions to shrink it), for profiling")
     return p.parse_args()
 
@@ -277,7 +278,7 @@ def time_device(stream, flush, fn, steps):
     return statistics.mean(times)
 
 
-def extra_configs(args, device, stream, flush, threads, which=("c2", "c3", "c4"), regions=0):
+def extra_configs(args, device, stream, flush, threads, which=("c2", "c3", "c4", "sw"), regions=0):
     """c2 (shared SNP haplotypes), c3 (PD-HMM) and c4 (adjoint), one device-timed line each
     (`regions` > 0 shrinks them, for profiling)."""
     from fgkl_b200 import BatchContext, Config, Precision, _lib, synthetic
@@ -364,8 +365,20 @@ def extra_configs(args, device, stream, flush, threads, which=("c2", "c3", "c4")
                                                    "restated in C (oracle/fgkl_cpu.c), FP32 with FP64 recomputation"}
             res[name]["device_over_cpu"] = (nominal / t / 1e9) / cpu
         ctx.close()
-    if "c4" not in which:
-        return res
+    if "c4" in which:
+        res["c4"] = adjoint_line(args, device, stream, flush, regions, threads)
+    if "sw" in which:
+        res["sw"] = smith_waterman_line(args, device, threads)
+    return res
+
+
+def adjoint_line(args, device, stream, flush, regions, threads):
+    """c4: the adjoint, device-timed, with an accuracy sample against the FP64 scalar adjoint."""
+    from fgkl_b200 import _lib, synthetic
+    from fgkl_b200.adjoint import AdjointContext, params_from_quals
+    from oracle import oracle
+
+    steps = max(2, min(args.steps, 3))
     # c4: the adjoint.
     w = synthetic.workload(4, seed=args.seed, regions=regions, threads=threads)
     p = params_from_quals(w)
@@ -397,7 +410,7 @@ def extra_configs(args, device, stream, flush, threads, which=("c2", "c3", "c4")
     fp32_peak = max(s_tf.value, p_tf.value)
     adj_tf = FLOP_ADJOINT * nominal / t / 1e12
     rel = [abs(ours_g[k][lo:hi].sum() - g_ref[k].sum()) / abs(g_ref[k].sum()) for k in range(4)]
-    res["c4"] = {"workload": "adjoint: 256 regions x 64 reads (151) x 8 haplotypes (350); gradients of the summed log10 "
+    line = {"workload": "adjoint: 256 regions x 64 reads (151) x 8 haplotypes (350); gradients of the summed log10 "
                              "likelihood w.r.t. gap-open (ins, del), gap continuation, base error per read position",
                  "regions": w.num_regions, "nominal_gcups": nominal / t / 1e9, "ms_per_step": 1e3 * t, "steps": steps,
                  "nominal_cells": nominal, "cells_per_pair_visited": "backward sweep twice (checkpoints, then blocks), forward once",
@@ -408,7 +421,64 @@ def extra_configs(args, device, stream, flush, threads, which=("c2", "c3", "c4")
                               "peak_source": "measured FP32 FMA probe on this GPU"},
                  "accuracy_sample": "region 0 against the FP64 scalar adjoint (summed gradients)"}
     actx.close()
-    return res
+    return line
+
+
+def sw_pairs(n_pairs, ref_len=500, alt_len=500, seed=5):
+    """fgkl's sw-bench pairs (crates/smithwaterman/src/bin/bench.rs:42-53): a uniform ACGT reference,
+    the alternate its first alt_len bases with 3 substitutions and 1 deletion (drawn with numpy)."""
+    rng = np.random.default_rng(seed)
+    acgt = np.frombuffer(b"ACGT", np.uint8)
+    pairs = []
+    for _ in range(n_pairs):
+        r = acgt[rng.integers(0, 4, ref_len)]
+        a = r[:min(alt_len, ref_len)].copy()
+        for _ in range(3):
+            a[rng.integers(0, a.size)] = acgt[rng.integers(0, 4)]
+        a = np.delete(a, rng.integers(0, a.size))
+        pairs.append((r.tobytes(), a.tobytes()))
+    return pairs
+
+
+def smith_waterman_line(args, device, threads):
+    """GATK's Smith-Waterman (fgkl crates/smithwaterman) on fgkl's sw-bench shape, one batch call."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from fgkl_b200 import BatchContext
+    from fgkl_b200.sw import HAPLOTYPE_TO_REFERENCE as P, OverhangStrategy, align_batch
+    from oracle import oracle
+
+    pairs = sw_pairs(args.sw_pairs)
+    cells = sum(len(r) * len(a) for r, a in pairs)
+    ctx = BatchContext(device=device)
+    align_batch(pairs[:64], P, OverhangStrategy.INDEL, ctx)  # untimed: the engine's buffers
+    times = []
+    for _ in range(max(2, min(args.steps, 3))):
+        t0 = time.perf_counter()
+        got = align_batch(pairs, P, OverhangStrategy.INDEL, ctx)
+        times.append(time.perf_counter() - t0)
+    ctx.close()
+    t = statistics.median(times)
+    params = (P.match_value, P.mismatch_penalty, P.gap_open_penalty, P.gap_extend_penalty)
+    sample = list(range(0, len(pairs), max(1, len(pairs) // 512)))
+
+    def one(k):
+        return oracle.sw_align(pairs[k][0], pairs[k][1], params, int(OverhangStrategy.INDEL))
+
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(threads) as ex:
+        ref = list(ex.map(one, sample))
+    cpu_secs = time.perf_counter() - t0
+    cpu_cells = sum(len(pairs[k][0]) * len(pairs[k][1]) for k in sample)
+    differ = sum((g.cigar, g.offset) != r for g, r in zip((got[k] for k in sample), ref))
+    return {"workload": f"Smith-Waterman: {len(pairs)} pairs, reference 500, alternate its first 500 bases with 3 substitutions "
+                        "and 1 deletion (fgkl's sw-bench shape), haplotype-to-reference scores, Indel strategy",
+            "gcups": cells / t / 1e9, "ms_per_step": 1e3 * t, "cells": cells,
+            "timing": "one fgkl_sw_align_batch call from host arrays (uploads, kernel, downloads), wall clock",
+            "alignments_differing_from_oracle": differ, "oracle_sample_pairs": len(sample),
+            "cpu_baseline": {"value": cpu_cells / cpu_secs / 1e9, "unit": "GCUPS", "cores": threads, "kind": "port",
+                             "sample": f"{len(sample)} pairs through the scalar restatement of GATK's aligner "
+                                       "(oracle/sw_oracle.c), one pair per thread"}}
 
 
 # ---------------------------------------------------------------------------------------------
