@@ -50,6 +50,7 @@ int AdjointEngine::check(cudaError_t e, const char* what) {
 template <class T>
 T* AdjointEngine::grow(T*& p, size_t& cap, size_t n) {
   const size_t bytes = std::max<size_t>(n * sizeof(T), 256);
+  if (over_allocation_limit(bytes)) return nullptr;  // the buffer held so far is kept
   if (bytes > cap) {
     // Half as much again as the old size: a caller whose batches vary in size stops reallocating
     // after a few calls (cudaFree waits for the whole device, other callers' streams included).

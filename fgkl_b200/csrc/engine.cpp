@@ -21,6 +21,11 @@ std::atomic<int64_t> g_allocation_limit{0};
 int64_t allocation_limit() { return g_allocation_limit.load(std::memory_order_relaxed); }
 int64_t set_allocation_limit(int64_t bytes) { return g_allocation_limit.exchange(bytes); }
 
+bool over_allocation_limit(size_t bytes) {
+  const int64_t lim = allocation_limit();
+  return lim > 0 && bytes > static_cast<size_t>(lim);
+}
+
 cudaError_t device_alloc(void** p, size_t bytes) {
   const int64_t lim = allocation_limit();
   if (lim > 0 && bytes > static_cast<size_t>(lim)) {
@@ -258,6 +263,7 @@ int Engine::check(cudaError_t e, const char* what) {
 template <class T>
 T* Engine::grow(T*& ptr, size_t& cap, size_t n) {
   const size_t bytes = std::max<size_t>(n * sizeof(T), 256);
+  if (over_allocation_limit(bytes)) return nullptr;  // the buffer held so far is kept
   if (bytes > cap) {
     // Half as much again as the old size: a caller whose batches vary in size stops reallocating
     // after a few calls (cudaFree waits for the whole device, other callers' streams included).
@@ -304,6 +310,7 @@ bool host_pinned(const void* p, size_t bytes) {
 // Grows a pinned host buffer to at least `bytes`, by half again at least (cudaFreeHost waits for the
 // whole device); false when the allocation fails.
 bool grow_pinned(uint8_t*& p, size_t& cap, size_t bytes) {
+  if (over_allocation_limit(bytes)) return false;
   if (bytes <= cap) return true;
   const size_t want = cap > 0 ? std::max(bytes, cap + cap / 2) : bytes;
   if (p) cudaFreeHost(p);
@@ -728,6 +735,7 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
   const size_t s_qoff = s_tasks + align_up(tasks.size() * sizeof(Task));
   const size_t s_out = s_qoff + align_up((kQueueBins + 1) * sizeof(int));
   const size_t stage_bytes = s_out + align_up(static_cast<size_t>(out_len_) * sizeof(double)) + align_up(sizeof(Counters));
+  if (over_allocation_limit(stage_bytes)) return fail(FGKL_E_OUT_OF_MEMORY, "pinned host allocation failed");
   if (stage_bytes > cap_stage_) {
     // Grown by half again at least, as the device buffers are (cudaFreeHost waits for the device).
     const size_t want = cap_stage_ > 0 ? std::max(stage_bytes, cap_stage_ + cap_stage_ / 2) : stage_bytes;

@@ -14,10 +14,12 @@
 
 namespace fgkl {
 
-// Failure injection (fgkl_set_allocation_limit): device and page-locked host allocations larger
-// than this many bytes fail as if out of memory; 0 = no limit.
+// Failure injection (fgkl_set_allocation_limit): a call that needs a device or page-locked host
+// buffer larger than this many bytes fails as if out of memory, whether or not a buffer that large
+// is already held (which is kept); 0 = no limit.
 int64_t allocation_limit();
 int64_t set_allocation_limit(int64_t bytes);
+bool over_allocation_limit(size_t bytes);
 // cudaMalloc / cudaMallocHost under that limit.
 cudaError_t device_alloc(void** p, size_t bytes);
 cudaError_t pinned_alloc(void** p, size_t bytes);

@@ -47,6 +47,7 @@ int SwEngine::check(cudaError_t e, const char* what) {
 template <class T>
 T* SwEngine::grow(T*& p, size_t& cap, size_t n) {
   const size_t bytes = std::max<size_t>(n * sizeof(T), 256);
+  if (over_allocation_limit(bytes)) return nullptr;  // the buffer held so far is kept
   if (bytes > cap) {
     const size_t want = cap > 0 ? std::max(bytes, cap + cap / 2) : bytes;
     cudaFree(p);

@@ -129,11 +129,12 @@ int fgkl_set_call_combining(int32_t max_batches);
 int fgkl_call_combining_stats(uint64_t* batches, uint64_t* requests);
 
 /* Failure injection (no counterpart in the reference; its Rust allocator aborts instead). From now on
- * every device or page-locked host allocation the library asks for that is larger than `bytes`
- * fails as if the device were out of memory, so a caller's handling of FGKL_E_OUT_OF_MEMORY can be
- * exercised without exhausting a real device. Buffers the library already holds are not touched,
- * and a call that fails leaves its engine or context usable for later calls. `bytes` = 0 removes
- * the limit. Process-wide; returns the previous limit, or FGKL_E_INVALID_ARGUMENT when negative. */
+ * every call that needs a device or page-locked host buffer larger than `bytes` fails with
+ * FGKL_E_OUT_OF_MEMORY, as if the device could not hold it, whether or not the library already holds
+ * a buffer that large; so a caller's handling of the error can be exercised without exhausting a
+ * real device. Buffers already held are kept, and a call that fails leaves its engine or context
+ * usable for later calls. `bytes` = 0 removes the limit. Process-wide; returns the previous limit, or
+ * FGKL_E_INVALID_ARGUMENT when negative. */
 int64_t fgkl_set_allocation_limit(int64_t bytes);
 
 /* Name of the backend, the analogue of backendNative (crates/jni/src/lib.rs:149-156). */
