@@ -63,7 +63,9 @@ struct AdjSizes {
   static constexpr int kStepBytes = kRecChunks * 32 * 16;
   static constexpr int kRawK = 28672 / kStepBytes;
   static constexpr int K = kRawK < 1 ? 1 : (kRawK > 8 ? 8 : kRawK);
-  static constexpr size_t kSmemPerWarp = static_cast<size_t>(K) * kStepBytes;
+  // Per warp: the K steps' records, then the next block's checkpoint, fetched a block ahead.
+  static constexpr size_t kStageOffset = static_cast<size_t>(K) * kStepBytes;
+  static constexpr size_t kSmemPerWarp = kStageOffset + static_cast<size_t>(kStateChunks) * 32 * 16;
 };
 
 constexpr int kFlushSteps = 32;  // forward steps between FP64 additions of the FP32 sums
@@ -416,6 +418,21 @@ __device__ typename P::V adj_forward(const AdjView& v, const AdjCoef<P, R>& c, i
 #pragma unroll
   for (int r = 0; r < R; ++r) gi[r] = gd[r] = ge[r] = gq[r] = P::zero();
   uint4* buf = reinterpret_cast<uint4*>(smem);
+  V* stage = reinterpret_cast<V*>(reinterpret_cast<char*>(smem) + Z::kStageOffset);
+  // The checkpoint a block starts from, copied into shared memory a block ahead (each lane its own
+  // chunks), so the restore does not wait on global memory.
+  auto fetch_state = [&](int t0n) {
+    const int lo_n = max(0, n - min(t0n + K, n));
+    if (t0n < n && lo_n > 0) {
+      const V* src = sc.state(blk, (n - lo_n) / K - 1);
+#pragma unroll
+      for (int ch = 0; ch < Z::kStateChunks; ++ch)
+        __pipeline_memcpy_async(reinterpret_cast<char*>(stage) + (ch * 32 + lane) * 16,
+                                reinterpret_cast<const char*>(src) + (ch * 32 + lane) * 16, 16);
+    }
+    __pipeline_commit();
+  };
+  fetch_state(0);
   for (int t0 = 0; t0 < n; t0 += K) {
     const int t1 = min(t0 + K, n);
     const int lo = max(0, n - t1), hi = n - 1 - t0;
@@ -423,10 +440,12 @@ __device__ typename P::V adj_forward(const AdjView& v, const AdjCoef<P, R>& c, i
     // the block buffer [step - lo][chunk][lane].
     {
       AdjBwd<P, R> st;
+      __pipeline_wait_prior(0);
       if (lo > 0)
-        st.restore(sc.state(blk, (n - lo) / K - 1), lane, c_fac);
+        st.restore(stage, lane, c_fac);
       else
         st.zero();
+      fetch_state(t0 + K);
       uint32_t next_code = adj_bwd_code(hap, m, lo - (31 - lane));
       for (int tb = lo; tb <= hi; ++tb) {
         const int p = tb - (31 - lane);
@@ -449,10 +468,13 @@ __device__ typename P::V adj_forward(const AdjView& v, const AdjCoef<P, R>& c, i
     }
     __syncwarp();
     const bool uniform = t0 >= 31 && t1 <= m;  // every lane inside the haplotype at every step
+    // The haplotype base of each step, loaded a step ahead.
+    uint32_t next_fcode = (t0 - lane >= 0 && t0 - lane < m) ? adj_code(__ldg(hap + t0 - lane)) : 0u;
     for (int t = t0; t < t1; ++t) {
       const int p = t - lane;  // column p + 1
       const bool live = p >= 0 && p < m;
-      const uint32_t code = live ? adj_code(__ldg(hap + p)) : 0u;
+      const uint32_t code = next_fcode;
+      next_fcode = (p + 1 >= 0 && p + 1 < m) ? adj_code(__ldg(hap + p + 1)) : 0u;
       V rec[Z::kRecVals];
       const int slot = n - 1 - t - lo;
 #pragma unroll
@@ -498,6 +520,7 @@ __device__ typename P::V adj_forward(const AdjView& v, const AdjCoef<P, R>& c, i
     }
     __syncwarp();
   }
+  __pipeline_wait_prior(0);
   return __shfl_sync(kFull, f.acc, 31);
 }
 
