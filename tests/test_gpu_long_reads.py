@@ -21,7 +21,8 @@ DOUBLE = Config(precision=Precision.DOUBLE)
 
 def assert_close(actual, expected, tol, what=""):
     assert actual.shape == expected.shape
-    d = np.abs(actual - expected)
+    same = actual == expected  # equal infinities: a likelihood of zero on both sides
+    d = np.where(same, 0.0, np.abs(actual - expected))
     worst = int(np.argmax(d))
     assert np.all(d <= tol), f"{what}: pair {worst}: got {actual[worst]}, expected {expected[worst]} (diff {d[worst]})"
     assert np.isfinite(d).all()
@@ -133,16 +134,22 @@ def test_batched_long_reads_have_the_per_call_bits(gpu):
     ctx.close()
 
 
-def many_byte_reads(seed, reads, classes):
-    """Reads whose bases are drawn from `classes` distinct bytes (more than 31), with ACGT among them."""
+def many_byte_reads(seed, reads, classes, every=0):
+    """Reads whose bases are drawn from `classes` distinct bytes (more than 31), with ACGT among them:
+    a random quarter of the bases replaced, or with `every` > 0 every `every`-th base, the alphabet's
+    bytes taken in turn (few enough substitutions that long reads keep a finite likelihood)."""
     rng = Rng(seed)
     alphabet = b"ACGTNacgtn" + bytes(range(ord("!"), ord("!") + classes - 10))  # punctuation and digits
     assert len(set(alphabet)) == classes
-    out = []
+    out, turn = [], 0
     for r in reads:
         b = bytearray(r.bases)
         for i in range(len(b)):
-            if rng.below(4) == 0:
+            if every > 0:
+                if i % every == every // 2:
+                    b[i] = alphabet[turn % len(alphabet)]
+                    turn += 1
+            elif rng.below(4) == 0:
                 b[i] = alphabet[rng.below(len(alphabet))]
         out.append(Read(bytes(b), r.quals, r.ins_gop, r.del_gop, r.gcp))
     return out
@@ -161,9 +168,12 @@ def test_pd_region_with_40_distinct_read_bytes(gpu):
 
 def test_pd_region_with_40_read_bytes_and_long_reads(gpu):
     reads, haps = pd_region(33, 3, 900, 3, 1000)
-    reads = many_byte_reads(6, reads, 40)
+    reads = many_byte_reads(6, reads, 40, every=60)
+    assert len({b for r in reads for b in r.bases}) >= 40
+    expected = O.compute_matrix(reads, haps)
+    assert np.isfinite(expected).all()
     got, _ = computed(PdPairHmm, FLOAT, reads, haps)
-    assert_close(got, O.compute_matrix(reads, haps), 1e-4)
+    assert_close(got, expected, 1e-4)
 
 
 def test_pd_region_with_more_than_256_match_sets(gpu):

@@ -163,9 +163,10 @@ def test_gpu_a_failed_allocation_raises_runtime_exception(gpu, shim):
     prev = set_allocation_limit(1024)
     try:
         exc, _, region_calls = call(shim, *flat(reads, haps))
+        message = _lib.last_error()  # read before the limit call below clears it
     finally:
         set_allocation_limit(prev)
-    assert exc is not None and exc[0] == RTE and exc[1] == _lib.last_error()
+    assert exc is not None and exc[0] == RTE and exc[1] == message
     assert "allocation failed" in exc[1]
     assert region_calls == 0
     exc, out, _ = call(shim, *flat(reads, haps))
