@@ -189,10 +189,15 @@ __device__ __forceinline__ void load_record(V (&dst)[N], const V* src) {
 
 __device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
 
+// The bracket of the match recurrence, which the caller multiplies by the prior. In the FP32 form
+// the row's match-to-match factor is folded into its priors (prior * mm) and out of k1 and k2
+// (divided by mm), so the diagonal M enters unscaled and k0 is not read: three operations a cell with
+// the prior instead of four. A row with mm = 0 makes k1 and k2 infinite and the cell NaN, which the
+// acceptance test sends to the FP64 recomputation.
 template <class P>
 __device__ __forceinline__ typename P::V cell_match(const typename P::V& dM, const typename P::V& dX, const typename P::V& dY,
                                                     const typename P::V& k0, const typename P::V& k1, const typename P::V& k2) {
-  if (P::kTransformed) return P::fma(dM, k0, P::fma(dX, k1, P::mul(dY, k2)));
+  if (P::kTransformed) return P::fma(dX, k1, P::fma(dY, k2, dM));
   // fgkl kernel.rs:1011: prior * (y_diag*im + (x_diag*im + m_diag*mm)).
   return P::fma(dY, k1, P::fma(dX, k1, P::mul(dM, k0)));
 }

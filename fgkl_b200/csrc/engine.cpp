@@ -658,7 +658,9 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
   for (auto& f : first) bins_.push_back(f.second);
   // Recomputation queues: room for every (read, distinct haplotype) pair of each rows-per-lane bin.
   // Pairs either pass loses (an FP32 underflow, or a joined FP64 result below the backward range)
-  // are recomputed in FP64 without sharing, which cannot lose a pair (lib.rs:461-487).
+  // are recomputed in FP64 (lib.rs:461-520): after an FP32 pass, a read lost against a third of its
+  // haplotypes or more once with its region's shared program, any pair that sweep loses again and
+  // every other lost pair without sharing, which cannot lose a pair.
   const bool queue_on = cfg.double_fallback;
   std::vector<int> queue_off(kQueueBins + 1, 0);
   {
@@ -693,9 +695,11 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
     const bool rescue = list == &rescue_bins_;
     size_t off = 0;
     for (Bin& b : *list) {
+      // Short-read recomputation bins also run dense reads' whole programs after an FP32 pass.
+      const bool whole = !rescue || !cfg.double_precision;
       b.stride = align_up(is_long(b.kind) ? long_scratch_bytes(b.kind, b.rows, max_hap_len)
-                          : rescue        ? scratch_bytes(b.kind, b.rows, 0, 0, 1)
-                                          : scratch_bytes(b.kind, b.rows, max_slots, max_nodes, max_segs));
+                          : whole         ? scratch_bytes(b.kind, b.rows, max_slots, max_nodes, max_segs)
+                                          : scratch_bytes(b.kind, b.rows, 0, 0, 1));
       b.scratch_off = off;
       off += static_cast<size_t>(b.blocks) * kWarpsPerBlock * b.stride;
     }
@@ -887,6 +891,7 @@ int Engine::run() {
       a.scratch = d_scratch_ + bin.scratch_off;
       a.scratch_stride = bin.stride;
       a.min_accept_plain = (!rescue && !cfg_.double_precision) ? 1 : 0;
+      a.only_lost = rescue ? 1 : 0;
       const int li = i - 1;  // this launch's index, for profiling events
       if (profile_ && (rc = check(cudaEventRecord(ev_[2 * li], s), "profiling event"))) return rc;
       if ((rc = check(launch(bin.kind, bin.rows, bin.blocks, a, s), rescue ? "recomputation launch" : "first-pass launch")))
@@ -902,7 +907,7 @@ int Engine::run() {
   };
   if ((rc = pass(bins_, false))) return rc;
   if (!rescue_bins_.empty()) {
-    CollectArgs c{view_, d_queue_, queue_off, queue_tail};
+    CollectArgs c{view_, d_queue_, queue_off, queue_tail, cfg_.double_precision ? 0 : 1};
     if ((rc = check(launch_collect(c, n_regions_, stream_), "lost-pair collection"))) return rc;
     planned_.kernel_launches++;
   }

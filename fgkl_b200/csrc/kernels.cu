@@ -12,7 +12,8 @@
 //   M = prior * (mm*M(i-1,j-1) + im*(X(i-1,j-1) + Y(i-1,j-1)))
 //   X = mi*M(i-1,j) + ii*X(i-1,j)          Y = md*M(i,j-1) + dd*Y(i,j-1)
 // The FP32 kernels carry X/mi and Y/md (per-row constants) instead of X and Y: every term stays
-// positive, the X and Y updates become one FMA each, 6 FP32 operations per cell instead of 8. An
+// positive, the X and Y updates become one FMA each. They also fold each row's mm into its priors
+// (M = (prior*mm) * (M(i-1,j-1) + k1*X^ + k2*Y^)), 5 FP32 operations per cell instead of 8. An
 // overflow this could cause for extreme gap-open ratios surfaces as a non-finite result, which is
 // recomputed in FP64 with the plain recurrence.
 //
@@ -67,13 +68,15 @@ struct Layout {
   }
 };
 
-// Priors of the lane's rows for every haplotype code, in shared memory (Layout::prior_at).
+// Priors of the lane's rows for every haplotype code, in shared memory (Layout::prior_at), times the
+// row's match-to-match factor in the FP32 form (cell_match).
 template <class P, int R>
 __device__ __forceinline__ void put_priors(typename P::V* table, int lane, int r, int c, const RowModel& m) {
   using S = typename P::S;
+  const double fold = (P::kTransformed && m.read) ? m.mm : 1.0;
   for (int code = 0; code < Layout<P, R>::kPriorCodes; ++code) {
     const bool match = code == m.oc || code == kCodeN;
-    P::put(table[Layout<P, R>::prior_at(code, r, lane)], c, static_cast<S>(match ? m.pm : m.px));
+    P::put(table[Layout<P, R>::prior_at(code, r, lane)], c, static_cast<S>((match ? m.pm : m.px) * fold));
   }
 }
 
@@ -113,12 +116,13 @@ struct FwdRows {
         const RowModel m = row_model(v, rd[c], g - rd[c].pad, codes);
         double k0, k1, k2, k3, k4;
         if (P::kTransformed) {
-          // S = mm*M + (im*mi')*X^ + (im*md')*Y^ with X = mi*X^, Y = md*Y^;
+          // S = mm*M + (im*mi')*X^ + (im*md')*Y^ with X = mi*X^, Y = md*Y^, taken as
+          // mm * (M + (im*mi'/mm)*X^ + (im*md'/mm)*Y^) with mm in the prior table (cell_match);
           // X^ = M_up + (gc*mi'/mi)*X^_up; Y^ = M_left + gc*Y^_left.
           if (m.read) {
             k0 = m.mm;
-            k1 = m.im * m.mi_prev;
-            k2 = m.im * m.md_prev;
+            k1 = m.im * m.mi_prev / m.mm;
+            k2 = m.im * m.md_prev / m.mm;
             k3 = m.gc * m.mi_prev / m.mi;
             k4 = m.gc;
           } else {
@@ -152,7 +156,9 @@ struct FwdRows {
 };
 
 // Backward coefficients: each row's own deletion transitions and the transitions and priors of the
-// row below it (rows l*R+1 .. l*R+R; the last comes from the next lane's top row).
+// row below it (rows l*R+1 .. l*R+R; the last comes from the next lane's top row). In the FP32 form
+// the row below's match-to-match factor sits in its prior table (put_priors), so `into` carries it
+// and im holds im/mm of the row below.
 template <class P, int R>
 struct BwdRows {
   using V = typename P::V;
@@ -180,7 +186,7 @@ struct BwdRows {
         P::put(md[r], c, static_cast<S>(self.read ? self.md : 0.0));
         P::put(dd[r], c, static_cast<S>(self.read ? self.gc : 1.0));
         P::put(mm[r], c, static_cast<S>(below.mm));
-        P::put(im[r], c, static_cast<S>(below.im));
+        P::put(im[r], c, static_cast<S>(P::kTransformed ? (below.read ? below.im / below.mm : 0.0) : below.im));
         P::put(mi[r], c, static_cast<S>(below.mi));
         P::put(ii[r], c, static_cast<S>(below.gc));
         P::put(pm[r], c, static_cast<S>(below.pm));
@@ -312,7 +318,7 @@ __device__ void backward_pass(const LaunchArgs& a, const Program& prog, const Re
       const V itm = P::mul(into, bp.im[r]);
       V bx = P::fma(belowX, bp.ii[r], itm);
       const V by = P::fma(BY[r], bp.dd[r], itm);
-      V bm = P::fma(BY[r], bp.md[r], P::fma(belowX, bp.mi[r], P::mul(into, bp.mm[r])));
+      V bm = P::fma(BY[r], bp.md[r], P::fma(belowX, bp.mi[r], P::kTransformed ? into : P::mul(into, bp.mm[r])));
       if (r == R - 1) {
         bm = P::add(bm, sink);
         bx = P::add(bx, sink);
@@ -629,6 +635,9 @@ __device__ void finalize(const LaunchArgs& a, const Task& task, const Region& re
     }
     return;
   }
+  // A dense read's recomputation (only_lost) fills in only the pairs the first pass lost and counts
+  // nothing: the pairs it loses again stay NaN for the unshared sweep that follows it.
+  const bool dense = a.only_lost != 0;
   unsigned long long lost_count = 0;
   for (int k = lane; k < region.n_haps; k += 32) {
     const HapInfo info = a.v.haps[region.hap_off + k];
@@ -638,6 +647,9 @@ __device__ void finalize(const LaunchArgs& a, const Task& task, const Region& re
 #pragma unroll
     for (int c = 0; c < P::NC; ++c) {
       if (task.read[c] < 0) continue;
+      const int read_local = task.read[c] - region.read_off;
+      double* dst = a.v.out + region.out_off + static_cast<int64_t>(read_local) * region.n_haps + info.order;
+      if (dense && !isnan(*dst)) continue;
       const double raw = __dmul_rn(sc.seg_raw[info.seg * P::NC + c], factor);
       bool lost;
       if (joined)
@@ -646,12 +658,11 @@ __device__ void finalize(const LaunchArgs& a, const Task& task, const Region& re
         lost = a.min_accept_plain ? !(raw >= C::kMinAccepted) : (raw != raw);
       if (!P::kDouble) lost |= isinf(raw);
       const double result = lost ? __longlong_as_double(0x7ff8000000000000ll) : log10(raw) - C::kLog10Initial;
-      const int read_local = task.read[c] - region.read_off;
-      a.v.out[region.out_off + static_cast<int64_t>(read_local) * region.n_haps + info.order] = result;
+      *dst = result;
       lost_count += lost;
     }
   }
-  if (lost_count) atomicAdd(&a.v.counters->lost_pairs, lost_count);
+  if (lost_count && !dense) atomicAdd(&a.v.counters->lost_pairs, lost_count);
 }
 
 template <class P, int R>
@@ -699,32 +710,94 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, (MinBlocks<P, R>::value))
       forward_pass<P, R>(a, prog, rd, codes, lane, sc, nullptr, 0);
       __syncwarp();
       finalize<P, R>(a, task, region, prog, rd, lane, sc);
+      if (P::kDouble && a.only_lost) {
+        // A dense read's shared FP64 sweep can lose a pair again (a joined result below the backward
+        // range): each such distinct haplotype is swept once more here without sharing, which
+        // cannot lose it (fgkl lib.rs:476-486).
+        __syncwarp();
+        const double* row = a.v.out + region.out_off + static_cast<int64_t>(task.read[0] - region.read_off) * region.n_haps;
+        for (int base = 0; base < region.n_haps; base += 32) {
+          const int k = base + lane;
+          bool again = false;
+          if (k < region.n_haps) {
+            const HapInfo info = a.v.haps[region.hap_off + k];
+            again = info.src == k && isnan(row[info.order]);
+          }
+          unsigned mask = __ballot_sync(kFull, again);
+          while (mask) {
+            Task one = task;
+            one.hap = base + __ffs(mask) - 1;
+            mask &= mask - 1;
+            const HapInfo info = a.v.haps[region.hap_off + one.hap];
+            Scratch<P, R> s1(scratch, smem, 0, 0, 1);
+            forward_pass<P, R>(a, prog, rd, codes, lane, s1, a.v.hap_codes + region.seq_off + info.seq, info.len);
+            __syncwarp();
+            finalize<P, R>(a, one, region, prog, rd, lane, s1);
+            __syncwarp();
+          }
+        }
+      }
     }
     __syncwarp();
   }
 }
 
-// Queues every pair the first pass lost -- its output is NaN -- as an FP64 recomputation task, one
-// per (read, distinct sorted haplotype), in the queue bin of its form and rows-per-lane (queue_bin).
-// One block per region; nothing to do (one load per block) when no pair was lost.
+// Queues what the first pass lost for FP64 recomputation, in the queue bin of the read's form and
+// rows-per-lane (queue_bin), one warp per read. After an FP32 pass, a read of a shared program lost
+// against at least a third of its haplotypes (duplicates counted, fgkl lib.rs:495-505) is queued once,
+// as a whole-program task that fills in every lost pair of the read with one shared sweep, when that
+// sweep is the cheaper one; any other lost pair is queued as (read, distinct sorted haplotype), swept
+// unshared. Both are FP64 sweeps of fgkl's recurrence and agree to rounding. One block per region;
+// nothing to do (one load per block) when no pair was lost.
 __global__ void __launch_bounds__(256) collect_kernel(CollectArgs a) {
   if (a.v.counters->lost_pairs == 0) return;
   const Region region = a.v.regions[blockIdx.x];
-  const int64_t pairs = static_cast<int64_t>(region.n_reads) * region.n_haps;
   const bool generic = (region.flags & kRegionGeneric) != 0;
-  for (int64_t e = threadIdx.x; e < pairs; e += blockDim.x) {
-    const int r = static_cast<int>(e / region.n_haps), k = static_cast<int>(e % region.n_haps);
-    const HapInfo info = a.v.haps[region.hap_off + k];
-    if (info.src != k) continue;
-    if (!isnan(a.v.out[region.out_off + static_cast<int64_t>(r) * region.n_haps + info.order])) continue;
+  const int lane = threadIdx.x & 31;
+  for (int r = threadIdx.x >> 5; r < region.n_reads; r += blockDim.x >> 5) {
+    const double* row = a.v.out + region.out_off + static_cast<int64_t>(r) * region.n_haps;
+    int lost_all = 0, lost_distinct = 0, lost_steps = 0;
+    for (int k = lane; k < region.n_haps; k += 32) {
+      const HapInfo info = a.v.haps[region.hap_off + k];
+      const bool lost = isnan(row[info.order]);
+      lost_all += lost;
+      lost_distinct += lost && info.src == k;
+      lost_steps += (lost && info.src == k) ? info.len + 32 : 0;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      lost_all += __shfl_xor_sync(kFull, lost_all, o);
+      lost_distinct += __shfl_xor_sync(kFull, lost_distinct, o);
+      lost_steps += __shfl_xor_sync(kFull, lost_steps, o);
+    }
+    if (lost_all == 0) continue;
     const int read = region.read_off + r;
     const int len = static_cast<int>(a.v.read_off[read + 1] - a.v.read_off[read]);
     const int bin = queue_bin(len, generic);
     const int rows = queue_bin_rows(bin);
-    const int slot = atomicAdd(a.queue_tail + bin, 1);
-    if (slot < a.queue_off[bin + 1] - a.queue_off[bin]) {
-      a.queue[a.queue_off[bin] + slot] = Task{static_cast<int32_t>(blockIdx.x), {read, -1}, rows, k};
-      atomicAdd(&a.v.counters->rescue_reads, 1ull);
+    const int cap = a.queue_off[bin + 1] - a.queue_off[bin];
+    // The shared sweep must also cost at most two thirds of the unshared ones in wavefront steps:
+    // a program that shares little (most PD regions) runs slower whole, in one warp, than its pairs
+    // spread over many.
+    const int prog_steps = region.prog.fwd_len + 32 + (region.prog.bwd_len > 0 ? region.prog.bwd_len + 32 : 0);
+    if (a.dense && bin < kRowBins && 3 * lost_all >= region.n_haps && 3 * prog_steps <= 2 * lost_steps) {
+      if (lane == 0) {
+        const int slot = atomicAdd(a.queue_tail + bin, 1);
+        if (slot < cap) {
+          a.queue[a.queue_off[bin] + slot] = Task{static_cast<int32_t>(blockIdx.x), {read, -1}, rows, -1};
+          atomicAdd(&a.v.counters->rescue_reads, static_cast<unsigned long long>(lost_distinct));
+        }
+      }
+      continue;
+    }
+    for (int k = lane; k < region.n_haps; k += 32) {
+      const HapInfo info = a.v.haps[region.hap_off + k];
+      if (info.src != k || !isnan(row[info.order])) continue;
+      const int slot = atomicAdd(a.queue_tail + bin, 1);
+      if (slot < cap) {
+        a.queue[a.queue_off[bin] + slot] = Task{static_cast<int32_t>(blockIdx.x), {read, -1}, rows, k};
+        atomicAdd(&a.v.counters->rescue_reads, 1ull);
+      }
     }
   }
 }

@@ -87,14 +87,17 @@ struct LaunchArgs {
   char* scratch;
   size_t scratch_stride; // bytes per warp
   int min_accept_plain;  // 1: results below the single-precision threshold are lost
+  int only_lost;         // recomputation: a whole-program task writes only pairs whose result is NaN
 };
 
 // The pass between the first pass and the recomputation: queues lost pairs.
 struct CollectArgs {
   BatchView v;
-  Task* queue;           // recomputation queue: (read, distinct haplotype) FP64 tasks
+  Task* queue;           // recomputation queue: (read, distinct haplotype) FP64 tasks, and dense reads
   const int* queue_off;  // per rows-per-lane bin: first queue index (one past the last bin at the end)
   int* queue_tail;       // per bin: tasks queued
+  int dense;             // 1 after an FP32 pass: a read lost against a third of its haplotypes or more
+                         // is queued once, as a whole-program FP64 task (fgkl lib.rs:495-520)
 };
 
 // Rows per lane the instantiations cover.

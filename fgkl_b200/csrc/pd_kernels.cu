@@ -102,10 +102,11 @@ struct PdRows {
         const RowModel m = row_model(v, rd[c], lane * R + r - rd[c].pad, classes);
         double k0, k1, k2, k3, k4;
         if (P::kTransformed) {
+          // The match-to-match factor moves into the priors (cell_match).
           if (m.read) {
             k0 = m.mm;
-            k1 = m.im * m.mi_prev;
-            k2 = m.im * m.md_prev;
+            k1 = m.im * m.mi_prev / m.mm;
+            k2 = m.im * m.md_prev / m.mm;
             k3 = m.gc * m.mi_prev / m.mi;
             k4 = m.gc;
           } else {
@@ -124,13 +125,14 @@ struct PdRows {
             k3 = 1.0;
           }
         }
+        const double fold = (P::kTransformed && m.read) ? m.mm : 1.0;
         P::put(c0[r], c, static_cast<S>(k0));
         P::put(c1[r], c, static_cast<S>(k1));
         P::put(c2[r], c, static_cast<S>(k2));
         P::put(c3[r], c, static_cast<S>(k3));
         P::put(c4[r], c, static_cast<S>(k4));
-        P::put(pm[r], c, static_cast<S>(m.pm));
-        P::put(px[r], c, static_cast<S>(m.px));
+        P::put(pm[r], c, static_cast<S>(m.pm * fold));
+        P::put(px[r], c, static_cast<S>(m.px * fold));
         cls[c][r] = m.read ? (1u << (m.oc & 31)) : 0u;
       }
     }
@@ -420,6 +422,9 @@ __device__ void pd_finalize(const LaunchArgs& a, const Task& task, const Region&
     }
     return;
   }
+  // A dense read's recomputation (only_lost) fills in only the pairs the first pass lost; a PD program
+  // has no joins, so in FP64 it loses none.
+  const bool dense = a.only_lost != 0;
   unsigned long long lost_count = 0;
   for (int k = lane; k < region.n_haps; k += 32) {
     const HapInfo info = a.v.haps[region.hap_off + k];
@@ -427,16 +432,18 @@ __device__ void pd_finalize(const LaunchArgs& a, const Task& task, const Region&
 #pragma unroll
     for (int c = 0; c < P::NC; ++c) {
       if (task.read[c] < 0) continue;
+      const int read_local = task.read[c] - region.read_off;
+      double* dst = a.v.out + region.out_off + static_cast<int64_t>(read_local) * region.n_haps + info.order;
+      if (dense && !isnan(*dst)) continue;
       const double raw = __dmul_rn(sc.seg_raw[info.seg * P::NC + c], factor);
       bool lost = a.min_accept_plain ? !(raw >= C::kMinAccepted) : (raw != raw);
       if (!P::kDouble) lost |= isinf(raw);
       const double result = lost ? __longlong_as_double(0x7ff8000000000000ll) : log10(raw) - C::kLog10Initial;
-      const int read_local = task.read[c] - region.read_off;
-      a.v.out[region.out_off + static_cast<int64_t>(read_local) * region.n_haps + info.order] = result;
+      *dst = result;
       lost_count += lost;
     }
   }
-  if (lost_count) atomicAdd(&a.v.counters->lost_pairs, lost_count);
+  if (lost_count && !dense) atomicAdd(&a.v.counters->lost_pairs, lost_count);
 }
 
 template <class P, int R>

@@ -402,3 +402,53 @@ def test_page_locked_inputs_and_outputs_give_the_same_bits(gpu):
     _check(_lib.lib().fgkl_batch_compute(ctx._ctx, C.byref(b2), C.byref(c), _ptr(out2, _lib.f64p), out2.size, C.byref(st)))
     assert out2.tobytes() == expected.tobytes()
     del t_bases, t_out, keep
+
+
+def two_family_region(seed, n_a=5, n_b=2, hap_len=260, read_len=120):
+    """Haplotypes of two unrelated families (n_a near copies of one sequence, n_b of another) and
+    reads sampled from each: a read of family B is lost in FP32 against every A haplotype (a dense
+    read when 3 n_a >= n_a + n_b and the shared program is the cheaper sweep, as here, where each
+    family's copies differ only in their last 40 bases), a read of family A only against the n_b B
+    haplotypes (a sparse read when 3 n_b < n_a + n_b)."""
+    rng = Rng(seed)
+    fam = [bytes(rng.base() for _ in range(hap_len)) for _ in range(2)]
+    haps = []
+    for f, count in ((0, n_a), (1, n_b)):
+        for _ in range(count):
+            h = bytearray(fam[f])
+            for _ in range(3):  # near the end, so the family shares long prefixes
+                h[hap_len - 40 + rng.below(40)] = rng.base()
+            haps.append(bytes(h))
+    reads, owner = [], []
+    for i in range(12):
+        f = i % 3 == 2  # every third read from family B
+        src = fam[int(f)]
+        start = rng.below(hap_len - read_len)
+        reads.append(Read(src[start:start + read_len], bytes(20 + rng.below(21) for _ in range(read_len)),
+                          bytes([45] * read_len), bytes([45] * read_len), bytes([10] * read_len)))
+        owner.append(int(f))
+    return reads, haps, owner
+
+
+def test_dense_reads_are_recomputed_with_their_shared_program(gpu):
+    """fgkl lib.rs:495-520: after an FP32 pass, a read lost against at least a third of the haplotypes
+    is recomputed once in FP64 against all of them with sharing, the others pair by pair. Every lost
+    pair comes back at FP64 accuracy; a dense read's lost pairs carry the bits of its FP64 program,
+    that is of the double-precision pass, and the pairs it did not lose keep their FP32 bits."""
+    reads, haps, owner = two_family_region(23)
+    expected = reference_all(reads, haps).reshape(len(reads), len(haps))
+    fam_of_hap = [0] * 5 + [1] * 2
+    lost_mask = np.array([[owner[r] != fam_of_hap[h] for h in range(len(haps))] for r in range(len(reads))])
+    assert (expected[lost_mask] < -70.0).all() and (expected[~lost_mask] > -60.0).all()
+    out, fallbacks = compute_counting(FLOAT, reads, haps)
+    out = out.reshape(len(reads), len(haps))
+    assert fallbacks == int(lost_mask.sum())
+    assert_close(out[lost_mask], expected[lost_mask], 1e-9, "lost pairs")
+    assert_close(out[~lost_mask], expected[~lost_mask], 1e-4, "kept pairs")
+    double = compute(DOUBLE, reads, haps).reshape(len(reads), len(haps))
+    dense = [r for r in range(len(reads)) if owner[r] == 1]
+    for r in dense:
+        assert out[r][lost_mask[r]].tobytes() == double[r][lost_mask[r]].tobytes(), r
+    alone = compute(FLOAT, [reads[r] for r in range(len(reads)) if owner[r] == 0], haps).reshape(-1, len(haps))
+    kept = out[[r for r in range(len(reads)) if owner[r] == 0]]
+    assert kept[:, :5].tobytes() == alone[:, :5].tobytes()

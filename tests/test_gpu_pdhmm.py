@@ -230,3 +230,43 @@ def test_one_or_two_reads_per_warp_give_the_same_bits_and_the_autotuner_tries_bo
     assert len(tried) == 18
     assert sorted({t["reads_per_warp"] for t in tried}) == [1, 2]
     assert chosen["ms"] == min(t["ms"] for t in tried)
+
+
+def test_dense_reads_are_recomputed_with_their_shared_program(gpu):
+    """fgkl lib.rs:495-520 for PD haplotypes: a read lost in FP32 against at least a third of them is
+    recomputed in FP64 with its region's shared program (its lost pairs get the double-precision
+    pass's bits), a read lost against fewer pair by pair; the pairs kept keep their FP32 bits."""
+    rng = Rng(29)
+    hap_len, read_len = 260, 120
+    fam = [bytes(rng.base() for _ in range(hap_len)) for _ in range(2)]
+    haps, fam_of_hap = [], []
+    for f, count in ((0, 5), (1, 2)):
+        for i in range(count):
+            flags = bytearray(hap_len)
+            for j in range(10, hap_len - 10, 53):
+                flags[j] = SNP | ALT_G
+            flags[100] |= DEL_START
+            flags[103] |= DEL_END
+            if i < 3:  # near the end (long shared prefixes); the family's last two are duplicates
+                flags[hap_len - 40 + rng.below(30)] |= SNP | ALT_T
+            haps.append(PdHaplotype(fam[f], bytes(flags)))
+            fam_of_hap.append(f)
+    reads, owner = [], []
+    for i in range(12):
+        f = int(i % 3 == 2)
+        start = rng.below(hap_len - read_len)
+        reads.append(Read(fam[f][start:start + read_len], bytes(20 + rng.below(21) for _ in range(read_len)),
+                          bytes([45] * read_len), bytes([45] * read_len), bytes([10] * read_len)))
+        owner.append(f)
+    expected = reference_all(reads, haps).reshape(len(reads), len(haps))
+    lost_mask = np.array([[owner[r] != fam_of_hap[h] for h in range(len(haps))] for r in range(len(reads))])
+    assert (expected[lost_mask] < -70.0).all() and (expected[~lost_mask] > -60.0).all()
+    out, fallbacks = compute_counting(FLOAT, reads, haps)
+    out = out.reshape(len(reads), len(haps))
+    assert fallbacks == int(lost_mask.sum())
+    assert_close(out[lost_mask], expected[lost_mask], 1e-9, "lost pairs")
+    assert_close(out[~lost_mask], expected[~lost_mask], 1e-4, "kept pairs")
+    double = compute(DOUBLE, reads, haps).reshape(len(reads), len(haps))
+    for r in range(len(reads)):
+        if owner[r] == 1:
+            assert out[r][lost_mask[r]].tobytes() == double[r][lost_mask[r]].tobytes(), r
