@@ -35,9 +35,14 @@
 // them top to bottom; lane 0's row above comes from the bottom row the block above stored, or GATK's
 // row 0 in the first block.
 //
-// Haplotype bases are compared as bytes: prior code = the byte with 'N' and byte 4 swapped, so N is
-// code kCodeN (matches every read base); a read N matches everything through its mismatch prior.
+// Haplotype bases are compared as bytes: a haplotype N matches every read base; a read N matches
+// everything through its mismatch prior, which equals its match prior.
+//
+// Most steps of a one-block read are interior: every lane lies strictly inside the haplotype in both
+// sweeps (steps 32 .. m - 1). Those steps, block by block, run without the column-0 resets, the
+// masks of lanes outside the haplotype and the row-block exchanges.
 #include <cmath>
+#include <type_traits>
 
 #include "adjoint.cuh"
 #include "dp_common.cuh"
@@ -45,8 +50,6 @@
 namespace fgkl {
 
 namespace {
-
-__device__ __forceinline__ uint32_t adj_code(uint32_t b) { return b == 'N' ? kCodeN : (b == kCodeN ? 'N' : b); }
 
 // Sizes of one instantiation: a lane's record of one backward step (BM, BX, BY rows) and its saved
 // backward state (BM, BY rows, the diagonal BM and the two values shuffled from the lane below), in
@@ -70,87 +73,124 @@ struct AdjSizes {
 
 constexpr int kFlushSteps = 32;  // forward steps between FP64 additions of the FP32 sums
 
-// The lane's rows: their own forward transitions and priors, and the row below each (backward).
-// Read row q = lane * R + r - pad, pad relative to the row block (negative below the first).
+// The lane's rows: their forward transitions and priors, and those of the row below the lane's last
+// row, which the backward step of that row reads (the backward step of row r < R - 1 reads row r + 1's
+// own). Read row q = lane * R + r - pad, pad relative to the row block (negative below the first).
+// Haplotype and read bases are compared as bytes; a haplotype N matches every read base, and a read N
+// has equal match and mismatch priors.
 template <class P, int R>
 struct AdjCoef {
   using V = typename P::V;
   using S = typename P::S;
   V mm[R], im[R], mi[R], ii[R], md[R], dd[R], pm[R], px[R];
-  V bmm[R], bim[R], bmi[R], bii[R], bpm[R], bpx[R];
-  int oc[R], boc[R];
-  uint32_t nmask;  // bit r: the row's read base is N
-  uint32_t real;   // bit r: a read row
+  V kqx[R];  // d prior / d e of a mismatch: 1/3, or -1 for a read N (whose prior is 1 - e either way)
+  int rb[R];                     // read byte; -1 for a padding row (no haplotype byte matches it)
+  V lmm, lim, lmi, lii, lpm, lpx;  // the row below row R - 1
+  int lrb;
+  uint32_t real;  // bit r: a read row
+
+  struct Row {
+    double mm, im, mi, ii, md, dd, pm, px, kqx;
+    int rb;
+    bool real;
+  };
+  __device__ static Row row(const AdjView& v, int64_t off, int len, int q) {
+    Row w;
+    w.real = q >= 0 && q < len;
+    if (w.real) {
+      const int64_t o = off + q;
+      const double di = v.d_ins[o], dl = v.d_del[o], ep = v.eps[o], e = v.err[o];
+      const int b = v.bases[o];
+      w.mm = 1.0 - di - dl;
+      w.im = 1.0 - ep;
+      w.mi = di;
+      w.ii = ep;
+      w.md = dl;
+      w.dd = ep;
+      w.pm = 1.0 - e;
+      w.px = b == 'N' ? w.pm : e / 3.0;
+      w.kqx = b == 'N' ? -1.0 : 1.0 / 3.0;
+      w.rb = b;
+    } else {
+      // Padding rows keep M = X = 0 and Y = INITIAL / hap_len: GATK's row 0.
+      w.mm = w.im = w.mi = w.ii = w.md = w.pm = w.px = w.kqx = 0.0;
+      w.dd = 1.0;
+      w.rb = -1;
+    }
+    return w;
+  }
 
   __device__ void load(const AdjView& v, int64_t off, int len, int pad, int lane) {
-    nmask = real = 0u;
+    real = 0u;
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      const int q = lane * R + r - pad;
-      if (q >= 0 && q < len) {
-        const int64_t o = off + q;
-        const double di = v.d_ins[o], dl = v.d_del[o], ep = v.eps[o], e = v.err[o];
-        const uint8_t b = v.bases[o];
-        mm[r] = static_cast<S>(1.0 - di - dl);
-        im[r] = static_cast<S>(1.0 - ep);
-        mi[r] = static_cast<S>(di);
-        ii[r] = static_cast<S>(ep);
-        md[r] = static_cast<S>(dl);
-        dd[r] = static_cast<S>(ep);
-        pm[r] = static_cast<S>(1.0 - e);
-        px[r] = b == 'N' ? pm[r] : static_cast<S>(e / 3.0);
-        oc[r] = static_cast<int>(adj_code(b));
-        real |= 1u << r;
-        if (b == 'N') nmask |= 1u << r;
-      } else {
-        // Padding rows keep M = X = 0 and Y = INITIAL / hap_len: GATK's row 0.
-        mm[r] = im[r] = mi[r] = ii[r] = md[r] = pm[r] = px[r] = P::zero();
-        dd[r] = static_cast<S>(1.0);
-        oc[r] = -1;
-      }
-      const int qb = q + 1;
-      if (qb >= 0 && qb < len) {
-        const int64_t o = off + qb;
-        const double di = v.d_ins[o], dl = v.d_del[o], ep = v.eps[o], e = v.err[o];
-        const uint8_t b = v.bases[o];
-        bmm[r] = static_cast<S>(1.0 - di - dl);
-        bim[r] = static_cast<S>(1.0 - ep);
-        bmi[r] = static_cast<S>(di);
-        bii[r] = static_cast<S>(ep);
-        bpm[r] = static_cast<S>(1.0 - e);
-        bpx[r] = b == 'N' ? bpm[r] : static_cast<S>(e / 3.0);
-        boc[r] = static_cast<int>(adj_code(b));
-      } else {
-        bmm[r] = bim[r] = bmi[r] = bii[r] = bpm[r] = bpx[r] = P::zero();
-        boc[r] = -1;
-      }
+      const Row w = row(v, off, len, lane * R + r - pad);
+      mm[r] = static_cast<S>(w.mm);
+      im[r] = static_cast<S>(w.im);
+      mi[r] = static_cast<S>(w.mi);
+      ii[r] = static_cast<S>(w.ii);
+      md[r] = static_cast<S>(w.md);
+      dd[r] = static_cast<S>(w.dd);
+      pm[r] = static_cast<S>(w.pm);
+      px[r] = static_cast<S>(w.px);
+      kqx[r] = static_cast<S>(w.kqx);
+      rb[r] = w.rb;
+      if (w.real) real |= 1u << r;
     }
+    const Row w = row(v, off, len, lane * R + R - pad);
+    lmm = static_cast<S>(w.mm);
+    lim = static_cast<S>(w.im);
+    lmi = static_cast<S>(w.mi);
+    lii = static_cast<S>(w.ii);
+    lpm = static_cast<S>(w.pm);
+    lpx = static_cast<S>(w.px);
+    lrb = w.rb;
   }
-  __device__ bool matches(uint32_t code, int r) const { return static_cast<int>(code) == oc[r] || code == kCodeN; }
-  __device__ V bprior(uint32_t code, int r) const {
-    return (static_cast<int>(code) == boc[r] || code == kCodeN) ? bpm[r] : bpx[r];
+  // Coefficients of the row below row r, for the backward step.
+  __device__ V bmm(int r) const { return r + 1 < R ? mm[r + 1 < R ? r + 1 : 0] : lmm; }
+  __device__ V bim(int r) const { return r + 1 < R ? im[r + 1 < R ? r + 1 : 0] : lim; }
+  __device__ V bmi(int r) const { return r + 1 < R ? mi[r + 1 < R ? r + 1 : 0] : lmi; }
+  __device__ V bii(int r) const { return r + 1 < R ? ii[r + 1 < R ? r + 1 : 0] : lii; }
+  __device__ V bprior(int code, bool hapN, int r) const {
+    if (r + 1 < R) {
+      const int k = r + 1 < R ? r + 1 : 0;
+      return (code == rb[k] || hapN) ? pm[k] : px[k];
+    }
+    return (code == lrb || hapN) ? lpm : lpx;
   }
 };
 
-// The backward sweep's state between two steps.
+// The backward sweep's state between two steps. The BM rows are double-buffered: a step reads the
+// column's old rows from one set (the diagonal of the row above) and writes the new ones to the
+// other, and consecutive steps swap the sets (the step's parity picks them), so no row is copied.
 template <class P, int R>
 struct AdjBwd {
   using V = typename P::V;
   using Z = AdjSizes<P, R>;
-  V BM[R], BY[R];
+  V BA[R], BB[R], BY[R];
   V dBM, topBM, topBX;
 
+  template <bool kB>
+  __device__ __forceinline__ V (&cur())[R] {
+    if constexpr (kB)
+      return BB;
+    else
+      return BA;
+  }
   __device__ __forceinline__ void zero() {
 #pragma unroll
-    for (int r = 0; r < R; ++r) BM[r] = BY[r] = P::zero();
+    for (int r = 0; r < R; ++r) BA[r] = BB[r] = BY[r] = P::zero();
     dBM = topBM = topBX = P::zero();
   }
-  // Saved as [chunk][lane] 16-byte chunks, so each chunk of the warp is 512 contiguous bytes.
-  __device__ __forceinline__ void save(V* dst, int lane) const {
+  // Saved as [chunk][lane] 16-byte chunks, so each chunk of the warp is 512 contiguous bytes; kB
+  // names the set holding the current rows.
+  template <bool kB>
+  __device__ __forceinline__ void save(V* dst, int lane) {
     V rec[Z::kStateChunks * Z::kPer16];
+    const V(&bm)[R] = cur<kB>();
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      rec[r] = BM[r];
+      rec[r] = bm[r];
       rec[R + r] = BY[r];
     }
     rec[2 * R] = dBM;
@@ -162,7 +202,7 @@ struct AdjBwd {
     for (int c = 0; c < Z::kStateChunks; ++c)
       reinterpret_cast<uint4*>(dst)[c * 32 + lane] = reinterpret_cast<const uint4*>(rec)[c];
   }
-  // Restores a saved state multiplied by `scale`.
+  // Restores a saved state multiplied by `scale` into the first set.
   __device__ __forceinline__ void restore(const V* src, int lane, V scale) {
     V rec[Z::kStateChunks * Z::kPer16];
 #pragma unroll
@@ -170,7 +210,7 @@ struct AdjBwd {
       reinterpret_cast<uint4*>(rec)[c] = reinterpret_cast<const uint4*>(src)[c * 32 + lane];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      BM[r] = P::mul(rec[r], scale);
+      BA[r] = P::mul(rec[r], scale);
       BY[r] = P::mul(rec[R + r], scale);
     }
     dBM = P::mul(rec[2 * R], scale);
@@ -179,40 +219,47 @@ struct AdjBwd {
   }
 };
 
-// One backward step at lane position p (column m - p). `sink` is the scale added at the read's last
-// row (lane 31 of the last row block). With `below` (lane 31 of a row block above another), the row
-// below comes from that block's stored top row: cBX its BX at this column, cBM its BM, the next
-// step's diagonal. kRec: keep the column's BM, BX, BY rows in `rec`.
-template <class P, int R, bool kRec>
-__device__ __forceinline__ void adj_bwd_step(AdjBwd<P, R>& s, const AdjCoef<P, R>& c, typename P::V sink, uint32_t code, int p,
+// One backward step at lane position p (column m - p), reading haplotype byte `code` (the diagonal
+// successor's base), from BM set kB to set !kB. `sink` is the scale added at the read's last row
+// (lane 31 of the last row block). kGeneral: a step where some lane is at or before column m (p <= 0:
+// the all-zero column beyond the haplotype is set at p == 0) or where lane 31 takes the row below from
+// the stored top row of the block below (`below`: cBX its BX at this column, cBM its BM, the next
+// step's diagonal); without it the step is an interior step of a one-block read and skips both.
+// kRec: keep the column's BM, BX, BY rows in `rec`.
+template <class P, int R, bool kRec, bool kGeneral, bool kB>
+__device__ __forceinline__ void adj_bwd_step(AdjBwd<P, R>& s, const AdjCoef<P, R>& c, typename P::V sink, int code, int p,
                                              bool below, typename P::V cBM, typename P::V cBX,
                                              typename P::V (&rec)[AdjSizes<P, R>::kRecVals]) {
   using V = typename P::V;
+  V(&old)[R] = s.template cur<kB>();
+  V(&nw)[R] = s.template cur<!kB>();
   V rBM = P::down(s.topBM), rBX = P::down(s.topBX);
-  if (below) {
-    rBM = cBM;
-    rBX = cBX;
-  }
-  if (p == 0) {
-    // The all-zero column beyond the haplotype.
+  if (kGeneral) {
+    if (below) {
+      rBM = cBM;
+      rBX = cBX;
+    }
+    if (p == 0) {
 #pragma unroll
-    for (int r = 0; r < R; ++r) s.BM[r] = s.BY[r] = P::zero();
-    s.dBM = P::zero();
+      for (int r = 0; r < R; ++r) old[r] = s.BY[r] = P::zero();
+      s.dBM = P::zero();
+    }
   }
-  V belowX = rBX, diagM = s.dBM;
+  const bool hapN = code == 'N';
+  V belowX = rBX;
 #pragma unroll
   for (int r = R - 1; r >= 0; --r) {
-    const V into = P::mul(c.bprior(code, r), diagM);
-    const V itm = P::mul(into, c.bim[r]);
-    V bx = P::fma(belowX, c.bii[r], itm);
+    const V diagM = r + 1 < R ? old[r + 1 < R ? r + 1 : 0] : s.dBM;
+    const V into = P::mul(c.bprior(code, hapN, r), diagM);
+    const V itm = P::mul(into, c.bim(r));
+    V bx = P::fma(belowX, c.bii(r), itm);
     const V by = P::fma(s.BY[r], c.dd[r], itm);
-    V bm = P::fma(s.BY[r], c.md[r], P::fma(belowX, c.bmi[r], P::mul(into, c.bmm[r])));
+    V bm = P::fma(s.BY[r], c.md[r], P::fma(belowX, c.bmi(r), P::mul(into, c.bmm(r))));
     if (r == R - 1) {
       bm = P::add(bm, sink);
       bx = P::add(bx, sink);
     }
-    diagM = s.BM[r];
-    s.BM[r] = bm;
+    nw[r] = bm;
     s.BY[r] = by;
     belowX = bx;
     if (kRec) {
@@ -221,16 +268,16 @@ __device__ __forceinline__ void adj_bwd_step(AdjBwd<P, R>& s, const AdjCoef<P, R
       rec[2 * R + r] = by;
     }
   }
-  s.topBM = s.BM[0];
+  s.topBM = nw[0];
   s.topBX = belowX;
   s.dBM = rBM;
 }
 
-// The base code the backward step at lane position p reads (the diagonal successor's base), none
-// beyond the haplotype.
-__device__ __forceinline__ uint32_t adj_bwd_code(const uint8_t* hap, int m, int p) {
+// The haplotype byte the backward step at lane position p reads (the diagonal successor's base),
+// 0 beyond the haplotype.
+__device__ __forceinline__ int adj_bwd_code(const uint8_t* hap, int m, int p) {
   const int jj = m - p;
-  return (p >= 0 && jj >= 0 && jj < m) ? adj_code(__ldg(hap + jj)) : 0u;
+  return (p >= 0 && jj >= 0 && jj < m) ? __ldg(hap + jj) : 0;
 }
 
 // A pair's per-warp scratch: checkpoints [row block][state][chunk][lane], then the top rows of row
@@ -270,6 +317,11 @@ struct AdjScratch {
   }
 };
 
+// Steps where every lane of a one-block read lies strictly inside the haplotype, in both sweeps:
+// forward step t (lane positions t - 31 .. t, columns 1 .. m) and backward step t (positions
+// t - 31 .. t) are interior for 32 <= t <= m - 1.
+constexpr int kAdjInteriorFirst = 32;
+
 // Backward sweep of row block `blk` over steps 0 .. m + 31, saving the state entering every K-th
 // step before the end (the state entering backward step n - (i + 1) K as checkpoint i, n = m + 31)
 // and, for a block below another, its top row (lane 0) at every column. Returns, in every lane, the
@@ -281,6 +333,7 @@ __device__ typename P::V adj_backward(const AdjCoef<P, R>& c, const uint8_t* hap
   using S = typename P::S;
   using Z = AdjSizes<P, R>;
   const bool last = blk == sc.blocks - 1;
+  const bool single = sc.blocks == 1 && pad >= R;  // one row block, lane 0 all padding
   const V sink = (lane == 31 && last) ? static_cast<S>(Consts<P::kDouble>::kBackwardScale) : P::zero();
   const bool below = lane == 31 && !last;
   AdjBwd<P, R> st;
@@ -289,13 +342,18 @@ __device__ typename P::V adj_backward(const AdjCoef<P, R>& c, const uint8_t* hap
   const int pad_lane = pad_row >= 0 ? pad_row / R : 0, pad_r = pad_row >= 0 ? pad_row % R : 0;
   const int n = m + 31;
   V start_mass = P::zero();
-  uint32_t next_code = adj_bwd_code(hap, m, -(31 - lane));
+  int next_code = adj_bwd_code(hap, m, -(31 - lane));
   V cBM = P::zero(), cBX = P::zero();
   V rec[Z::kRecVals];
-  for (int t = 0; t < m + 32; ++t) {
-    if (t > 0 && t < n && (n - t) % Z::K == 0) st.save(sc.state(blk, (n - t) / Z::K - 1), lane);
+  auto general = [&](int t) {
+    if (t > 0 && t < n && (n - t) % Z::K == 0) {
+      if (t & 1)
+        st.template save<true>(sc.state(blk, (n - t) / Z::K - 1), lane);
+      else
+        st.template save<false>(sc.state(blk, (n - t) / Z::K - 1), lane);
+    }
     const int p = t - (31 - lane);
-    const uint32_t code = next_code;
+    const int code = next_code;
     next_code = adj_bwd_code(hap, m, p + 1);
     if (below) {
       // Lane 31 is at position t: column m - t of the block below's top row.
@@ -307,7 +365,10 @@ __device__ typename P::V adj_backward(const AdjCoef<P, R>& c, const uint8_t* hap
         cBM = cBX = P::zero();
       }
     }
-    adj_bwd_step<P, R, false>(st, c, sink, code, p, below, cBM, cBX, rec);
+    if (t & 1)
+      adj_bwd_step<P, R, false, true, true>(st, c, sink, code, p, below, cBM, cBX, rec);
+    else
+      adj_bwd_step<P, R, false, true, false>(st, c, sink, code, p, below, cBM, cBX, rec);
     if (blk > 0 && lane == 0 && p >= 0 && p <= m) {
       V* u = sc.up(blk, m - p);
       u[0] = st.topBM;
@@ -318,7 +379,25 @@ __device__ typename P::V adj_backward(const AdjCoef<P, R>& c, const uint8_t* hap
       for (int r = 0; r < R; ++r)
         if (r == pad_r) start_mass = st.BY[r];
     }
+  };
+  int t = 0;
+  const int fast_end = single ? m - 1 : -1;  // last interior step
+  for (; t <= n && (t < kAdjInteriorFirst || t > fast_end); ++t) general(t);
+  // Interior steps, two at a time from an even step: the next step's byte is in range
+  // (m - t + 30 - lane in [0, m - 2]).
+  auto interior = [&](int t, auto flip) {
+    constexpr bool kB = decltype(flip)::value;
+    if ((n - t) % Z::K == 0) st.template save<kB>(sc.state(0, (n - t) / Z::K - 1), lane);
+    const int code = next_code;
+    next_code = __ldg(hap + (m - t + 30 - lane));
+    adj_bwd_step<P, R, false, false, kB>(st, c, sink, code, 0, false, cBM, cBX, rec);
+  };
+  for (; t + 1 <= fast_end; t += 2) {
+    interior(t, std::false_type{});
+    interior(t + 1, std::true_type{});
   }
+  if (t <= fast_end) interior(t++, std::false_type{});
+  for (; t <= n; ++t) general(t);
   return __shfl_sync(kFull, start_mass, pad_lane);
 }
 
@@ -336,20 +415,22 @@ struct AdjFwd {
 // BY rows, already multiplied by c). kMask: steps where some lane lies outside the haplotype, whose
 // terms are dropped.
 template <class P, int R, bool kMask>
-__device__ __forceinline__ void adj_fwd_step(AdjFwd<P, R>& f, const AdjCoef<P, R>& c, uint32_t code, bool live,
+__device__ __forceinline__ void adj_fwd_step(AdjFwd<P, R>& f, const AdjCoef<P, R>& c, int code, bool live,
                                              const typename P::V (&rec)[AdjSizes<P, R>::kRecVals], typename P::V uM,
                                              typename P::V uX, typename P::V (&gi)[R], typename P::V (&gd)[R],
                                              typename P::V (&ge)[R], typename P::V (&gq)[R]) {
   using V = typename P::V;
   using S = typename P::S;
-  const V third = static_cast<S>(1.0 / 3.0), minus_one = static_cast<S>(-1.0);
+  const V minus_one = static_cast<S>(-1.0);
+  const bool hapN = code == 'N';
   // Match and deletion values from the bottom row up (each row reads the old row above).
 #pragma unroll
   for (int r = R - 1; r >= 0; --r) {
     const V pM = r ? f.M[r - 1] : f.dM, pX = r ? f.X[r - 1] : f.dX, pY = r ? f.Y[r - 1] : f.dY;
     const V mOld = f.M[r], yOld = f.Y[r];
-    const bool match = c.matches(code, r);
+    const bool match = code == c.rb[r] || hapN;
     const V prior = match ? c.pm[r] : c.px[r];
+    const V kq = match ? minus_one : c.kqx[r];
     const V sxy = P::add(pX, pY);
     const V s = P::fma(pM, c.mm[r], P::mul(sxy, c.im[r]));
     f.Y[r] = P::fma(yOld, c.dd[r], P::mul(mOld, c.md[r]));
@@ -360,7 +441,6 @@ __device__ __forceinline__ void adj_fwd_step(AdjFwd<P, R>& f, const AdjCoef<P, R
     gi[r] = P::fma(-pM, bmp, gi[r]);
     gd[r] = P::fma(-pM, bmp, P::fma(mOld, by, gd[r]));
     ge[r] = P::fma(-sxy, bmp, P::fma(yOld, by, ge[r]));
-    const V kq = (match || ((c.nmask >> r) & 1u)) ? minus_one : third;
     gq[r] = P::fma(s, P::mul(bm, kq), gq[r]);
   }
   // Insertion values from the top row down (each row reads the new row above).
@@ -373,7 +453,7 @@ __device__ __forceinline__ void adj_fwd_step(AdjFwd<P, R>& f, const AdjCoef<P, R
     gi[r] = P::fma(qM, bx, gi[r]);
     ge[r] = P::fma(qX, bx, ge[r]);
   }
-  if (live) f.acc = P::add(f.acc, P::add(f.M[R - 1], f.X[R - 1]));
+  if (!kMask || live) f.acc = P::add(f.acc, P::add(f.M[R - 1], f.X[R - 1]));
 }
 
 // Adds the lane's FP32 (FP64) sums into the per-position gradients and clears them.
@@ -397,7 +477,8 @@ __device__ __forceinline__ void adj_flush(const AdjView& v, const AdjCoef<P, R>&
 // Forward sweep of row block `blk`, block by block of K steps with the backward values recomputed
 // into shared memory first, accumulating the gradient terms; returns lane 31's accumulated result
 // (meaningful in the last row block). `c_fac` scales the recomputed backward values, `init` is the
-// row-0 constant of the scaled forward values.
+// row-0 constant of the scaled forward values. Blocks whose steps are all interior steps of a
+// one-block read (kAdjInteriorFirst) run both sweeps without the edge and row-block code.
 template <class P, int R>
 __device__ typename P::V adj_forward(const AdjView& v, const AdjCoef<P, R>& c, int64_t off, int pad, const uint8_t* hap, int m, int lane,
                                      const AdjScratch<P, R>& sc, int blk, typename P::V* smem, typename P::V c_fac,
@@ -407,6 +488,7 @@ __device__ typename P::V adj_forward(const AdjView& v, const AdjCoef<P, R>& c, i
   using Z = AdjSizes<P, R>;
   constexpr int K = Z::K;
   const bool first = blk == 0, last = blk == sc.blocks - 1;
+  const bool single = sc.blocks == 1 && pad >= R;  // one row block, lane 0 all padding
   const int n = m + 31;
   const V sink = (lane == 31 && last) ? P::mul(static_cast<S>(Consts<P::kDouble>::kBackwardScale), c_fac) : P::zero();
   const bool below = lane == 31 && !last;
@@ -432,10 +514,23 @@ __device__ typename P::V adj_forward(const AdjView& v, const AdjCoef<P, R>& c, i
     }
     __pipeline_commit();
   };
+  auto store_rec = [&](int slot, V (&rec)[Z::kRecVals]) {
+#pragma unroll
+    for (int i = 3 * R; i < Z::kRecVals; ++i) rec[i] = P::zero();
+#pragma unroll
+    for (int ch = 0; ch < Z::kRecChunks; ++ch) buf[(slot * Z::kRecChunks + ch) * 32 + lane] = reinterpret_cast<const uint4*>(rec)[ch];
+  };
+  auto load_rec = [&](int t, int lo, V (&rec)[Z::kRecVals]) {
+    const int slot = n - 1 - t - lo;
+#pragma unroll
+    for (int ch = 0; ch < Z::kRecChunks; ++ch) reinterpret_cast<uint4*>(rec)[ch] = buf[(slot * Z::kRecChunks + ch) * 32 + lane];
+  };
   fetch_state(0);
+  int flushed = 0;
   for (int t0 = 0; t0 < n; t0 += K) {
     const int t1 = min(t0 + K, n);
     const int lo = max(0, n - t1), hi = n - 1 - t0;
+    const bool interior = single && t0 >= kAdjInteriorFirst && t1 <= m - 1;
     // Backward steps [lo, hi] from the checkpoint entering lo (or the start), scaled by c_fac, into
     // the block buffer [step - lo][chunk][lane].
     {
@@ -446,77 +541,111 @@ __device__ typename P::V adj_forward(const AdjView& v, const AdjCoef<P, R>& c, i
       else
         st.zero();
       fetch_state(t0 + K);
-      uint32_t next_code = adj_bwd_code(hap, m, lo - (31 - lane));
-      for (int tb = lo; tb <= hi; ++tb) {
-        const int p = tb - (31 - lane);
-        const uint32_t code = next_code;
-        next_code = adj_bwd_code(hap, m, p + 1);
-        V cBM = P::zero(), cBX = P::zero();
-        if (below && tb <= m) {
-          const V* u = sc.up(blk + 1, m - tb);
-          cBM = P::mul(u[0], c_fac);
-          cBX = P::mul(u[1], c_fac);
+      // Step tb uses BM set (tb - lo) & 1; the restored state is in the first set.
+      if (interior) {
+        // Backward steps lo..hi are interior (lo >= 32, hi <= m - 2): step tb reads byte
+        // m - tb + 31 - lane, inside [2, m - 1].
+        int next_code = __ldg(hap + (m - lo + 31 - lane));
+        auto rstep = [&](int tb, auto flip) {
+          const int code = next_code;
+          next_code = __ldg(hap + (m - tb + 30 - lane));
+          V rec[Z::kRecVals];
+          adj_bwd_step<P, R, true, false, decltype(flip)::value>(st, c, sink, code, 0, false, P::zero(), P::zero(), rec);
+          store_rec(tb - lo, rec);
+        };
+        int tb = lo;
+        for (; tb + 1 <= hi; tb += 2) {
+          rstep(tb, std::false_type{});
+          rstep(tb + 1, std::true_type{});
         }
-        V rec[Z::kRecVals];
-        adj_bwd_step<P, R, true>(st, c, sink, code, p, below, cBM, cBX, rec);
-#pragma unroll
-        for (int i = 3 * R; i < Z::kRecVals; ++i) rec[i] = P::zero();
-#pragma unroll
-        for (int ch = 0; ch < Z::kRecChunks; ++ch)
-          buf[((tb - lo) * Z::kRecChunks + ch) * 32 + lane] = reinterpret_cast<const uint4*>(rec)[ch];
+        if (tb <= hi) rstep(tb, std::false_type{});
+      } else {
+        int next_code = adj_bwd_code(hap, m, lo - (31 - lane));
+        for (int tb = lo; tb <= hi; ++tb) {
+          const int p = tb - (31 - lane);
+          const int code = next_code;
+          next_code = adj_bwd_code(hap, m, p + 1);
+          V cBM = P::zero(), cBX = P::zero();
+          if (below && tb <= m) {
+            const V* u = sc.up(blk + 1, m - tb);
+            cBM = P::mul(u[0], c_fac);
+            cBX = P::mul(u[1], c_fac);
+          }
+          V rec[Z::kRecVals];
+          if ((tb - lo) & 1)
+            adj_bwd_step<P, R, true, true, true>(st, c, sink, code, p, below, cBM, cBX, rec);
+          else
+            adj_bwd_step<P, R, true, true, false>(st, c, sink, code, p, below, cBM, cBX, rec);
+          store_rec(tb - lo, rec);
+        }
       }
     }
     __syncwarp();
-    const bool uniform = t0 >= 31 && t1 <= m;  // every lane inside the haplotype at every step
-    // The haplotype base of each step, loaded a step ahead.
-    uint32_t next_fcode = (t0 - lane >= 0 && t0 - lane < m) ? adj_code(__ldg(hap + t0 - lane)) : 0u;
-    for (int t = t0; t < t1; ++t) {
-      const int p = t - lane;  // column p + 1
-      const bool live = p >= 0 && p < m;
-      const uint32_t code = next_fcode;
-      next_fcode = (p + 1 >= 0 && p + 1 < m) ? adj_code(__ldg(hap + p + 1)) : 0u;
-      V rec[Z::kRecVals];
-      const int slot = n - 1 - t - lo;
-#pragma unroll
-      for (int ch = 0; ch < Z::kRecChunks; ++ch) reinterpret_cast<uint4*>(rec)[ch] = buf[(slot * Z::kRecChunks + ch) * 32 + lane];
-      V uM = P::up(f.M[R - 1]), uX = P::up(f.X[R - 1]), uY = P::up(f.Y[R - 1]);
-      if (lane == 0) {
-        if (first) {
-          uM = uX = P::zero();
-          uY = init;
-        } else if (p >= 0 && p < m) {
-          const V* d = sc.down(p);
-          uM = d[0];
-          uX = d[1];
-          uY = d[2];
-        }
-      }
-      if (p == 0) {
-        // Column 0: the row-0 constant in the padding rows (and above the lane's top row when that
-        // is padding).
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-          f.M[r] = f.X[r] = P::zero();
-          f.Y[r] = lane * R + r < pad ? init : P::zero();
-        }
-        f.dM = f.dX = P::zero();
-        f.dY = lane * R - 1 < pad ? init : P::zero();
-        f.acc = P::zero();
-      }
-      if (uniform)
+    if (interior) {
+      // Every lane inside the haplotype at every step (step t reads byte t - lane, inside [1, m - 1]),
+      // no row block above or below: lane 0's rows are all padding and feed themselves the row-0
+      // constant through the shuffle.
+      int next_fcode = __ldg(hap + t0 - lane);
+      for (int t = t0; t < t1; ++t) {
+        const int code = next_fcode;
+        next_fcode = __ldg(hap + (t + 1 - lane));
+        V rec[Z::kRecVals];
+        load_rec(t, lo, rec);
+        const V uM = P::up(f.M[R - 1]), uX = P::up(f.X[R - 1]), uY = P::up(f.Y[R - 1]);
         adj_fwd_step<P, R, false>(f, c, code, true, rec, uM, uX, gi, gd, ge, gq);
-      else
-        adj_fwd_step<P, R, true>(f, c, code, live, rec, uM, uX, gi, gd, ge, gq);
-      f.dM = uM;
-      f.dX = uX;
-      f.dY = uY;
-      if (!last && lane == 31 && live) {
-        V* d = sc.down(p);
-        d[0] = f.M[R - 1];
-        d[1] = f.X[R - 1];
-        d[2] = f.Y[R - 1];
+        f.dM = uM;
+        f.dX = uX;
+        f.dY = uY;
       }
-      if ((t + 1) % kFlushSteps == 0 || t + 1 == n) adj_flush<P, R>(v, c, off, pad, lane, gi, gd, ge, gq);
+    } else {
+      // The haplotype base of each step, loaded a step ahead.
+      int next_fcode = (t0 - lane >= 0 && t0 - lane < m) ? __ldg(hap + t0 - lane) : 0;
+      for (int t = t0; t < t1; ++t) {
+        const int p = t - lane;  // column p + 1
+        const bool live = p >= 0 && p < m;
+        const int code = next_fcode;
+        next_fcode = (p + 1 >= 0 && p + 1 < m) ? __ldg(hap + p + 1) : 0;
+        V rec[Z::kRecVals];
+        load_rec(t, lo, rec);
+        V uM = P::up(f.M[R - 1]), uX = P::up(f.X[R - 1]), uY = P::up(f.Y[R - 1]);
+        if (lane == 0) {
+          if (first) {
+            uM = uX = P::zero();
+            uY = init;
+          } else if (p >= 0 && p < m) {
+            const V* d = sc.down(p);
+            uM = d[0];
+            uX = d[1];
+            uY = d[2];
+          }
+        }
+        if (p == 0) {
+          // Column 0: the row-0 constant in the padding rows (and above the lane's top row when
+          // that is padding).
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            f.M[r] = f.X[r] = P::zero();
+            f.Y[r] = lane * R + r < pad ? init : P::zero();
+          }
+          f.dM = f.dX = P::zero();
+          f.dY = lane * R - 1 < pad ? init : P::zero();
+          f.acc = P::zero();
+        }
+        adj_fwd_step<P, R, true>(f, c, code, live, rec, uM, uX, gi, gd, ge, gq);
+        f.dM = uM;
+        f.dX = uX;
+        f.dY = uY;
+        if (!last && lane == 31 && live) {
+          V* d = sc.down(p);
+          d[0] = f.M[R - 1];
+          d[1] = f.X[R - 1];
+          d[2] = f.Y[R - 1];
+        }
+      }
+    }
+    if (t1 - flushed >= kFlushSteps || t1 == n) {
+      adj_flush<P, R>(v, c, off, pad, lane, gi, gd, ge, gq);
+      flushed = t1;
     }
     __syncwarp();
   }
