@@ -303,8 +303,8 @@ def extra_configs(args, device, stream, flush, threads, which=("c2", "c3", "c4",
             tw = synthetic.workload(cfg_id, seed=args.seed + 7919, regions=min(512, w.num_regions), threads=threads)
             chosen, _ = tctx.autotune(tw, Config(precision=Precision.FLOAT), repeats=3)
             tctx.close()
-            tuning = {k: chosen[k] for k in ("streams", "grid_percent", "reads_per_warp")}
-            ctx.set_tuning(tuning["streams"], tuning["grid_percent"], tuning["reads_per_warp"])
+            tuning = {k: chosen[k] for k in ("streams", "grid_percent", "reads_per_warp", "rows_extra", "warps_per_block")}
+            ctx.set_tuning(**tuning)
         ctx.prepare(w, Config(precision=Precision.FLOAT))
         for _ in range(2):
             ctx.run()
@@ -514,8 +514,10 @@ def ours(args, rank, world, local, pg):
         tctx = BatchContext(device=device, stream=stream.cuda_stream)
         chosen, tried = tctx.autotune(tw, cfg, repeats=3)
         tctx.close()
-        tuning = {"chosen": {k: chosen[k] for k in ("streams", "grid_percent", "reads_per_warp")},
-                  "candidates_ms": {f"streams={t['streams']},grid={t['grid_percent']}%": round(t["ms"], 3) for t in tried},
+        tuning = {"chosen": {k: chosen[k] for k in ("streams", "grid_percent", "reads_per_warp", "rows_extra", "warps_per_block")},
+                  "candidates_ms": {f"s{t['streams']}/g{t['grid_percent']}/r{t['reads_per_warp']}/x{t['rows_extra']}"
+                                    f"/w{t['warps_per_block']}": round(t["ms"], 2) for t in tried},
+                  "key": "streams/grid %/reads per warp/rows-per-lane step up/warps per block",
                   "tuned_on": f"{tw.num_regions} regions of the same generator, another seed (untimed)"}
 
     def tuned(c):

@@ -100,7 +100,8 @@ class SwBatch(C.Structure):
 
 
 class Tuning(C.Structure):
-    _fields_ = [("streams", C.c_int32), ("grid_percent", C.c_int32), ("reads_per_warp", C.c_int32), ("ms", C.c_double)]
+    _fields_ = [("streams", C.c_int32), ("grid_percent", C.c_int32), ("reads_per_warp", C.c_int32), ("rows_extra", C.c_int32),
+                ("warps_per_block", C.c_int32), ("ms", C.c_double)]
 
 
 class LaunchProfile(C.Structure):

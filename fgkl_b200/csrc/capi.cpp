@@ -701,9 +701,12 @@ int fgkl_context_set_tuning(fgkl_context* ctx, const fgkl_tuning* t) {
   t_error.clear();
   if (!ctx || !t) return set_error(FGKL_E_INVALID_ARGUMENT, "null argument");
   if (t->streams < 1 || t->streams > 8 || t->grid_percent < 10 || t->grid_percent > 100 ||
-      (t->reads_per_warp != 1 && t->reads_per_warp != 2))
-    return set_error(FGKL_E_INVALID_ARGUMENT, "streams must be 1-8, grid_percent 10-100 and reads_per_warp 1 or 2");
-  ctx->engine->set_tuning(fgkl::Engine::Tuning{t->streams, t->grid_percent, t->reads_per_warp});
+      (t->reads_per_warp != 1 && t->reads_per_warp != 2) || (t->rows_extra != 0 && t->rows_extra != 1) ||
+      (t->warps_per_block != 1 && t->warps_per_block != 2 && t->warps_per_block != 4))
+    return set_error(FGKL_E_INVALID_ARGUMENT,
+                     "streams must be 1-8, grid_percent 10-100, reads_per_warp 1 or 2, rows_extra 0 or 1 and "
+                     "warps_per_block 1, 2 or 4");
+  ctx->engine->set_tuning(fgkl::Engine::Tuning{t->streams, t->grid_percent, t->reads_per_warp, t->rows_extra, t->warps_per_block});
   ctx->graph_current = false;
   return FGKL_OK;
 }
@@ -715,6 +718,8 @@ int fgkl_context_get_tuning(const fgkl_context* ctx, fgkl_tuning* t) {
   t->streams = k.streams;
   t->grid_percent = k.grid_percent;
   t->reads_per_warp = k.reads_per_warp;
+  t->rows_extra = k.rows_extra;
+  t->warps_per_block = k.warps_per_block;
   t->ms = 0.0;
   return FGKL_OK;
 }
@@ -729,28 +734,43 @@ int fgkl_context_autotune(fgkl_context* ctx, const fgkl_batch* batch, const fgkl
   const fgkl::Engine::Tuning before = e.tuning();
   e.set_profiling(false);
   // Candidates: every streams x grid pair with two reads per warp, then, for an FP32 PD-HMM batch,
-  // one read per warp at 4 and 8 streams with full grids.
+  // one read per warp at 4 and 8 streams with full grids; then the tile shapes around the fastest.
   std::vector<fgkl::Engine::Tuning> cands;
   for (int gp : {100, 90, 75, 60})
-    for (int st : {1, 2, 4, 8}) cands.push_back(fgkl::Engine::Tuning{st, gp, 2});
-  if (batch->hap_flags && !config->double_precision)
-    for (int st : {4, 8}) cands.push_back(fgkl::Engine::Tuning{st, 100, 1});
+    for (int st : {1, 2, 4, 8}) cands.push_back(fgkl::Engine::Tuning{st, gp, 2, 0, 4});
+  const bool fp32_pd = batch->hap_flags && !config->double_precision;
+  if (fp32_pd)
+    for (int st : {4, 8}) cands.push_back(fgkl::Engine::Tuning{st, 100, 1, 0, 4});
   fgkl::Engine::Tuning best{};
   double best_ms = -1.0;
   int n = 0, rc = FGKL_OK;
-  for (const auto& c : cands) {
+  auto try_one = [&](const fgkl::Engine::Tuning& c) {
     e.set_tuning(c);
-    if ((rc = fgkl_batch_prepare(ctx, batch, config))) break;
+    if ((rc = fgkl_batch_prepare(ctx, batch, config))) return;
     double ms = 0.0;
     if ((rc = e.time_run(repeats, &ms))) {
       rc = set_error(rc, e.error());
-      break;
+      return;
     }
-    if (tried && n < tried_cap) tried[n] = fgkl_tuning{c.streams, c.grid_percent, c.reads_per_warp, ms};
+    if (tried && n < tried_cap) tried[n] = fgkl_tuning{c.streams, c.grid_percent, c.reads_per_warp, c.rows_extra, c.warps_per_block, ms};
     ++n;
     if (best_ms < 0 || ms < best_ms) {
       best_ms = ms;
       best = c;
+    }
+  };
+  for (const auto& c : cands) {
+    try_one(c);
+    if (rc) break;
+  }
+  if (!rc && !config->double_precision) {
+    const fgkl::Engine::Tuning base = best;
+    std::vector<fgkl::Engine::Tuning> shapes;
+    for (int w : {1, 2}) shapes.push_back(fgkl::Engine::Tuning{base.streams, base.grid_percent, base.reads_per_warp, 0, w});
+    if (!batch->hap_flags) shapes.push_back(fgkl::Engine::Tuning{base.streams, base.grid_percent, base.reads_per_warp, 1, 4});
+    for (const auto& c : shapes) {
+      try_one(c);
+      if (rc) break;
     }
   }
   e.set_profiling(was_profiling);
@@ -764,7 +784,7 @@ int fgkl_context_autotune(fgkl_context* ctx, const fgkl_batch* batch, const fgkl
   }
   e.set_tuning(best);
   if ((rc = fgkl_batch_prepare(ctx, batch, config))) return rc;
-  if (chosen) *chosen = fgkl_tuning{best.streams, best.grid_percent, best.reads_per_warp, best_ms};
+  if (chosen) *chosen = fgkl_tuning{best.streams, best.grid_percent, best.reads_per_warp, best.rows_extra, best.warps_per_block, best_ms};
   return FGKL_OK;
 }
 

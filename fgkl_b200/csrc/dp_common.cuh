@@ -16,7 +16,10 @@ namespace fgkl {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
+// Warps per block: the default and largest. The first-pass kernels (pairhmm_kernel, pd_kernel) also
+// launch with 1 or 2 (a tuning axis); a warp's index comes from blockDim there.
 constexpr int kWarpsPerBlock = 4;
+__host__ __device__ constexpr int warps_index(int warps) { return warps <= 1 ? 0 : (warps == 2 ? 1 : 2); }
 
 // ---------------------------------------------------------------------------------------------
 // Arithmetic policies.
@@ -209,8 +212,10 @@ __device__ __forceinline__ typename P::V cell_match(const typename P::V& dM, con
 // attribute is set and the occupancy queried on the first call only, so each later batch's planning
 // makes no CUDA call for it while other batches run.
 constexpr int kMaxDevices = 64;
+// `smem_limit` (default: `smem`) is the kernel's dynamic shared-memory limit to set, the largest block
+// any launch of it uses.
 template <class K>
-int resident_blocks(K* kernel, size_t smem, int threads, std::atomic<int>* cache) {
+int resident_blocks(K* kernel, size_t smem, int threads, std::atomic<int>* cache, size_t smem_limit = 0) {
   int dev = 0;
   cudaGetDevice(&dev);
   const bool keep = dev >= 0 && dev < kMaxDevices;
@@ -219,7 +224,7 @@ int resident_blocks(K* kernel, size_t smem, int threads, std::atomic<int>* cache
     if (c) return c - 1;
   }
   int blocks = 0;
-  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem_limit > smem ? smem_limit : smem));
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, threads, smem);
   if (keep) cache[dev].store(blocks + 1, std::memory_order_release);
   return blocks;

@@ -597,8 +597,13 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
     } else if (cfg.double_precision || plans[g].extra_codes) {
       for (; i < order.size(); ++i) one(Kind::kOneF64, single_rows(len_of(order[i])), i);
     } else {
-      for (; i < order.size() && packed_rows(len_of(order[i])) > 8; ++i) one(Kind::kOneF32, single_rows(len_of(order[i])), i);
-      for (; i < order.size(); i += 2) two(Kind::kPackedF32, packed_rows(len_of(order[i])), i);
+      // The tile-shape axis: rows_extra moves each read to the next instantiated rows-per-lane
+      // (more padding rows, other registers and occupancy; the same bits).
+      const bool up = tuning_.rows_extra != 0;
+      auto single_up = [&](int rows) { return up && rows + 2 <= max_rows(Kind::kOneF32) ? rows + 2 : rows; };  // even, 10..20
+      auto packed_up = [&](int rows) { return up && rows < 8 ? rows + 1 : rows; };
+      for (; i < order.size() && packed_rows(len_of(order[i])) > 8; ++i) one(Kind::kOneF32, single_up(single_rows(len_of(order[i]))), i);
+      for (; i < order.size(); i += 2) two(Kind::kPackedF32, packed_up(packed_rows(len_of(order[i]))), i);
     }
   });
   {
@@ -646,11 +651,13 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
         tasks.push_back(e.second);
         cost += e.first;
       }
+      const bool fp32 = b.kind == Kind::kPackedF32 || b.kind == Kind::kOneF32 || b.kind == Kind::kPackedF32Pd || b.kind == Kind::kOneF32Pd;
+      b.warps = fp32 ? tuning_.warps_per_block : kWarpsPerBlock;
       int per_sm = 0, threads = 0;
-      occupancy(b.kind, b.rows, &per_sm, &threads);
+      occupancy(b.kind, b.rows, &per_sm, &threads, b.warps);
       if (per_sm <= 0) return fail(FGKL_E_CUDA, "kernel instantiation unavailable on this device");
       const int grid = std::max(sms_, per_sm * sms_ * tuning_.grid_percent / 100);
-      b.blocks = std::max(1, std::min((b.n_tasks + kWarpsPerBlock - 1) / kWarpsPerBlock, grid));
+      b.blocks = std::max(1, std::min((b.n_tasks + b.warps - 1) / b.warps, grid));
       first.push_back({cost, b});
     }
   // The bin with the most work launches first; the others fill the SMs its tail frees.
@@ -701,7 +708,7 @@ int Engine::prepare(const BatchInput& in, const EngineConfig& cfg) {
                           : whole         ? scratch_bytes(b.kind, b.rows, max_slots, max_nodes, max_segs)
                                           : scratch_bytes(b.kind, b.rows, 0, 0, 1));
       b.scratch_off = off;
-      off += static_cast<size_t>(b.blocks) * kWarpsPerBlock * b.stride;
+      off += static_cast<size_t>(b.blocks) * b.warps * b.stride;
     }
     scratch_total = std::max(scratch_total, off);
   }
@@ -894,7 +901,7 @@ int Engine::run() {
       a.only_lost = rescue ? 1 : 0;
       const int li = i - 1;  // this launch's index, for profiling events
       if (profile_ && (rc = check(cudaEventRecord(ev_[2 * li], s), "profiling event"))) return rc;
-      if ((rc = check(launch(bin.kind, bin.rows, bin.blocks, a, s), rescue ? "recomputation launch" : "first-pass launch")))
+      if ((rc = check(launch(bin.kind, bin.rows, bin.blocks, a, s, bin.warps), rescue ? "recomputation launch" : "first-pass launch")))
         return rc;
       if (profile_ && (rc = check(cudaEventRecord(ev_[2 * li + 1], s), "profiling event"))) return rc;
       planned_.kernel_launches++;
@@ -919,6 +926,8 @@ void Engine::set_tuning(const Tuning& t) {
   tuning_.streams = std::max(1, std::min(t.streams, kAuxStreams));
   tuning_.grid_percent = std::max(10, std::min(t.grid_percent, 100));
   tuning_.reads_per_warp = t.reads_per_warp == 1 ? 1 : 2;
+  tuning_.rows_extra = t.rows_extra ? 1 : 0;
+  tuning_.warps_per_block = (t.warps_per_block == 1 || t.warps_per_block == 2) ? t.warps_per_block : kWarpsPerBlock;
 }
 
 int Engine::time_run(int repeats, double* ms) {

@@ -129,12 +129,17 @@ class Engine {
 
   // Launch configuration of the batched form: how many streams the launches of one pass spread
   // over (1: one after another; more: bins overlap, the largest first), each first-pass persistent
-  // grid as a percentage of the resident-block limit, and how many reads an FP32 PD-HMM warp
-  // carries (two in FP32x2 at 8 warps per SM, or one at 12). Applies from the next prepare().
+  // grid as a percentage of the resident-block limit, how many reads an FP32 PD-HMM warp carries
+  // (two in FP32x2 at 8 warps per SM, or one at 12), and the first pass's tile shape: rows per lane
+  // of the plain FP32 reads (the fewest that hold the read, or the next the kernels instantiate)
+  // and warps per block of the FP32 first-pass kernels. None changes a result bit. Applies from the
+  // next prepare().
   struct Tuning {
     int streams = 8;
     int grid_percent = 100;
-    int reads_per_warp = 2;  // FP32 PD-HMM reads of at most 248 bases: 2 (FP32x2 pairs) or 1
+    int reads_per_warp = 2;   // FP32 PD-HMM reads of at most 248 bases: 2 (FP32x2 pairs) or 1
+    int rows_extra = 0;       // 1: plain FP32 reads one rows-per-lane step above the fewest
+    int warps_per_block = 4;  // FP32 first-pass kernels: 1, 2 or 4
   };
   void set_tuning(const Tuning& t);
   const Tuning& tuning() const { return tuning_; }
@@ -153,6 +158,7 @@ class Engine {
     size_t scratch_off;  // this bin's slice of the scratch
     uint64_t fwd_cells = 0, bwd_cells = 0;  // DP cells its tasks compute (first pass)
     int queue_bin = 0;   // recomputation bins: the queue bin (queue_bin) the tasks come from
+    int warps = 4;       // warps per block
   };
   static constexpr int kAuxStreams = 8;
   Tuning tuning_;

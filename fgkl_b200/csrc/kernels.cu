@@ -671,7 +671,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, (MinBlocks<P, R>::value))
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31;
   const int warp_in_block = threadIdx.x >> 5;
-  const int warp = blockIdx.x * kWarpsPerBlock + warp_in_block;
+  const int warp = blockIdx.x * static_cast<int>(blockDim.x >> 5) + warp_in_block;
   V* smem = reinterpret_cast<V*>(smem_raw + warp_in_block * Layout<P, R>::kSmemPerWarp);
   const int count = a.count ? min(*a.count, a.n_tasks) : a.n_tasks;
   for (;;) {
@@ -961,29 +961,30 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, (LongMinBlocks<P, R>::val
 }
 
 template <class P, int R>
-void occ(int* blocks, int* threads) {
-  *threads = kWarpsPerBlock * 32;
-  static std::atomic<int> cache[kMaxDevices];
-  *blocks = resident_blocks(pairhmm_kernel<P, R>, kWarpsPerBlock * Layout<P, R>::kSmemPerWarp, kWarpsPerBlock * 32, cache);
+void occ(int* blocks, int* threads, int warps) {
+  *threads = warps * 32;
+  static std::atomic<int> cache[3][kMaxDevices];
+  *blocks = resident_blocks(pairhmm_kernel<P, R>, warps * Layout<P, R>::kSmemPerWarp, warps * 32, cache[warps_index(warps)],
+                            kWarpsPerBlock * Layout<P, R>::kSmemPerWarp);
 }
 
 template <class P, int R>
-cudaError_t go(int blocks, const LaunchArgs& a, cudaStream_t s) {
-  const size_t smem = kWarpsPerBlock * Layout<P, R>::kSmemPerWarp;
-  pairhmm_kernel<P, R><<<blocks, kWarpsPerBlock * 32, smem, s>>>(a);
+cudaError_t go(int blocks, const LaunchArgs& a, cudaStream_t s, int warps) {
+  const size_t smem = warps * Layout<P, R>::kSmemPerWarp;
+  pairhmm_kernel<P, R><<<blocks, warps * 32, smem, s>>>(a);
   return cudaGetLastError();
 }
 
 template <class P, int R>
 struct OccF {
-  static int run(int* b, int* t) {
-    occ<P, R>(b, t);
+  static int run(int* b, int* t, int warps) {
+    occ<P, R>(b, t, warps);
     return 0;
   }
 };
 template <class P, int R>
 struct GoF {
-  static cudaError_t run(int blocks, const LaunchArgs& a, cudaStream_t s) { return go<P, R>(blocks, a, s); }
+  static cudaError_t run(int blocks, const LaunchArgs& a, cudaStream_t s, int warps) { return go<P, R>(blocks, a, s, warps); }
 };
 template <class P, int R>
 struct SizeF {
@@ -1148,13 +1149,13 @@ size_t scratch_bytes(Kind k, int rows, int max_slots, int max_nodes, int max_seg
   return dispatch<SizeF>(k, rows, max_slots, max_nodes, max_segs);
 }
 
-void occupancy(Kind k, int rows, int* blocks, int* threads) {
+void occupancy(Kind k, int rows, int* blocks, int* threads, int warps) {
   *blocks = 0;
   *threads = kWarpsPerBlock * 32;
-  if (!valid_rows(k, rows)) return;
+  if (!valid_rows(k, rows) || (warps != 1 && warps != 2 && warps != 4)) return;
   if (is_long(k)) return long_occupancy(k, rows, blocks, threads);
-  if (is_pd(k)) return pd_occupancy(pd_form(k), rows, blocks, threads);
-  dispatch<OccF>(k, rows, blocks, threads);
+  if (is_pd(k)) return pd_occupancy(pd_form(k), rows, blocks, threads, warps);
+  dispatch<OccF>(k, rows, blocks, threads, warps);
 }
 
 cudaError_t launch_collect(const CollectArgs& args, int n_regions, cudaStream_t stream) {
@@ -1163,11 +1164,11 @@ cudaError_t launch_collect(const CollectArgs& args, int n_regions, cudaStream_t 
   return cudaGetLastError();
 }
 
-cudaError_t launch(Kind k, int rows, int blocks, const LaunchArgs& args, cudaStream_t stream) {
-  if (!valid_rows(k, rows)) return cudaErrorInvalidValue;
+cudaError_t launch(Kind k, int rows, int blocks, const LaunchArgs& args, cudaStream_t stream, int warps) {
+  if (!valid_rows(k, rows) || (warps != 1 && warps != 2 && warps != 4)) return cudaErrorInvalidValue;
   if (is_long(k)) return long_launch(k, rows, blocks, args, stream);
-  if (is_pd(k)) return pd_launch(pd_form(k), rows, blocks, args, stream);
-  return dispatch<GoF>(k, rows, blocks, args, stream);
+  if (is_pd(k)) return pd_launch(pd_form(k), rows, blocks, args, stream, warps);
+  return dispatch<GoF>(k, rows, blocks, args, stream, warps);
 }
 
 // ---------------------------------------------------------------------------------------------

@@ -105,13 +105,13 @@ int max_rows(Kind k);
 // Bytes of per-warp scratch one task of this instantiation needs.
 size_t scratch_bytes(Kind k, int rows, int max_slots, int max_nodes, int max_segs);
 // Resident blocks per SM and threads per block of an instantiation.
-void occupancy(Kind k, int rows, int* blocks_per_sm, int* threads_per_block);
+void occupancy(Kind k, int rows, int* blocks_per_sm, int* threads_per_block, int warps_per_block = 4);
 // Launches one persistent grid of `blocks` blocks.
-cudaError_t launch(Kind k, int rows, int blocks, const LaunchArgs& args, cudaStream_t stream);
+cudaError_t launch(Kind k, int rows, int blocks, const LaunchArgs& args, cudaStream_t stream, int warps_per_block = 4);
 // PD-HMM instantiations (pd_kernels.cu).
 size_t pd_scratch_bytes(PdForm form, int rows, int max_slots, int max_segs);
-void pd_occupancy(PdForm form, int rows, int* blocks_per_sm, int* threads_per_block);
-cudaError_t pd_launch(PdForm form, int rows, int blocks, const LaunchArgs& args, cudaStream_t stream);
+void pd_occupancy(PdForm form, int rows, int* blocks_per_sm, int* threads_per_block, int warps_per_block = 4);
+cudaError_t pd_launch(PdForm form, int rows, int blocks, const LaunchArgs& args, cudaStream_t stream, int warps_per_block = 4);
 // Strip-mined kinds (is_long): per-warp scratch for haplotypes of at most `max_hap_len` bases (the
 // bottom row a block hands to the next, plus the pair's result), occupancy and launch. The plain
 // ones live in kernels.cu, the PD ones in pd_kernels.cu.

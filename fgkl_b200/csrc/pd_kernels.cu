@@ -457,7 +457,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, (PdMinBlocks<P, R>::value
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31;
   const int warp_in_block = threadIdx.x >> 5;
-  const int warp = blockIdx.x * kWarpsPerBlock + warp_in_block;
+  const int warp = blockIdx.x * static_cast<int>(blockDim.x >> 5) + warp_in_block;
   V* smem = reinterpret_cast<V*>(smem_raw + warp_in_block * PdLayout<P, R>::kSmemPerWarp);
   const int count = a.count ? min(*a.count, a.n_tasks) : a.n_tasks;
   for (;;) {
@@ -643,15 +643,16 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, (P::kDouble ? 1 : 2)) pd_
 }
 
 template <class P, int R>
-void pd_occ(int* blocks) {
-  static std::atomic<int> cache[kMaxDevices];
-  *blocks = resident_blocks(pd_kernel<P, R>, kWarpsPerBlock * PdLayout<P, R>::kSmemPerWarp, kWarpsPerBlock * 32, cache);
+void pd_occ(int* blocks, int warps) {
+  static std::atomic<int> cache[3][kMaxDevices];
+  *blocks = resident_blocks(pd_kernel<P, R>, warps * PdLayout<P, R>::kSmemPerWarp, warps * 32, cache[warps_index(warps)],
+                            kWarpsPerBlock * PdLayout<P, R>::kSmemPerWarp);
 }
 
 template <class P, int R>
-cudaError_t pd_go(int blocks, const LaunchArgs& a, cudaStream_t s) {
-  const size_t smem = kWarpsPerBlock * PdLayout<P, R>::kSmemPerWarp;
-  pd_kernel<P, R><<<blocks, kWarpsPerBlock * 32, smem, s>>>(a);
+cudaError_t pd_go(int blocks, const LaunchArgs& a, cudaStream_t s, int warps) {
+  const size_t smem = warps * PdLayout<P, R>::kSmemPerWarp;
+  pd_kernel<P, R><<<blocks, warps * 32, smem, s>>>(a);
   return cudaGetLastError();
 }
 
@@ -755,38 +756,38 @@ size_t pd_scratch_bytes(PdForm form, int rows, int max_slots, int max_segs) {
   }
 }
 
-void pd_occupancy(PdForm form, int rows, int* blocks, int* threads) {
-  *threads = kWarpsPerBlock * 32;
+void pd_occupancy(PdForm form, int rows, int* blocks, int* threads, int warps) {
+  *threads = warps * 32;
   *blocks = 0;
   switch (form) {
     case PdForm::kOneF64:
       pd_rows<OneF64>(rows, [&](auto r) {
-        pd_occ<OneF64, decltype(r)::value>(blocks);
+        pd_occ<OneF64, decltype(r)::value>(blocks, warps);
         return 0;
       });
       break;
     case PdForm::kPackedF32:
       pd_rows8(rows, [&](auto r) {
-        pd_occ<PackedF32, decltype(r)::value>(blocks);
+        pd_occ<PackedF32, decltype(r)::value>(blocks, warps);
         return 0;
       });
       break;
     default:
       pd_rows<OneF32>(rows, [&](auto r) {
-        pd_occ<OneF32, decltype(r)::value>(blocks);
+        pd_occ<OneF32, decltype(r)::value>(blocks, warps);
         return 0;
       });
   }
 }
 
-cudaError_t pd_launch(PdForm form, int rows, int blocks, const LaunchArgs& a, cudaStream_t s) {
+cudaError_t pd_launch(PdForm form, int rows, int blocks, const LaunchArgs& a, cudaStream_t s, int warps) {
   switch (form) {
     case PdForm::kOneF64:
-      return pd_rows<OneF64>(rows, [&](auto r) { return pd_go<OneF64, decltype(r)::value>(blocks, a, s); });
+      return pd_rows<OneF64>(rows, [&](auto r) { return pd_go<OneF64, decltype(r)::value>(blocks, a, s, warps); });
     case PdForm::kPackedF32:
-      return pd_rows8(rows, [&](auto r) { return pd_go<PackedF32, decltype(r)::value>(blocks, a, s); });
+      return pd_rows8(rows, [&](auto r) { return pd_go<PackedF32, decltype(r)::value>(blocks, a, s, warps); });
     default:
-      return pd_rows<OneF32>(rows, [&](auto r) { return pd_go<OneF32, decltype(r)::value>(blocks, a, s); });
+      return pd_rows<OneF32>(rows, [&](auto r) { return pd_go<OneF32, decltype(r)::value>(blocks, a, s, warps); });
   }
 }
 

@@ -384,7 +384,8 @@ class BatchContext:
     def autotune(self, workload, config: Config | None = None, repeats: int = 3) -> tuple[dict, list[dict]]:
         """Times the launch configurations on ``workload`` (or a sample of the caller's work), keeps the
         fastest for this context's later batches and leaves ``workload`` prepared with it. Returns the
-        chosen configuration and every candidate, each ``{"streams", "grid_percent", "reads_per_warp", "ms"}``."""
+        chosen configuration and every candidate, each ``{"streams", "grid_percent", "reads_per_warp",
+        "rows_extra", "warps_per_block", "ms"}``."""
         b = workload.as_batch()
         self._keep = (workload, b)
         cfg = (config or Config())._c()
@@ -394,16 +395,21 @@ class BatchContext:
         _check(lib().fgkl_context_autotune(self._ctx, C.byref(b), C.byref(cfg), int(repeats), C.byref(chosen), tried, 32,
                                            C.byref(n)))
         as_dict = lambda t: {"streams": int(t.streams), "grid_percent": int(t.grid_percent),
-                             "reads_per_warp": int(t.reads_per_warp), "ms": float(t.ms)}
+                             "reads_per_warp": int(t.reads_per_warp), "rows_extra": int(t.rows_extra),
+                             "warps_per_block": int(t.warps_per_block), "ms": float(t.ms)}
         return as_dict(chosen), [as_dict(tried[i]) for i in range(min(n.value, 32))]
 
-    def set_tuning(self, streams: int, grid_percent: int, reads_per_warp: int = 2) -> None:
-        _check(lib().fgkl_context_set_tuning(self._ctx, C.byref(_lib.Tuning(streams, grid_percent, reads_per_warp, 0.0))))
+    def set_tuning(self, streams: int, grid_percent: int, reads_per_warp: int = 2, rows_extra: int = 0,
+                   warps_per_block: int = 4) -> None:
+        """Launch configuration for the next prepare (fgkl_tuning); no value changes a result bit."""
+        _check(lib().fgkl_context_set_tuning(
+            self._ctx, C.byref(_lib.Tuning(streams, grid_percent, reads_per_warp, rows_extra, warps_per_block, 0.0))))
 
     def tuning(self) -> dict:
         t = _lib.Tuning()
         _check(lib().fgkl_context_get_tuning(self._ctx, C.byref(t)))
-        return {"streams": int(t.streams), "grid_percent": int(t.grid_percent), "reads_per_warp": int(t.reads_per_warp)}
+        return {"streams": int(t.streams), "grid_percent": int(t.grid_percent), "reads_per_warp": int(t.reads_per_warp),
+                "rows_extra": int(t.rows_extra), "warps_per_block": int(t.warps_per_block)}
 
     def set_profiling(self, on: bool) -> None:
         """Direct launches timed with CUDA events (no graph); see ``launch_profile``."""

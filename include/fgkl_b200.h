@@ -194,19 +194,24 @@ int64_t fgkl_batch_output_len(const fgkl_context* ctx);
 
 /* Launch configuration of a context's batched form (the autotuner's search space). */
 typedef struct fgkl_tuning {
-  int32_t streams;         /* streams the launches of one pass spread over, 1-8 (1: one after another) */
-  int32_t grid_percent;    /* each first-pass persistent grid, % of the kernel's resident-block limit, 10-100 */
-  int32_t reads_per_warp;  /* FP32 PD-HMM reads of at most 248 bases: 2 (FP32x2 pairs, the default) or 1 */
-  double ms;               /* autotuner: median device time of one run of the batch with this configuration */
+  int32_t streams;          /* streams the launches of one pass spread over, 1-8 (1: one after another) */
+  int32_t grid_percent;     /* each first-pass persistent grid, % of the kernel's resident-block limit, 10-100 */
+  int32_t reads_per_warp;   /* FP32 PD-HMM reads of at most 248 bases: 2 (FP32x2 pairs, the default) or 1 */
+  int32_t rows_extra;       /* tile shape: 1 runs plain FP32 reads one rows-per-lane step above the fewest
+                               that hold them (0, the default: the fewest) */
+  int32_t warps_per_block;  /* tile shape: warps per block of the FP32 first-pass kernels, 1, 2 or 4 (default) */
+  double ms;                /* autotuner: median device time of one run of the batch with this configuration */
 } fgkl_tuning;
 
-/* Autotuner. Plans `batch` once per candidate configuration (streams in {1, 2, 4, 8} x grid in
- * {100, 90, 75, 60} %; for an FP32 PD-HMM batch also one read per warp at 4 and 8 streams, full
- * grids). It times the candidate's kernels with CUDA events: one untimed run, then the median of
- * `repeats` runs. It keeps the fastest for the context's later batches and leaves `batch`
- * prepared with it. `tried` (may be NULL) receives up to `tried_cap` candidates in the order they
- * ran, and `n_tried` their count. Host-synchronous; a batch that represents the caller's workload
- * (a sample of it will do) gives the configuration that workload runs fastest with. */
+/* Autotuner. Plans `batch` once per candidate configuration and times its kernels with CUDA events:
+ * one untimed run, then the median of `repeats` runs. The candidates: streams in {1, 2, 4, 8} x grid
+ * in {100, 90, 75, 60} % (two reads per warp, default tile shape); for an FP32 PD-HMM batch also one
+ * read per warp at 4 and 8 streams, full grids; then, from the fastest so far, the tile shapes 1 and 2
+ * warps per block and, for a plain FP32 batch, one rows-per-lane step up. No configuration changes a
+ * result bit. It keeps the fastest for the context's later batches and leaves `batch` prepared with
+ * it. `tried` (may be NULL) receives up to `tried_cap` candidates in the order they ran, and
+ * `n_tried` their count. Host-synchronous; a batch that represents the caller's workload (a sample of
+ * it will do) gives the configuration that workload runs fastest with. */
 int fgkl_context_autotune(fgkl_context* ctx, const fgkl_batch* batch, const fgkl_config* config, int32_t repeats,
                           fgkl_tuning* chosen, fgkl_tuning* tried, int32_t tried_cap, int32_t* n_tried);
 /* Sets or reads a context's launch configuration directly (applies from the next prepare). */

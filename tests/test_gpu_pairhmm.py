@@ -342,11 +342,17 @@ def test_autotuner_times_every_launch_configuration_and_keeps_the_bits(gpu):
     default, _ = BatchContext().compute(w, FLOAT)
     ctx = BatchContext()
     chosen, tried = ctx.autotune(w, FLOAT, repeats=2)
-    assert len(tried) == 16
-    assert {(t["streams"], t["grid_percent"]) for t in tried} == {(s, g) for s in (1, 2, 4, 8) for g in (100, 90, 75, 60)}
+    assert len(tried) == 19
+    launch = [t for t in tried if t["rows_extra"] == 0 and t["warps_per_block"] == 4]
+    assert {(t["streams"], t["grid_percent"]) for t in launch[:16]} == {(s, g) for s in (1, 2, 4, 8) for g in (100, 90, 75, 60)}
+    # The tile shapes are tried around the fastest launch configuration of the first 16.
+    best16 = min(tried[:16], key=lambda t: t["ms"])
+    shapes = [(t["streams"], t["grid_percent"], t["rows_extra"], t["warps_per_block"]) for t in tried[16:]]
+    assert shapes == [(best16["streams"], best16["grid_percent"], 0, 1), (best16["streams"], best16["grid_percent"], 0, 2),
+                      (best16["streams"], best16["grid_percent"], 1, 4)]
     assert all(t["ms"] > 0 for t in tried)
     assert chosen["ms"] == min(t["ms"] for t in tried)
-    assert ctx.tuning() == {"streams": chosen["streams"], "grid_percent": chosen["grid_percent"], "reads_per_warp": 2}
+    assert ctx.tuning() == {k: chosen[k] for k in ("streams", "grid_percent", "reads_per_warp", "rows_extra", "warps_per_block")}
     # The batch stays prepared with the chosen configuration; launch shapes never change a result.
     ctx.run()
     tuned, _ = ctx.fetch()
@@ -354,6 +360,34 @@ def test_autotuner_times_every_launch_configuration_and_keeps_the_bits(gpu):
     ctx.set_tuning(1, 10)
     narrow, _ = ctx.compute(w, FLOAT)
     assert narrow.tobytes() == default.tobytes()
+
+
+@pytest.mark.parametrize("rows_extra,warps", [(1, 4), (0, 1), (0, 2), (1, 2)])
+def test_tile_shapes_keep_the_bits(gpu, rows_extra, warps):
+    """Rows per lane one step up (more padding rows) and 1 or 2 warps per block change no result bit:
+    a cell's arithmetic does not depend on the rows beside it, and the joins sum in read-row order."""
+    from fgkl_b200 import BatchContext
+
+    parts = [region(11, 70, 120, 24, 300), region(12, 9, 260, 5, 400), region(13, 30, 60, 7, 200)]
+    w = synthetic.from_regions(parts)
+    base = BatchContext()
+    base.set_profiling(True)
+    default, _ = base.compute(w, FLOAT)
+    ctx = BatchContext()
+    ctx.set_tuning(8, 100, 2, rows_extra, warps)
+    assert ctx.tuning()["rows_extra"] == rows_extra and ctx.tuning()["warps_per_block"] == warps
+    ctx.set_profiling(True)
+    shaped, _ = ctx.compute(w, FLOAT)
+    assert shaped.tobytes() == default.tobytes()
+
+    def bins(c):
+        return {(p["kind"], p["rows"]) for p in c.launch_profile() if not p["recomputation"]}
+
+    # Kind 0 (two reads, FP32x2) moves up one row up to 8, kind 1 (one read, 10-20 rows) one even step.
+    up = lambda k, r: (k, r + 1 if k == 0 and r < 8 else (r + 2 if k == 1 and r < 20 else r))
+    expected = {up(k, r) for k, r in bins(base)} if rows_extra else bins(base)
+    assert bins(ctx) == expected
+    assert any(k == 1 for k, _ in expected) and any(k == 0 for k, _ in expected)
 
 
 def test_page_locked_inputs_and_outputs_give_the_same_bits(gpu):

@@ -226,9 +226,15 @@ def test_one_or_two_reads_per_warp_give_the_same_bits_and_the_autotuner_tries_bo
     assert one.tobytes() == two.tobytes()
     expected = np.concatenate([reference_all(r, h) for r, h in parts])
     assert_close(one, expected, 1e-4, "one read per warp")
+    for warps in (1, 2):
+        shaped = BatchContext()
+        shaped.set_tuning(8, 100, 2, 0, warps)
+        assert shaped.compute(w, FLOAT)[0].tobytes() == two.tobytes(), warps
     chosen, tried = BatchContext().autotune(w, FLOAT, repeats=1)
-    assert len(tried) == 18
+    assert len(tried) == 20  # 16 launch configurations, 2 with one read per warp, 2 tile shapes (warps)
     assert sorted({t["reads_per_warp"] for t in tried}) == [1, 2]
+    assert sorted({t["warps_per_block"] for t in tried}) == [1, 2, 4]
+    assert all(t["rows_extra"] == 0 for t in tried)
     assert chosen["ms"] == min(t["ms"] for t in tried)
 
 
