@@ -281,13 +281,51 @@ __device__ __forceinline__ void pd_step(const LaunchArgs& a, const Program& prog
       if (next_slot >= 0) prefetch(sc.staged(st.seg_i + 1, lane), sc.slot(next_slot, lane), L::kSnap);
     }
   }
-  // Some lane is nearly always at a column carrying DEL_START or DEL_END or right after a deletion;
-  // the general path is exact for every column, so the warp takes it whenever any lane needs it
-  // rather than running both paths divergently.
-  if (__any_sync(kFull, (ev & kPdSlowMask) != 0)) {
-    // A column carrying DEL_START or DEL_END, or right after a deletion.
+  // A slow step (some lane at a column carrying DEL_START or DEL_END, or right after a deletion) runs
+  // the branch-value path for the whole warp; it is exact for every column, so lanes do not diverge
+  // between it and the plain recurrence.
+  const bool slow = __any_sync(kFull, (ev & kPdSlowMask) != 0);
+  const uint32_t s_first = (ev >> kPdFirstShift) & 3u, s_later = (ev >> kPdLaterShift) & 3u;
+  if (slow && __all_sync(kFull, s_first == s_later)) {
+    // A column carrying DEL_START or DEL_END, or right after a deletion, where every row of each lane
+    // is in one deletion state (the read's first row starts NORMAL, the later rows in the state the
+    // row above ended in, and the two differ only when a deletion runs to the haplotype's end): the
+    // merges and holds are then one predicate a lane, not a select a row.
     const bool mat = (ev & PD_MAT) != 0, de = (ev & PD_DE) != 0;
-    const uint32_t s_first = (ev >> kPdFirstShift) & 3u, s_later = (ev >> kPdLaterShift) & 3u;
+    const bool after = s_later == kPdAfterDel, keep = mat && s_later != kPdInsideDel;
+#pragma unroll
+    for (int r = R - 1; r >= 0; --r) {
+      V pM = r ? st.M[r - 1] : d.M, pX = r ? st.X[r - 1] : d.X, pY = r ? st.Y[r - 1] : d.Y;
+      V lM = st.M[r], lX = st.X[r], lY = st.Y[r];
+      if (after) {
+        pM = P::max(r ? st.BM[r - 1] : d.BM, pM);
+        pX = P::max(r ? st.BX[r - 1] : d.BX, pX);
+        pY = P::max(r ? st.BY[r - 1] : d.BY, pY);
+        lM = P::max(st.BM[r], lM);
+        lX = P::max(st.BX[r], lX);
+        lY = P::max(st.BY[r], lY);
+      }
+      if (keep) {
+        st.BM[r] = lM;
+        st.BX[r] = lX;
+        st.BY[r] = lY;
+      }
+      const V prior = kGeneric ? pr.prior_generic(ev, r) : pr.prior(sig, r);
+      st.Y[r] = P::kTransformed ? P::fma(lY, pr.c4[r], lM) : P::fma(lY, pr.c3[r], P::mul(lM, pr.c4[r]));
+      st.M[r] = P::mul(prior, cell_match<P>(pM, pX, pY, pr.c0[r], pr.c1[r], pr.c2[r]));
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      V qM = r ? st.M[r - 1] : u.M, qX = r ? st.X[r - 1] : u.X;
+      if (de) {
+        qM = P::max(r ? st.BM[r - 1] : u.BM, qM);
+        qX = P::max(r ? st.BX[r - 1] : u.BX, qX);
+      }
+      st.X[r] = P::kTransformed ? P::fma(qX, pr.c3[r], qM) : P::fma(qX, pr.c3[r], P::mul(qM, pr.c2[r]));
+    }
+  } else if (slow) {
+    // A slow column where some lane's first read row is in another state than its later rows.
+    const bool mat = (ev & PD_MAT) != 0, de = (ev & PD_DE) != 0;
 #pragma unroll
     for (int r = R - 1; r >= 0; --r) {
       bool after[P::NC], inside[P::NC];
