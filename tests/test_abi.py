@@ -167,3 +167,21 @@ def test_call_combining_python_mirror():
         fgkl_b200.set_call_combining(9)
     batches, requests = fgkl_b200.call_combining_stats()
     assert requests >= 2 * batches
+
+
+def test_allocation_free_entry_checks_its_bounds_on_the_host():
+    """The allocation-free entry refuses, before any device work, a call of more than
+    FGKL_NOALLOC_MAX_PAIRS (2^31 - 1) pairs and a max_read_len outside 1..620 (its ticket counter
+    is 64-bit, so no count up to the bound can wrap)."""
+    L = _lib.lib()
+    r = _lib.DeviceRegion()
+    r.num_reads, r.num_haplotypes, r.max_read_len = 65536, 32768, 151  # 2^31 pairs: one past the bound
+    assert L.fgkl_pairhmm_compute_device_noalloc(C.byref(r), None, None) == _lib.FGKL_E_INVALID_ARGUMENT
+    assert "2^31 - 1" in _lib.last_error()
+    r.num_reads, r.num_haplotypes = -1, 4
+    assert L.fgkl_pairhmm_compute_device_noalloc(C.byref(r), None, None) == _lib.FGKL_E_INVALID_ARGUMENT
+    for bad_len in (0, 621):
+        r.num_reads, r.num_haplotypes, r.max_read_len = 4, 4, bad_len
+        assert L.fgkl_pairhmm_compute_device_noalloc(C.byref(r), None, None) == _lib.FGKL_E_UNSUPPORTED
+    r.num_reads, r.num_haplotypes, r.max_read_len = 0, 4, 151  # no pairs: nothing to do
+    assert L.fgkl_pairhmm_compute_device_noalloc(C.byref(r), None, None) == 0
