@@ -15,13 +15,16 @@
 // per column into the stream entry (program.h), with the column's prior code (a match set: its base
 // and, on a SNP column, the flagged alternates).
 //
-// Branch values are only ever read at a column following one that carries DEL_START or DEL_END (and
-// one row down from a DEL_END column), so a lane keeps them lazily: its per-row branch registers are
-// updated only on columns carrying either flag (B = V(left), held, or merged by the state), and
-// hold a stale value elsewhere that nothing reads. Columns with no flag and not right after a
-// deletion (the vast majority) run the plain recurrence. The branch values of the lane above arrive
-// by shuffle every step like its match, insertion and deletion values, one set for the column and
-// the previous set for the diagonal.
+// A column right after DEL_END is AFTER_DEL in every row (the state machine sets it from the
+// DEL_END flag alone), and there the diagonal and the left cell enter only as max(B, V). So a lane
+// takes that max once, at the DEL_END column itself: after computing the column, each row's M, X
+// and Y become max(B, V) (row by row down the insertion sweep, so the next row's X reads U =
+// max(B(up), V(up)) as GATK's DEL_END rule asks, and the last row after the result has taken its
+// unmerged values). Every later reader of those values is a max reader, and the max is idempotent,
+// so the AFTER_DEL column itself needs no branch values at all. Branch values are then only the
+// lane's own rows: set to V(left) on a column carrying DEL_START or DEL_END (held inside a
+// deletion), read on DEL_END columns, stale elsewhere where nothing reads them; the lane above's
+// never cross. Columns carrying neither flag (the vast majority) run the plain recurrence.
 //
 // Priors. A PD region maps its reads' distinct bytes to classes 0..30; each match-set code carries
 // the bit set of classes it accepts, so a row's prior is pm or px by one bit test.
@@ -40,8 +43,8 @@ struct PdLayout {
   using V = typename P::V;
   static constexpr int kRound = 16 / static_cast<int>(sizeof(V)) > 1 ? 16 / static_cast<int>(sizeof(V)) : 1;
   static constexpr int up(int x) { return (x + kRound - 1) / kRound * kRound; }
-  // M, X, Y rows; branch M, X, Y rows; above-row M, X, Y and branch M, X, Y; accumulated result.
-  static constexpr int kSnap = up(6 * R + 7);
+  // M, X, Y rows; branch M, X, Y rows; above-row M, X, Y; accumulated result.
+  static constexpr int kSnap = up(6 * R + 4);
   static constexpr size_t kStageBytes = 32ull * kSnap * sizeof(V);
   static constexpr size_t kSmemPerWarp = kStageBytes;
 };
@@ -162,16 +165,16 @@ struct PdState {
   V BM[R], BX[R], BY[R];
   V acc;
   int seg_i;
-  // Strip-mined reads: the row above lane 0's top row for this step's column, values and branch
-  // values (read only by pd_step<..., kCarry = true>).
-  V cM, cX, cY, cBM, cBX, cBY;
+  // Strip-mined reads: the row above lane 0's top row for this step's column (read only by
+  // pd_step<..., kCarry = true>).
+  V cM, cX, cY;
 };
 
-// The lane above's bottom row: values and branch values.
+// The lane above's bottom row.
 template <class P>
 struct PdEdge {
   using V = typename P::V;
-  V M, X, Y, BM, BX, BY;
+  V M, X, Y;
 };
 
 // One PD forward step: events, then the column. `u` receives the lane above's bottom row for this
@@ -190,16 +193,10 @@ __device__ __forceinline__ void pd_step(const LaunchArgs& a, const Program& prog
   u.M = P::up(st.M[R - 1]);
   u.X = P::up(st.X[R - 1]);
   u.Y = P::up(st.Y[R - 1]);
-  u.BM = P::up(st.BM[R - 1]);
-  u.BX = P::up(st.BX[R - 1]);
-  u.BY = P::up(st.BY[R - 1]);
   if (kCarry && lane == 0) {
     u.M = st.cM;
     u.X = st.cX;
     u.Y = st.cY;
-    u.BM = st.cBM;
-    u.BX = st.cBX;
-    u.BY = st.cBY;
   }
   // END and ACC act in lane 31 alone (the read's last row); the other lanes pass them by without
   // entering the event code, which every lane otherwise reaches at its own step.
@@ -224,10 +221,7 @@ __device__ __forceinline__ void pd_step(const LaunchArgs& a, const Program& prog
         o[6 * R] = d.M;
         o[6 * R + 1] = d.X;
         o[6 * R + 2] = d.Y;
-        o[6 * R + 3] = d.BM;
-        o[6 * R + 4] = d.BX;
-        o[6 * R + 5] = d.BY;
-        o[6 * R + 6] = st.acc;
+        o[6 * R + 3] = st.acc;
       }
     }
     if ((ev & EV_END) && lane == 31) {
@@ -256,10 +250,7 @@ __device__ __forceinline__ void pd_step(const LaunchArgs& a, const Program& prog
         d.M = s[6 * R];
         d.X = s[6 * R + 1];
         d.Y = s[6 * R + 2];
-        d.BM = s[6 * R + 3];
-        d.BX = s[6 * R + 4];
-        d.BY = s[6 * R + 5];
-        st.acc = s[6 * R + 6];
+        st.acc = s[6 * R + 3];
       } else {
         // The origin: the row-0 constant in the padding rows, zero branch values (GATK never writes
         // branch column zero).
@@ -267,7 +258,7 @@ __device__ __forceinline__ void pd_step(const LaunchArgs& a, const Program& prog
                              : (P::kDouble ? static_cast<S>(rec->init_d) : static_cast<S>(rec->init_f));
 #pragma unroll
         for (int r = 0; r < R; ++r) st.M[r] = st.X[r] = st.Y[r] = st.BM[r] = st.BX[r] = st.BY[r] = P::zero();
-        d.M = d.X = d.Y = d.BM = d.BX = d.BY = st.acc = P::zero();
+        d.M = d.X = d.Y = st.acc = P::zero();
         if (lane * R <= pad_hi) {
 #pragma unroll
           for (int c = 0; c < P::NC; ++c) {
@@ -281,86 +272,62 @@ __device__ __forceinline__ void pd_step(const LaunchArgs& a, const Program& prog
       if (next_slot >= 0) prefetch(sc.staged(st.seg_i + 1, lane), sc.slot(next_slot, lane), L::kSnap);
     }
   }
-  // A slow step (some lane at a column carrying DEL_START or DEL_END, or right after a deletion) runs
-  // the branch-value path for the whole warp; it is exact for every column, so lanes do not diverge
-  // between it and the plain recurrence.
+  // A slow step (some lane at a column carrying DEL_START or DEL_END) runs the branch-value path for
+  // the whole warp; it is exact for every column, so lanes do not diverge between it and the plain
+  // recurrence.
   const bool slow = __any_sync(kFull, (ev & kPdSlowMask) != 0);
-  const uint32_t s_first = (ev >> kPdFirstShift) & 3u, s_later = (ev >> kPdLaterShift) & 3u;
-  if (slow && __all_sync(kFull, s_first == s_later)) {
-    // A column carrying DEL_START or DEL_END, or right after a deletion, where every row of each lane
-    // is in one deletion state (the read's first row starts NORMAL, the later rows in the state the
-    // row above ended in, and the two differ only when a deletion runs to the haplotype's end): the
-    // merges and holds are then one predicate a lane, not a select a row.
-    const bool mat = (ev & PD_MAT) != 0, de = (ev & PD_DE) != 0;
-    const bool after = s_later == kPdAfterDel, keep = mat && s_later != kPdInsideDel;
+  const bool de = slow && (ev & PD_DE) != 0;
+  if (slow) {
+    const bool mat = (ev & PD_MAT) != 0;
+    const uint32_t s_first = (ev >> kPdFirstShift) & 3u, s_later = (ev >> kPdLaterShift) & 3u;
+    if (__all_sync(kFull, s_first == s_later)) {
+      // Every row of each lane in one deletion state (the read's first row starts NORMAL, the later
+      // rows in the state the row above ended in; the two differ only when a deletion runs to the
+      // haplotype's end): a column carrying either flag keeps V(left) as the branch values unless
+      // inside a deletion, one predicate a lane.
+      const bool keep = mat && s_later != kPdInsideDel;
 #pragma unroll
-    for (int r = R - 1; r >= 0; --r) {
-      V pM = r ? st.M[r - 1] : d.M, pX = r ? st.X[r - 1] : d.X, pY = r ? st.Y[r - 1] : d.Y;
-      V lM = st.M[r], lX = st.X[r], lY = st.Y[r];
-      if (after) {
-        pM = P::max(r ? st.BM[r - 1] : d.BM, pM);
-        pX = P::max(r ? st.BX[r - 1] : d.BX, pX);
-        pY = P::max(r ? st.BY[r - 1] : d.BY, pY);
-        lM = P::max(st.BM[r], lM);
-        lX = P::max(st.BX[r], lX);
-        lY = P::max(st.BY[r], lY);
+      for (int r = R - 1; r >= 0; --r) {
+        const V pM = r ? st.M[r - 1] : d.M, pX = r ? st.X[r - 1] : d.X, pY = r ? st.Y[r - 1] : d.Y;
+        if (keep) {
+          st.BM[r] = st.M[r];
+          st.BX[r] = st.X[r];
+          st.BY[r] = st.Y[r];
+        }
+        const V prior = kGeneric ? pr.prior_generic(ev, r) : pr.prior(sig, r);
+        st.Y[r] = P::kTransformed ? P::fma(st.Y[r], pr.c4[r], st.M[r]) : P::fma(st.Y[r], pr.c3[r], P::mul(st.M[r], pr.c4[r]));
+        st.M[r] = P::mul(prior, cell_match<P>(pM, pX, pY, pr.c0[r], pr.c1[r], pr.c2[r]));
       }
-      if (keep) {
-        st.BM[r] = lM;
-        st.BX[r] = lX;
-        st.BY[r] = lY;
+    } else {
+      // Some lane's first read row is in another state than its later rows.
+#pragma unroll
+      for (int r = R - 1; r >= 0; --r) {
+        bool inside[P::NC];
+#pragma unroll
+        for (int c = 0; c < P::NC; ++c) inside[c] = ((lane * R + r == rd[c].pad) ? s_first : s_later) == kPdInsideDel;
+        const V pM = r ? st.M[r - 1] : d.M, pX = r ? st.X[r - 1] : d.X, pY = r ? st.Y[r - 1] : d.Y;
+        if (mat) {
+          st.BM[r] = P::sel(inside[0], inside[P::NC - 1], st.BM[r], st.M[r]);
+          st.BX[r] = P::sel(inside[0], inside[P::NC - 1], st.BX[r], st.X[r]);
+          st.BY[r] = P::sel(inside[0], inside[P::NC - 1], st.BY[r], st.Y[r]);
+        }
+        const V prior = kGeneric ? pr.prior_generic(ev, r) : pr.prior(sig, r);
+        st.Y[r] = P::kTransformed ? P::fma(st.Y[r], pr.c4[r], st.M[r]) : P::fma(st.Y[r], pr.c3[r], P::mul(st.M[r], pr.c4[r]));
+        st.M[r] = P::mul(prior, cell_match<P>(pM, pX, pY, pr.c0[r], pr.c1[r], pr.c2[r]));
       }
-      const V prior = kGeneric ? pr.prior_generic(ev, r) : pr.prior(sig, r);
-      st.Y[r] = P::kTransformed ? P::fma(lY, pr.c4[r], lM) : P::fma(lY, pr.c3[r], P::mul(lM, pr.c4[r]));
-      st.M[r] = P::mul(prior, cell_match<P>(pM, pX, pY, pr.c0[r], pr.c1[r], pr.c2[r]));
     }
+    // Insertion values from the top row down. On a DEL_END column each row's values take the max
+    // with its branch values once its X is computed (the last row's after the result below), so
+    // the next row's X reads U = max(B(up), V(up)); the lane above's bottom row arrives merged.
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      V qM = r ? st.M[r - 1] : u.M, qX = r ? st.X[r - 1] : u.X;
-      if (de) {
-        qM = P::max(r ? st.BM[r - 1] : u.BM, qM);
-        qX = P::max(r ? st.BX[r - 1] : u.BX, qX);
-      }
+      const V qM = r ? st.M[r - 1] : u.M, qX = r ? st.X[r - 1] : u.X;
       st.X[r] = P::kTransformed ? P::fma(qX, pr.c3[r], qM) : P::fma(qX, pr.c3[r], P::mul(qM, pr.c2[r]));
-    }
-  } else if (slow) {
-    // A slow column where some lane's first read row is in another state than its later rows.
-    const bool mat = (ev & PD_MAT) != 0, de = (ev & PD_DE) != 0;
-#pragma unroll
-    for (int r = R - 1; r >= 0; --r) {
-      bool after[P::NC], inside[P::NC];
-#pragma unroll
-      for (int c = 0; c < P::NC; ++c) {
-        const uint32_t s = (lane * R + r == rd[c].pad) ? s_first : s_later;
-        after[c] = s == kPdAfterDel;
-        inside[c] = s == kPdInsideDel;
+      if (de && r + 1 < R) {
+        st.M[r] = P::max(st.BM[r], st.M[r]);
+        st.X[r] = P::max(st.BX[r], st.X[r]);
+        st.Y[r] = P::max(st.BY[r], st.Y[r]);
       }
-      const bool a0 = after[0], a1 = after[P::NC - 1];
-      const V qBM = r ? st.BM[r - 1] : d.BM, qBX = r ? st.BX[r - 1] : d.BX, qBY = r ? st.BY[r - 1] : d.BY;
-      V pM = r ? st.M[r - 1] : d.M, pX = r ? st.X[r - 1] : d.X, pY = r ? st.Y[r - 1] : d.Y;
-      pM = P::sel(a0, a1, P::max(qBM, pM), pM);
-      pX = P::sel(a0, a1, P::max(qBX, pX), pX);
-      pY = P::sel(a0, a1, P::max(qBY, pY), pY);
-      const V lM = P::sel(a0, a1, P::max(st.BM[r], st.M[r]), st.M[r]);
-      const V lX = P::sel(a0, a1, P::max(st.BX[r], st.X[r]), st.X[r]);
-      const V lY = P::sel(a0, a1, P::max(st.BY[r], st.Y[r]), st.Y[r]);
-      if (mat) {
-        st.BM[r] = P::sel(inside[0], inside[P::NC - 1], st.BM[r], lM);
-        st.BX[r] = P::sel(inside[0], inside[P::NC - 1], st.BX[r], lX);
-        st.BY[r] = P::sel(inside[0], inside[P::NC - 1], st.BY[r], lY);
-      }
-      const V prior = kGeneric ? pr.prior_generic(ev, r) : pr.prior(sig, r);
-      st.Y[r] = P::kTransformed ? P::fma(lY, pr.c4[r], lM) : P::fma(lY, pr.c3[r], P::mul(lM, pr.c4[r]));
-      st.M[r] = P::mul(prior, cell_match<P>(pM, pX, pY, pr.c0[r], pr.c1[r], pr.c2[r]));
-    }
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      V qM = r ? st.M[r - 1] : u.M, qX = r ? st.X[r - 1] : u.X;
-      if (de) {
-        qM = P::max(r ? st.BM[r - 1] : u.BM, qM);
-        qX = P::max(r ? st.BX[r - 1] : u.BX, qX);
-      }
-      st.X[r] = P::kTransformed ? P::fma(qX, pr.c3[r], qM) : P::fma(qX, pr.c3[r], P::mul(qM, pr.c2[r]));
     }
   } else {
 #pragma unroll
@@ -377,6 +344,11 @@ __device__ __forceinline__ void pd_step(const LaunchArgs& a, const Program& prog
     }
   }
   st.acc = P::fma(st.X[R - 1], an, P::add(st.acc, st.M[R - 1]));
+  if (de) {
+    st.M[R - 1] = P::max(st.BM[R - 1], st.M[R - 1]);
+    st.X[R - 1] = P::max(st.BX[R - 1], st.X[R - 1]);
+    st.Y[R - 1] = P::max(st.BY[R - 1], st.Y[R - 1]);
+  }
 }
 
 // Entry p of a recomputation stream: the haplotype's forward entries (code and deletion bits),
@@ -410,7 +382,7 @@ __device__ void pd_forward_pass(const LaunchArgs& a, const Program& prog, const 
   st.acc = P::zero();
   st.seg_i = -1;
   PdEdge<P> ea, eb;
-  ea.M = ea.X = ea.Y = ea.BM = ea.BX = ea.BY = P::zero();
+  ea.M = ea.X = ea.Y = P::zero();
   eb = ea;
   if (P::kDouble && synth_len > 0) {
     const int n = synth_len;
@@ -540,15 +512,15 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, (PdMinBlocks<P, R>::value
 // Strip-mined PD pairs (reads longer than 620 bases), and every pair of a region whose reads hold
 // more distinct bytes than the class bits cover (kGeneric): one read against one distinct
 // haplotype, unshared, over the haplotype's forward entries, the rows cut into blocks of 32 R rows
-// run one after another. Lane 0's row above -- values and branch values -- comes from a carry row:
-// GATK's row 0 in the first block (M = X = 0, Y = INITIAL / hap_len, no branch values), after that
+// run one after another. Lane 0's row above comes from a carry row (merged on DEL_END columns like
+// every row): GATK's row 0 in the first block (M = X = 0, Y = INITIAL / hap_len), after that
 // the previous block's bottom row, written by lane 31 column by column and read by lane 0 31 steps
 // before lane 31 of the next block overwrites it (the plain strip-mined kernel's scheme). The
 // state a block's top row starts in is the previous row's, which the entries' later-row state
 // carries; only the read's first row (in the first block) takes the first-row state.
 // ---------------------------------------------------------------------------------------------
 
-constexpr int kPdCarryVals = 8;  // M, X, Y, BM, BX, BY, padded to 16 bytes
+constexpr int kPdCarryVals = 4;  // M, X, Y, padded to 16 bytes
 
 template <class P>
 constexpr size_t pd_long_scratch_size(int max_hap_len) {
@@ -559,8 +531,7 @@ template <class P, int R>
 __device__ __forceinline__ void pd_long_store(typename P::V* carry, const PdState<P, R>& st, int lane, int t, int n, bool last) {
   const int p = t - 31;
   if (!last && lane == 31 && p >= 0 && p < n) {
-    typename P::V rec[kPdCarryVals] = {st.M[R - 1],  st.X[R - 1],  st.Y[R - 1], st.BM[R - 1],
-                                       st.BX[R - 1], st.BY[R - 1], P::zero(),   P::zero()};
+    typename P::V rec[kPdCarryVals] = {st.M[R - 1], st.X[R - 1], st.Y[R - 1], P::zero()};
     store_record(carry + static_cast<size_t>(p) * kPdCarryVals, rec);
   }
 }
@@ -576,9 +547,6 @@ __device__ __forceinline__ void pd_set_carry(PdState<P, R>& st, const typename P
   st.cM = c[0];
   st.cX = c[1];
   st.cY = c[2];
-  st.cBM = c[3];
-  st.cBX = c[4];
-  st.cBY = c[5];
 }
 
 template <class P, int R, bool kGeneric>
@@ -593,11 +561,11 @@ __device__ void pd_long_block(const LaunchArgs& a, const ReadRef* rd, int lane, 
   for (int r = 0; r < R; ++r) st.M[r] = st.X[r] = st.Y[r] = st.BM[r] = st.BX[r] = st.BY[r] = P::zero();
   st.acc = P::zero();
   st.seg_i = -1;
-  st.cM = st.cX = st.cBM = st.cBX = st.cBY = P::zero();
+  st.cM = st.cX = P::zero();
   st.cY = first ? static_cast<S>(Consts<P::kDouble>::kInitial / n) : P::zero();
   const Program prog{};
   PdEdge<P> ea, eb;
-  ea.M = ea.X = ea.Y = ea.BM = ea.BX = ea.BY = P::zero();
+  ea.M = ea.X = ea.Y = P::zero();
   eb = ea;
   V n0[kPdCarryVals], n1[kPdCarryVals];
 #pragma unroll

@@ -44,8 +44,9 @@ constexpr uint32_t PD_DE = 1u << 15;   // DEL_END: insertion from the branch val
 constexpr int kPdFirstShift = 16;      // 2 bits: deletion state in the read's first row
 constexpr int kPdLaterShift = 18;      // 2 bits: deletion state in the later rows
 constexpr uint32_t kPdNormal = 0, kPdInsideDel = 1, kPdAfterDel = 2;
-// Any column a PD lane cannot compute with the plain recurrence.
-constexpr uint32_t kPdSlowMask = PD_MAT | PD_DE | (kPdAfterDel << kPdFirstShift) | (kPdAfterDel << kPdLaterShift);
+// Any column a PD lane cannot compute with the plain recurrence. The column after DEL_END (AFTER_DEL
+// in every row) is not one of them: its max merges are taken at the DEL_END column itself.
+constexpr uint32_t kPdSlowMask = PD_MAT | PD_DE;
 constexpr int kPdPayloadShift = 20;
 constexpr uint32_t kPdPayloadNone = (1u << (32 - kPdPayloadShift)) - 1;
 // Read bytes a PD region distinguishes (classes 0..30; 31 marks a padding row).
