@@ -456,9 +456,12 @@ __device__ void pd_finalize(const LaunchArgs& a, const Task& task, const Region&
   if (lost_count && !dense) atomicAdd(&a.v.counters->lost_pairs, lost_count);
 }
 
+// Resident blocks of 4 warps the register budget is cut for (measured on c3): one-read FP32 at 4
+// (128 registers, no spill), the FP32x2 form at 2 (up to 255), FP64 at 3 for R <= 5 (168 registers,
+// a few spilled values: the recomputation sweeps run faster at 12 warps per SM than at 8), else 1.
 template <class P, int R>
 struct PdMinBlocks {
-  static constexpr int value = P::kDouble ? 1 : 2;  // the packed form (two reads) too: up to 255 registers
+  static constexpr int value = P::kDouble ? (R <= 5 ? 3 : 1) : (P::NC == 2 ? 2 : 4);
 };
 
 template <class P, int R>
