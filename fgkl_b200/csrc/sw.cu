@@ -197,32 +197,61 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 8) sw_kernel(SwArgs a) {
     __threadfence_block();
     __syncwarp();
 
-    // End cell and traceback (reference.rs:113-203), lane 0.
-    if (lane == 0) {
-      int p1 = 0, p2 = m, seg = 0;
-      int best = INT_MIN;
-      if (a.strategy == kSwIndel) {
-        p1 = n;
-      } else {
-        for (int i = 1; i <= n; ++i) {
-          const int cur = sc.last_col[i - 1];
-          if (cur >= best) {
-            p1 = i;
-            best = cur;
-          }
-        }
-        if (a.strategy != kSwLeadingIndel) {
-          for (int j = 1; j <= m; ++j) {
-            const int cur = sc.last_row[j - 1];
-            if (cur > best || (cur == best && abs(n - j) < abs(p1 - p2))) {
-              p1 = n;
-              p2 = j;
-              best = cur;
-              seg = m - j;
-            }
-          }
+    // End cell (reference.rs:113-143), by the warp: the best of the last column, ties to the lowest
+    // row (the scan runs down the column and keeps the last of equal values), then, unless the
+    // strategy is LeadingIndel, the last row's cells, each taking over when higher, or equal and
+    // nearer the diagonal (|n - j| below the current |p1 - p2|, ties to the earlier column). Each
+    // lane scans a strided share; the shares combine in the scan's order.
+    int p1 = 0, p2 = m, seg = 0;
+    if (a.strategy == kSwIndel) {
+      p1 = n;
+    } else {
+      int cv = INT_MIN, ci = 0;
+      for (int i = lane + 1; i <= n; i += 32) {
+        const int cur = sc.last_col[i - 1];
+        if (cur >= cv) {
+          cv = cur;
+          ci = i;
         }
       }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const int ov = __shfl_xor_sync(kFull, cv, o), oi = __shfl_xor_sync(kFull, ci, o);
+        if (ov > cv || (ov == cv && oi > ci)) {
+          cv = ov;
+          ci = oi;
+        }
+      }
+      p1 = ci;
+      if (a.strategy != kSwLeadingIndel) {
+        int rv = INT_MIN, rj = 0, rd = INT_MAX;
+        for (int j = lane + 1; j <= m; j += 32) {
+          const int cur = sc.last_row[j - 1], d = abs(n - j);
+          if (cur > rv || (cur == rv && d < rd)) {
+            rv = cur;
+            rj = j;
+            rd = d;
+          }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          const int ov = __shfl_xor_sync(kFull, rv, o), oj = __shfl_xor_sync(kFull, rj, o), od = __shfl_xor_sync(kFull, rd, o);
+          if (ov > rv || (ov == rv && (od < rd || (od == rd && oj < rj)))) {
+            rv = ov;
+            rj = oj;
+            rd = od;
+          }
+        }
+        if (rv > cv || (rv == cv && rd < abs(ci - m))) {
+          p1 = n;
+          p2 = rj;
+          seg = m - rj;
+        }
+      }
+    }
+
+    // Traceback (reference.rs:144-203), lane 0.
+    if (lane == 0) {
       // Elements last to first, reversed at the end.
       int e = 0;
       if (seg > 0 && a.strategy == kSwSoftClip) {
@@ -284,9 +313,56 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 8) sw_kernel(SwArgs a) {
   }
 }
 
+// Packs every pair's CIGAR elements (counts[k] of them from cigar_slot[k]) into one dense run,
+// pair after pair, so the host downloads only the elements the batch produced rather than every
+// slot's capacity. One block: each thread sums a contiguous share of the counts, the block scans the
+// 1024 sums, each thread then copies its share's pairs.
+constexpr int kCompactThreads = 1024;
+__global__ void __launch_bounds__(kCompactThreads) sw_compact_kernel(const uint32_t* cigar, const int64_t* slot, const int32_t* count,
+                                                                     int n_pairs, uint32_t* packed) {
+  __shared__ int64_t warp_sum[kCompactThreads / 32];
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int64_t share = (static_cast<int64_t>(n_pairs) + kCompactThreads - 1) / kCompactThreads;
+  const int64_t lo = min(static_cast<int64_t>(n_pairs), tid * share), hi = min(static_cast<int64_t>(n_pairs), lo + share);
+  int64_t own = 0;
+  for (int64_t k = lo; k < hi; ++k) own += count[k];
+  // Exclusive scan of the per-thread sums: within each warp, then over the warps.
+  int64_t incl = own;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int64_t v = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += v;
+  }
+  if (lane == 31) warp_sum[w] = incl;
+  __syncthreads();
+  if (w == 0) {
+    int64_t ws = warp_sum[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int64_t v = __shfl_up_sync(kFull, ws, o);
+      if (lane >= o) ws += v;
+    }
+    warp_sum[lane] = ws;  // inclusive over the warps
+  }
+  __syncthreads();
+  int64_t pos = (w > 0 ? warp_sum[w - 1] : 0) + incl - own;
+  for (int64_t k = lo; k < hi; ++k) {
+    const uint32_t* src = cigar + slot[k];
+    for (int i = 0; i < count[k]; ++i) packed[pos + i] = src[i];
+    pos += count[k];
+  }
+}
+
 }  // namespace
 
 size_t sw_scratch_bytes(int64_t ref_len, int64_t alt_len) { return SwScratch::bytes(ref_len, alt_len); }
+
+cudaError_t sw_compact(const uint32_t* cigar, const int64_t* slot, const int32_t* count, int n_pairs, uint32_t* packed,
+                       cudaStream_t stream) {
+  if (n_pairs <= 0) return cudaSuccess;
+  sw_compact_kernel<<<1, kCompactThreads, 0, stream>>>(cigar, slot, count, n_pairs, packed);
+  return cudaGetLastError();
+}
 
 void sw_occupancy(int* blocks_per_sm, int* threads_per_block) {
   *threads_per_block = kWarpsPerBlock * 32;

@@ -39,5 +39,9 @@ struct SwArgs {
 size_t sw_scratch_bytes(int64_t ref_len, int64_t alt_len);
 void sw_occupancy(int* blocks_per_sm, int* threads_per_block);
 cudaError_t sw_launch(int blocks, const SwArgs& a, cudaStream_t stream);
+// Packs the pairs' CIGAR elements, pair after pair, into `packed` (as many elements as the counts
+// sum to), after sw_launch on the same stream.
+cudaError_t sw_compact(const uint32_t* cigar, const int64_t* slot, const int32_t* count, int n_pairs, uint32_t* packed,
+                       cudaStream_t stream);
 
 }  // namespace fgkl

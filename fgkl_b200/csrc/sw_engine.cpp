@@ -107,7 +107,7 @@ int SwEngine::align(const SwBatch& in, const SwScores& s, int strategy, uint32_t
 
   const int64_t ref_bytes = in.ref_off[P], alt_bytes = in.alt_off[P];
   if (!grow(d_seq_, cap_seq_, static_cast<size_t>(ref_bytes + alt_bytes) + 16) || !grow(d_idx_, cap_idx_, 3 * static_cast<size_t>(P + 1)) ||
-      !grow(d_small_, cap_small_, 3 * static_cast<size_t>(P) + 1) || !grow(d_cigar_, cap_cigar_, static_cast<size_t>(slot[P])) ||
+      !grow(d_small_, cap_small_, 3 * static_cast<size_t>(P) + 1) || !grow(d_cigar_, cap_cigar_, 2 * static_cast<size_t>(slot[P])) ||
       !grow(d_scratch_, cap_scratch_, static_cast<size_t>(blocks) * kWarps * stride))
     return fail(FGKL_E_OUT_OF_MEMORY, "device allocation failed");
   int rc;
@@ -149,11 +149,31 @@ int SwEngine::align(const SwBatch& in, const SwScores& s, int strategy, uint32_t
   a.offset = d_offsets;
   a.counter = d_counter;
   if ((rc = check(sw_launch(static_cast<int>(blocks), a, stream_), "Smith-Waterman launch"))) return rc;
-  if ((rc = check(cudaMemcpyAsync(cigar, d_cigar_, 4 * static_cast<size_t>(slot[P]), cudaMemcpyDeviceToHost, stream_), "download CIGARs")) ||
+  // Only the elements produced cross to the host: packed pair after pair on the device, then
+  // scattered into the caller's slots (a CIGAR is a few elements; its slot holds ref + alt + 2).
+  uint32_t* d_packed = d_cigar_ + slot[P];
+  if ((rc = check(sw_compact(d_cigar_, d_slot, d_counts, static_cast<int>(P), d_packed, stream_), "CIGAR packing")) ||
       (rc = check(cudaMemcpyAsync(counts, d_counts, 4 * static_cast<size_t>(P), cudaMemcpyDeviceToHost, stream_), "download counts")) ||
-      (rc = check(cudaMemcpyAsync(offsets, d_offsets, 4 * static_cast<size_t>(P), cudaMemcpyDeviceToHost, stream_), "download offsets")))
+      (rc = check(cudaMemcpyAsync(offsets, d_offsets, 4 * static_cast<size_t>(P), cudaMemcpyDeviceToHost, stream_), "download offsets")) ||
+      (rc = check(cudaStreamSynchronize(stream_), "Smith-Waterman kernel")))
     return rc;
-  return check(cudaStreamSynchronize(stream_), "Smith-Waterman kernel");
+  int64_t total = 0;
+  for (int64_t k = 0; k < P; ++k) {
+    if (counts[k] < 0 || counts[k] > sw_cigar_slot(in.ref_off[k + 1] - in.ref_off[k], in.alt_off[k + 1] - in.alt_off[k]))
+      return fail(FGKL_E_CUDA, "Smith-Waterman kernel returned an impossible CIGAR length");
+    total += counts[k];
+  }
+  packed_.resize(static_cast<size_t>(total));
+  if (total > 0 &&
+      ((rc = check(cudaMemcpyAsync(packed_.data(), d_packed, 4 * static_cast<size_t>(total), cudaMemcpyDeviceToHost, stream_),
+                   "download CIGARs")) ||
+       (rc = check(cudaStreamSynchronize(stream_), "download CIGARs"))))
+    return rc;
+  for (int64_t k = 0, pos = 0; k < P; ++k) {
+    std::copy(packed_.begin() + pos, packed_.begin() + pos + counts[k], cigar + slot[k]);
+    pos += counts[k];
+  }
+  return FGKL_OK;
 }
 
 }  // namespace fgkl

@@ -6,6 +6,7 @@
 
 #include <cstdint>
 #include <string>
+#include <vector>
 
 #include "sw.cuh"
 
@@ -57,10 +58,11 @@ class SwEngine {
   size_t cap_idx_ = 0;
   int32_t* d_small_ = nullptr;  // order | counts | offsets | counter
   size_t cap_small_ = 0;
-  uint32_t* d_cigar_ = nullptr;
+  uint32_t* d_cigar_ = nullptr;  // slot layout | packed elements
   size_t cap_cigar_ = 0;
   char* d_scratch_ = nullptr;
   size_t cap_scratch_ = 0;
+  std::vector<uint32_t> packed_;  // the batch's CIGAR elements, pair after pair
 };
 
 }  // namespace fgkl
