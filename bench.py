@@ -38,6 +38,10 @@ WORKLOAD = ("batched uneven PairHMM: 4096 regions, 8-256 reads (75% of length 15
 FLOP_FORWARD = 12  # 4 FMUL + 4 FFMA per forward cell (fgkl kernel.rs:1011-1013)
 FLOP_BACKWARD = 11  # 3 FMUL + 4 FFMA per backward cell (kernel.rs:1080-1088)
 FLOP_ADJOINT = 40   # adjoint cell: backward 11 + forward 11 + gradient terms 18
+# Smith-Waterman cell (GATK's recurrences, reference.rs:69-110), integer operations: the diagonal's
+# score (compare, add), each gap (two adds, the compare that picks open or extend), the three-way
+# choice of H (two compares), the -1e8 floor, and the traceback byte (direction and two gap bits).
+SW_OPS_PER_CELL = 13
 L2_BYTES = 126 * 1024 * 1024
 
 
@@ -478,15 +482,22 @@ def smith_waterman_line(args, device, threads):
     counts = np.zeros(len(pairs), np.int32)
     offsets = np.zeros(len(pairs), np.int32)
     prm = P._c()
-    times = []
+    times, kernel = [], []
+    kms = C.c_float()
     for _ in range(max(3, min(args.steps, 5))):
         t0 = time.perf_counter()
         _check(_lib.lib().fgkl_sw_align_batch(ctx._ctx, C.byref(b), C.byref(prm), int(OverhangStrategy.INDEL),
                                               cigar.ctypes.data_as(C.POINTER(C.c_uint32)), cap,
                                               counts.ctypes.data_as(_lib.i32p), offsets.ctypes.data_as(_lib.i32p)))
         times.append(time.perf_counter() - t0)
+        _check(_lib.lib().fgkl_sw_last_kernel_ms(ctx._ctx, C.byref(kms)))
+        kernel.append(kms.value / 1e3)
     ctx.close()
     t = statistics.median(times)
+    tk = statistics.median(kernel)
+    alu = C.c_double()
+    _check(_lib.lib().fgkl_probe_int32_alu_gops(device, C.byref(alu)))
+    sw_gops = SW_OPS_PER_CELL * cells / tk / 1e9
     same = all(int(offsets[k]) == got[k].offset and counts[k] == len(_cigar_ops(got[k].cigar)) for k in range(0, len(pairs), 97))
     params = (P.match_value, P.mismatch_penalty, P.gap_open_penalty, P.gap_extend_penalty)
     sample = list(range(0, len(pairs), max(1, len(pairs) // 512)))
@@ -503,6 +514,11 @@ def smith_waterman_line(args, device, threads):
     return {"workload": f"Smith-Waterman: {len(pairs)} pairs, reference 500, alternate its first 500 bases with 3 substitutions "
                         "and 1 deletion (fgkl's sw-bench shape), haplotype-to-reference scores, Indel strategy",
             "gcups": cells / t / 1e9, "ms_per_step": 1e3 * t, "cells": cells,
+            "kernel": {"ms": 1e3 * tk, "gcups": cells / tk / 1e9,
+                       "timing": "CUDA events around the fill-and-traceback launch of each timed call, median"},
+            "roofline": {"bound": "int32 alu", "unit": "Gop/s", "achieved": sw_gops, "peak": alu.value,
+                         "frac": sw_gops / alu.value, "ops_per_cell": SW_OPS_PER_CELL,
+                         "peak_source": "measured XOR and signed-max chains on this GPU (fgkl_probe_int32_alu_gops)"},
             "timing": "one fgkl_sw_align_batch call (C ABI) from host arrays built once: uploads, kernel, CIGAR packing, "
                       "downloads, wall clock",
             "timed_calls_match_the_python_call": same,

@@ -180,6 +180,8 @@ def lib() -> C.CDLL:
     L.fgkl_sw_align_batch.argtypes = [C.c_void_p, C.POINTER(SwBatch), C.POINTER(SwParams), C.c_int32, C.POINTER(C.c_uint32),
                                       C.c_int64, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
     L.fgkl_sw_align_batch.restype = C.c_int
+    L.fgkl_sw_last_kernel_ms.argtypes = [C.c_void_p, C.POINTER(C.c_float)]
+    L.fgkl_sw_last_kernel_ms.restype = C.c_int
     L.fgkl_set_allocation_limit.argtypes = [C.c_int64]
     L.fgkl_set_allocation_limit.restype = C.c_int64
     L.fgkl_backend.restype = C.c_char_p
@@ -210,6 +212,7 @@ def lib() -> C.CDLL:
                                      C.POINTER(C.c_uint64)]
     L.fgkl_plan_sweeps.argtypes = [u8p, i32p, C.c_int32, i32p, C.c_int32, i32p, C.c_int32]
     L.fgkl_probe_fp32_tflops.argtypes = [C.c_int32, f64p, f64p, f64p]
+    L.fgkl_probe_int32_alu_gops.argtypes = [C.c_int32, f64p]
     L.fgkl_context_profile.argtypes = [C.c_void_p, C.c_int32]
     L.fgkl_batch_launch_profile.argtypes = [C.c_void_p, C.POINTER(LaunchProfile), C.c_int32, C.POINTER(C.c_int32)]
     L.fgkl_adjoint_prepare.argtypes = [C.c_void_p, C.POINTER(AdjointBatch), C.c_int32]
@@ -243,5 +246,5 @@ EXPORTED = [
     "fgkl_synth_reference_region", "fgkl_synth_view", "fgkl_synth_free", "fgkl_plan_describe", "fgkl_plan_region_cells", "fgkl_plan_sweeps", "fgkl_probe_fp32_tflops",
     "fgkl_pairhmm_compute_device_noalloc", "fgkl_context_profile", "fgkl_batch_launch_profile", "fgkl_adjoint_prepare", "fgkl_adjoint_run", "fgkl_adjoint_fetch",
     "fgkl_adjoint_compute", "fgkl_adjoint_output_len", "fgkl_adjoint_grad_len", "fgkl_pd_row_states", "fgkl_pd_plan_describe", "fgkl_pd_match_accepts",
-    "fgkl_sw_align", "fgkl_sw_cigar_capacity", "fgkl_sw_align_batch",
+    "fgkl_sw_align", "fgkl_sw_cigar_capacity", "fgkl_sw_align_batch", "fgkl_sw_last_kernel_ms", "fgkl_probe_int32_alu_gops",
 ]

@@ -1090,6 +1090,14 @@ int fgkl_sw_align_batch(fgkl_context* ctx, const fgkl_sw_batch* b, const fgkl_sw
   return set_error(FGKL_E_OUT_OF_MEMORY, "host memory allocation failed");
 }
 
+int fgkl_sw_last_kernel_ms(fgkl_context* ctx, float* ms) {
+  t_error.clear();
+  if (!ctx || !ms) return set_error(FGKL_E_INVALID_ARGUMENT, "null argument");
+  if (!ctx->sw || ctx->sw->last_kernel_ms() < 0.f) return set_error(FGKL_E_INVALID_ARGUMENT, "no Smith-Waterman batch has run on this context");
+  *ms = ctx->sw->last_kernel_ms();
+  return FGKL_OK;
+}
+
 int fgkl_pairhmm_compute_device_noalloc(const fgkl_device_region* region, double* out, void* stream) {
   t_error.clear();
   if (!region) return set_error(FGKL_E_INVALID_ARGUMENT, "null region");

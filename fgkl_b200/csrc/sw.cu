@@ -121,6 +121,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 8) sw_kernel(SwArgs a) {
         H[r] = 0;
         E[r] = kLowInit;
       }
+      const int last_r = (n - top >= 0 && n - top < kSwRows) ? n - top : -1;  // row n among the lane's rows
       int dH = 0;                  // H of the row above at the previous column (the top row's diagonal)
       int bH = 0, bF = kLowInit;   // this lane's bottom row at its last column, for the lane below
       uint8_t* tbb = sc.tb + static_cast<size_t>(b) * (m + 31) * kBlockRows;
@@ -182,11 +183,24 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 8) sw_kernel(SwArgs a) {
             H[r] = h;
             upH = h;
             upF = F;
-            if (top + r == n) sc.last_row[j - 1] = h;
-            if (j == m && top + r <= n) sc.last_col[top + r - 1] = h;
           }
           bH = upH;
           bF = upF;
+          // The last row and the last column, for the end cell: the lane holding the reference's last
+          // row stores its H at every column, and each lane stores its rows once, at the last column.
+          // Kept out of the row loop, where they were a compare and a predicated store per cell.
+          if (last_r >= 0) {
+            int v = H[0];
+#pragma unroll
+            for (int r = 1; r < kSwRows; ++r)
+              if (r == last_r) v = H[r];
+            sc.last_row[j - 1] = v;
+          }
+          if (j == m) {
+#pragma unroll
+            for (int r = 0; r < kSwRows; ++r)
+              if (top + r <= n) sc.last_col[top + r - 1] = H[r];
+          }
           if (lane == 31 && b + 1 < blocks) sc.carry[j - 1] = make_int2(bH, bF);
         }
         dH = uH;

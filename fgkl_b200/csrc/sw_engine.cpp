@@ -31,6 +31,8 @@ SwEngine::~SwEngine() {
   cudaFree(d_small_);
   cudaFree(d_cigar_);
   cudaFree(d_scratch_);
+  for (cudaEvent_t e : ev_)
+    if (e) cudaEventDestroy(e);
   if (own_stream_) cudaStreamDestroy(stream_);
 }
 
@@ -70,6 +72,7 @@ int SwEngine::align(const SwBatch& in, const SwScores& s, int strategy, uint32_t
                     int32_t* offsets) {
   DeviceGuard device_guard(device_);
   error_.clear();
+  kernel_ms_ = -1.f;
   const int64_t P = in.num_pairs;
   if (P < 0) return fail(FGKL_E_INVALID_ARGUMENT, "negative pair count");
   if (strategy < kSwSoftClip || strategy > kSwIgnore) return fail(FGKL_E_INVALID_ARGUMENT, "unknown overhang strategy code " + std::to_string(strategy));
@@ -148,14 +151,20 @@ int SwEngine::align(const SwBatch& in, const SwScores& s, int strategy, uint32_t
   a.count = d_counts;
   a.offset = d_offsets;
   a.counter = d_counter;
-  if ((rc = check(sw_launch(static_cast<int>(blocks), a, stream_), "Smith-Waterman launch"))) return rc;
+  if (!ev_[0] && (cudaEventCreate(&ev_[0]) != cudaSuccess || cudaEventCreate(&ev_[1]) != cudaSuccess))
+    return fail(FGKL_E_CUDA, "event creation failed");
+  if ((rc = check(cudaEventRecord(ev_[0], stream_), "event")) ||
+      (rc = check(sw_launch(static_cast<int>(blocks), a, stream_), "Smith-Waterman launch")) ||
+      (rc = check(cudaEventRecord(ev_[1], stream_), "event")))
+    return rc;
   // Only the elements produced cross to the host: packed pair after pair on the device, then
   // scattered into the caller's slots (a CIGAR is a few elements; its slot holds ref + alt + 2).
   uint32_t* d_packed = d_cigar_ + slot[P];
   if ((rc = check(sw_compact(d_cigar_, d_slot, d_counts, static_cast<int>(P), d_packed, stream_), "CIGAR packing")) ||
       (rc = check(cudaMemcpyAsync(counts, d_counts, 4 * static_cast<size_t>(P), cudaMemcpyDeviceToHost, stream_), "download counts")) ||
       (rc = check(cudaMemcpyAsync(offsets, d_offsets, 4 * static_cast<size_t>(P), cudaMemcpyDeviceToHost, stream_), "download offsets")) ||
-      (rc = check(cudaStreamSynchronize(stream_), "Smith-Waterman kernel")))
+      (rc = check(cudaStreamSynchronize(stream_), "Smith-Waterman kernel")) ||
+      (rc = check(cudaEventElapsedTime(&kernel_ms_, ev_[0], ev_[1]), "kernel time")))
     return rc;
   int64_t total = 0;
   for (int64_t k = 0; k < P; ++k) {

@@ -41,6 +41,9 @@ class SwEngine {
   int align(const SwBatch& in, const SwScores& s, int strategy, uint32_t* cigar, int64_t cigar_len, int32_t* counts,
             int32_t* offsets);
   const std::string& error() const { return error_; }
+  // Duration of the last align call's fill-and-traceback launch (CUDA events on the engine's stream),
+  // or -1 before the first.
+  float last_kernel_ms() const { return kernel_ms_; }
 
  private:
   int fail(int code, const std::string& msg);
@@ -63,6 +66,8 @@ class SwEngine {
   char* d_scratch_ = nullptr;
   size_t cap_scratch_ = 0;
   std::vector<uint32_t> packed_;  // the batch's CIGAR elements, pair after pair
+  cudaEvent_t ev_[2] = {nullptr, nullptr};  // around the fill-and-traceback launch
+  float kernel_ms_ = -1.f;
 };
 
 }  // namespace fgkl

@@ -324,6 +324,9 @@ int64_t fgkl_sw_cigar_capacity(const fgkl_sw_batch* batch);
  * them; offsets[k] its offset. Synchronous. */
 int fgkl_sw_align_batch(fgkl_context* ctx, const fgkl_sw_batch* batch, const fgkl_sw_params* params, int32_t strategy,
                         uint32_t* cigar, int64_t cigar_len, int32_t* counts, int32_t* offsets);
+/* Duration (ms, CUDA events on the context's stream) of the fill-and-traceback launch of the context's
+ * last fgkl_sw_align_batch call; no counterpart in the reference (measurement support). */
+int fgkl_sw_last_kernel_ms(fgkl_context* ctx, float* ms);
 
 /* ---- allocation-free form (no counterpart in the reference) ----
  *
@@ -380,6 +383,9 @@ int fgkl_pairhmm_compute_device_noalloc(const fgkl_device_region* region, double
 /* Measured FP32 FMA throughput of `device` (TFLOP/s) with scalar FFMA and packed FP32x2 FFMA chains:
  * the denominator of the kernels' FP32 roofline. */
 int fgkl_probe_fp32_tflops(int32_t device, double* scalar_tflops, double* packed_tflops, double* sm_clock_mhz);
+/* Measured integer ALU throughput of `device` (Gop/s: independent chains of 32-bit XOR and signed
+ * max): the denominator of the Smith-Waterman kernel's roofline. */
+int fgkl_probe_int32_alu_gops(int32_t device, double* gops);
 
 /* ---- synthetic workloads (the analogue of fgkl's crates/pairhmm/src/synthetic.rs) ---- */
 

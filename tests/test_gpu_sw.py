@@ -109,3 +109,41 @@ def test_batch_and_per_call_agree(gpu):
     pairs = [related_pair(rng, 30 + rng.below(400), 10 + rng.below(300)) for _ in range(40)]
     batch = align_batch(pairs, READ_TO_HAP, OverhangStrategy.SOFTCLIP)
     assert batch == [align(r, a, READ_TO_HAP, OverhangStrategy.SOFTCLIP) for r, a in pairs]
+
+
+def test_the_batch_kernel_time_is_reported_for_the_last_call(gpu):
+    import ctypes as C
+    import time
+
+    from fgkl_b200 import BatchContext
+
+    ctx = BatchContext()
+    try:
+        ms = C.c_float()
+        # No batch yet on this context: an error, not a stale number.
+        assert _lib.lib().fgkl_sw_last_kernel_ms(ctx._ctx, C.byref(ms)) != 0
+        rng = Rng(41)
+        pairs = [related_pair(rng, 300, 280) for _ in range(64)]
+        t0 = time.perf_counter()
+        check_batch_on(ctx, pairs)
+        wall_ms = 1e3 * (time.perf_counter() - t0)
+        assert _lib.lib().fgkl_sw_last_kernel_ms(ctx._ctx, C.byref(ms)) == 0
+        assert 0.0 < ms.value < wall_ms
+    finally:
+        ctx.close()
+
+
+def check_batch_on(ctx, pairs):
+    got = align_batch(pairs, HAP_TO_REF, OverhangStrategy.INDEL, ctx)
+    for (r, a), g in zip(pairs, got):
+        assert g == expected(r, a, HAP_TO_REF, OverhangStrategy.INDEL)
+
+
+def test_the_integer_alu_probe_measures_a_plausible_rate(gpu):
+    import ctypes as C
+
+    gops = C.c_double()
+    assert _lib.lib().fgkl_probe_int32_alu_gops(0, C.byref(gops)) == 0
+    # 148 SMs at up to 64 ALU operations a cycle near 2 GHz: some thousands of Gop/s, never above the
+    # 128-lane FP32 rate.
+    assert 1000.0 < gops.value < 148 * 128 * 2.1
