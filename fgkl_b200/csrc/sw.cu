@@ -155,26 +155,18 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 8) sw_kernel(SwArgs a) {
 #pragma unroll
           for (int r = 0; r < kSwRows; ++r) {
             const int sd = dg + (rb[r] == ab ? a.match : a.mismatch);
+            // A gap extends the neighbour's unless opening here scores strictly more. H is the largest
+            // of the three: the diagonal when it is at least both gaps, else the horizontal gap when it
+            // is at least the vertical one (so max(sd, max(E, F)) and one compare decide it).
             const int fe = upF + extend, fo = upH + open;
-            const bool vreset = fo > fe;
-            const int F = vreset ? fo : fe;
+            const int F = max(fe, fo);
             const int ee = E[r] + extend, eo = H[r] + open;
-            const bool hreset = eo > ee;
-            E[r] = hreset ? eo : ee;
-            int h;
-            uint32_t dir;
-            if (sd >= F && sd >= E[r]) {
-              h = sd;
-              dir = 0;
-            } else if (E[r] >= F) {
-              h = E[r];
-              dir = 1;
-            } else {
-              h = F;
-              dir = 2;
-            }
+            E[r] = max(ee, eo);
+            const int gap = max(E[r], F);
+            const uint32_t dir = sd >= gap ? 0u : (E[r] >= F ? 1u : 2u);
+            int h = max(sd, gap);
             h = h > kCutoff ? h : kCutoff;
-            const uint32_t byte = dir | (vreset ? 0u : kExtV) | (hreset ? 0u : kExtH);
+            const uint32_t byte = dir | (fe >= fo ? kExtV : 0u) | (ee >= eo ? kExtH : 0u);
             if (r < 4)
               lo |= byte << (8 * r);
             else
