@@ -399,15 +399,13 @@ void emit_program(const SortedHaps& s, bool with_suffix, ProgramBuild& out) {
     v.push_back(e | pending);
     pending = 0;
   };
-  std::vector<int32_t> eff_len(m, 0);
   for (int32_t i = 0; i < m; ++i) {
     const Seg& g = segs[i];
-    eff_len[i] = g.start > 0 ? eff_len[writer[i]] : g.len;
     Segment rec{};
     rec.hap = g.hap;
     rec.node = g.cut.column >= 0 ? g.cut.node : -1;
     rec.staged = g.start > 0 ? 1 : 0;
-    rec.factor = static_cast<double>(eff_len[i]) / static_cast<double>(g.len);
+    rec.scale = g.start > 0 ? static_cast<double>(segs[writer[i]].len) / static_cast<double>(g.len) : 1.0;
     rec.init_d = init_f64 / static_cast<double>(g.len);
     rec.init_f = static_cast<float>(init_f32 / static_cast<double>(g.len));
     rec.next_slot = -1;

@@ -61,12 +61,13 @@ constexpr uint8_t kNoCode = 0xFF;
 // column (the origin or a staged snapshot), then either finished or, for a cut, continued through
 // the cut column, whose match and deletion rows are joined with backward node `node`.
 //
-// Snapshots are never rescaled: the recurrence is linear in the row-0 constant INITIAL / length, so
-// a segment keeps the constant of the first segment of its snapshot chain (length eff_len) and its
-// raw result is multiplied by eff_len / hap_len at the end (fgkl rescales at every resume,
-// kernel.rs:641, :673-678; the two agree up to rounding).
+// The recurrence is linear in the row-0 constant INITIAL / length, so a segment that resumes from
+// another haplotype's snapshot multiplies the restored state by writer_len / hap_len, as fgkl does at
+// every resume (kernel.rs:641, :673-678): each segment runs at its own constant, and no value exceeds
+// what its own haplotype's recurrence reaches (a chain kept at a short first haplotype's constant
+// overflowed for short reads).
 struct Segment {
-  double factor;      // eff_len / hap_len
+  double scale;       // writer_len / hap_len for a resumed segment, 1 for one from the origin
   float init_f;       // 2^120 / hap_len narrowed to f32 (kernel.rs:640), for origin segments
   int32_t staged;     // 1: start from the staging buffer; 0: from the origin (column 0)
   double init_d;      // 2^1020 / hap_len

@@ -486,3 +486,19 @@ def test_dense_reads_are_recomputed_with_their_shared_program(gpu):
     alone = compute(FLOAT, [reads[r] for r in range(len(reads)) if owner[r] == 0], haps).reshape(-1, len(haps))
     kept = out[[r for r in range(len(reads)) if owner[r] == 0]]
     assert kept[:, :5].tobytes() == alone[:, :5].tobytes()
+
+
+@pytest.mark.parametrize("long_len", [149, 2000])
+def test_a_long_haplotype_resumed_from_a_one_base_prefix_keeps_its_own_scale(gpu, long_len):
+    # The one-base haplotype "C" sorts first and the long one resumes from its column 1. A resumed
+    # segment rescales the restored state to its own initial constant (kernel.rs:641-678); kept at the
+    # first haplotype's constant, a short read's likelihood near 1 overflowed (FP64 from about 16x the
+    # constant, FP32 from 256x).
+    rng = Rng(77)
+    long_hap = b"C" + bytes(rng.base() for _ in range(long_len - 1))
+    haps = [long_hap, b"C", long_hap[:long_len // 2]]
+    reads = [simple_read(b"A"), simple_read(b"CT"), simple_read(b"GCA"), simple_read(long_hap[10:40])]
+    expected = reference_all(reads, haps)
+    for precision, tol in ((Precision.DOUBLE, 1e-9), (Precision.FLOAT, 1e-4)):
+        for share in (True, False):
+            assert_close(compute(cfg(precision, share), reads, haps), expected, tol, f"{precision}, share {share}")

@@ -70,7 +70,11 @@ def test_flagged_alternates_and_deletions_change_the_result(gpu):
     without = compute(DOUBLE, reads, unflagged)
     changed = int(np.sum(np.abs(with_flags - without) > 1.0))
     assert changed >= 20, f"{changed} of {with_flags.size} pairs changed"
-    assert np.all(with_flags >= without), "flags never lower a likelihood"
+    # fgkl asserts this exactly (pd.rs:201), its FP64 arithmetic being the oracle's own. Here a pair
+    # the flags do not affect is computed through other sharing chains (the PD sort key includes the
+    # flags, and each resume rescales the state), so the two sides agree only to FP64 rounding:
+    # 5.7e-14 in log10 at most on this region, each within that of the oracle.
+    assert np.all(with_flags >= without - 1e-12), "flags never lower a likelihood"
 
 
 def test_haplotypes_without_flags_agree_with_the_plain_kernel(gpu):
@@ -276,3 +280,19 @@ def test_dense_reads_are_recomputed_with_their_shared_program(gpu):
     for r in range(len(reads)):
         if owner[r] == 1:
             assert out[r][lost_mask[r]].tobytes() == double[r][lost_mask[r]].tobytes(), r
+
+
+def test_a_long_pd_haplotype_resumed_from_a_one_base_prefix_keeps_its_own_scale(gpu):
+    # As in the plain kernel: the resumed segment, branch values included, is rescaled to its own
+    # initial constant, so a short read's likelihood near 1 does not overflow.
+    rng = Rng(78)
+    bases = b"C" + bytes(rng.base() for _ in range(1999))
+    flags = bytearray(len(bases))
+    flags[40] = DEL_START
+    flags[43] = DEL_END
+    flags[900] = SNP | ALT_G
+    haps = [PdHaplotype(bases, bytes(flags)), PdHaplotype(b"C", b"\x00"), PdHaplotype(bases[:700], bytes(flags[:700]))]
+    reads = [read(b"A"), read(b"CT"), read(b"GCA"), read(bases[30:60])]
+    expected = reference_all(reads, haps)
+    assert_close(compute(DOUBLE, reads, haps), expected, 1e-9, "double")
+    assert_close(compute(Config(precision=Precision.FLOAT, double_fallback=True), reads, haps), expected, 1e-4, "float")
