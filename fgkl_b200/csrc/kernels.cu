@@ -349,7 +349,7 @@ struct FwdState {
   int seg_i;
   // The next segment's record, loaded a segment ahead so a BEGIN never waits on memory.
   int nx_staged, nx_slot;
-  S nx_init, nx_scale;
+  S nx_init;
   // Strip-mined reads: the row above lane 0's top row for this step's column (the previous block's
   // bottom row, or GATK's row 0 in the first block). Read only by forward_step<..., kCarry = true>.
   V cM, cX, cY;
@@ -360,12 +360,10 @@ struct FwdState {
       nx_staged = rec->staged;
       nx_slot = rec->next_slot;
       nx_init = P::kDouble ? static_cast<S>(rec->init_d) : static_cast<S>(rec->init_f);
-      nx_scale = static_cast<S>(rec->scale);
     } else {
       nx_staged = 0;
       nx_slot = -1;
       nx_init = S(0);
-      nx_scale = S(1);
     }
   }
 };
@@ -439,39 +437,36 @@ __device__ __forceinline__ void forward_step(const LaunchArgs& a, const Program&
       const int next_slot = synth ? -1 : st.nx_slot;
       const bool staged = !synth && st.nx_staged;
       const S init = st.nx_init;
-      const V scale = P::splat(st.nx_scale);
       if (!synth) st.load_next(a.v, prog, st.seg_i + 1);
       if (staged) {
-        // The writer's state, rescaled to this haplotype's initial constant (kernel.rs:641-678).
         __pipeline_wait_prior(0);
         V s[L::kSnap];
         load_record(s, sc.staged(st.seg_i, lane));
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-          st.M[r] = P::mul(s[r], scale);
-          st.X[r] = P::mul(s[R + r], scale);
-          st.Y[r] = P::mul(s[2 * R + r], scale);
+          st.M[r] = s[r];
+          st.X[r] = s[R + r];
+          st.Y[r] = s[2 * R + r];
         }
-        dM = P::mul(s[3 * R], scale);
-        dX = P::mul(s[3 * R + 1], scale);
-        dY = P::mul(s[3 * R + 2], scale);
-        st.acc = P::mul(s[3 * R + 3], scale);
+        dM = s[3 * R];
+        dX = s[3 * R + 1];
+        dY = s[3 * R + 2];
+        st.acc = s[3 * R + 3];
       } else {
-        // The origin: nothing but the row-0 constant.
+        // The origin: nothing but the row-0 constant, in the padding rows (and the row above the
+        // lane when that is padding).
+        const S in_s = synth ? static_cast<S>(Consts<P::kDouble>::kInitial / synth_len) : init;
 #pragma unroll
         for (int r = 0; r < R; ++r) st.M[r] = st.X[r] = st.Y[r] = P::zero();
         dM = dX = dY = st.acc = P::zero();
-      }
-      // The padding rows (and the row above the lane when that is padding) hold this haplotype's
-      // row-0 constant exactly, from the origin or after a resume (GATK's row 0, kernel.rs:652-660).
-      const S in_s = synth ? static_cast<S>(Consts<P::kDouble>::kInitial / synth_len) : init;
-      if (lane * R <= pad_hi) {
+        if (lane * R <= pad_hi) {
 #pragma unroll
-        for (int c = 0; c < P::NC; ++c) {
+          for (int c = 0; c < P::NC; ++c) {
 #pragma unroll
-          for (int r = 0; r < R; ++r)
-            if (lane * R + r < rd[c].pad) P::put(st.Y[r], c, in_s);
-          if (lane * R - 1 < rd[c].pad) P::put(dY, c, in_s);
+            for (int r = 0; r < R; ++r)
+              if (lane * R + r < rd[c].pad) P::put(st.Y[r], c, in_s);
+            if (lane * R - 1 < rd[c].pad) P::put(dY, c, in_s);
+          }
         }
       }
       if (next_slot >= 0) prefetch(sc.staged(st.seg_i + 1, lane), sc.slot(next_slot, lane), L::kSnap);
@@ -648,13 +643,14 @@ __device__ void finalize(const LaunchArgs& a, const Task& task, const Region& re
     const HapInfo info = a.v.haps[region.hap_off + k];
     const Segment* seg = a.v.segs + prog.seg_off + info.seg;
     const bool joined = seg->node >= 0;
+    const double factor = seg->factor;
 #pragma unroll
     for (int c = 0; c < P::NC; ++c) {
       if (task.read[c] < 0) continue;
       const int read_local = task.read[c] - region.read_off;
       double* dst = a.v.out + region.out_off + static_cast<int64_t>(read_local) * region.n_haps + info.order;
       if (dense && !isnan(*dst)) continue;
-      const double raw = sc.seg_raw[info.seg * P::NC + c];
+      const double raw = __dmul_rn(sc.seg_raw[info.seg * P::NC + c], factor);
       bool lost;
       if (joined)
         lost = !(raw >= C::kMinAcceptedJoined);

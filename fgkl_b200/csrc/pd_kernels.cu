@@ -235,48 +235,38 @@ __device__ __forceinline__ void pd_step(const LaunchArgs& a, const Program& prog
       const Segment* rec = a.v.segs + prog.seg_off + st.seg_i;
       if (!synth && st.seg_i + 1 < prog.n_segs) prefetch_l1(rec + 1);
       const int next_slot = synth ? -1 : rec->next_slot;
-      const bool staged = !synth && rec->staged;
-      if (staged) {
-        // The writer's state, branch values included, rescaled to this haplotype's initial constant
-        // (kernel.rs:641-678).
-        const V scale = P::splat(static_cast<S>(rec->scale));
+      if (!synth && rec->staged) {
         __pipeline_wait_prior(0);
         const V* s = sc.staged(st.seg_i, lane);
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-          st.M[r] = P::mul(s[r], scale);
-          st.X[r] = P::mul(s[R + r], scale);
-          st.Y[r] = P::mul(s[2 * R + r], scale);
-          st.BM[r] = P::mul(s[3 * R + r], scale);
-          st.BX[r] = P::mul(s[4 * R + r], scale);
-          st.BY[r] = P::mul(s[5 * R + r], scale);
+          st.M[r] = s[r];
+          st.X[r] = s[R + r];
+          st.Y[r] = s[2 * R + r];
+          st.BM[r] = s[3 * R + r];
+          st.BX[r] = s[4 * R + r];
+          st.BY[r] = s[5 * R + r];
         }
-        d.M = P::mul(s[6 * R], scale);
-        d.X = P::mul(s[6 * R + 1], scale);
-        d.Y = P::mul(s[6 * R + 2], scale);
-        st.acc = P::mul(s[6 * R + 3], scale);
+        d.M = s[6 * R];
+        d.X = s[6 * R + 1];
+        d.Y = s[6 * R + 2];
+        st.acc = s[6 * R + 3];
       } else {
-        // The origin: zero branch values (GATK never writes branch column zero).
+        // The origin: the row-0 constant in the padding rows, zero branch values (GATK never writes
+        // branch column zero).
+        const S in_s = synth ? static_cast<S>(Consts<P::kDouble>::kInitial / synth_len)
+                             : (P::kDouble ? static_cast<S>(rec->init_d) : static_cast<S>(rec->init_f));
 #pragma unroll
         for (int r = 0; r < R; ++r) st.M[r] = st.X[r] = st.Y[r] = st.BM[r] = st.BX[r] = st.BY[r] = P::zero();
         d.M = d.X = d.Y = st.acc = P::zero();
-      }
-      // The padding rows (and the row above the lane when that is padding) hold this haplotype's
-      // row-0 constant exactly, from the origin or after a resume. A padding row's deletion branch
-      // value is 0 or that constant, and a DEL_END merge with the row's own Y gives the constant
-      // either way, so after a resume it is set to the constant too.
-      const S in_s = synth ? static_cast<S>(Consts<P::kDouble>::kInitial / synth_len)
-                           : (P::kDouble ? static_cast<S>(rec->init_d) : static_cast<S>(rec->init_f));
-      if (lane * R <= pad_hi) {
+        if (lane * R <= pad_hi) {
 #pragma unroll
-        for (int c = 0; c < P::NC; ++c) {
+          for (int c = 0; c < P::NC; ++c) {
 #pragma unroll
-          for (int r = 0; r < R; ++r)
-            if (lane * R + r < rd[c].pad) {
-              P::put(st.Y[r], c, in_s);
-              if (staged) P::put(st.BY[r], c, in_s);
-            }
-          if (lane * R - 1 < rd[c].pad) P::put(d.Y, c, in_s);
+            for (int r = 0; r < R; ++r)
+              if (lane * R + r < rd[c].pad) P::put(st.Y[r], c, in_s);
+            if (lane * R - 1 < rd[c].pad) P::put(d.Y, c, in_s);
+          }
         }
       }
       if (next_slot >= 0) prefetch(sc.staged(st.seg_i + 1, lane), sc.slot(next_slot, lane), L::kSnap);
@@ -448,13 +438,14 @@ __device__ void pd_finalize(const LaunchArgs& a, const Task& task, const Region&
   unsigned long long lost_count = 0;
   for (int k = lane; k < region.n_haps; k += 32) {
     const HapInfo info = a.v.haps[region.hap_off + k];
+    const double factor = a.v.segs[prog.seg_off + info.seg].factor;
 #pragma unroll
     for (int c = 0; c < P::NC; ++c) {
       if (task.read[c] < 0) continue;
       const int read_local = task.read[c] - region.read_off;
       double* dst = a.v.out + region.out_off + static_cast<int64_t>(read_local) * region.n_haps + info.order;
       if (dense && !isnan(*dst)) continue;
-      const double raw = sc.seg_raw[info.seg * P::NC + c];
+      const double raw = __dmul_rn(sc.seg_raw[info.seg * P::NC + c], factor);
       bool lost = a.min_accept_plain ? !(raw >= C::kMinAccepted) : (raw != raw);
       if (!P::kDouble) lost |= isinf(raw);
       const double result = lost ? __longlong_as_double(0x7ff8000000000000ll) : log10(raw) - C::kLog10Initial;

@@ -399,15 +399,22 @@ void emit_program(const SortedHaps& s, bool with_suffix, ProgramBuild& out) {
     v.push_back(e | pending);
     pending = 0;
   };
+  // Each sharing tree runs at the constant of its longest haplotype (program.h, Segment).
+  std::vector<int32_t> root(m, 0), tree_len(m, 0);
+  for (int32_t i = 0; i < m; ++i) {
+    root[i] = segs[i].start > 0 ? root[writer[i]] : i;
+    tree_len[root[i]] = std::max(tree_len[root[i]], segs[i].len);
+  }
   for (int32_t i = 0; i < m; ++i) {
     const Seg& g = segs[i];
+    const double t_len = static_cast<double>(tree_len[root[i]]);
     Segment rec{};
     rec.hap = g.hap;
     rec.node = g.cut.column >= 0 ? g.cut.node : -1;
     rec.staged = g.start > 0 ? 1 : 0;
-    rec.scale = g.start > 0 ? static_cast<double>(segs[writer[i]].len) / static_cast<double>(g.len) : 1.0;
-    rec.init_d = init_f64 / static_cast<double>(g.len);
-    rec.init_f = static_cast<float>(init_f32 / static_cast<double>(g.len));
+    rec.factor = t_len / static_cast<double>(g.len);
+    rec.init_d = init_f64 / t_len;
+    rec.init_f = static_cast<float>(init_f32 / t_len);
     rec.next_slot = -1;
     if (i + 1 < m && writer[i + 1] >= 0 && writer[i + 1] < i) rec.next_slot = writes.at({writer[i + 1], segs[i + 1].start}).second;
     out.segs.push_back(rec);

@@ -61,16 +61,22 @@ constexpr uint8_t kNoCode = 0xFF;
 // column (the origin or a staged snapshot), then either finished or, for a cut, continued through
 // the cut column, whose match and deletion rows are joined with backward node `node`.
 //
-// The recurrence is linear in the row-0 constant INITIAL / length, so a segment that resumes from
-// another haplotype's snapshot multiplies the restored state by writer_len / hap_len, as fgkl does at
-// every resume (kernel.rs:641, :673-678): each segment runs at its own constant, and no value exceeds
-// what its own haplotype's recurrence reaches (a chain kept at a short first haplotype's constant
-// overflowed for short reads).
+// The recurrence is linear in the row-0 constant INITIAL / length. fgkl rescales a snapshot at every
+// resume (kernel.rs:641, :673-678). Here a sharing tree (a segment from the origin and every segment
+// that resumes from it, directly or not) runs at one constant, INITIAL / tree_len with tree_len its
+// longest haplotype's length, and each raw result is multiplied by tree_len / hap_len at the end, so
+// a resume costs nothing (rescaling at each resume, inside the event windows, cost 5.5% on 4096
+// uneven regions). No value then exceeds what its own haplotype's recurrence reaches, so nothing
+// overflows that fgkl's does not. A tree kept at its first haplotype's constant overflows when that
+// one is much shorter (a one-base haplotype prefixing a long one, with short reads). A member shorter
+// than its tree's longest runs that ratio below fgkl's scale. That matters only where 2^1020 L is an
+// FP64 subnormal (log10 L below -614.7), where fgkl's own value has lost precision too; equal lengths
+// run at fgkl's own scale.
 struct Segment {
-  double scale;       // writer_len / hap_len for a resumed segment, 1 for one from the origin
-  float init_f;       // 2^120 / hap_len narrowed to f32 (kernel.rs:640), for origin segments
+  double factor;      // tree_len / hap_len
+  float init_f;       // 2^120 / tree_len narrowed to f32 (kernel.rs:640), for origin segments
   int32_t staged;     // 1: start from the staging buffer; 0: from the origin (column 0)
-  double init_d;      // 2^1020 / hap_len
+  double init_d;      // 2^1020 / tree_len
   int32_t next_slot;  // global snapshot slot to prefetch for the NEXT segment at this BEGIN, or -1
   int32_t node;       // backward node joined at the cut; -1 = no cut
   int32_t hap;        // sorted haplotype index
