@@ -185,3 +185,17 @@ def test_allocation_free_entry_checks_its_bounds_on_the_host():
         assert L.fgkl_pairhmm_compute_device_noalloc(C.byref(r), None, None) == _lib.FGKL_E_UNSUPPORTED
     r.num_reads, r.num_haplotypes, r.max_read_len = 0, 4, 151  # no pairs: nothing to do
     assert L.fgkl_pairhmm_compute_device_noalloc(C.byref(r), None, None) == 0
+
+
+def test_measurement_entries_check_their_arguments():
+    # No context: an error, not a crash; the probe needs somewhere to write.
+    ms = C.c_float()
+    assert _lib.lib().fgkl_sw_last_kernel_ms(None, C.byref(ms)) == _lib.FGKL_E_INVALID_ARGUMENT
+    assert _lib.lib().fgkl_probe_int32_alu_gops(0, None) == _lib.FGKL_E_INVALID_ARGUMENT
+
+
+@pytest.mark.skipif(has_gpu(), reason="checks the no-device path")
+def test_the_alu_probe_without_a_device_fails_loudly():
+    gops = C.c_double(-1.0)
+    assert _lib.lib().fgkl_probe_int32_alu_gops(0, C.byref(gops)) == _lib.FGKL_E_NO_DEVICE
+    assert gops.value == -1.0
