@@ -502,3 +502,22 @@ def test_a_long_haplotype_resumed_from_a_one_base_prefix_keeps_its_own_scale(gpu
     for precision, tol in ((Precision.DOUBLE, 1e-9), (Precision.FLOAT, 1e-4)):
         for share in (True, False):
             assert_close(compute(cfg(precision, share), reads, haps), expected, tol, f"{precision}, share {share}")
+
+
+def test_an_fp32_overflow_is_recomputed_in_fp64(gpu):
+    # A 1-base read N (prior near 1 in every column) against two 528-base haplotypes that differ at
+    # position 150: with suffix sharing, row 0's backward start mass sums the 377 shared suffix
+    # columns at the 2^120 backward scale, past FP32's range. fgkl's finish_lane accepts the
+    # resulting +inf (kernel.rs:897-914), and its CPU restatement here returns +inf; this build counts
+    # a non-finite FP32 result as lost and recomputes it in FP64, which gives GATK's value.
+    rng = Rng(91)
+    hap = bytes(rng.base() for _ in range(528))
+    other = bytearray(hap)
+    other[150] = ord("A") if hap[150] != ord("A") else ord("C")
+    haps = [hap, bytes(other)]
+    reads = [Read(b"N", bytes([30]), bytes([45]), bytes([38]), bytes([8])), simple_read(b"A"), simple_read(hap[100:130])]
+    expected = reference_all(reads, haps)
+    assert np.isfinite(expected).all()
+    for share in (True, False):
+        assert_close(compute(cfg(Precision.FLOAT, share), reads, haps), expected, 1e-4, f"float, share {share}")
+        assert_close(compute(cfg(Precision.DOUBLE, share), reads, haps), expected, 1e-9, f"double, share {share}")
