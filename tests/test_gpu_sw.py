@@ -147,3 +147,51 @@ def test_the_integer_alu_probe_measures_a_plausible_rate(gpu):
     # 148 SMs at up to 64 ALU operations a cycle near 2 GHz: some thousands of Gop/s, never above the
     # 128-lane FP32 rate.
     assert 1000.0 < gops.value < 148 * 128 * 2.1
+
+
+def test_weak_alignments_of_unrelated_700_mers(gpu):
+    # fgkl's weak_alignments_saturate_the_narrow_lanes_and_fall_back_exactly (lib.rs:855-866): its
+    # 16-bit lanes saturate here; the 32-bit scores here have no narrow form, but the case stands.
+    rng = Rng(23)
+    r = bytes(rng.base() for _ in range(700))
+    a = bytes(rng.base() for _ in range(700))
+    want = expected(r, a, HAP_TO_REF, OverhangStrategy.SOFTCLIP)
+    assert align(r, a, HAP_TO_REF, OverhangStrategy.SOFTCLIP) == want
+    assert align_batch([(r, a)], HAP_TO_REF, OverhangStrategy.SOFTCLIP) == [want]
+
+
+def test_a_haplotype_matching_the_far_end_of_the_reference(gpu):
+    # fgkl's a_haplotype_matching_the_far_end_of_the_reference_stays_in_narrow_lanes (lib.rs:869-881).
+    rng = Rng(29)
+    r = bytes(rng.base() for _ in range(600))
+    a = bytearray(r[380:])
+    a[100] = ord("C") if a[100] == ord("A") else ord("A")
+    a = bytes(a)
+    want = expected(r, a, HAP_TO_REF, OverhangStrategy.SOFTCLIP)
+    assert align(r, a, HAP_TO_REF, OverhangStrategy.SOFTCLIP) == want
+    assert align_batch([(r, a)], HAP_TO_REF, OverhangStrategy.SOFTCLIP) == [want]
+
+
+def test_a_reused_context_matches_the_oracle_as_pair_sizes_shrink_and_grow(gpu):
+    # fgkl's a_reused_aligner_matches_the_reference_as_pair_sizes_shrink_and_grow (lib.rs:1023-1065):
+    # the first pair is unrelated, and the scratch each later pair finds is what the earlier ones left.
+    from fgkl_b200 import BatchContext
+
+    rng = Rng(11)
+    sizes = [(600, 520), (500, 150), (40, 30), (320, 310), (8, 5), (590, 600), (60, 200)]
+    pairs = []
+    for k, (n, m) in enumerate(sizes):
+        if k == 0:
+            pairs.append((bytes(rng.base() for _ in range(n)), bytes(rng.base() for _ in range(m))))
+        else:
+            pairs.append(related_pair(rng, n, m))
+    ctx = BatchContext()
+    try:
+        for r, a in pairs:
+            for params in (HAP_TO_REF, READ_TO_HAP):
+                for strategy in STRATEGIES:
+                    want = expected(r, a, params, strategy)
+                    assert align(r, a, params, strategy) == want, (len(r), len(a), strategy)
+                    assert align_batch([(r, a)], params, strategy, ctx) == [want], (len(r), len(a), strategy)
+    finally:
+        ctx.close()
