@@ -151,8 +151,11 @@ int SwEngine::align(const SwBatch& in, const SwScores& s, int strategy, uint32_t
   a.count = d_counts;
   a.offset = d_offsets;
   a.counter = d_counter;
-  if (!ev_[0] && (cudaEventCreate(&ev_[0]) != cudaSuccess || cudaEventCreate(&ev_[1]) != cudaSuccess))
-    return fail(FGKL_E_CUDA, "event creation failed");
+  if (!ev_[0] || !ev_[1]) {
+    for (cudaEvent_t& e : ev_)
+      if (!e && cudaEventCreate(&e) != cudaSuccess) e = nullptr;
+    if (!ev_[0] || !ev_[1]) return fail(FGKL_E_CUDA, "event creation failed");
+  }
   if ((rc = check(cudaEventRecord(ev_[0], stream_), "event")) ||
       (rc = check(sw_launch(static_cast<int>(blocks), a, stream_), "Smith-Waterman launch")) ||
       (rc = check(cudaEventRecord(ev_[1], stream_), "event")))
@@ -163,9 +166,13 @@ int SwEngine::align(const SwBatch& in, const SwScores& s, int strategy, uint32_t
   if ((rc = check(sw_compact(d_cigar_, d_slot, d_counts, static_cast<int>(P), d_packed, stream_), "CIGAR packing")) ||
       (rc = check(cudaMemcpyAsync(counts, d_counts, 4 * static_cast<size_t>(P), cudaMemcpyDeviceToHost, stream_), "download counts")) ||
       (rc = check(cudaMemcpyAsync(offsets, d_offsets, 4 * static_cast<size_t>(P), cudaMemcpyDeviceToHost, stream_), "download offsets")) ||
-      (rc = check(cudaStreamSynchronize(stream_), "Smith-Waterman kernel")) ||
-      (rc = check(cudaEventElapsedTime(&kernel_ms_, ev_[0], ev_[1]), "kernel time")))
+      (rc = check(cudaStreamSynchronize(stream_), "Smith-Waterman kernel")))
     return rc;
+  // Measurement only: a failed query leaves the time unknown (-1) and the alignment stands.
+  if (cudaEventElapsedTime(&kernel_ms_, ev_[0], ev_[1]) != cudaSuccess) {
+    kernel_ms_ = -1.f;
+    cudaGetLastError();
+  }
   int64_t total = 0;
   for (int64_t k = 0; k < P; ++k) {
     if (counts[k] < 0 || counts[k] > sw_cigar_slot(in.ref_off[k + 1] - in.ref_off[k], in.alt_off[k + 1] - in.alt_off[k]))
